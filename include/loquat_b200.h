@@ -1,0 +1,152 @@
+/*
+ * LOQUAT-B200 C ABI.
+ *
+ * Plain C entry points over the sm_100a kernels of the per-step SPH path.
+ * Every function returns an int status (LQ_OK = 0); lq_last_error() gives the
+ * message of the last failure on the calling thread.  No function exits the
+ * process.  The C++ drop-in surface (loquat_grid.h, particle_interaction.h,
+ * predictor_corrector.h, adami_boundary.h, field_smoothing.h) is a thin layer
+ * over these calls that keeps the reference's print-and-exit behaviour.
+ *
+ * Conventions
+ *   par            pointer to a 208-byte Parameters record (types.h); "host"
+ *                  means host memory, "device" means device memory.
+ *   float4 arrays  float[np][4]  (pospres, velrhop, idep, accad, spin)
+ *   tensor2d arrays float[np][6] (str, stn, acestn), order xx yy zz xy xz yz
+ *   stream         a cudaStream_t; NULL is the legacy default stream, which
+ *                  is what the reference uses for every launch.
+ *   Device arrays are caller-owned unless stated otherwise.
+ */
+#ifndef LOQUAT_B200_C_ABI_H
+#define LOQUAT_B200_C_ABI_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LQ_OK            0
+#define LQ_ERR_ARG       1   /* bad argument (null pointer, size, layout)     */
+#define LQ_ERR_CUDA      2   /* CUDA runtime error                            */
+#define LQ_ERR_ALLOC     3   /* device or host allocation failed              */
+#define LQ_ERR_IO        4   /* file missing, malformed or truncated          */
+#define LQ_ERR_STATE     5   /* simulation health check failed                */
+#define LQ_ERR_NOTFOUND  6   /* required XML key absent                       */
+
+#define LQ_ABI_VERSION   1
+
+/* ---- library ------------------------------------------------------------ */
+int         lq_abi_version(void);
+size_t      lq_parameters_size(void);            /* == sizeof(Parameters) = 208 */
+const char* lq_last_error(void);
+const char* lq_status_string(int status);
+
+/* Derived constants: h, 1/h, eta, m, cell counts, layer size, Wendland C2
+ * constants, W(0), W(dr).  Replaces LoquatSph::InitializeParameters
+ * (reference src/loquat.cu:111-139), same float arithmetic. */
+int lq_initialize_parameters(void* par_host);
+
+/* dt = cfl * h / cs (reference src/loquat.cu:325-333; dynamic dt is not
+ * implemented there either). Writes par_host->dt. */
+int lq_update_time_step(void* par_host);
+
+/* ---- neighbour grid (replaces LoquatGrid, reference src/loquat_grid.h:28-66) */
+/* Allocates the grid arrays for np particles and ncell cells
+ * (GridConfig, ResizeArrayLength). */
+int lq_grid_create(int np, int ncell, void** grid);
+int lq_grid_resize(void* grid, int np, int ncell);
+int lq_grid_destroy(void* grid);
+/* Hash, stable sort and cell bounds (LoquatGrid::NeighborSearch,
+ * reference src/loquat_grid.h:60).  pospres/idep: device float4[np]. */
+int lq_grid_neighbor_search(void* grid, const void* par_host, const void* par_device,
+                            const float* pospres, const float* idep, void* stream);
+/* Device pointers owned by the grid.  cell_start has ncell + 1 entries:
+ * the particles of cell c are the sorted slots [cell_start[c], cell_start[c+1]). */
+int lq_grid_arrays(void* grid, const int** part_cel, const int** part_idx,
+                   const int** cell_beg, const int** cell_end, const int** cell_start);
+/* data[i] <- data[part_idx[i]] through cache (LoquatGrid::SortArrayFloat4 /
+ * SortArrayTensor2d, reference src/loquat_grid.h:62-64). */
+int lq_grid_sort_float4(void* grid, int np, float* data, float* cache, void* stream);
+int lq_grid_sort_tensor2d(void* grid, int np, float* data, float* cache, void* stream);
+
+/* ---- per-stage operators ------------------------------------------------ */
+/* reference src/particle_interaction.h:27-40 */
+int lq_particle_interaction(const void* par_host, const void* par_device,
+                            const float* pospres, const float* velrhop, const float* idep,
+                            const float* str, const float* stn,
+                            float* accad, float* spin, float* acestn,
+                            const int* cell_beg, const int* cell_end, void* stream);
+
+/* reference src/adami_boundary.h:27-34 */
+int lq_adami_boundary(const void* par_host, const void* par_device,
+                      const float* pospres, const float* velrhop, float* str,
+                      const int* cell_beg, const int* cell_end, void* stream);
+
+/* reference src/field_smoothing.h:27-35 */
+int lq_stress_regularization(const void* par_host, const void* par_device,
+                             const float* pospres, const float* velrhop, float* str,
+                             float* tensor2d_cache,
+                             const int* cell_beg, const int* cell_end, void* stream);
+
+/* reference src/predictor_corrector.h:30-48 */
+int lq_predictor(const void* par_host, const void* par_device,
+                 float* pospres, float* velrhop, float* idep, float* str, float* stn,
+                 float* pospres_ini, float* velrhop_ini, float* idep_ini,
+                 float* str_ini, float* stn_ini,
+                 const float* accad, const float* spin, const float* acestn, void* stream);
+
+/* reference src/predictor_corrector.h:51-67 */
+int lq_corrector(const void* par_host, const void* par_device,
+                 float* pospres, float* velrhop, float* idep, float* str, float* stn,
+                 const float* pospres_ini, const float* velrhop_ini, const float* idep_ini,
+                 const float* str_ini, const float* stn_ini,
+                 const float* accad, const float* spin, const float* acestn, void* stream);
+
+/* ---- whole-step driver (the hot loop of LoquatSph::RunSimulation,
+ *      reference src/loquat.cu:322-409) ------------------------------------ */
+#define LQ_SIM_GRAPH   1   /* replay each step as one captured CUDA graph      */
+
+/* Creates a simulation from host arrays (np = par->np particles, boundary
+ * first).  par must have been through lq_initialize_parameters.  The state
+ * is uploaded, sorted once (reference src/loquat.cu:297-298) and kept on
+ * the device. */
+int lq_sim_create(const void* par_host,
+                  const float* pospres, const float* velrhop, const float* idep,
+                  const float* str, const float* stn, int flags, void** sim);
+int lq_sim_destroy(void* sim);
+/* Advances nsteps time steps, queued on the simulation's stream. */
+int lq_sim_step(void* sim, int nsteps);
+int lq_sim_synchronize(void* sim);
+int lq_sim_stream(void* sim, void** stream);
+/* Host <-> device copies of the whole state, in the current sorted order. */
+int lq_sim_upload(void* sim, const float* pospres, const float* velrhop, const float* idep,
+                  const float* str, const float* stn);
+int lq_sim_download(void* sim, float* pospres, float* velrhop, float* idep,
+                    float* str, float* stn);
+/* Device pointers of the current state (valid until the next lq_sim_step). */
+int lq_sim_state(void* sim, float** pospres, float** velrhop, float** idep,
+                 float** str, float** stn);
+/* Step counter and simulated time. */
+int lq_sim_clock(void* sim, long long* step, double* time);
+/* Health word: [0] non-finite material values, [1] material particles
+ * outside the cell lattice, [2] boundary particles outside the lattice,
+ * [3] reserved.  Reading it synchronises the stream. */
+int lq_sim_health(void* sim, int* health4);
+/* Kernel launches per time step of this simulation (without/with Shepard). */
+int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard);
+
+/* ---- XML / .dat formats (reference src/loquat_io.cu:69-370) ------------ */
+int lq_io_load_parameters(const char* xml_path, void* par_host);
+int lq_io_save_parameters(const char* xml_path, const void* par_host);
+int lq_io_load_particles(const char* dat_path, int np,
+                         float* pospres, float* velrhop, float* idep, float* str, float* stn);
+int lq_io_save_particles(const char* dat_path, int np,
+                         const float* pospres, const float* velrhop, const float* idep,
+                         const float* str, const float* stn);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LOQUAT_B200_C_ABI_H */

@@ -1,0 +1,95 @@
+"""Build the LOQUAT-B200 shared library for sm_100a.
+
+    python -m loquat_b200.build [--verbose-ptxas] [--force]
+
+Compiles every ``csrc/*.cu`` / ``csrc/*.cpp`` with nvcc
+(``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3``) into objects under
+``loquat_b200/_build/`` and links ``loquat_b200/liblqb200.so`` in-tree, with
+the CUDA runtime linked statically so the library needs no loader path.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+INCLUDE = ROOT / "include"
+BUILD = PKG / "_build"
+LIB = PKG / "liblqb200.so"
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = [
+    "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
+    "-Xcompiler", "-fPIC,-O3,-fvisibility=default",
+    f"-I{INCLUDE}", f"-I{CSRC}",
+]
+
+
+def _sources():
+    return sorted(list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cpp")))
+
+
+def _headers():
+    return sorted(list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(INCLUDE.glob("*.h")))
+
+
+def _stale(obj: Path, src: Path, hdr_mtime: float) -> bool:
+    if not obj.exists():
+        return True
+    m = obj.stat().st_mtime
+    return m < src.stat().st_mtime or m < hdr_mtime
+
+
+def _compile(src: Path, ptxas_verbose: bool) -> tuple[Path, str]:
+    obj = BUILD / (src.name + ".o")
+    cmd = [NVCC, *ARCH, *COMMON, "-c", str(src), "-o", str(obj)]
+    if ptxas_verbose and src.suffix == ".cu":
+        cmd += ["-Xptxas", "-v"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {src.name}:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    return obj, r.stderr
+
+
+def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = True) -> Path:
+    """Compile and link the library; returns its path."""
+    BUILD.mkdir(exist_ok=True)
+    hdr_mtime = max((h.stat().st_mtime for h in _headers()), default=0.0)
+    srcs = _sources()
+    todo = [s for s in srcs if force or ptxas_verbose or _stale(BUILD / (s.name + ".o"), s, hdr_mtime)]
+    reports = []
+    if todo:
+        with cf.ThreadPoolExecutor(max_workers=min(8, len(todo))) as ex:
+            for obj, err in ex.map(lambda s: _compile(s, ptxas_verbose), todo):
+                if err.strip():
+                    reports.append((obj.name, err))
+    objs = [BUILD / (s.name + ".o") for s in srcs]
+    if force or todo or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
+        cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-cudart", "static"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    if not quiet or ptxas_verbose:
+        for name, err in reports:
+            print(f"== {name}\n{err}", file=sys.stderr)
+    return LIB
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--verbose-ptxas", action="store_true")
+    a = ap.parse_args(argv)
+    lib = build(force=a.force, ptxas_verbose=a.verbose_ptxas, quiet=False)
+    print(lib)
+
+
+if __name__ == "__main__":
+    main()

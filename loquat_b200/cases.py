@@ -1,0 +1,238 @@
+"""Seeded synthetic cases in LOQUAT's input conventions.
+
+The reference ships one example whose particle file is absent, so every input
+is generated here: soil on a jittered cubic lattice, Adami dummy particles in
+layers on the floor (and walls), geostatic K0 stress, boundary particles
+stored first (reference src/loquat_io.cu:204-237 reads them in file order and
+the kernels index material particles from npb).  Coordinates start at 0
+because the reference grid hashes raw coordinates (src/adami_boundary.cu:80-82).
+
+Parameter conventions pinned by the reference's example
+(examples/sand_collapse_plane.xml:12-28): cs = sqrt(K / rho0), dt = cfl h / cs,
+k_phi = 6 sin(phi) / (sqrt(3) (3 + sin(phi))).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .params import Parameters, dp_cone, elastic_moduli
+
+
+@dataclass
+class Case:
+    name: str
+    par: Parameters
+    pospres: np.ndarray   # (np, 4) x, y, z, pressure
+    velrhop: np.ndarray   # (np, 4) vx, vy, vz, density
+    idep: np.ndarray      # (np, 4) object id, plastic strain, 0, 0
+    str_: np.ndarray      # (np, 6) stress, tension positive
+    stn: np.ndarray       # (np, 6) strain
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def np_(self) -> int:
+        return self.pospres.shape[0]
+
+    def arrays(self):
+        return self.pospres, self.velrhop, self.idep, self.str_, self.stn
+
+    def with_ids(self) -> "Case":
+        """Copy whose idep.w holds each particle's original index (exact in
+        float below 2**24), so particles can be matched after re-sorting;
+        no kernel reads idep.z or idep.w."""
+        idep = self.idep.copy()
+        n = idep.shape[0]
+        idep[:, 3] = np.arange(n, dtype=np.float64).astype(np.float32)
+        if n >= 1 << 24:
+            idep[:, 2] = (np.arange(n) >> 24).astype(np.float32)
+            idep[:, 3] = (np.arange(n) & ((1 << 24) - 1)).astype(np.float32)
+        return Case(self.name, self.par.copy(), self.pospres.copy(), self.velrhop.copy(), idep,
+                    self.str_.copy(), self.stn.copy(), dict(self.meta))
+
+
+def _lattice(nx, ny, nz, dr, origin):
+    i, j, k = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    pts = np.stack([i.ravel(), j.ravel(), k.ravel()], axis=1).astype(np.float64)
+    return (pts + 0.5) * dr + np.asarray(origin, np.float64)
+
+
+def _base_parameters(dr, hdr, rho0, domain, E, nu, cfl, model, model_pars, shepard, alpha, gravity):
+    p = Parameters()
+    p.domain_size_x, p.domain_size_y, p.domain_size_z = map(float, domain)
+    p.domain_min_x = p.domain_min_y = p.domain_min_z = 0.0
+    p.dr, p.hdr, p.rho0 = dr, hdr, rho0
+    K, G = elastic_moduli(E, nu)
+    p.cs = math.sqrt(K / rho0)
+    p.cfl = cfl
+    p.constitutive_model = model
+    (p.model_par_1, p.model_par_2, p.model_par_3, p.model_par_4, p.model_par_5) = model_pars(K, G)
+    p.density_shepard_filter = 0
+    p.stress_shepard_filter = shepard
+    p.dynamic_time_step = 0
+    p.integration_method = 1
+    p.viscosity_type = 1
+    p.artificial_viscosity_alpha = alpha
+    p.artificial_pressure = 0
+    p.artificial_pressure_coefficient = 0.0
+    p.acc_x, p.acc_y, p.acc_z = gravity
+    p.time = 0.0
+    p.output_frequency = 1.0
+    p.output_number = 0
+    p.output_format = 1
+    return p
+
+
+def assemble(name, par, boundary_xyz, soil_xyz, rng, jitter, rho0, gravity_z, top_z, floor_z, K0,
+             object_ids=(0, 1), meta=None) -> Case:
+    """Stacks boundary then soil particles, jitters them, sets geostatic stress.
+
+    Soil stress: sigma_zz = rho0 g (top - z) (negative: compression), sigma_xx =
+    sigma_yy = K0 sigma_zz, pressure = -tr(sigma)/3.  Boundary stress starts at
+    0 (the Adami pass overwrites it)."""
+    from . import initialize_parameters
+
+    nb, ns = boundary_xyz.shape[0], soil_xyz.shape[0]
+    xyz = np.concatenate([boundary_xyz, soil_xyz], axis=0)
+    if jitter > 0:
+        xyz = xyz + rng.uniform(-jitter, jitter, size=xyz.shape)
+    n = nb + ns
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = xyz.astype(np.float32)
+    vel = np.zeros((n, 4), np.float32)
+    vel[:, 3] = rho0
+    idep = np.zeros((n, 4), np.float32)
+    idep[:nb, 0] = object_ids[0]
+    idep[nb:, 0] = object_ids[1]
+    s = np.zeros((n, 6), np.float32)
+    z = pos[nb:, 2].astype(np.float64)
+    top = top_z(pos[nb:, :3].astype(np.float64)) if callable(top_z) else top_z
+    szz = rho0 * gravity_z * (top - z)  # gravity_z < 0 -> compression below the top
+    szz = np.minimum(szz, 0.0)
+    s[nb:, 2] = szz
+    s[nb:, 0] = K0 * szz
+    s[nb:, 1] = K0 * szz
+    pos[nb:, 3] = (-(s[nb:, 0].astype(np.float64) + s[nb:, 1] + s[nb:, 2]) / 3.0).astype(np.float32)
+    stn = np.zeros((n, 6), np.float32)
+    par.np, par.npb, par.npm = n, nb, ns
+    initialize_parameters(par)
+    par.dt = par.cfl * par.h / par.cs
+    m = dict(meta or {})
+    m.update(np=n, npb=nb, npm=ns)
+    return Case(name, par, pos, vel, idep, s, stn, m)
+
+
+def column_collapse(dr=0.002, length=0.2, height=0.1, thickness=0.02, runout=0.6, layers=3, hdr=1.2,
+                    rho0=2650.0, E=0.84e6, nu=0.3, phi=19.8, psi=0.0, cohesion=0.0, cfl=0.1, alpha=0.25,
+                    shepard=30, seed=1, jitter_frac=0.01, side_walls=True, name="column_collapse") -> Case:
+    """Granular column collapse: the 3D slab of the reference's
+    sand_collapse_plane shape class.  Soil block length x height x thickness
+    against a back wall at x = 0, on a floor, between two side walls (y),
+    all of `layers` Adami layers; the floor and side walls run `runout` in x."""
+    b = layers * dr
+    nsx, nsy, nsz = round(length / dr), round(thickness / dr), round(height / dr)
+    nrx = round(runout / dr)
+    nwy = nsy + 2 * layers if side_walls else nsy
+    wall_top = height + 0.1 * height
+    nwz = round(wall_top / dr)
+    y0 = b if side_walls else 0.0
+    soil = _lattice(nsx, nsy, nsz, dr, (b, y0, b))
+    parts = [_lattice(nrx + layers, nwy, layers, dr, (0.0, 0.0, 0.0))]          # floor
+    parts.append(_lattice(layers, nsy, nwz, dr, (0.0, y0, b)))                   # back wall
+    if side_walls:
+        parts.append(_lattice(nrx + layers, layers, nwz, dr, (0.0, 0.0, b)))     # y = 0 side
+        parts.append(_lattice(nrx + layers, layers, nwz, dr, (0.0, y0 + nsy * dr, b)))
+    bnd = np.concatenate(parts, axis=0)
+    domain = ((nrx + layers) * dr, nwy * dr, b + 1.5 * height)
+    kphi, kpsi, kc = dp_cone(phi, psi, cohesion)
+    par = _base_parameters(dr, hdr, rho0, domain, E, nu, cfl, 1, lambda K, G: (K, G, kphi, kpsi, kc), shepard,
+                           alpha, (0.0, 0.0, -9.81))
+    K0 = 1.0 - math.sin(math.radians(phi))
+    rng = np.random.default_rng(seed)
+    return assemble(name, par, bnd, soil, rng, jitter_frac * dr, rho0, -9.81, b + height, b, K0,
+                    meta=dict(config="column", dr=dr, soil_lattice=(nsx, nsy, nsz), phi=phi))
+
+
+def cylinder_collapse(dr=0.002949, radius=0.2, height=0.4, floor_radius_factor=2.5, layers=3, hdr=1.3,
+                      rho0=2000.0, E=5.0e6, nu=0.3, phi=30.0, psi=0.0, cohesion=0.0, cfl=0.1, alpha=0.25,
+                      shepard=30, seed=1, jitter_frac=0.01, name="cylinder_collapse") -> Case:
+    """Axisymmetric cylinder collapse on a square Adami floor of half-width
+    floor_radius_factor * radius.  At dr = 2.949 mm the cylinder holds about
+    1.96 M soil particles (at 4 mm it would hold 0.79 M)."""
+    b = layers * dr
+    half = floor_radius_factor * radius
+    nf = round(2 * half / dr)
+    side = nf * dr
+    cx = cy = side / 2.0
+    nr = int(math.ceil(radius / dr)) + 1
+    nz = round(height / dr)
+    ii = np.arange(-nr, nr)
+    gx, gy = np.meshgrid(ii, ii, indexing="ij")
+    px = (gx.ravel() + 0.5) * dr
+    py = (gy.ravel() + 0.5) * dr
+    inside = px * px + py * py <= radius * radius
+    px, py = px[inside] + cx, py[inside] + cy
+    zs = (np.arange(nz) + 0.5) * dr + b
+    soil = np.stack([np.repeat(px[None, :], nz, 0).ravel(), np.repeat(py[None, :], nz, 0).ravel(),
+                     np.repeat(zs[:, None], px.size, 1).ravel()], axis=1)
+    bnd = _lattice(nf, nf, layers, dr, (0.0, 0.0, 0.0))
+    domain = (side, side, b + 1.15 * height)
+    kphi, kpsi, kc = dp_cone(phi, psi, cohesion)
+    par = _base_parameters(dr, hdr, rho0, domain, E, nu, cfl, 1, lambda K, G: (K, G, kphi, kpsi, kc), shepard,
+                           alpha, (0.0, 0.0, -9.81))
+    K0 = 1.0 - math.sin(math.radians(phi))
+    rng = np.random.default_rng(seed)
+    return assemble(name, par, bnd, soil, rng, jitter_frac * dr, rho0, -9.81, b + height, b, K0,
+                    meta=dict(config="cylinder", dr=dr, radius=radius, height=height, phi=phi))
+
+
+def small_column(nsx=16, nsy=6, nsz=12, dr=0.002, layers=3, hdr=1.2, model=1, seed=3, jitter_frac=0.01,
+                 velocity_noise=0.0, shepard=5, hypo_pars=(-106.5, -801.5, -797.1, 1077.7, 0.0),
+                 E=0.84e6, nu=0.3, phi=19.8, cohesion=0.0, rho0=2650.0, alpha=0.25, front_wall=False,
+                 name="small_column") -> Case:
+    """A few-thousand-particle column for parity tests.  `velocity_noise`
+    (m/s) adds a seeded random velocity to the soil so every term of the
+    interaction pass is exercised from the first step.  model 2 uses the
+    four-parameter hypoplastic law with `hypo_pars` = (c1, c2, c3, c4, cohesion).
+    `front_wall` closes the box at the soil's free face (a confined block)."""
+    b = layers * dr
+    nrx = nsx + (0 if front_wall else 10)
+    soil = _lattice(nsx, nsy, nsz, dr, (b, b, b))
+    nwy = nsy + 2 * layers
+    nwz = nsz + 2
+    parts = [
+        _lattice(nrx + 2 * layers, nwy, layers, dr, (0.0, 0.0, 0.0)),
+        _lattice(layers, nsy, nwz, dr, (0.0, b, b)),
+        _lattice(nrx + 2 * layers, layers, nwz, dr, (0.0, 0.0, b)),
+        _lattice(nrx + 2 * layers, layers, nwz, dr, (0.0, b + nsy * dr, b)),
+    ]
+    if front_wall:
+        parts.append(_lattice(layers, nsy, nwz, dr, (b + nsx * dr, b, b)))
+    bnd = np.concatenate(parts)
+    domain = ((nrx + 2 * layers) * dr, nwy * dr, b + 1.6 * nsz * dr)
+    if model == 1:
+        kphi, kpsi, kc = dp_cone(phi, 0.0, cohesion)
+        pars = lambda K, G: (K, G, kphi, kpsi, kc)  # noqa: E731
+    else:
+        pars = lambda K, G: tuple(hypo_pars)  # noqa: E731
+    par = _base_parameters(dr, hdr, rho0, domain, E, nu, 0.1, model, pars, shepard, alpha, (0.0, 0.0, -9.81))
+    K0 = 1.0 - math.sin(math.radians(phi))
+    rng = np.random.default_rng(seed)
+    c = assemble(name, par, bnd, soil, rng, jitter_frac * dr, rho0, -9.81, b + nsz * dr, b, K0,
+                 meta=dict(config="small", dr=dr, top=b + nsz * dr))
+    if velocity_noise > 0:
+        nb = c.par.npb
+        c.velrhop[nb:, :3] = rng.uniform(-velocity_noise, velocity_noise, size=(c.par.npm, 3)).astype(np.float32)
+    return c
+
+
+def config_case(index: int, **kw) -> Case:
+    """Case of one of the benchmark configurations (0-based):
+    0 column collapse 50k, 1 cylinder collapse ~1.96M (plain FP32 form)."""
+    if index == 0:
+        return column_collapse(**kw)
+    if index == 1:
+        return cylinder_collapse(**kw)
+    raise ValueError(f"configuration {index} has no generator yet")

@@ -1,0 +1,248 @@
+/*
+ * LOQUAT-B200 predictor-corrector integrator with the Drucker-Prager and
+ * hypoplastic stress updates (reference src/predictor_corrector.cu:169-336),
+ * its C ABI entry points and the C++ drop-in functions.
+ *
+ * The reference issues five device-to-device snapshot copies and then the
+ * predictor kernel; here the snapshot is written by the same kernel that
+ * reads the state, so the state is read once.  The native driver skips the
+ * snapshot entirely: the predictor writes into a second buffer and the
+ * corrector reads the untouched first buffer through the new sort
+ * permutation.
+ */
+#include <cstdio>
+#include <cstdlib>
+
+#include "lq_internal.cuh"
+#include "lq_device.cuh"
+#include <predictor_corrector.h>
+
+namespace lqb {
+
+namespace {
+
+constexpr int kBlock = 128;
+
+inline int blocks_for(long long n, int b) { return (int)((n + b - 1) / b); }
+
+/* Half step of the material slots (reference src/predictor_corrector.cu:169-218):
+ * v += dt/2 a; rho += dt/2 drho; x += dt/2 v_new; eps += dt/2 deps;
+ * stress and plastic strain from the model at dt/2. */
+__global__ void __launch_bounds__(kBlock) k_predict(const Parameters* __restrict__ P, int np, int npb, State in,
+                                                    State out, State snap, bool do_snap, Rates rt)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    const float4 x0 = in.pos[i];
+    const float4 v0 = in.vel[i];
+    const float4 id = in.idep[i];
+    const tensor2d s0 = load_t2_rw(in.str, i);
+    const tensor2d e0 = load_t2_rw(in.stn, i);
+    if (do_snap) {
+        snap.pos[i] = x0;
+        snap.vel[i] = v0;
+        snap.idep[i] = id;
+        store_t2(snap.str, i, s0);
+        store_t2(snap.stn, i, e0);
+    }
+    if (i < npb) {
+        if (out.pos != in.pos) {
+            out.pos[i] = x0;
+            out.vel[i] = v0;
+            out.idep[i] = id;
+            store_t2(out.str, i, s0);
+            store_t2(out.stn, i, e0);
+        }
+        return;
+    }
+    const float dt = __ldg(&P->dt);
+    const Material M = load_material(P);
+    const float4 a = __ldg(rt.accad + i);
+    const float4 w = __ldg(rt.spin + i);
+    const tensor2d de = load_t2(rt.acestn, i);
+
+    float4 v = v0;
+    v.x += 0.5f * dt * a.x;
+    v.y += 0.5f * dt * a.y;
+    v.z += 0.5f * dt * a.z;
+    v.w += 0.5f * dt * a.w;
+    float4 x = x0;
+    x.x += 0.5f * dt * v.x;
+    x.y += 0.5f * dt * v.y;
+    x.z += 0.5f * dt * v.z;
+    const tensor2d e = e0 + de * (0.5f * dt);
+
+    float p = x0.w;
+    float ep = id.y;
+    tensor2d s = s0;
+    if (M.model == 1) {
+        dp_update(M, 0.5f * dt, w, de, p, ep, s);
+    } else {
+        hypo_update(M, 0.5f * dt, de, w, s);
+        ep = sqrtf(2.0f / 3.0f * J2(e));
+    }
+    x.w = p;
+    out.pos[i] = x;
+    out.vel[i] = v;
+    out.idep[i] = make_float4(id.x, ep, id.z, id.w);
+    store_t2(out.str, i, s);
+    store_t2(out.stn, i, e);
+}
+
+/* Full step from the snapshot (reference src/predictor_corrector.cu:256-307):
+ * v = v0 + dt a; x = x0 + dt/2 (v + v0); eps = eps0 + dt deps; the model
+ * restarts from the snapshot stress and plastic strain; the pressure passed
+ * in is the current one. */
+__global__ void __launch_bounds__(kBlock) k_correct(const Parameters* __restrict__ P, int np, int npb, State cur,
+                                                    State ini, const int* __restrict__ ini_idx, Rates rt,
+                                                    int* __restrict__ health)
+{
+    const int i = npb + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    const int k = ini_idx ? __ldg(ini_idx + i) : i;
+    const float dt = __ldg(&P->dt);
+    const Material M = load_material(P);
+    const float4 a = __ldg(rt.accad + i);
+    const float4 w = __ldg(rt.spin + i);
+    const tensor2d de = load_t2(rt.acestn, i);
+    const float4 x0 = ini.pos[k];
+    const float4 v0 = ini.vel[k];
+    const float ep0 = ini.idep[k].y;
+    const tensor2d s0 = load_t2_rw(ini.str, k);
+    const tensor2d e0 = load_t2_rw(ini.stn, k);
+    const float4 xc = cur.pos[i];
+    const float4 id = cur.idep[i];
+
+    float4 v;
+    v.x = v0.x + dt * a.x;
+    v.y = v0.y + dt * a.y;
+    v.z = v0.z + dt * a.z;
+    v.w = v0.w + dt * a.w;
+    float4 x;
+    x.x = 0.5f * (v.x + v0.x) * dt + x0.x;
+    x.y = 0.5f * (v.y + v0.y) * dt + x0.y;
+    x.z = 0.5f * (v.z + v0.z) * dt + x0.z;
+    const tensor2d e = e0 + de * dt;
+
+    float p = xc.w;
+    float ep = ep0;
+    tensor2d s = s0;
+    if (M.model == 1) {
+        dp_update(M, dt, w, de, p, ep, s);
+    } else {
+        hypo_update(M, dt, de, w, s);
+        ep = sqrtf(2.0f / 3.0f * J2(e));
+    }
+    x.w = p;
+    cur.pos[i] = x;
+    cur.vel[i] = v;
+    cur.idep[i] = make_float4(id.x, ep, id.z, id.w);
+    store_t2(cur.str, i, s);
+    store_t2(cur.stn, i, e);
+    if (health) {
+        const bool ok = isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(v.x) && isfinite(v.y) &&
+                        isfinite(v.z) && isfinite(v.w) && isfinite(s.xx) && isfinite(s.yy) && isfinite(s.zz) &&
+                        isfinite(s.xy) && isfinite(s.xz) && isfinite(s.yz);
+        if (!ok) atomicAdd(health + HEALTH_NONFINITE, 1);
+    }
+}
+
+}  // namespace
+
+int launch_predict(const Parameters* ph, const Parameters* pd, const State& in, const State& out, const State* snap,
+                   const Rates& r, cudaStream_t s)
+{
+    if (ph->np <= 0) return LQ_OK;
+    const bool do_snap = snap && snap->pos;
+    State sn = do_snap ? *snap : State{nullptr, nullptr, nullptr, nullptr, nullptr};
+    k_predict<<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_predict");
+    return LQ_OK;
+}
+
+int launch_correct(const Parameters* ph, const Parameters* pd, const State& cur, const State& ini,
+                   const int* ini_idx, const Rates& r, int* health, cudaStream_t s)
+{
+    if (ph->npm <= 0) return LQ_OK;
+    k_correct<<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, ini_idx, r, health);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_correct");
+    return LQ_OK;
+}
+
+}  // namespace lqb
+
+/* ------------------------------------------------------------------ C ABI */
+
+extern "C" int lq_predictor(const void* par_host, const void* par_device, float* pospres, float* velrhop,
+                            float* idep, float* str, float* stn, float* pospres_ini, float* velrhop_ini,
+                            float* idep_ini, float* str_ini, float* stn_ini, const float* accad, const float* spin,
+                            const float* acestn, void* stream)
+{
+    if (!par_host || !par_device) return lqb::set_error(LQ_ERR_ARG, "lq_predictor: null Parameters");
+    const Parameters* ph = static_cast<const Parameters*>(par_host);
+    if (ph->npm == 0) return LQ_OK; /* reference returns before the snapshot too */
+    if (!pospres || !velrhop || !idep || !str || !stn || !pospres_ini || !velrhop_ini || !idep_ini || !str_ini ||
+        !stn_ini || !accad || !spin || !acestn)
+        return lqb::set_error(LQ_ERR_ARG, "lq_predictor: null array");
+    lqb::State st{(float4*)pospres, (float4*)velrhop, (float4*)idep, (tensor2d*)str, (tensor2d*)stn};
+    lqb::State sn{(float4*)pospres_ini, (float4*)velrhop_ini, (float4*)idep_ini, (tensor2d*)str_ini,
+                  (tensor2d*)stn_ini};
+    lqb::Rates r{(float4*)accad, (float4*)spin, (tensor2d*)acestn};
+    return lqb::launch_predict(ph, static_cast<const Parameters*>(par_device), st, st, &sn, r,
+                               static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int lq_corrector(const void* par_host, const void* par_device, float* pospres, float* velrhop,
+                            float* idep, float* str, float* stn, const float* pospres_ini, const float* velrhop_ini,
+                            const float* idep_ini, const float* str_ini, const float* stn_ini, const float* accad,
+                            const float* spin, const float* acestn, void* stream)
+{
+    if (!par_host || !par_device) return lqb::set_error(LQ_ERR_ARG, "lq_corrector: null Parameters");
+    const Parameters* ph = static_cast<const Parameters*>(par_host);
+    if (ph->npm == 0) return LQ_OK;
+    if (!pospres || !velrhop || !idep || !str || !stn || !pospres_ini || !velrhop_ini || !idep_ini || !str_ini ||
+        !stn_ini || !accad || !spin || !acestn)
+        return lqb::set_error(LQ_ERR_ARG, "lq_corrector: null array");
+    lqb::State st{(float4*)pospres, (float4*)velrhop, (float4*)idep, (tensor2d*)str, (tensor2d*)stn};
+    lqb::State in{(float4*)pospres_ini, (float4*)velrhop_ini, (float4*)idep_ini, (tensor2d*)str_ini,
+                  (tensor2d*)stn_ini};
+    lqb::Rates r{(float4*)accad, (float4*)spin, (tensor2d*)acestn};
+    return lqb::launch_correct(ph, static_cast<const Parameters*>(par_device), st, in, nullptr, r, nullptr,
+                               static_cast<cudaStream_t>(stream));
+}
+
+/* ------------------------------------------- C++ drop-in functions */
+
+namespace {
+
+void check_or_die(int st, const char* what)
+{
+    if (st != LQ_OK) {
+        fprintf(stderr, "%s failed: %s\n", what, lq_last_error());
+        exit(EXIT_FAILURE);
+    }
+}
+
+}  // namespace
+
+void Predictor(Parameters* par_host, Parameters* par_device, float4* pospres, float4* velrhop, float4* idep,
+               tensor2d* str, tensor2d* stn, float4* pospres_ini, float4* velrhop_ini, float4* idep_ini,
+               tensor2d* str_ini, tensor2d* stn_ini, float4* accad, float4* spin, tensor2d* acestn)
+{
+    check_or_die(lq_predictor(par_host, par_device, (float*)pospres, (float*)velrhop, (float*)idep, (float*)str,
+                              (float*)stn, (float*)pospres_ini, (float*)velrhop_ini, (float*)idep_ini,
+                              (float*)str_ini, (float*)stn_ini, (const float*)accad, (const float*)spin,
+                              (const float*)acestn, nullptr),
+                 "Predictor");
+}
+
+void Corrector(Parameters* par_host, Parameters* par_device, float4* pospres, float4* velrhop, float4* idep,
+               tensor2d* str, tensor2d* stn, float4* pospres_ini, float4* velrhop_ini, float4* idep_ini,
+               tensor2d* str_ini, tensor2d* stn_ini, float4* accad, float4* spin, tensor2d* acestn)
+{
+    check_or_die(lq_corrector(par_host, par_device, (float*)pospres, (float*)velrhop, (float*)idep, (float*)str,
+                              (float*)stn, (const float*)pospres_ini, (const float*)velrhop_ini,
+                              (const float*)idep_ini, (const float*)str_ini, (const float*)stn_ini,
+                              (const float*)accad, (const float*)spin, (const float*)acestn, nullptr),
+                 "Corrector");
+}

@@ -1,0 +1,191 @@
+/*
+ * LOQUAT-B200 device helpers: cell arithmetic, neighbour-range lookup and
+ * the constitutive updates.  Everything here is inlined into the kernels.
+ */
+#pragma once
+
+#include <cuda_runtime.h>
+#include <types.h>
+#include "lq_internal.cuh"
+
+namespace lqb {
+
+/* 8-byte accesses of a 24-byte tensor2d (the widest aligned access). */
+__device__ __forceinline__ tensor2d load_t2(const tensor2d* p, int i)
+{
+    const float2* q = reinterpret_cast<const float2*>(p) + 3 * (size_t)i;
+    float2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+    return make_tensor2d(a.x, a.y, b.x, b.y, c.x, c.y);
+}
+
+__device__ __forceinline__ tensor2d load_t2_rw(const tensor2d* p, int i)
+{
+    const float2* q = reinterpret_cast<const float2*>(p) + 3 * (size_t)i;
+    float2 a = q[0], b = q[1], c = q[2];
+    return make_tensor2d(a.x, a.y, b.x, b.y, c.x, c.y);
+}
+
+__device__ __forceinline__ void store_t2(tensor2d* p, int i, const tensor2d& t)
+{
+    float2* q = reinterpret_cast<float2*>(p) + 3 * (size_t)i;
+    q[0] = make_float2(t.xx, t.yy);
+    q[1] = make_float2(t.zz, t.xy);
+    q[2] = make_float2(t.xz, t.yz);
+}
+
+/* Cell coordinate along one axis: floor((0.5 x) / h) from the raw
+ * coordinate (reference src/adami_boundary.cu:80-82).  Returns -1 outside
+ * [0, n) and for NaN. */
+__device__ __forceinline__ int cell_axis(float x, float i_h, int n)
+{
+    float s = floorf(0.5f * x * i_h);
+    return (s >= 0.0f && s < (float)n) ? (int)s : -1;
+}
+
+/* Unclamped coordinate used as the centre of a 27-cell stencil. */
+__device__ __forceinline__ int stencil_axis(float x, float i_h)
+{
+    return (int)floorf(0.5f * x * i_h);
+}
+
+/* The particles of the three cells (X, Y, zlo..zhi) of one layer are one
+ * contiguous slot range because keys are z-fastest and the sort is by key.
+ * Returns false when the range is empty. */
+__device__ __forceinline__ bool zrun_range(const Cells& c, int base, int zlo, int zhi, int& s, int& e)
+{
+    if (c.start) {
+        s = __ldg(c.start + base + zlo);
+        e = __ldg(c.start + base + zhi + 1);
+        return e > s;
+    }
+    s = -1;
+    for (int z = zlo; z <= zhi; ++z) {
+        int b = __ldg(c.beg + base + z);
+        if (b != -1) {
+            if (s < 0) s = b;
+            e = __ldg(c.end + base + z);
+        }
+    }
+    return s >= 0;
+}
+
+/* Jaumann co-rotational term with spin (W_yx, W_zx, W_zy)
+ * (reference src/predictor_corrector.cu:40-45). */
+__device__ __forceinline__ tensor2d jaumann(const float4& w, const tensor2d& s)
+{
+    tensor2d r;
+    r.xx = -2.0f * (w.x * s.xy + w.y * s.xz);
+    r.yy = 2.0f * (w.x * s.xy - w.z * s.yz);
+    r.zz = 2.0f * (w.y * s.xz + w.z * s.yz);
+    r.xy = w.x * (s.xx - s.yy) - w.z * s.xz - w.y * s.yz;
+    r.xz = w.y * (s.xx - s.zz) + w.z * s.xy - w.x * s.yz;
+    r.yz = w.z * (s.yy - s.zz) + w.x * s.xz + w.y * s.xy;
+    return r;
+}
+
+struct Material {
+    int model;
+    float p1, p2, p3, p4, p5;
+};
+
+__device__ __forceinline__ Material load_material(const Parameters* P)
+{
+    Material m;
+    m.model = __ldg(&P->constitutive_model);
+    m.p1 = __ldg(&P->model_par_1);
+    m.p2 = __ldg(&P->model_par_2);
+    m.p3 = __ldg(&P->model_par_3);
+    m.p4 = __ldg(&P->model_par_4);
+    m.p5 = __ldg(&P->model_par_5);
+    return m;
+}
+
+/* Drucker-Prager: elastic trial with Jaumann rate, tension cut-off, radial
+ * return to the cone (reference src/predictor_corrector.cu:30-105).
+ * K = p1, G = p2, k_phi = p3, k_psi = p4, k_c = p5. */
+__device__ __forceinline__ void dp_update(const Material& M, float dtp, const float4& w, const tensor2d& d,
+                                          float& p, float& ep, tensor2d& s)
+{
+    const float K = M.p1, G = M.p2, kphi = M.p3, kpsi = M.p4, kc = M.p5;
+    tensor2d r = jaumann(w, s);
+    r = r + d * (2.0f * G);
+    float ace = (K - 2.0f / 3.0f * G) * (d.xx + d.yy + d.zz);
+    r.xx += ace;
+    r.yy += ace;
+    r.zz += ace;
+    s = s + r * dtp;
+
+    float sm = (s.xx + s.yy + s.zz) / 3.0f;
+    s.xx -= sm;
+    s.yy -= sm;
+    s.zz -= sm;
+
+    float tenf = (kphi == 0.0f) ? 0.0f : kc / kphi;
+    float over = sm - tenf;                      /* tension cut-off */
+    if (over >= 0.0f) {
+        float dl = over / K;
+        sm = tenf;
+        ep += dl * (1.0f / 3.0f) * sqrtf(2.0f);
+    }
+    float tau = sqrtf(0.5f * J2(s));
+    float f = tau + kphi * sm - kc;              /* shear yield function */
+    if (f > 0.0f) {
+        float dl = f / (G + K * kphi * kpsi);
+        sm -= K * kpsi * dl;
+        float ratio = tau < 1e-10f ? 1.0f : (kc - kphi * sm) / tau;
+        s.xx *= ratio;
+        s.yy *= ratio;
+        s.zz *= ratio;
+        s.xy *= ratio;
+        s.xz *= ratio;
+        s.yz *= ratio;
+        ep += dl * sqrtf(1.0f / 3.0f + 2.0f / 9.0f * kpsi * kpsi);
+    }
+    s.xx += sm;
+    s.yy += sm;
+    s.zz += sm;
+    p = -sm;
+}
+
+/* Four-parameter hypoplastic rate (c1..c4 = p1..p4, cohesion = p5) with the
+ * Jaumann term, cohesion shift and tension cap
+ * (reference src/predictor_corrector.cu:111-165).  The near-zero-stress
+ * reset leaves T_xz as it is, as the reference does. */
+__device__ __forceinline__ void hypo_update(const Material& M, float dtp, const tensor2d& d, const float4& w,
+                                            tensor2d& s)
+{
+    const float c1 = M.p1, c2 = M.p2, c3 = M.p3, c4 = M.p4, coh = M.p5;
+    tensor2d jau = jaumann(w, s);
+    tensor2d T = s;
+    if (coh > 0.0f) {
+        T.xx -= coh;
+        T.yy -= coh;
+        T.zz -= coh;
+    }
+    float t1 = T.xx + T.yy + T.zz;
+    if (fabsf(t1) < 4.0f) {
+        t1 = -4.0f;
+        T.xx = -1.0f;
+        T.yy = -1.0f;
+        T.zz = -2.0f;
+        T.xy = 0.0f;
+        T.yz = 0.0f;
+    }
+    tensor2d Ts = T;
+    Ts.xx -= t1 / 3.0f;
+    Ts.yy -= t1 / 3.0f;
+    Ts.zz -= t1 / 3.0f;
+    float d1 = d.xx + d.yy + d.zz;
+    float td = J2(T, d);
+    float nd = sqrtf(J2(d));
+    tensor2d rate = jau + d * (c1 * t1) + T * (c2 * d1 + c3 * td / t1) + (T + Ts) * (c4 * nd);
+    s = s + rate * dtp;
+    float pres = (s.xx + s.yy + s.zz) / 3.0f;
+    if (pres > coh) {
+        s.xx -= (pres - coh);
+        s.yy -= (pres - coh);
+        s.zz -= (pres - coh);
+    }
+}
+
+}  // namespace lqb

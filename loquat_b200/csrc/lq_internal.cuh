@@ -1,0 +1,112 @@
+/*
+ * LOQUAT-B200 internal declarations shared by the translation units of the
+ * library: array bundles, launch wrappers and error reporting.
+ */
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include <types.h>
+#include <loquat_b200.h>
+
+namespace lqb {
+
+/* ---------------------------------------------------------------- errors */
+int set_error(int status, const char* fmt, ...);
+int cuda_status(cudaError_t e, const char* what);
+
+#define LQ_TRY_CUDA(expr, what)                                    \
+    do {                                                           \
+        cudaError_t lq_e_ = (expr);                                \
+        if (lq_e_ != cudaSuccess) return ::lqb::cuda_status(lq_e_, what); \
+    } while (0)
+
+#define LQ_TRY(expr)                                               \
+    do {                                                           \
+        int lq_s_ = (expr);                                        \
+        if (lq_s_ != LQ_OK) return lq_s_;                          \
+    } while (0)
+
+/* --------------------------------------------------------------- arrays */
+/* The five sorted state arrays (reference src/loquat.h:61-66). */
+struct State {
+    float4* pos;     /* x, y, z, pressure                 */
+    float4* vel;     /* vx, vy, vz, density               */
+    float4* idep;    /* object id, plastic strain, -, -   */
+    tensor2d* str;   /* Cauchy stress, tension positive   */
+    tensor2d* stn;   /* total strain                      */
+};
+
+/* Per-stage rates written by the interaction pass (reference src/loquat.h:74-77). */
+struct Rates {
+    float4* accad;     /* dv/dt, drho/dt   */
+    float4* spin;      /* W_yx, W_zx, W_zy */
+    tensor2d* acestn;  /* strain rate      */
+};
+
+/* Cell lookup.  With `start` (ncell + 1 entries) the particles of cell c are
+ * [start[c], start[c+1]).  Otherwise `beg`/`end` hold the reference's
+ * per-cell bounds with -1 for an empty cell. */
+struct Cells {
+    const int* start;
+    const int* beg;
+    const int* end;
+};
+
+/* Health counters written by the kernels (see lq_sim_health). */
+enum { HEALTH_NONFINITE = 0, HEALTH_MAT_OUT = 1, HEALTH_BND_OUT = 2, HEALTH_WORDS = 4 };
+
+/* ----------------------------------------------------------------- grid */
+struct GridBuffers {
+    int np_cap = 0, ncell_cap = 0;
+    int* key = nullptr;       /* unsorted cell key              np */
+    int* rank = nullptr;      /* rank inside the cell           np */
+    int* count = nullptr;     /* particles per cell             ncell + 1 */
+    int* start = nullptr;     /* exclusive scan of count        ncell + 1 */
+    int* part_idx = nullptr;  /* sorted slot -> previous slot   np */
+    int* part_cel = nullptr;  /* sorted key                     np */
+    int* beg = nullptr;       /* optional per-cell bounds       ncell */
+    int* end = nullptr;
+    void* scan_tmp = nullptr;
+    size_t scan_bytes = 0;
+};
+
+/* Sizes the scan scratch for n_cells + 1 entries. */
+int scan_scratch_bytes(int ncell, size_t* bytes);
+
+/* Hash, count, scan, scatter and in-cell ordering: a stable sort of the
+ * particles by cell key.  Writes key, rank, count, start, part_idx,
+ * part_cel, and beg/end when `bounds` is set.  `health` may be null. */
+int grid_search(const Parameters* par_host, const Parameters* par_dev, const float4* pos, GridBuffers& g,
+                bool bounds, int* health, cudaStream_t s);
+
+int gather_float4(int n, const int* idx, const float4* in, float4* out, cudaStream_t s);
+int gather_tensor2d(int n, const int* idx, const tensor2d* in, tensor2d* out, cudaStream_t s);
+/* Gathers all five state arrays in one pass: out[i] = in[idx[i]]. */
+int gather_state(int n, const int* idx, const State& in, const State& out, cudaStream_t s);
+
+/* ------------------------------------------------------------ operators */
+int launch_interaction(const Parameters* par_host, const Parameters* par_dev, const State& st, const Rates& r,
+                       const Cells& c, cudaStream_t s);
+int launch_adami(const Parameters* par_host, const Parameters* par_dev, const State& st, const Cells& c,
+                 cudaStream_t s);
+/* Shepard filter of material stress into out_str[npb, np).  When `full` is
+ * set the kernel also copies every other array (and the boundary stress)
+ * from `st` to `out`, producing a complete new state. */
+int launch_shepard(const Parameters* par_host, const Parameters* par_dev, const State& st, tensor2d* out_str,
+                   const State* full, const Cells& c, cudaStream_t s);
+/* Predictor: out <- in advanced by dt/2 on material slots, boundary slots
+ * copied when out != in; `snap` (may be all-null) receives a copy of `in`. */
+int launch_predict(const Parameters* par_host, const Parameters* par_dev, const State& in, const State& out,
+                   const State* snap, const Rates& r, cudaStream_t s);
+/* Corrector in place on `cur`; ini values read at ini_idx[i] (identity when
+ * ini_idx is null).  Non-finite results are counted in health. */
+int launch_correct(const Parameters* par_host, const Parameters* par_dev, const State& cur, const State& ini,
+                   const int* ini_idx, const Rates& r, int* health, cudaStream_t s);
+
+/* Host-side copy of Parameters derivation (reference src/loquat.cu:111-139). */
+void initialize_parameters(Parameters* p);
+
+}  // namespace lqb
