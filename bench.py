@@ -1,0 +1,345 @@
+#!/usr/bin/env python
+"""Benchmark of LOQUAT's per-step SPH path on B200: particle-steps/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default): 3D cylinder collapse, R = 0.2 m, H = 0.4 m,
+dr = 2.949 mm (about 1.96 M soil particles) on a 3-layer Adami floor,
+Drucker-Prager phi = 30 deg, E = 5 MPa, nu = 0.3, rho = 2000 kg/m^3,
+Wendland C2 with h = 1.3 dr, plain FP32 form.  Seeded synthetic input.
+One step = predictor + corrector stages (search, gather, Adami,
+interaction, integration) plus the Shepard pass every 30 steps.
+
+`value` is material particle-steps/s of the whole job with the state
+resident in HBM (device time, CUDA events on the simulation's stream, max
+over ranks).  `e2e` is the same metric through the C ABI from pinned host
+buffers: state upload, every step followed by a device->host read of the
+16-byte health word, and the final state download, all inside the timed
+region.  Under torchrun every rank runs an independent replica (weak
+scaling, no collective in the data path).
+
+`--impl reference` times the CPU FP64 OpenMP restatement of the reference's
+algorithm (the reference has no CPU implementation of its own and its GPU
+build cannot be assembled: two of its libraries are not distributed) on a
+bounded sample of the workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+BYTES_INTERACTION_PER_PARTICLE = 112   # 56 B read (pos, velrhop, str) + 56 B written (accad, spin, acestn)
+FLOPS_PER_PAIR = 80                    # counted from the interaction kernel's pair body
+FLOPS_PER_CANDIDATE = 8                # distance test
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=250)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=["cylinder", "column"], default="cylinder")
+    ap.add_argument("--dr", type=float, default=None, help="override the particle spacing")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=10)
+    return ap.parse_args(argv)
+
+
+def make_case(args, rank=0):
+    from loquat_b200 import cases
+
+    if args.config == "cylinder":
+        kw = {} if args.dr is None else {"dr": args.dr}
+        return cases.cylinder_collapse(seed=1 + rank, **kw)
+    kw = {} if args.dr is None else {"dr": args.dr}
+    return cases.column_collapse(seed=1 + rank, **kw)
+
+
+def cpu_sample_case(args):
+    """Bounded CPU sample of the workload: the same material, spacing and
+    smoothing length on a cylinder scaled down to about 100 k soil particles."""
+    from loquat_b200 import cases
+
+    if args.config == "cylinder":
+        s = (1.0e5 / 1.96e6) ** (1.0 / 3.0)
+        return cases.cylinder_collapse(radius=0.2 * s, height=0.4 * s, seed=1), "cylinder R=%.4f m H=%.4f m" % (
+            0.2 * s, 0.4 * s)
+    return cases.column_collapse(seed=1), "column collapse 50k"
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profiles(workload: str):
+    """DRAM bytes per interaction launch from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / "interaction_traffic.json"
+    if not f.exists():
+        return None
+    try:
+        d = json.loads(f.read_text())
+        return d.get(workload)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.proc = None
+        self.path = None
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+            if gpu_id:
+                cmd += ["-i", gpu_id]
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def gpu_uuid(torch, dev):
+    try:
+        return "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        return None
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_cpu_baseline(args, steps=5, warmup=1):
+    """The FP64 oracle on all host threads on the bounded sample."""
+    import oracle
+
+    case, desc = cpu_sample_case(args)
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    sim = oracle.OracleSim(case.par, *case.arrays())
+    sim.step(warmup)
+    t0 = time.perf_counter()
+    sim.step(steps)
+    dt = time.perf_counter() - t0
+    sim.close()
+    value = case.par.npm * steps / dt
+    return {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{desc} at dr={case.meta['dr'] * 1e3:.3f} mm ({case.par.npm} soil + {case.par.npb} boundary "
+                      f"particles), {warmup} warm-up + {steps} timed steps, FP64"}, dt
+
+
+def bench_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    import oracle
+
+    case, desc = cpu_sample_case(args)
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    sim = oracle.OracleSim(case.par, *case.arrays())
+    sim.step(args.warmup)
+    t0 = time.perf_counter()
+    sim.step(args.steps)
+    dt = time.perf_counter() - t0
+    value = case.par.npm * args.steps / dt
+    out = {
+        "impl": "reference",
+        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / max(args.steps, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name(args), "sample": desc, "np": case.par.np, "npm": case.par.npm},
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+                         "sample": f"{desc} ({case.par.npm} soil particles), FP64 OpenMP restatement of the "
+                                   "reference algorithm"},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def workload_name(args):
+    if args.config == "cylinder":
+        return "cylinder collapse R=0.2 m H=0.4 m dr=%.3f mm h=1.3dr DP phi=30 (plain FP32)" % (
+            1e3 * (args.dr or 0.002949))
+    return "column collapse 0.2x0.1x0.02 m dr=2 mm h=1.2dr DP phi=19.8 (plain FP32)"
+
+
+def bench_ours(args):
+    import torch
+
+    world, rank, local = dist_setup()
+    if not torch.cuda.is_available():
+        print(json.dumps({"error": "no CUDA device"}))
+        return 1
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    import loquat_b200 as lq
+
+    case = make_case(args, rank)
+    par = case.par
+    npm, np_ = par.npm, par.np
+    sim = lq.Simulation(par, *case.arrays(), graph=True)
+    ext = torch.cuda.ExternalStream(sim.stream())
+    plain, with_shep = sim.launches_per_step()
+
+    sim.step(args.warmup)
+    sim.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    s0, _ = sim.clock()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(gpu_uuid(torch, local)) if rank == 0 else None
+    start.record(ext)
+    sim.step(args.steps)
+    end.record(ext)
+    sim.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop() if clocks else None
+    s1, _ = sim.clock()
+    ms = start.elapsed_time(end)
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    shep_steps = sum(1 for s in range(s0, s1) if par.stress_shepard_filter and s % par.stress_shepard_filter == 0
+                     and s != 0)
+    launches = (s1 - s0) * plain + shep_steps * (with_shep - plain)
+    value = npm * args.steps * world / (ms / 1e3)
+    health = sim.health()
+
+    # live per-phase device times (eager launches, CUDA events on the same stream)
+    prof = sim.profile(args.profile_steps) if args.profile_steps > 0 else {}
+    inter_ms, inter_n = prof.get("interaction", (0.0, 0))
+    t_int = inter_ms / max(inter_n, 1) / 1e3
+    peak, peak_kind = measured_peaks()
+    achieved_gbs = BYTES_INTERACTION_PER_PARTICLE * npm / t_int / 1e9 if t_int > 0 else None
+    workload = workload_name(args)
+    traffic = traffic_from_profiles(workload)
+
+    e2e = None
+    if not args.no_e2e:
+        host = [torch.empty(a.shape, dtype=torch.float32, pin_memory=True).numpy() for a in case.arrays()]
+        for h, a in zip(host, case.arrays()):
+            h[...] = a
+        out = [torch.empty(a.shape, dtype=torch.float32, pin_memory=True).numpy() for a in case.arrays()]
+        sim.synchronize()
+        if dist:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        sim.upload(*host)
+        for _ in range(args.steps):
+            sim.step(1)
+            sim.health()             # device -> host read of the step's result
+        sim.download(out)
+        e1.record(ext)
+        sim.synchronize()
+        ems = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ems], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        state_bytes = sum(a.nbytes for a in host)
+        e2e = {"value": npm * args.steps * world / (ems / 1e3), "unit": "particle-steps/s",
+               "h2d_bytes_per_step": state_bytes / args.steps,
+               "d2h_bytes_per_step": (state_bytes + 16 * args.steps) / args.steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu, _ = run_cpu_baseline(args)
+
+    if rank == 0:
+        line = {
+            "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload, "np": np_, "npm": npm, "npb": par.npb, "ncell": par.ncell,
+                       "form": "plain FP32, CUDA-graph step",
+                       "l2": "state larger than L2 (3 x %.0f MB state buffers)" % (np_ * 96 / 1e6),
+                       "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved_gbs / peak) if achieved_gbs else None, "traffic": traffic,
+                         "kernel": "k_interaction", "peak_kind": peak_kind,
+                         "bytes_per_launch": BYTES_INTERACTION_PER_PARTICLE * npm,
+                         "ms_per_launch": t_int * 1e3},
+            "phases_ms_per_step": {k: v[0] / max(args.profile_steps, 1) for k, v in prof.items()},
+            "gpu_launches": launches,
+            "health": [int(x) for x in health],
+            "clocks": clk,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    sim.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        return bench_reference(args)
+    return bench_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -135,6 +135,13 @@ int lq_sim_clock(void* sim, long long* step, double* time);
 int lq_sim_health(void* sim, int* health4);
 /* Kernel launches per time step of this simulation (without/with Shepard). */
 int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard);
+/* Advances nsteps steps launching kernels one by one with CUDA events
+ * around each phase, then synchronises and returns the summed device time
+ * per phase in phase_ms[6]: search, gather, Adami, interaction, integrate,
+ * Shepard (the phases of the reference's Timer, include/types.h:158-173,
+ * timed on the device instead of with std::clock).  phase_launches[6]
+ * (may be NULL) receives how many times each phase ran. */
+int lq_sim_profile(void* sim, int nsteps, double* phase_ms, int* phase_launches);
 
 /* ---- XML / .dat formats (reference src/loquat_io.cu:69-370) ------------ */
 int lq_io_load_parameters(const char* xml_path, void* par_host);

@@ -63,6 +63,7 @@ _SIGNATURES = {
     "lq_sim_clock": (_I, [_VP, ctypes.POINTER(_LL), ctypes.POINTER(_D)]),
     "lq_sim_health": (_I, [_VP, _VP]),
     "lq_sim_launches_per_step": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "lq_sim_profile": (_I, [_VP, _I, _VP, _VP]),
     "lq_io_load_parameters": (_I, [ctypes.c_char_p, _VP]),
     "lq_io_save_parameters": (_I, [ctypes.c_char_p, _VP]),
     "lq_io_load_particles": (_I, [ctypes.c_char_p, _I] + [_VP] * 5),
@@ -247,6 +248,16 @@ class Simulation:
         h = np.zeros(4, np.int32)
         check(lib().lq_sim_health(self.handle, h.ctypes.data), "lq_sim_health")
         return h
+
+    PHASES = ("search", "gather", "adami", "interaction", "integrate", "shepard")
+
+    def profile(self, n: int) -> dict:
+        """Runs n steps eagerly with CUDA events around each phase; returns
+        {phase: (total_ms, launches)}."""
+        ms = np.zeros(6, np.float64)
+        cnt = np.zeros(6, np.int32)
+        check(lib().lq_sim_profile(self.handle, n, ms.ctypes.data, cnt.ctypes.data), "lq_sim_profile")
+        return {p: (float(ms[k]), int(cnt[k])) for k, p in enumerate(self.PHASES)}
 
     def launches_per_step(self):
         a, b = _I(), _I()

@@ -42,10 +42,13 @@ __device__ __forceinline__ int cell_axis(float x, float i_h, int n)
     return (s >= 0.0f && s < (float)n) ? (int)s : -1;
 }
 
-/* Unclamped coordinate used as the centre of a 27-cell stencil. */
+/* Coordinate used as the centre of a 27-cell stencil.  Values far outside
+ * the lattice (and NaN) are clamped to -2 or 2^30 so that neighbour offsets
+ * cannot overflow; such stencils touch no cell. */
 __device__ __forceinline__ int stencil_axis(float x, float i_h)
 {
-    return (int)floorf(0.5f * x * i_h);
+    const float s = floorf(0.5f * x * i_h);
+    return (int)fminf(fmaxf(s, -2.0f), 1073741824.0f);
 }
 
 /* The particles of the three cells (X, Y, zlo..zhi) of one layer are one

@@ -98,6 +98,63 @@ int enqueue_step(LqSim* S)
     return LQ_OK;
 }
 
+/* Phases timed by lq_sim_profile, the reference's Timer phases
+ * (reference include/types.h:158-173, src/loquat.cu:345-395) with the
+ * search split from the gathers. */
+enum { PH_SEARCH = 0, PH_GATHER, PH_ADAMI, PH_INTERACTION, PH_INTEGRATE, PH_SHEPARD, PH_COUNT };
+
+struct PhaseTimer {
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> phase;
+    int used = 0;
+    int mark(cudaStream_t s, int ph)
+    {
+        if (used + 2 > (int)ev.size()) return lqb::set_error(LQ_ERR_ARG, "profile: event pool exhausted");
+        phase.push_back(ph);
+        LQ_TRY_CUDA(cudaEventRecord(ev[used], s), "profile event");
+        used += 1;
+        return LQ_OK;
+    }
+    int close(cudaStream_t s)
+    {
+        LQ_TRY_CUDA(cudaEventRecord(ev[used], s), "profile event");
+        used += 1;
+        return LQ_OK;
+    }
+};
+
+/* One eager time step with an event pair around every phase. */
+int enqueue_step_timed(LqSim* S, PhaseTimer& T)
+{
+    const Parameters* ph = &S->ph;
+    const Parameters* pd = S->pd;
+    cudaStream_t s = S->stream;
+    const lqb::Cells cells{S->g.start, nullptr, nullptr};
+    State* in[2] = {&S->C, &S->B};
+    State* out[2] = {&S->A, &S->C};
+    for (int stage = 0; stage < 2; ++stage) {
+        LQ_TRY(T.mark(s, PH_SEARCH));
+        LQ_TRY(lqb::grid_search(ph, pd, in[stage]->pos, S->g, false, S->health, s));
+        LQ_TRY(T.close(s));
+        LQ_TRY(T.mark(s, PH_GATHER));
+        LQ_TRY(lqb::gather_state(S->np, S->g.part_idx, *in[stage], *out[stage], s));
+        LQ_TRY(T.close(s));
+        LQ_TRY(T.mark(s, PH_ADAMI));
+        LQ_TRY(lqb::launch_adami(ph, pd, *out[stage], cells, s));
+        LQ_TRY(T.close(s));
+        LQ_TRY(T.mark(s, PH_INTERACTION));
+        LQ_TRY(lqb::launch_interaction(ph, pd, *out[stage], S->R, cells, s));
+        LQ_TRY(T.close(s));
+        LQ_TRY(T.mark(s, PH_INTEGRATE));
+        if (stage == 0)
+            LQ_TRY(lqb::launch_predict(ph, pd, S->A, S->B, nullptr, S->R, s));
+        else
+            LQ_TRY(lqb::launch_correct(ph, pd, S->C, S->A, S->g.part_idx, S->R, S->health, s));
+        LQ_TRY(T.close(s));
+    }
+    return LQ_OK;
+}
+
 /* Shepard stress filter (reference src/loquat.cu:400-409). */
 int enqueue_shepard(LqSim* S)
 {
@@ -338,4 +395,45 @@ extern "C" int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard
     if (plain) *plain = 2 * stage;
     if (with_shepard) *with_shepard = 2 * stage + per_search + 1 + 1;
     return LQ_OK;
+}
+
+extern "C" int lq_sim_profile(void* sim, int nsteps, double* phase_ms, int* phase_launches)
+{
+    if (!sim || nsteps < 0 || !phase_ms) return lqb::set_error(LQ_ERR_ARG, "lq_sim_profile: bad argument");
+    LqSim* S = static_cast<LqSim*>(sim);
+    PhaseTimer T;
+    const int per_step = 2 * 5 * 2 + 2;
+    T.ev.resize((size_t)nsteps * per_step + 4);
+    for (auto& e : T.ev) LQ_TRY_CUDA(cudaEventCreate(&e), "profile event create");
+    int st = LQ_OK;
+    const int N = S->ph.stress_shepard_filter;
+    for (int k = 0; k < nsteps && st == LQ_OK; ++k) {
+        S->ph.time = (float)S->time;
+        st = enqueue_step_timed(S, T);
+        if (st == LQ_OK && N != 0 && S->step % N == 0 && S->step != 0) {
+            st = T.mark(S->stream, PH_SHEPARD);
+            if (st == LQ_OK) st = enqueue_shepard(S);
+            if (st == LQ_OK) st = T.close(S->stream);
+        }
+        S->time += (double)S->ph.dt;
+        S->step++;
+    }
+    if (st == LQ_OK) {
+        cudaError_t e = cudaStreamSynchronize(S->stream);
+        if (e != cudaSuccess) st = lqb::cuda_status(e, "profile synchronize");
+    }
+    for (int p = 0; p < PH_COUNT; ++p) {
+        phase_ms[p] = 0.0;
+        if (phase_launches) phase_launches[p] = 0;
+    }
+    if (st == LQ_OK) {
+        for (size_t k = 0; k < T.phase.size(); ++k) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, T.ev[2 * k], T.ev[2 * k + 1]);
+            phase_ms[T.phase[k]] += ms;
+            if (phase_launches) phase_launches[T.phase[k]] += 1;
+        }
+    }
+    for (auto& e : T.ev) cudaEventDestroy(e);
+    return st;
 }

@@ -36,7 +36,8 @@ int main()
         (const void*)&lq_sim_create, (const void*)&lq_sim_destroy, (const void*)&lq_sim_step,
         (const void*)&lq_sim_synchronize, (const void*)&lq_sim_stream, (const void*)&lq_sim_upload,
         (const void*)&lq_sim_download, (const void*)&lq_sim_state, (const void*)&lq_sim_clock,
-        (const void*)&lq_sim_health, (const void*)&lq_sim_launches_per_step, (const void*)&lq_io_load_parameters,
+        (const void*)&lq_sim_health, (const void*)&lq_sim_launches_per_step, (const void*)&lq_sim_profile,
+        (const void*)&lq_io_load_parameters,
         (const void*)&lq_io_save_parameters, (const void*)&lq_io_load_particles, (const void*)&lq_io_save_particles,
     };
     int n = 0;
