@@ -70,6 +70,24 @@ int lq_grid_arrays(void* grid, const int** part_cel, const int** part_idx,
 int lq_grid_sort_float4(void* grid, int np, float* data, float* cache, void* stream);
 int lq_grid_sort_tensor2d(void* grid, int np, float* data, float* cache, void* stream);
 
+/* Neighbour search that allocates nothing; this entry point has no
+ * counterpart in the reference.  It is for callers that cannot allocate
+ * device memory themselves (a host code whose memory pool already holds
+ * the GPU's memory, a step loop that cannot take cudaMalloc's device-wide
+ * synchronisation).  Same result as lq_grid_neighbor_search, but the
+ * caller passes the outputs (part_cel, part_idx: int[np]; cell_beg,
+ * cell_end: int[ncell]) and the working arrays live in one fixed 17 MiB
+ * device array inside the library, held on every device that loads it
+ * until exit.  Limits: np <= LQ_NOALLOC_MAX_PARTICLES, ncell <=
+ * LQ_NOALLOC_MAX_CELLS, else LQ_ERR_ARG.  All calls on a device share that
+ * array: calls that overlap on the GPU race.  The first call on a device
+ * looks up the array's device address (with that device current); make
+ * it before any stream capture begins. */
+#define LQ_NOALLOC_MAX_PARTICLES 1048576
+#define LQ_NOALLOC_MAX_CELLS     1048575
+int lq_grid_neighbor_search_noalloc(const void* par_host, const void* par_device, const float* pospres,
+                                    int* part_cel, int* part_idx, int* cell_beg, int* cell_end, void* stream);
+
 /* ---- per-stage operators ------------------------------------------------ */
 /* reference src/particle_interaction.h:27-40 */
 int lq_particle_interaction(const void* par_host, const void* par_device,

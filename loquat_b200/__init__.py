@@ -47,6 +47,7 @@ _SIGNATURES = {
     "lq_grid_arrays": (_I, [_VP] + [ctypes.POINTER(_VP)] * 5),
     "lq_grid_sort_float4": (_I, [_VP, _I, _VP, _VP, _VP]),
     "lq_grid_sort_tensor2d": (_I, [_VP, _I, _VP, _VP, _VP]),
+    "lq_grid_neighbor_search_noalloc": (_I, [_VP] * 8),
     "lq_particle_interaction": (_I, [_VP] * 13),
     "lq_adami_boundary": (_I, [_VP] * 8),
     "lq_stress_regularization": (_I, [_VP] * 9),
@@ -125,6 +126,20 @@ def initialize_parameters(par: Parameters) -> Parameters:
 def update_time_step(par: Parameters) -> Parameters:
     check(lib().lq_update_time_step(ctypes.byref(par)), "lq_update_time_step")
     return par
+
+
+LQ_NOALLOC_MAX_PARTICLES = 1048576
+LQ_NOALLOC_MAX_CELLS = 1048575
+
+
+def grid_neighbor_search_noalloc(par_host, par_dev, pospres, part_cel, part_idx, cell_beg, cell_end, stream=None):
+    """lq_grid_neighbor_search_noalloc: the neighbour search for callers that
+    cannot allocate device memory; outputs are caller-provided device arrays
+    and the working arrays are a fixed array inside the library (see
+    include/loquat_b200.h for the limits and the sharing rules)."""
+    check(lib().lq_grid_neighbor_search_noalloc(ptr(par_host), ptr(par_dev), ptr(pospres), ptr(part_cel),
+                                                ptr(part_idx), ptr(cell_beg), ptr(cell_end), stream),
+          "lq_grid_neighbor_search_noalloc")
 
 
 # ------------------------------------------------------------------ operators

@@ -31,7 +31,7 @@ int main()
         (const void*)&lq_status_string, (const void*)&lq_initialize_parameters, (const void*)&lq_update_time_step,
         (const void*)&lq_grid_create, (const void*)&lq_grid_resize, (const void*)&lq_grid_destroy,
         (const void*)&lq_grid_neighbor_search, (const void*)&lq_grid_arrays, (const void*)&lq_grid_sort_float4,
-        (const void*)&lq_grid_sort_tensor2d, (const void*)&lq_particle_interaction, (const void*)&lq_adami_boundary,
+        (const void*)&lq_grid_sort_tensor2d, (const void*)&lq_grid_neighbor_search_noalloc, (const void*)&lq_particle_interaction, (const void*)&lq_adami_boundary,
         (const void*)&lq_stress_regularization, (const void*)&lq_predictor, (const void*)&lq_corrector,
         (const void*)&lq_sim_create, (const void*)&lq_sim_destroy, (const void*)&lq_sim_step,
         (const void*)&lq_sim_synchronize, (const void*)&lq_sim_stream, (const void*)&lq_sim_upload,
