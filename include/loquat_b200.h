@@ -147,18 +147,29 @@ int lq_sim_state(void* sim, float** pospres, float** velrhop, float** idep,
                  float** str, float** stn);
 /* Step counter and simulated time. */
 int lq_sim_clock(void* sim, long long* step, double* time);
-/* Health word: [0] non-finite material values, [1] material particles
- * outside the cell lattice, [2] boundary particles outside the lattice,
- * [3] reserved.  Reading it synchronises the stream. */
+/* Health word, counted since the last read: [0] non-finite material values,
+ * [1] material and [2] boundary particles found outside the cell lattice by
+ * a search, [3] particles with more than 192 neighbours within 2h + skin.
+ * Reading it synchronises the stream and clears it. */
 int lq_sim_health(void* sim, int* health4);
-/* Kernel launches per time step of this simulation (without/with Shepard). */
+/* Neighbour lists are kept across steps and rebuilt (search, sort, list
+ * build) only when a particle's displacement since the last build plus a
+ * bound on its next step's motion reaches half the skin; the lists hold
+ * every pair within 2h + skin.  Default skin 0.1 h; setting it forces a
+ * rebuild before the next step.  lq_sim_rebuilds counts rebuilds so far. */
+int lq_sim_set_skin(void* sim, float skin_over_h);
+int lq_sim_rebuilds(void* sim, long long* count);
+/* Own kernel launches of a step without a rebuild (plain) and of a step
+ * with the Shepard pass; a rebuild adds lq_sim_rebuild_launches more. */
 int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard);
+int lq_sim_rebuild_launches(void* sim, int* launches);
 /* Advances nsteps steps launching kernels one by one with CUDA events
  * around each phase, then synchronises and returns the summed device time
- * per phase in phase_ms[6]: search, gather, Adami, interaction, integrate,
- * Shepard (the phases of the reference's Timer, include/types.h:158-173,
- * timed on the device instead of with std::clock).  phase_launches[6]
- * (may be NULL) receives how many times each phase ran. */
+ * per phase in phase_ms[7]: search, gather, Adami, interaction pairs,
+ * integrate, Shepard, neighbour-list build (the phases of the reference's
+ * Timer, include/types.h:158-173, timed on the device instead of with
+ * std::clock, with the search and the list build split out).
+ * phase_launches[7] (may be NULL) receives how many times each phase ran. */
 int lq_sim_profile(void* sim, int nsteps, double* phase_ms, int* phase_launches);
 
 /* ---- XML / .dat formats (reference src/loquat_io.cu:69-370) ------------ */

@@ -65,6 +65,9 @@ _SIGNATURES = {
     "lq_sim_health": (_I, [_VP, _VP]),
     "lq_sim_launches_per_step": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "lq_sim_profile": (_I, [_VP, _I, _VP, _VP]),
+    "lq_sim_set_skin": (_I, [_VP, _F]),
+    "lq_sim_rebuilds": (_I, [_VP, ctypes.POINTER(_LL)]),
+    "lq_sim_rebuild_launches": (_I, [_VP, ctypes.POINTER(_I)]),
     "lq_io_load_parameters": (_I, [ctypes.c_char_p, _VP]),
     "lq_io_save_parameters": (_I, [ctypes.c_char_p, _VP]),
     "lq_io_load_particles": (_I, [ctypes.c_char_p, _I] + [_VP] * 5),
@@ -264,15 +267,28 @@ class Simulation:
         check(lib().lq_sim_health(self.handle, h.ctypes.data), "lq_sim_health")
         return h
 
-    PHASES = ("search", "gather", "adami", "interaction", "integrate", "shepard")
+    PHASES = ("search", "gather", "adami", "interaction", "integrate", "shepard", "list")
 
     def profile(self, n: int) -> dict:
         """Runs n steps eagerly with CUDA events around each phase; returns
         {phase: (total_ms, launches)}."""
-        ms = np.zeros(6, np.float64)
-        cnt = np.zeros(6, np.int32)
+        ms = np.zeros(len(self.PHASES), np.float64)
+        cnt = np.zeros(len(self.PHASES), np.int32)
         check(lib().lq_sim_profile(self.handle, n, ms.ctypes.data, cnt.ctypes.data), "lq_sim_profile")
         return {p: (float(ms[k]), int(cnt[k])) for k, p in enumerate(self.PHASES)}
+
+    def set_skin(self, skin_over_h: float):
+        check(lib().lq_sim_set_skin(self.handle, skin_over_h), "lq_sim_set_skin")
+
+    def rebuilds(self) -> int:
+        c = _LL()
+        check(lib().lq_sim_rebuilds(self.handle, ctypes.byref(c)), "lq_sim_rebuilds")
+        return c.value
+
+    def rebuild_launches(self) -> int:
+        c = _I()
+        check(lib().lq_sim_rebuild_launches(self.handle, ctypes.byref(c)), "lq_sim_rebuild_launches")
+        return c.value
 
     def launches_per_step(self):
         a, b = _I(), _I()

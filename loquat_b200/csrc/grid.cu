@@ -67,6 +67,14 @@ __global__ void __launch_bounds__(kBlock) k_hash_count(const Parameters* __restr
     rank[i] = base + __popc(peers & ((1u << lane) - 1u));
 }
 
+__global__ void __launch_bounds__(kBlock) k_fill_int(int* __restrict__ p, int n, int v)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+__global__ void k_add_int(int* __restrict__ p, int v) { *p += v; }
+
 __global__ void __launch_bounds__(kBlock) k_scatter(int np, const int* __restrict__ key, const int* __restrict__ rank,
                                                     const int* __restrict__ start, int* __restrict__ part_idx,
                                                     int* __restrict__ part_cel)
@@ -138,6 +146,21 @@ __global__ void __launch_bounds__(kBlock) k_gather_state(int n, const int* __res
 
 }  // namespace
 
+int fill_int(int* p, int n, int v, cudaStream_t s)
+{
+    if (n <= 0) return LQ_OK;
+    k_fill_int<<<blocks_for(n), kBlock, 0, s>>>(p, n, v);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_fill_int");
+    return LQ_OK;
+}
+
+int add_int(int* p, int v, cudaStream_t s)
+{
+    k_add_int<<<1, 1, 0, s>>>(p, v);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_add_int");
+    return LQ_OK;
+}
+
 int scan_scratch_bytes(int ncell, size_t* bytes)
 {
     *bytes = 0;
@@ -157,7 +180,7 @@ int grid_search(const Parameters* ph, const Parameters* pd, const float4* pos, G
                          g.np_cap, g.ncell_cap);
     if (ph->ncell != 2 * ph->ncell_one_layer + 1 || ph->ncell_delete != ncell - 1)
         return set_error(LQ_ERR_ARG, "grid_search: Parameters cell counts are not initialised");
-    LQ_TRY_CUDA(cudaMemsetAsync(g.count, 0, sizeof(int) * (size_t)(ncell + 1), s), "count reset");
+    LQ_TRY(fill_int(g.count, ncell + 1, 0, s));
     if (np > 0) {
         k_hash_count<<<blocks_for(np), kBlock, 0, s>>>(pd, np, npb, pos, g.key, g.rank, g.count, health);
         LQ_TRY_CUDA(cudaGetLastError(), "k_hash_count");

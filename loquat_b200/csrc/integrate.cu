@@ -92,13 +92,33 @@ __global__ void __launch_bounds__(kBlock) k_predict(const Parameters* __restrict
 /* Full step from the snapshot (reference src/predictor_corrector.cu:256-307):
  * v = v0 + dt a; x = x0 + dt/2 (v + v0); eps = eps0 + dt deps; the model
  * restarts from the snapshot stress and plastic strain; the pressure passed
- * in is the current one. */
+ * in is the current one.  Reads the current state `cur` and the snapshot
+ * `ini` (at ini_idx[i], or i), writes `out` (which may be `cur` or `ini`).
+ * When out differs from cur, boundary slots are copied from cur (their
+ * stress is the latest Adami extrapolation).  With `verlet`, each material
+ * particle also checks whether neighbour lists built at positions xbuild
+ * stay valid through the next step: it raises *rebuild when twice its
+ * displacement plus a bound on its next step's motion reaches the skin. */
+struct VerletCheck {
+    const float4* xbuild;
+    int* rebuild;
+    float half_skin;
+};
+
 __global__ void __launch_bounds__(kBlock) k_correct(const Parameters* __restrict__ P, int np, int npb, State cur,
-                                                    State ini, const int* __restrict__ ini_idx, Rates rt,
-                                                    int* __restrict__ health)
+                                                    State ini, const int* __restrict__ ini_idx, State out, Rates rt,
+                                                    int* __restrict__ health, VerletCheck verlet, int first)
 {
-    const int i = npb + blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = first + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
+    if (i < npb) {
+        out.pos[i] = cur.pos[i];
+        out.vel[i] = cur.vel[i];
+        out.idep[i] = cur.idep[i];
+        store_t2(out.str, i, load_t2_rw(cur.str, i));
+        store_t2(out.stn, i, load_t2_rw(cur.stn, i));
+        return;
+    }
     const int k = ini_idx ? __ldg(ini_idx + i) : i;
     const float dt = __ldg(&P->dt);
     const Material M = load_material(P);
@@ -134,16 +154,27 @@ __global__ void __launch_bounds__(kBlock) k_correct(const Parameters* __restrict
         ep = sqrtf(2.0f / 3.0f * J2(e));
     }
     x.w = p;
-    cur.pos[i] = x;
-    cur.vel[i] = v;
-    cur.idep[i] = make_float4(id.x, ep, id.z, id.w);
-    store_t2(cur.str, i, s);
-    store_t2(cur.stn, i, e);
+    out.pos[i] = x;
+    out.vel[i] = v;
+    out.idep[i] = make_float4(id.x, ep, id.z, id.w);
+    store_t2(out.str, i, s);
+    store_t2(out.stn, i, e);
     if (health) {
         const bool ok = isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(v.x) && isfinite(v.y) &&
                         isfinite(v.z) && isfinite(v.w) && isfinite(s.xx) && isfinite(s.yy) && isfinite(s.zz) &&
                         isfinite(s.xy) && isfinite(s.xz) && isfinite(s.yz);
         if (!ok) atomicAdd(health + HEALTH_NONFINITE, 1);
+    }
+    if (verlet.xbuild) {
+        const float4 xb = __ldg(verlet.xbuild + i);
+        const float dx = x.x - xb.x, dy = x.y - xb.y, dz = x.z - xb.z;
+        const float moved = sqrtf(dx * dx + dy * dy + dz * dz);
+        const float speed = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
+        const float accel = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
+        /* next step: the predictor half step and the corrector full step
+         * move a particle by at most dt |v| + dt^2 |a| each; 2x covers both */
+        const float ahead = 2.0f * dt * (speed + dt * accel);
+        if (!(moved + ahead < verlet.half_skin)) atomicOr(verlet.rebuild, 1);
     }
 }
 
@@ -164,7 +195,19 @@ int launch_correct(const Parameters* ph, const Parameters* pd, const State& cur,
                    const int* ini_idx, const Rates& r, int* health, cudaStream_t s)
 {
     if (ph->npm <= 0) return LQ_OK;
-    k_correct<<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, ini_idx, r, health);
+    k_correct<<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, ini_idx, cur, r, health,
+                                                             VerletCheck{nullptr, nullptr, 0.0f}, ph->npb);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_correct");
+    return LQ_OK;
+}
+
+int launch_correct_into(const Parameters* ph, const Parameters* pd, const State& cur, const State& ini,
+                        const State& out, const Rates& r, int* health, const float4* xbuild, int* rebuild,
+                        float skin, cudaStream_t s)
+{
+    if (ph->np <= 0) return LQ_OK;
+    k_correct<<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health,
+                                                            VerletCheck{xbuild, rebuild, 0.5f * skin}, 0);
     LQ_TRY_CUDA(cudaGetLastError(), "k_correct");
     return LQ_OK;
 }

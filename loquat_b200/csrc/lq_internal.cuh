@@ -56,7 +56,7 @@ struct Cells {
 };
 
 /* Health counters written by the kernels (see lq_sim_health). */
-enum { HEALTH_NONFINITE = 0, HEALTH_MAT_OUT = 1, HEALTH_BND_OUT = 2, HEALTH_WORDS = 4 };
+enum { HEALTH_NONFINITE = 0, HEALTH_MAT_OUT = 1, HEALTH_BND_OUT = 2, HEALTH_NBR_OVERFLOW = 3, HEALTH_WORDS = 4 };
 
 /* ----------------------------------------------------------------- grid */
 struct GridBuffers {
@@ -87,9 +87,24 @@ int gather_tensor2d(int n, const int* idx, const tensor2d* in, tensor2d* out, cu
 /* Gathers all five state arrays in one pass: out[i] = in[idx[i]]. */
 int gather_state(int n, const int* idx, const State& in, const State& out, cudaStream_t s);
 
+/* ------------------------------------------------------ neighbour lists */
+/* Neighbours stored per material particle; a particle with more walks its
+ * 27 cells directly instead. */
+#define LQ_NBR_CAP 192
+
+struct NeighborList {
+    int* list = nullptr;    /* int[LQ_NBR_CAP * stride], entry k of particle t at k * stride + t */
+    int* count = nullptr;   /* int[stride] */
+    int stride = 0;         /* >= npm, multiple of 32 */
+};
+
 /* ------------------------------------------------------------ operators */
 int launch_interaction(const Parameters* par_host, const Parameters* par_dev, const State& st, const Rates& r,
                        const Cells& c, cudaStream_t s);
+int launch_neighbor_list(const Parameters* par_host, const Parameters* par_dev, const float4* pos, const Cells& c,
+                         const NeighborList& nl, cudaStream_t s);
+int launch_interaction_list(const Parameters* par_host, const Parameters* par_dev, const State& st, const Rates& r,
+                            const Cells& c, const NeighborList& nl, cudaStream_t s);
 int launch_adami(const Parameters* par_host, const Parameters* par_dev, const State& st, const Cells& c,
                  cudaStream_t s);
 /* Shepard filter of material stress into out_str[npb, np).  When `full` is
@@ -105,6 +120,28 @@ int launch_predict(const Parameters* par_host, const Parameters* par_dev, const 
  * ini_idx is null).  Non-finite results are counted in health. */
 int launch_correct(const Parameters* par_host, const Parameters* par_dev, const State& cur, const State& ini,
                    const int* ini_idx, const Rates& r, int* health, cudaStream_t s);
+
+/* Corrector from snapshot `ini` and current `cur` into `out` (boundary slots
+ * copied from cur); material particles raise *rebuild when neighbour lists
+ * built at xbuild with this skin may not hold through the next step. */
+int launch_correct_into(const Parameters* par_host, const Parameters* par_dev, const State& cur, const State& ini,
+                        const State& out, const Rates& r, int* health, const float4* xbuild, int* rebuild,
+                        float skin, cudaStream_t s);
+
+/* List-driven Adami (boundary targets, material neighbours) and Shepard. */
+int launch_adami_list(const Parameters* par_host, const Parameters* par_dev, const State& st, const NeighborList& nl,
+                      cudaStream_t s);
+int launch_shepard_list(const Parameters* par_host, const Parameters* par_dev, const State& st, tensor2d* out_str,
+                        const NeighborList& nl, cudaStream_t s);
+/* Neighbour lists of targets [first, first + n) from grid layers
+ * layer_lo..1 with cut-off radius `cut` (2h plus skin); list overflows are
+ * counted in health[HEALTH_NBR_OVERFLOW]. */
+int launch_neighbor_list_range(const Parameters* par_host, const Parameters* par_dev, int first, int n, int layer_lo,
+                               float cut, const float4* pos, const Cells& c, const NeighborList& nl, int* health,
+                               cudaStream_t s);
+/* Fills n ints with v; adds v to one int. */
+int fill_int(int* p, int n, int v, cudaStream_t s);
+int add_int(int* p, int v, cudaStream_t s);
 
 /* Host-side copy of Parameters derivation (reference src/loquat.cu:111-139). */
 void initialize_parameters(Parameters* p);

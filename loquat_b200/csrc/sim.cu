@@ -1,23 +1,29 @@
 /*
  * LOQUAT-B200 native time-step driver: the hot loop of
- * LoquatSph::RunSimulation (reference src/loquat.cu:322-409) with the same
- * stage order, re-planned for one B200:
+ * LoquatSph::RunSimulation (reference src/loquat.cu:322-409), re-planned
+ * for one B200.
  *
- *   reference (per step)                      here
- *   search + 5 gathers (+copy back each)      search + 1 fused 5-array gather
- *   Adami, interaction                        Adami, interaction
- *   5 snapshot copies + predictor             predictor A -> B (A is the snapshot)
- *   search + 10 gathers (+copy back each)     search + 1 fused 5-array gather B -> C
- *   Adami, interaction                        Adami, interaction
- *   corrector (snapshot re-sorted)            corrector in place on C, reading the
- *                                             snapshot A through the new permutation
- *   every N steps: search + 5 gathers +       every N steps: search + gather C -> A,
- *   Shepard + copy back                       Shepard A -> C
- *   per-step H2D Parameters + 8 host syncs    one CUDA graph launch per step, no sync
+ * The reference searches and re-sorts the particles before every stage
+ * (twice per step) and every phase visits the 27 neighbouring cells again.
+ * Here the particle order and neighbour lists are kept across steps,
+ * Verlet-style: the lists hold every pair within 2h + skin, and they are
+ * rebuilt (search, stable sort, gather, list build) only when the particles
+ * could have moved far enough for a pair to cross the 2h cut-off unseen.
+ * Every evaluation therefore sees exactly the pairs within 2h, as a fresh
+ * search would; only the float summation order differs.
  *
- * Buffer roles are fixed (the state is in C at every step boundary), so a
- * step and a Shepard pass are each captured once as a CUDA graph and
- * replayed.  dt = cfl h / cs is constant, as in the reference.
+ *   per step (state in S, order fixed between rebuilds)
+ *     [rebuild if flagged: search S, gather S -> T, copy T -> S, record the
+ *      positions, build material and boundary lists]
+ *     Adami(S), interaction(S), predictor S -> S2          (S is the snapshot)
+ *     Adami(S2), interaction(S2), corrector (S2, S) -> S   (raises the flag)
+ *   every N steps: Shepard(S) -> T.str, copy back            (reference :400-409)
+ *
+ * The rebuild decision stays on the device: a one-thread kernel turns the
+ * flag into the condition of an IF node of the step's CUDA graph.  Without
+ * graphs (or if the driver cannot build the conditional node) the host
+ * reads the flag before each step, which gives the same sequence of
+ * rebuilds.  dt = cfl h / cs is constant, as in the reference.
  */
 #include <cstring>
 #include <vector>
@@ -28,6 +34,8 @@ namespace {
 
 using lqb::State;
 
+constexpr float kDefaultSkinOverH = 0.1f;
+
 struct LqSim {
     Parameters ph{};
     Parameters* pd = nullptr;
@@ -35,21 +43,29 @@ struct LqSim {
     long long step = 0;
     double time = 0.0;
     int flags = 0;
+    float skin = 0.0f;                 /* list cut-off = 2h + skin */
     cudaStream_t stream = nullptr;
-    State A{}, B{}, C{};
+    cudaStream_t side = nullptr;       /* captures the rebuild body */
+    State S{}, S2{}, T{};
+    float4* xbuild = nullptr;          /* positions when the lists were built */
     lqb::Rates R{};
     lqb::GridBuffers g;
+    lqb::NeighborList nlm, nlb;        /* material targets, boundary targets */
     int* health = nullptr;
+    int* rebuild = nullptr;            /* device flag: rebuild before the next step */
+    int* rebuilds = nullptr;           /* device counter of rebuilds */
+    int* host_flag = nullptr;          /* pinned mirror for the eager path */
     std::vector<void*> allocs;
     cudaGraphExec_t step_exec = nullptr;
     cudaGraphExec_t shep_exec = nullptr;
+    bool conditional = false;
 };
 
 int dev_alloc(LqSim* S, void** p, size_t bytes)
 {
     cudaError_t e = cudaMalloc(p, bytes > 0 ? bytes : 16);
-    if (e != cudaSuccess) return lqb::set_error(LQ_ERR_ALLOC, "sim: cudaMalloc(%zu) failed: %s", bytes,
-                                                cudaGetErrorString(e));
+    if (e != cudaSuccess)
+        return lqb::set_error(LQ_ERR_ALLOC, "sim: cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
     S->allocs.push_back(*p);
     return LQ_OK;
 }
@@ -67,112 +83,178 @@ int alloc_state(LqSim* S, State& st)
 
 void release(LqSim* S)
 {
+    if (S->stream) cudaStreamSynchronize(S->stream);
     if (S->step_exec) cudaGraphExecDestroy(S->step_exec);
     if (S->shep_exec) cudaGraphExecDestroy(S->shep_exec);
-    if (S->stream) cudaStreamSynchronize(S->stream);
+    S->step_exec = S->shep_exec = nullptr;
     for (void* p : S->allocs) cudaFree(p);
     S->allocs.clear();
+    if (S->host_flag) cudaFreeHost(S->host_flag);
+    S->host_flag = nullptr;
+    if (S->side) cudaStreamDestroy(S->side);
     if (S->stream) cudaStreamDestroy(S->stream);
-    S->stream = nullptr;
+    S->side = S->stream = nullptr;
 }
 
-/* One time step; the state is in C before and after. */
-int enqueue_step(LqSim* S)
+/* ------------------------------------------------------------- kernels */
+
+__global__ void k_copy_state(int n, State in, State out, float4* __restrict__ xbuild)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 x = in.pos[i];
+    out.pos[i] = x;
+    xbuild[i] = x;
+    out.vel[i] = in.vel[i];
+    out.idep[i] = in.idep[i];
+    const float2* a = reinterpret_cast<const float2*>(in.str) + 3 * (size_t)i;
+    float2* b = reinterpret_cast<float2*>(out.str) + 3 * (size_t)i;
+    b[0] = a[0];
+    b[1] = a[1];
+    b[2] = a[2];
+    a = reinterpret_cast<const float2*>(in.stn) + 3 * (size_t)i;
+    b = reinterpret_cast<float2*>(out.stn) + 3 * (size_t)i;
+    b[0] = a[0];
+    b[1] = a[1];
+    b[2] = a[2];
+}
+
+__global__ void k_copy_t2(int first, int n, const tensor2d* __restrict__ in, tensor2d* __restrict__ out)
+{
+    const int i = first + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= first + n) return;
+    const float2* a = reinterpret_cast<const float2*>(in) + 3 * (size_t)i;
+    float2* b = reinterpret_cast<float2*>(out) + 3 * (size_t)i;
+    b[0] = a[0];
+    b[1] = a[1];
+    b[2] = a[2];
+}
+
+/* Turns the rebuild flag into the IF condition and clears it. */
+__global__ void k_decide(cudaGraphConditionalHandle h, int* flag, int* count)
+{
+    const int f = *flag;
+    cudaGraphSetConditional(h, f ? 1u : 0u);
+    if (f) {
+        *flag = 0;
+        *count += 1;
+    }
+}
+
+inline int blocks(int n) { return (n + 255) / 256; }
+
+/* ------------------------------------------------------------ sequences */
+
+/* Search, sort and list build; leaves the state in S with fresh lists. */
+int enqueue_rebuild(LqSim* S, cudaStream_t s)
 {
     const Parameters* ph = &S->ph;
     const Parameters* pd = S->pd;
-    cudaStream_t s = S->stream;
+    const lqb::Cells cells{S->g.start, nullptr, nullptr};
+    LQ_TRY(lqb::grid_search(ph, pd, S->S.pos, S->g, false, S->health, s));
+    LQ_TRY(lqb::gather_state(S->np, S->g.part_idx, S->S, S->T, s));
+    k_copy_state<<<blocks(S->np), 256, 0, s>>>(S->np, S->T, S->S, S->xbuild);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_copy_state");
+    const float cut = 2.0f * ph->h + S->skin;
+    LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, S->npb, S->npm, 0, cut, S->S.pos, cells, S->nlm, S->health, s));
+    LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, S->nlb, S->health, s));
+    return LQ_OK;
+}
+
+/* The two stages of a step on the current lists. */
+int enqueue_stages(LqSim* S, cudaStream_t s)
+{
+    const Parameters* ph = &S->ph;
+    const Parameters* pd = S->pd;
     const lqb::Cells cells{S->g.start, nullptr, nullptr};
     /* predictor stage (reference src/loquat.cu:343-368) */
-    LQ_TRY(lqb::grid_search(ph, pd, S->C.pos, S->g, false, S->health, s));
-    LQ_TRY(lqb::gather_state(S->np, S->g.part_idx, S->C, S->A, s));
-    LQ_TRY(lqb::launch_adami(ph, pd, S->A, cells, s));
-    LQ_TRY(lqb::launch_interaction(ph, pd, S->A, S->R, cells, s));
-    LQ_TRY(lqb::launch_predict(ph, pd, S->A, S->B, nullptr, S->R, s));
+    LQ_TRY(lqb::launch_adami_list(ph, pd, S->S, S->nlb, s));
+    LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S, S->R, cells, S->nlm, s));
+    LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s));
     /* corrector stage (reference src/loquat.cu:371-396) */
-    LQ_TRY(lqb::grid_search(ph, pd, S->B.pos, S->g, false, S->health, s));
-    LQ_TRY(lqb::gather_state(S->np, S->g.part_idx, S->B, S->C, s));
-    LQ_TRY(lqb::launch_adami(ph, pd, S->C, cells, s));
-    LQ_TRY(lqb::launch_interaction(ph, pd, S->C, S->R, cells, s));
-    LQ_TRY(lqb::launch_correct(ph, pd, S->C, S->A, S->g.part_idx, S->R, S->health, s));
+    LQ_TRY(lqb::launch_adami_list(ph, pd, S->S2, S->nlb, s));
+    LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S2, S->R, cells, S->nlm, s));
+    LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild, S->skin, s));
     return LQ_OK;
 }
 
-/* Phases timed by lq_sim_profile, the reference's Timer phases
- * (reference include/types.h:158-173, src/loquat.cu:345-395) with the
- * search split from the gathers. */
-enum { PH_SEARCH = 0, PH_GATHER, PH_ADAMI, PH_INTERACTION, PH_INTEGRATE, PH_SHEPARD, PH_COUNT };
-
-struct PhaseTimer {
-    std::vector<cudaEvent_t> ev;
-    std::vector<int> phase;
-    int used = 0;
-    int mark(cudaStream_t s, int ph)
-    {
-        if (used + 2 > (int)ev.size()) return lqb::set_error(LQ_ERR_ARG, "profile: event pool exhausted");
-        phase.push_back(ph);
-        LQ_TRY_CUDA(cudaEventRecord(ev[used], s), "profile event");
-        used += 1;
-        return LQ_OK;
-    }
-    int close(cudaStream_t s)
-    {
-        LQ_TRY_CUDA(cudaEventRecord(ev[used], s), "profile event");
-        used += 1;
-        return LQ_OK;
-    }
-};
-
-/* One eager time step with an event pair around every phase. */
-int enqueue_step_timed(LqSim* S, PhaseTimer& T)
+/* Shepard stress filter (reference src/loquat.cu:400-409) on the lists. */
+int enqueue_shepard(LqSim* S, cudaStream_t s)
 {
-    const Parameters* ph = &S->ph;
-    const Parameters* pd = S->pd;
-    cudaStream_t s = S->stream;
-    const lqb::Cells cells{S->g.start, nullptr, nullptr};
-    State* in[2] = {&S->C, &S->B};
-    State* out[2] = {&S->A, &S->C};
-    for (int stage = 0; stage < 2; ++stage) {
-        LQ_TRY(T.mark(s, PH_SEARCH));
-        LQ_TRY(lqb::grid_search(ph, pd, in[stage]->pos, S->g, false, S->health, s));
-        LQ_TRY(T.close(s));
-        LQ_TRY(T.mark(s, PH_GATHER));
-        LQ_TRY(lqb::gather_state(S->np, S->g.part_idx, *in[stage], *out[stage], s));
-        LQ_TRY(T.close(s));
-        LQ_TRY(T.mark(s, PH_ADAMI));
-        LQ_TRY(lqb::launch_adami(ph, pd, *out[stage], cells, s));
-        LQ_TRY(T.close(s));
-        LQ_TRY(T.mark(s, PH_INTERACTION));
-        LQ_TRY(lqb::launch_interaction(ph, pd, *out[stage], S->R, cells, s));
-        LQ_TRY(T.close(s));
-        LQ_TRY(T.mark(s, PH_INTEGRATE));
-        if (stage == 0)
-            LQ_TRY(lqb::launch_predict(ph, pd, S->A, S->B, nullptr, S->R, s));
-        else
-            LQ_TRY(lqb::launch_correct(ph, pd, S->C, S->A, S->g.part_idx, S->R, S->health, s));
-        LQ_TRY(T.close(s));
+    LQ_TRY(lqb::launch_shepard_list(&S->ph, S->pd, S->S, S->T.str, S->nlm, s));
+    if (S->npm > 0) {
+        k_copy_t2<<<blocks(S->npm), 256, 0, s>>>(S->npb, S->npm, S->T.str, S->S.str);
+        LQ_TRY_CUDA(cudaGetLastError(), "k_copy_t2");
     }
     return LQ_OK;
 }
 
-/* Shepard stress filter (reference src/loquat.cu:400-409). */
-int enqueue_shepard(LqSim* S)
+/* Step graph: decide -> IF(rebuild) -> stages. */
+int capture_step(LqSim* S)
 {
-    const Parameters* ph = &S->ph;
-    const Parameters* pd = S->pd;
     cudaStream_t s = S->stream;
-    const lqb::Cells cells{S->g.start, nullptr, nullptr};
-    LQ_TRY(lqb::grid_search(ph, pd, S->C.pos, S->g, false, S->health, s));
-    LQ_TRY(lqb::gather_state(S->np, S->g.part_idx, S->C, S->A, s));
-    LQ_TRY(lqb::launch_shepard(ph, pd, S->A, S->C.str, &S->C, cells, s));
+    LQ_TRY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+    int st = LQ_OK;
+    cudaGraph_t graph = nullptr;
+    do {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t cg = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &ndeps);
+        if (e != cudaSuccess) { st = lqb::cuda_status(e, "capture info"); break; }
+        cudaGraphConditionalHandle h;
+        e = cudaGraphConditionalHandleCreate(&h, cg, 0, 0);
+        if (e != cudaSuccess) { st = lqb::cuda_status(e, "conditional handle"); break; }
+        k_decide<<<1, 1, 0, s>>>(h, S->rebuild, S->rebuilds);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) { st = lqb::cuda_status(e, "k_decide"); break; }
+        e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &ndeps);
+        if (e != cudaSuccess) { st = lqb::cuda_status(e, "capture info"); break; }
+        /* the parameter record's C union has no usable C++ default
+         * constructor: zero raw storage and view it as the record */
+        alignas(cudaGraphNodeParams) unsigned char cp_raw[sizeof(cudaGraphNodeParams)];
+        memset(cp_raw, 0, sizeof(cp_raw));
+        cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_raw);
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cnode;
+        e = cudaGraphAddNode(&cnode, cg, deps, ndeps, &cp);
+        if (e != cudaSuccess) { st = lqb::cuda_status(e, "conditional node"); break; }
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(S->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) { st = lqb::cuda_status(e, "body capture"); break; }
+        st = enqueue_rebuild(S, S->side);
+        cudaGraph_t body_out = nullptr;
+        e = cudaStreamEndCapture(S->side, &body_out);
+        if (st != LQ_OK) break;
+        if (e != cudaSuccess) { st = lqb::cuda_status(e, "body end capture"); break; }
+        e = cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies);
+        if (e != cudaSuccess) { st = lqb::cuda_status(e, "capture dependencies"); break; }
+        st = enqueue_stages(S, s);
+    } while (0);
+    cudaError_t e = cudaStreamEndCapture(s, &graph);
+    if (st != LQ_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+    }
+    if (e != cudaSuccess) return lqb::cuda_status(e, "end capture");
+    e = cudaGraphInstantiate(&S->step_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        S->step_exec = nullptr;
+        return lqb::cuda_status(e, "graph instantiate");
+    }
     return LQ_OK;
 }
 
-int capture(LqSim* S, int (*fn)(LqSim*), cudaGraphExec_t* exec)
+int capture_plain(LqSim* S, int (*fn)(LqSim*, cudaStream_t), cudaGraphExec_t* exec)
 {
     cudaGraph_t graph = nullptr;
     LQ_TRY_CUDA(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-    int st = fn(S);
+    int st = fn(S, S->stream);
     cudaError_t e = cudaStreamEndCapture(S->stream, &graph);
     if (st != LQ_OK) {
         if (graph) cudaGraphDestroy(graph);
@@ -185,6 +267,29 @@ int capture(LqSim* S, int (*fn)(LqSim*), cudaGraphExec_t* exec)
     return LQ_OK;
 }
 
+/* Reads the rebuild flag on the host; clears it and counts the rebuild when set. */
+int host_take_flag(LqSim* S, bool* set)
+{
+    cudaStream_t s = S->stream;
+    LQ_TRY_CUDA(cudaMemcpyAsync(S->host_flag, S->rebuild, sizeof(int), cudaMemcpyDeviceToHost, s), "flag read");
+    LQ_TRY_CUDA(cudaStreamSynchronize(s), "flag read");
+    *set = *S->host_flag != 0;
+    if (*set) {
+        LQ_TRY(lqb::fill_int(S->rebuild, 1, 0, s));
+        LQ_TRY(lqb::add_int(S->rebuilds, 1, s));
+    }
+    return LQ_OK;
+}
+
+/* One step without the step graph: the host reads the flag. */
+int eager_step(LqSim* S)
+{
+    bool rebuild = false;
+    LQ_TRY(host_take_flag(S, &rebuild));
+    if (rebuild) LQ_TRY(enqueue_rebuild(S, S->stream));
+    return enqueue_stages(S, S->stream);
+}
+
 int upload(LqSim* S, const float* pos, const float* vel, const float* idep, const float* str, const float* stn,
            State& dst)
 {
@@ -195,6 +300,25 @@ int upload(LqSim* S, const float* pos, const float* vel, const float* idep, cons
     LQ_TRY_CUDA(cudaMemcpyAsync(dst.idep, idep, n * sizeof(float4), cudaMemcpyHostToDevice, s), "upload idep");
     LQ_TRY_CUDA(cudaMemcpyAsync(dst.str, str, n * sizeof(tensor2d), cudaMemcpyHostToDevice, s), "upload str");
     LQ_TRY_CUDA(cudaMemcpyAsync(dst.stn, stn, n * sizeof(tensor2d), cudaMemcpyHostToDevice, s), "upload stn");
+    return LQ_OK;
+}
+
+int set_flag(LqSim* S, int v) { return lqb::fill_int(S->rebuild, 1, v, S->stream); }
+
+int build_graphs(LqSim* S)
+{
+    if (S->step_exec) cudaGraphExecDestroy(S->step_exec);
+    if (S->shep_exec) cudaGraphExecDestroy(S->shep_exec);
+    S->step_exec = S->shep_exec = nullptr;
+    S->conditional = false;
+    if (!(S->flags & LQ_SIM_GRAPH)) return LQ_OK;
+    if (capture_step(S) == LQ_OK) {
+        S->conditional = true;
+    } else {
+        cudaGetLastError(); /* fall back to host-decided rebuilds */
+        S->step_exec = nullptr;
+    }
+    LQ_TRY(capture_plain(S, enqueue_shepard, &S->shep_exec));
     return LQ_OK;
 }
 
@@ -217,16 +341,28 @@ int create(LqSim* S, const Parameters* par, const float* pos, const float* vel, 
         return lqb::set_error(LQ_ERR_ARG, "lq_sim_create: constitutive_model must be 1 or 2");
     S->ph.dt = S->ph.cfl * S->ph.h / S->ph.cs; /* reference src/loquat.cu:333 */
     S->time = (double)S->ph.time;
+    S->skin = kDefaultSkinOverH * S->ph.h;
     LQ_TRY_CUDA(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking), "stream create");
+    LQ_TRY_CUDA(cudaStreamCreateWithFlags(&S->side, cudaStreamNonBlocking), "stream create");
+    LQ_TRY_CUDA(cudaMallocHost((void**)&S->host_flag, sizeof(int)), "pinned flag");
     LQ_TRY(dev_alloc(S, (void**)&S->pd, sizeof(Parameters)));
-    LQ_TRY(alloc_state(S, S->A));
-    LQ_TRY(alloc_state(S, S->B));
-    LQ_TRY(alloc_state(S, S->C));
+    LQ_TRY(alloc_state(S, S->S));
+    LQ_TRY(alloc_state(S, S->S2));
+    LQ_TRY(alloc_state(S, S->T));
     const size_t n = (size_t)S->np;
+    LQ_TRY(dev_alloc(S, (void**)&S->xbuild, n * sizeof(float4)));
     LQ_TRY(dev_alloc(S, (void**)&S->R.accad, n * sizeof(float4)));
     LQ_TRY(dev_alloc(S, (void**)&S->R.spin, n * sizeof(float4)));
     LQ_TRY(dev_alloc(S, (void**)&S->R.acestn, n * sizeof(tensor2d)));
     LQ_TRY(dev_alloc(S, (void**)&S->health, sizeof(int) * lqb::HEALTH_WORDS));
+    LQ_TRY(dev_alloc(S, (void**)&S->rebuild, sizeof(int)));
+    LQ_TRY(dev_alloc(S, (void**)&S->rebuilds, sizeof(int)));
+    S->nlm.stride = ((S->npm > 0 ? S->npm : 1) + 31) / 32 * 32;
+    LQ_TRY(dev_alloc(S, (void**)&S->nlm.list, sizeof(int) * (size_t)LQ_NBR_CAP * S->nlm.stride));
+    LQ_TRY(dev_alloc(S, (void**)&S->nlm.count, sizeof(int) * (size_t)S->nlm.stride));
+    S->nlb.stride = ((S->npb > 0 ? S->npb : 1) + 31) / 32 * 32;
+    LQ_TRY(dev_alloc(S, (void**)&S->nlb.list, sizeof(int) * (size_t)LQ_NBR_CAP * S->nlb.stride));
+    LQ_TRY(dev_alloc(S, (void**)&S->nlb.count, sizeof(int) * (size_t)S->nlb.stride));
     const int ncell = S->ph.ncell;
     lqb::GridBuffers& g = S->g;
     LQ_TRY(lqb::scan_scratch_bytes(ncell, &g.scan_bytes));
@@ -244,17 +380,14 @@ int create(LqSim* S, const Parameters* par, const float* pos, const float* vel, 
     LQ_TRY_CUDA(cudaMemsetAsync(S->R.spin, 0, n * sizeof(float4), S->stream), "zero rates");
     LQ_TRY_CUDA(cudaMemsetAsync(S->R.acestn, 0, n * sizeof(tensor2d), S->stream), "zero rates");
     LQ_TRY_CUDA(cudaMemsetAsync(S->health, 0, sizeof(int) * lqb::HEALTH_WORDS, S->stream), "zero health");
+    LQ_TRY_CUDA(cudaMemsetAsync(S->rebuilds, 0, sizeof(int), S->stream), "zero counter");
     LQ_TRY_CUDA(cudaMemcpyAsync(S->pd, &S->ph, sizeof(Parameters), cudaMemcpyHostToDevice, S->stream),
                 "upload Parameters");
-    /* initial search + primary sort (reference src/loquat.cu:297-298) */
-    LQ_TRY(upload(S, pos, vel, idep, str, stn, S->A));
-    LQ_TRY(lqb::grid_search(&S->ph, S->pd, S->A.pos, S->g, false, S->health, S->stream));
-    LQ_TRY(lqb::gather_state(S->np, S->g.part_idx, S->A, S->C, S->stream));
+    LQ_TRY(upload(S, pos, vel, idep, str, stn, S->S));
+    /* the first step searches and sorts (reference src/loquat.cu:297-298) */
+    LQ_TRY(set_flag(S, 1));
     LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "sim create");
-    if (S->flags & LQ_SIM_GRAPH) {
-        LQ_TRY(capture(S, enqueue_step, &S->step_exec));
-        LQ_TRY(capture(S, enqueue_shepard, &S->shep_exec));
-    }
+    LQ_TRY(build_graphs(S));
     return LQ_OK;
 }
 
@@ -297,13 +430,13 @@ extern "C" int lq_sim_step(void* sim, int nsteps)
         if (S->step_exec) {
             LQ_TRY_CUDA(cudaGraphLaunch(S->step_exec, S->stream), "step graph launch");
         } else {
-            LQ_TRY(enqueue_step(S));
+            LQ_TRY(eager_step(S));
         }
         if (N != 0 && S->step % N == 0 && S->step != 0) {
             if (S->shep_exec) {
                 LQ_TRY_CUDA(cudaGraphLaunch(S->shep_exec, S->stream), "Shepard graph launch");
             } else {
-                LQ_TRY(enqueue_shepard(S));
+                LQ_TRY(enqueue_shepard(S, S->stream));
             }
         }
         S->time += (double)S->ph.dt;
@@ -332,7 +465,8 @@ extern "C" int lq_sim_upload(void* sim, const float* pospres, const float* velrh
     if (!sim || !pospres || !velrhop || !idep || !str || !stn)
         return lqb::set_error(LQ_ERR_ARG, "lq_sim_upload: null argument");
     LqSim* S = static_cast<LqSim*>(sim);
-    return upload(S, pospres, velrhop, idep, str, stn, S->C);
+    LQ_TRY(upload(S, pospres, velrhop, idep, str, stn, S->S));
+    return set_flag(S, 1); /* new positions: search and rebuild the lists first */
 }
 
 extern "C" int lq_sim_download(void* sim, float* pospres, float* velrhop, float* idep, float* str, float* stn)
@@ -341,11 +475,11 @@ extern "C" int lq_sim_download(void* sim, float* pospres, float* velrhop, float*
     LqSim* S = static_cast<LqSim*>(sim);
     const size_t n = (size_t)S->np;
     cudaStream_t s = S->stream;
-    if (pospres) LQ_TRY_CUDA(cudaMemcpyAsync(pospres, S->C.pos, n * sizeof(float4), cudaMemcpyDeviceToHost, s), "dl");
-    if (velrhop) LQ_TRY_CUDA(cudaMemcpyAsync(velrhop, S->C.vel, n * sizeof(float4), cudaMemcpyDeviceToHost, s), "dl");
-    if (idep) LQ_TRY_CUDA(cudaMemcpyAsync(idep, S->C.idep, n * sizeof(float4), cudaMemcpyDeviceToHost, s), "dl");
-    if (str) LQ_TRY_CUDA(cudaMemcpyAsync(str, S->C.str, n * sizeof(tensor2d), cudaMemcpyDeviceToHost, s), "dl");
-    if (stn) LQ_TRY_CUDA(cudaMemcpyAsync(stn, S->C.stn, n * sizeof(tensor2d), cudaMemcpyDeviceToHost, s), "dl");
+    if (pospres) LQ_TRY_CUDA(cudaMemcpyAsync(pospres, S->S.pos, n * sizeof(float4), cudaMemcpyDeviceToHost, s), "dl");
+    if (velrhop) LQ_TRY_CUDA(cudaMemcpyAsync(velrhop, S->S.vel, n * sizeof(float4), cudaMemcpyDeviceToHost, s), "dl");
+    if (idep) LQ_TRY_CUDA(cudaMemcpyAsync(idep, S->S.idep, n * sizeof(float4), cudaMemcpyDeviceToHost, s), "dl");
+    if (str) LQ_TRY_CUDA(cudaMemcpyAsync(str, S->S.str, n * sizeof(tensor2d), cudaMemcpyDeviceToHost, s), "dl");
+    if (stn) LQ_TRY_CUDA(cudaMemcpyAsync(stn, S->S.stn, n * sizeof(tensor2d), cudaMemcpyDeviceToHost, s), "dl");
     LQ_TRY_CUDA(cudaStreamSynchronize(s), "download");
     return LQ_OK;
 }
@@ -354,11 +488,11 @@ extern "C" int lq_sim_state(void* sim, float** pospres, float** velrhop, float**
 {
     if (!sim) return lqb::set_error(LQ_ERR_ARG, "lq_sim_state: null sim");
     LqSim* S = static_cast<LqSim*>(sim);
-    if (pospres) *pospres = (float*)S->C.pos;
-    if (velrhop) *velrhop = (float*)S->C.vel;
-    if (idep) *idep = (float*)S->C.idep;
-    if (str) *str = (float*)S->C.str;
-    if (stn) *stn = (float*)S->C.stn;
+    if (pospres) *pospres = (float*)S->S.pos;
+    if (velrhop) *velrhop = (float*)S->S.vel;
+    if (idep) *idep = (float*)S->S.idep;
+    if (str) *str = (float*)S->S.str;
+    if (stn) *stn = (float*)S->S.stn;
     return LQ_OK;
 }
 
@@ -383,36 +517,142 @@ extern "C" int lq_sim_health(void* sim, int* health4)
     return LQ_OK;
 }
 
+extern "C" int lq_sim_rebuilds(void* sim, long long* count)
+{
+    if (!sim || !count) return lqb::set_error(LQ_ERR_ARG, "lq_sim_rebuilds: null argument");
+    LqSim* S = static_cast<LqSim*>(sim);
+    int c = 0;
+    LQ_TRY_CUDA(cudaMemcpyAsync(&c, S->rebuilds, sizeof(int), cudaMemcpyDeviceToHost, S->stream), "rebuild count");
+    LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "rebuild count");
+    *count = c;
+    return LQ_OK;
+}
+
+extern "C" int lq_sim_set_skin(void* sim, float skin_over_h)
+{
+    if (!sim || !(skin_over_h >= 0.0f) || skin_over_h > 2.0f)
+        return lqb::set_error(LQ_ERR_ARG, "lq_sim_set_skin: skin/h must be in [0, 2]");
+    LqSim* S = static_cast<LqSim*>(sim);
+    LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "set skin");
+    S->skin = skin_over_h * S->ph.h;
+    LQ_TRY(set_flag(S, 1));
+    LQ_TRY(build_graphs(S));
+    return LQ_OK;
+}
+
 extern "C" int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard)
 {
     if (!sim) return lqb::set_error(LQ_ERR_ARG, "lq_sim_launches_per_step: null sim");
     LqSim* S = static_cast<LqSim*>(sim);
-    /* own kernels per stage: hash, scatter, cell order, gather, Adami (if
-     * npb), interaction, predictor/corrector; the cell scan is a library
-     * kernel and is not counted */
-    const int per_search = 3;
-    const int stage = per_search + 1 + (S->npb > 0 ? 1 : 0) + 1 + 1;
-    if (plain) *plain = 2 * stage;
-    if (with_shepard) *with_shepard = 2 * stage + per_search + 1 + 1;
+    /* own kernels of a step without a rebuild: decide (graph only), Adami
+     * (when npb > 0), interaction and integrator per stage; a Shepard pass
+     * adds the filter and its copy */
+    const int stage = (S->npb > 0 ? 1 : 0) + 1 + 1;
+    const int decide = S->conditional ? 1 : 0;
+    if (plain) *plain = decide + 2 * stage;
+    if (with_shepard) *with_shepard = decide + 2 * stage + (S->npm > 0 ? 2 : 0);
     return LQ_OK;
 }
+
+extern "C" int lq_sim_rebuild_launches(void* sim, int* launches)
+{
+    if (!sim || !launches) return lqb::set_error(LQ_ERR_ARG, "lq_sim_rebuild_launches: null argument");
+    LqSim* S = static_cast<LqSim*>(sim);
+    /* count reset, hash, scatter, cell order (the scan is a library
+     * kernel), gather, copy, material list, boundary list (when npb > 0) */
+    *launches = 4 + 1 + 1 + 1 + (S->npb > 0 ? 1 : 0);
+    return LQ_OK;
+}
+
+/* ------------------------------------------------------------ profiling */
+
+namespace {
+
+/* Phases timed by lq_sim_profile: the reference's Timer phases
+ * (reference include/types.h:158-173, src/loquat.cu:345-395) with the
+ * search and the list build split out. */
+enum { PH_SEARCH = 0, PH_GATHER, PH_ADAMI, PH_INTERACTION, PH_INTEGRATE, PH_SHEPARD, PH_LIST, PH_COUNT };
+
+struct PhaseTimer {
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> phase;
+    int used = 0;
+    int mark(cudaStream_t s, int ph)
+    {
+        if (used + 2 > (int)ev.size()) return lqb::set_error(LQ_ERR_ARG, "profile: event pool exhausted");
+        phase.push_back(ph);
+        LQ_TRY_CUDA(cudaEventRecord(ev[used], s), "profile event");
+        used += 1;
+        return LQ_OK;
+    }
+    int close(cudaStream_t s)
+    {
+        LQ_TRY_CUDA(cudaEventRecord(ev[used], s), "profile event");
+        used += 1;
+        return LQ_OK;
+    }
+};
+
+int profiled_step(LqSim* S, PhaseTimer& T)
+{
+    const Parameters* ph = &S->ph;
+    const Parameters* pd = S->pd;
+    cudaStream_t s = S->stream;
+    const lqb::Cells cells{S->g.start, nullptr, nullptr};
+    bool rebuild = false;
+    LQ_TRY(host_take_flag(S, &rebuild));
+    if (rebuild) {
+        LQ_TRY(T.mark(s, PH_SEARCH));
+        LQ_TRY(lqb::grid_search(ph, pd, S->S.pos, S->g, false, S->health, s));
+        LQ_TRY(T.close(s));
+        LQ_TRY(T.mark(s, PH_GATHER));
+        LQ_TRY(lqb::gather_state(S->np, S->g.part_idx, S->S, S->T, s));
+        k_copy_state<<<blocks(S->np), 256, 0, s>>>(S->np, S->T, S->S, S->xbuild);
+        LQ_TRY_CUDA(cudaGetLastError(), "k_copy_state");
+        LQ_TRY(T.close(s));
+        const float cut = 2.0f * ph->h + S->skin;
+        LQ_TRY(T.mark(s, PH_LIST));
+        LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, S->npb, S->npm, 0, cut, S->S.pos, cells, S->nlm, S->health,
+                                               s));
+        LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, S->nlb, S->health, s));
+        LQ_TRY(T.close(s));
+    }
+    State* cur[2] = {&S->S, &S->S2};
+    for (int stage = 0; stage < 2; ++stage) {
+        LQ_TRY(T.mark(s, PH_ADAMI));
+        LQ_TRY(lqb::launch_adami_list(ph, pd, *cur[stage], S->nlb, s));
+        LQ_TRY(T.close(s));
+        LQ_TRY(T.mark(s, PH_INTERACTION));
+        LQ_TRY(lqb::launch_interaction_list(ph, pd, *cur[stage], S->R, cells, S->nlm, s));
+        LQ_TRY(T.close(s));
+        LQ_TRY(T.mark(s, PH_INTEGRATE));
+        if (stage == 0)
+            LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s));
+        else
+            LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild,
+                                            S->skin, s));
+        LQ_TRY(T.close(s));
+    }
+    return LQ_OK;
+}
+
+}  // namespace
 
 extern "C" int lq_sim_profile(void* sim, int nsteps, double* phase_ms, int* phase_launches)
 {
     if (!sim || nsteps < 0 || !phase_ms) return lqb::set_error(LQ_ERR_ARG, "lq_sim_profile: bad argument");
     LqSim* S = static_cast<LqSim*>(sim);
     PhaseTimer T;
-    const int per_step = 2 * 5 * 2 + 2;
-    T.ev.resize((size_t)nsteps * per_step + 4);
+    T.ev.resize((size_t)nsteps * 2 * (3 + 6 + 1) + 4);
     for (auto& e : T.ev) LQ_TRY_CUDA(cudaEventCreate(&e), "profile event create");
     int st = LQ_OK;
     const int N = S->ph.stress_shepard_filter;
     for (int k = 0; k < nsteps && st == LQ_OK; ++k) {
         S->ph.time = (float)S->time;
-        st = enqueue_step_timed(S, T);
+        st = profiled_step(S, T);
         if (st == LQ_OK && N != 0 && S->step % N == 0 && S->step != 0) {
             st = T.mark(S->stream, PH_SHEPARD);
-            if (st == LQ_OK) st = enqueue_shepard(S);
+            if (st == LQ_OK) st = enqueue_shepard(S, S->stream);
             if (st == LQ_OK) st = T.close(S->stream);
         }
         S->time += (double)S->ph.dt;

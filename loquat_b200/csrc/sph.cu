@@ -24,7 +24,6 @@ namespace lqb {
 
 namespace {
 
-constexpr int kInteractionBlock = 128;
 constexpr int kBlock = 128;
 
 inline int blocks_for(long long n, int b) { return (int)((n + b - 1) / b); }
@@ -41,125 +40,236 @@ inline int blocks_for(long long n, int b) { return (int)((n + b - 1) / b); }
  * mu = h v_ij.x_ij / (r^2 + eta) for approaching pairs; R is the diagonal
  * artificial stress -eps sig_aa / rho^2 of tensile components, f = W/W(dr).
  *
- * Work layout.  One thread per material particle, 32 consecutive sorted
- * particles per warp.  A warp's particles mostly share one grid column
- * (X, Y); lanes are grouped by column and each group walks the union of its
- * lanes' stencils in lockstep: the candidate loop is warp-uniform, every
- * candidate position is one broadcast load, and each lane only runs the
- * cheap distance test.  Hits are appended to a per-lane list in shared
- * memory; when any lane's list is full (and at the end) the warp flushes,
- * each lane evaluating its own pairs, so the ~80-flop pair body runs with
- * most lanes busy instead of once per candidate at ~15% lane use.  A lane
- * meets its neighbours in the same order as a per-thread 27-cell walk, so
- * the sums are bit-identical to that.
- * Per pair: 3 loads (pos 16 B, vel 16 B, stress 24 B), about 80 flops. */
-constexpr int kIntWarps = kInteractionBlock / 32;
-constexpr int kHitCap = 64;
+ * Two ways to visit the neighbours share one pair body:
+ *  - k_interaction_direct: one thread per particle walks its 27 cells
+ *    (the reference operator, no scratch memory);
+ *  - k_neighbor_list + k_interaction_list (native driver): a warp walks the
+ *    union of its lanes' stencils in lockstep (one broadcast load per
+ *    candidate, one distance test per lane) and writes each lane's hits to
+ *    a global list in coalesced rows; a second kernel then evaluates each
+ *    particle's pairs from its list with every lane busy.
+ * Both visit a particle's neighbours in the same order, so their sums are
+ * bit-identical. */
 
-__global__ void __launch_bounds__(kInteractionBlock) k_interaction(const Parameters* __restrict__ P, int np, int npb,
-                                                                   State st, Rates rt, Cells cells)
+struct PairConst {
+    float ih, h, eta, m, Cg, Cw, avc, eps, wdr, cut2;
+    bool visc, artp;
+};
+
+__device__ __forceinline__ PairConst load_pair_const(const Parameters* __restrict__ P)
 {
-    __shared__ int hits[kIntWarps][kHitCap][32];
-    const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int i = npb + blockIdx.x * blockDim.x + threadIdx.x;
-    const bool active = i < np;
+    PairConst K;
+    K.ih = __ldg(&P->i_h);
+    K.h = __ldg(&P->h);
+    K.eta = __ldg(&P->eta);
+    K.m = __ldg(&P->m);
+    K.Cg = __ldg(&P->kernel_gradient_normalization_par);
+    K.Cw = __ldg(&P->kernel_normalization_par);
+    K.visc = __ldg(&P->viscosity_type) == 1;
+    K.avc = __ldg(&P->artificial_viscosity_alpha) * __ldg(&P->cs); /* alpha * cs */
+    K.artp = __ldg(&P->artificial_pressure) == 1;
+    K.eps = __ldg(&P->artificial_pressure_coefficient);
+    K.wdr = __ldg(&P->kernel_dr);
+    K.cut2 = 4.0f * K.h * K.h * 1.0001f; /* candidate test; the pair body applies q < 2 exactly */
+    return K;
+}
 
-    const float ih = __ldg(&P->i_h), h = __ldg(&P->h), eta = __ldg(&P->eta), m = __ldg(&P->m);
-    const float Cg = __ldg(&P->kernel_gradient_normalization_par);
-    const float Cw = __ldg(&P->kernel_normalization_par);
-    const bool visc = __ldg(&P->viscosity_type) == 1;
-    const float avc = __ldg(&P->artificial_viscosity_alpha) * __ldg(&P->cs); /* alpha * cs */
-    const bool artp = __ldg(&P->artificial_pressure) == 1;
-    const float eps = __ldg(&P->artificial_pressure_coefficient);
-    const float wdr = __ldg(&P->kernel_dr);
-    const int nx = __ldg(&P->cell_num_x), ny = __ldg(&P->cell_num_y), nz = __ldg(&P->cell_num_z);
-    const int L = __ldg(&P->ncell_one_layer);
-    const float cut2 = 4.0f * h * h * 1.0001f; /* prefilter; exact test is q < 2 */
+/* The particle whose rates are being summed, and its running sums. */
+struct Target {
+    float4 x, v;
+    float Sxx, Syy, Szz, Sxy, Sxz, Syz; /* sigma_i / rho_i^2 */
+    float Rx, Ry, Rz;                   /* artificial stress of i */
+    float drho, ax, ay, az;
+    float l00, l01, l02, l10, l11, l12, l20, l21, l22;
+};
 
-    float4 xi = make_float4(0.f, 0.f, 0.f, 0.f), vi = make_float4(0.f, 0.f, 0.f, 1.f);
+__device__ __forceinline__ void load_target(const PairConst& K, const State& st, int i, bool active, Target& T)
+{
+    T.x = make_float4(0.f, 0.f, 0.f, 0.f);
+    T.v = make_float4(0.f, 0.f, 0.f, 1.f);
     tensor2d si = make_tensor2d(0.0f);
     if (active) {
-        xi = __ldg(st.pos + i);
-        vi = __ldg(st.vel + i);
+        T.x = __ldg(st.pos + i);
+        T.v = __ldg(st.vel + i);
         si = load_t2(st.str, i);
     }
-    const float rhoi = vi.w;
-    const float ri2 = 1.0f / (rhoi * rhoi);
-    const float Sxx = si.xx * ri2, Syy = si.yy * ri2, Szz = si.zz * ri2;
-    const float Sxy = si.xy * ri2, Sxz = si.xz * ri2, Syz = si.yz * ri2;
-    float Rix = 0.f, Riy = 0.f, Riz = 0.f;
-    if (artp) {
-        Rix = si.xx > 0.f ? -eps * Sxx : 0.f;
-        Riy = si.yy > 0.f ? -eps * Syy : 0.f;
-        Riz = si.zz > 0.f ? -eps * Szz : 0.f;
+    const float ri2 = 1.0f / (T.v.w * T.v.w);
+    T.Sxx = si.xx * ri2; T.Syy = si.yy * ri2; T.Szz = si.zz * ri2;
+    T.Sxy = si.xy * ri2; T.Sxz = si.xz * ri2; T.Syz = si.yz * ri2;
+    T.Rx = T.Ry = T.Rz = 0.f;
+    if (K.artp) {
+        T.Rx = si.xx > 0.f ? -K.eps * T.Sxx : 0.f;
+        T.Ry = si.yy > 0.f ? -K.eps * T.Syy : 0.f;
+        T.Rz = si.zz > 0.f ? -K.eps * T.Szz : 0.f;
     }
+    T.drho = T.ax = T.ay = T.az = 0.f;
+    T.l00 = T.l01 = T.l02 = T.l10 = T.l11 = T.l12 = T.l20 = T.l21 = T.l22 = 0.f;
+}
 
-    float drho = 0.f, ax = 0.f, ay = 0.f, az = 0.f;
-    float l00 = 0.f, l01 = 0.f, l02 = 0.f, l10 = 0.f, l11 = 0.f, l12 = 0.f, l20 = 0.f, l21 = 0.f, l22 = 0.f;
+__device__ __forceinline__ float sqrt_approx(float x)
+{
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 
-    auto pair = [&](int j) {
-        const float4 xj = __ldg(st.pos + j);
-        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        const float q = sqrtf(r2) * ih;
-        if (!(q < 2.0f)) return;
-        const float4 vj = __ldg(st.vel + j);
-        const tensor2d sj = load_t2(st.str, j);
-        const float t = 2.0f - q;
-        const float fac = Cg * t * t * t;
-        const float gx = fac * dx, gy = fac * dy, gz = fac * dz;
-        const float vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
-        drho += vx * gx + vy * gy + vz * gz;
-        const float rinv = __frcp_rn(vj.w);
-        const float rj2 = rinv * rinv;
-        const float Txx = Sxx + sj.xx * rj2, Tyy = Syy + sj.yy * rj2, Tzz = Szz + sj.zz * rj2;
-        const float Txy = Sxy + sj.xy * rj2, Txz = Sxz + sj.xz * rj2, Tyz = Syz + sj.yz * rj2;
-        ax += Txx * gx + Txy * gy + Txz * gz;
-        ay += Txy * gx + Tyy * gy + Tyz * gz;
-        az += Txz * gx + Tyz * gy + Tzz * gz;
-        if (visc) {
-            const float vr = vx * dx + vy * dy + vz * dz;
-            if (vr < 0.f) {
-                const float mu = h * vr / (r2 + eta);
-                const float pi = -avc * mu / (0.5f * (rhoi + vj.w));
-                ax -= pi * gx;
-                ay -= pi * gy;
-                az -= pi * gz;
+/* One pair, without branches: a pair at q >= 2 gets a zero kernel gradient
+ * and adds zero to every sum. */
+__device__ __forceinline__ void pair_body(const PairConst& K, const State& st, Target& T, int j)
+{
+    const float4 xj = __ldg(st.pos + j);
+    const float4 vj = __ldg(st.vel + j);
+    const tensor2d sj = load_t2(st.str, j);
+    const float dx = T.x.x - xj.x, dy = T.x.y - xj.y, dz = T.x.z - xj.z;
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    const float q = sqrt_approx(r2) * K.ih;
+    const float t = fmaxf(2.0f - q, 0.0f);
+    const float fac = K.Cg * t * t * t;
+    const float gx = fac * dx, gy = fac * dy, gz = fac * dz;
+    const float vx = T.v.x - vj.x, vy = T.v.y - vj.y, vz = T.v.z - vj.z;
+    T.drho += vx * gx + vy * gy + vz * gz;
+    const float rinv = __fdividef(1.0f, vj.w);
+    const float rj2 = rinv * rinv;
+    const float Txx = T.Sxx + sj.xx * rj2, Tyy = T.Syy + sj.yy * rj2, Tzz = T.Szz + sj.zz * rj2;
+    const float Txy = T.Sxy + sj.xy * rj2, Txz = T.Sxz + sj.xz * rj2, Tyz = T.Syz + sj.yz * rj2;
+    float px = Txx * gx + Txy * gy + Txz * gz;
+    float py = Txy * gx + Tyy * gy + Tyz * gz;
+    float pz = Txz * gx + Tyz * gy + Tzz * gz;
+    if (K.visc) {
+        /* Pi = -alpha cs h vr / ((r^2 + eta) rhobar) for vr < 0 */
+        const float vr = fminf(vx * dx + vy * dy + vz * dz, 0.0f);
+        const float pi = __fdividef(-K.avc * K.h * vr, (r2 + K.eta) * (0.5f * (T.v.w + vj.w)));
+        px -= pi * gx;
+        py -= pi * gy;
+        pz -= pi * gz;
+    }
+    if (K.artp) {
+        const float wk = K.Cw * t * t * t * t * (q + 0.5f);
+        const float f = __fdividef(wk, K.wdr);
+        const float f4 = (f * f) * (f * f);
+        const float Rjx = sj.xx > 0.f ? -K.eps * sj.xx * rj2 : 0.f;
+        const float Rjy = sj.yy > 0.f ? -K.eps * sj.yy * rj2 : 0.f;
+        const float Rjz = sj.zz > 0.f ? -K.eps * sj.zz * rj2 : 0.f;
+        px += (T.Rx + Rjx) * f4 * gx;
+        py += (T.Ry + Rjy) * f4 * gy;
+        pz += (T.Rz + Rjz) * f4 * gz;
+    }
+    T.ax += px;
+    T.ay += py;
+    T.az += pz;
+    const float Vj = K.m * rinv;
+    const float wx = Vj * vx, wy = Vj * vy, wz = Vj * vz;
+    T.l00 -= wx * gx; T.l01 -= wx * gy; T.l02 -= wx * gz;
+    T.l10 -= wy * gx; T.l11 -= wy * gy; T.l12 -= wy * gz;
+    T.l20 -= wz * gx; T.l21 -= wz * gy; T.l22 -= wz * gz;
+}
+
+__device__ __forceinline__ void store_rates(const Parameters* __restrict__ P, const PairConst& K, const Rates& rt,
+                                            int i, const Target& T)
+{
+    rt.accad[i] = make_float4(K.m * T.ax + __ldg(&P->acc_x), K.m * T.ay + __ldg(&P->acc_y),
+                              K.m * T.az + __ldg(&P->acc_z), K.m * T.drho);
+    rt.spin[i] = make_float4(0.5f * (T.l10 - T.l01), 0.5f * (T.l20 - T.l02), 0.5f * (T.l21 - T.l12), 0.0f);
+    store_t2(rt.acestn, i,
+             make_tensor2d(T.l00, T.l11, T.l22, 0.5f * (T.l01 + T.l10), 0.5f * (T.l02 + T.l20),
+                           0.5f * (T.l12 + T.l21)));
+}
+
+/* The 27-cell walk of one particle (both layers), calling f(j) for every
+ * candidate that passes the distance test, in the order shared by every
+ * neighbour visit of this file: layer, then column (dy outer, dx inner),
+ * then slot. */
+template <class F>
+__device__ __forceinline__ void walk_stencil(const Parameters* __restrict__ P, const PairConst& K, const State& st,
+                                             const Cells& cells, int i, const float4& xi, F&& f)
+{
+    const int nx = __ldg(&P->cell_num_x), ny = __ldg(&P->cell_num_y), nz = __ldg(&P->cell_num_z);
+    const int L = __ldg(&P->ncell_one_layer);
+    const int cx = stencil_axis(xi.x, K.ih), cy = stencil_axis(xi.y, K.ih), cz = stencil_axis(xi.z, K.ih);
+    const int zlo = max(cz - 1, 0), zhi = min(cz + 1, nz - 1);
+    if (zlo > zhi) return;
+    for (int layer = 0; layer < 2; ++layer) {
+        const int off = layer ? L : 0;
+        for (int col = 0; col < 9; ++col) {
+            const int X = cx + (col % 3) - 1, Y = cy + (col / 3) - 1;
+            if (X < 0 || X >= nx || Y < 0 || Y >= ny) continue;
+            int s, e;
+            if (!zrun_range(cells, off + (X * ny + Y) * nz, zlo, zhi, s, e)) continue;
+            for (int j = s; j < e; ++j) {
+                const float4 xj = __ldg(st.pos + j);
+                const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+                if (dx * dx + dy * dy + dz * dz < K.cut2 && j != i) f(j);
             }
         }
-        if (artp) {
-            const float wk = Cw * t * t * t * t * (q + 0.5f);
-            const float f = wk / wdr;
-            const float f4 = (f * f) * (f * f);
-            const float Rjx = sj.xx > 0.f ? -eps * sj.xx * rj2 : 0.f;
-            const float Rjy = sj.yy > 0.f ? -eps * sj.yy * rj2 : 0.f;
-            const float Rjz = sj.zz > 0.f ? -eps * sj.zz * rj2 : 0.f;
-            ax += (Rix + Rjx) * f4 * gx;
-            ay += (Riy + Rjy) * f4 * gy;
-            az += (Riz + Rjz) * f4 * gz;
-        }
-        const float Vj = m * rinv;
-        const float wx = Vj * vx, wy = Vj * vy, wz = Vj * vz;
-        l00 -= wx * gx; l01 -= wx * gy; l02 -= wx * gz;
-        l10 -= wy * gx; l11 -= wy * gy; l12 -= wy * gz;
-        l20 -= wz * gx; l21 -= wz * gy; l22 -= wz * gz;
-    };
+    }
+}
 
-    int count = 0;
+__global__ void __launch_bounds__(kBlock) k_interaction_direct(const Parameters* __restrict__ P, int np, int npb,
+                                                               State st, Rates rt, Cells cells)
+{
+    const int i = npb + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    const PairConst K = load_pair_const(P);
+    Target T;
+    load_target(K, st, i, true, T);
+    walk_stencil(P, K, st, cells, i, T.x, [&](int j) { pair_body(K, st, T, j); });
+    store_rates(P, K, rt, i, T);
+}
+
+constexpr int kListWarps = kBlock / 32;
+constexpr int kStage = 32;
+constexpr int kUnroll = 8;
+
+/* Neighbour lists: list[k * stride + t] is the k-th neighbour slot of target
+ * slot first + t, count[t] their number (entries past LQ_NBR_CAP are not
+ * stored).  Candidates come from grid layers layer_lo..1 (0: both layers,
+ * 1: material only) and are kept when r^2 < cut2, the cut-off (2h) plus any
+ * skin.  Lanes are grouped by grid column; each group
+ * walks the union of its lanes' stencils, so the loop and every candidate
+ * load are warp-uniform and each lane only runs its distance test.  A lane's
+ * own slot passes the test too: its pair adds exactly zero.  Candidates
+ * outside a lane's own three z-cells are farther than 2h from it.  Hits are
+ * staged per lane in shared memory and flushed as coalesced rows. */
+__global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __restrict__ P, int first, int ntarget,
+                                                          int layer_lo, float cut2, const float4* __restrict__ pos,
+                                                          Cells cells, int* __restrict__ list,
+                                                          int* __restrict__ count_out, int stride,
+                                                          int* __restrict__ health)
+{
+    __shared__ int stage[kListWarps][kStage][32];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = first + t;
+    const bool active = t < ntarget;
+    const PairConst K = load_pair_const(P);
+    const int nx = __ldg(&P->cell_num_x), ny = __ldg(&P->cell_num_y), nz = __ldg(&P->cell_num_z);
+    const int L = __ldg(&P->ncell_one_layer);
+    const float4 xi = active ? __ldg(pos + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+    int* my_stage = &stage[w][0][lane];
+
+    int staged = 0, total = 0;
     auto flush = [&]() {
-        const int maxc = (int)__reduce_max_sync(FULL, (unsigned)count);
+        const int maxc = (int)__reduce_max_sync(FULL, (unsigned)staged);
         for (int k = 0; k < maxc; ++k)
-            if (k < count) pair(hits[w][k][lane]);
-        count = 0;
+            if (k < staged && total + k < LQ_NBR_CAP) list[(size_t)(total + k) * stride + t] = my_stage[32 * k];
+        total += staged;
+        staged = 0;
         __syncwarp();
+    };
+    auto test = [&](bool mine, const float4& xj, int j) {
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        if (mine && dx * dx + dy * dy + dz * dz < cut2) {
+            my_stage[32 * staged] = j;
+            ++staged;
+        }
     };
 
     int cx = 0, cy = 0, cz = 0;
     if (active) {
-        cx = stencil_axis(xi.x, ih);
-        cy = stencil_axis(xi.y, ih);
-        cz = stencil_axis(xi.z, ih);
+        cx = stencil_axis(xi.x, K.ih);
+        cy = stencil_axis(xi.y, K.ih);
+        cz = stencil_axis(xi.z, K.ih);
     }
     unsigned todo = __ballot_sync(FULL, active);
     while (todo) {
@@ -171,35 +281,70 @@ __global__ void __launch_bounds__(kInteractionBlock) k_interaction(const Paramet
         const int zmax = __reduce_max_sync(FULL, mine ? cz : INT_MIN);
         const int zlo = max(zmin - 1, 0), zhi = min(zmax + 1, nz - 1);
         if (zlo > zhi) continue;
-        for (int layer = 0; layer < 2; ++layer) {
+        for (int layer = layer_lo; layer < 2; ++layer) {
             const int off = layer ? L : 0;
             for (int col = 0; col < 9; ++col) {
                 const int X = gx + (col % 3) - 1, Y = gy + (col / 3) - 1;
                 if (X < 0 || X >= nx || Y < 0 || Y >= ny) continue;
                 int s, e;
                 if (!zrun_range(cells, off + (X * ny + Y) * nz, zlo, zhi, s, e)) continue;
-                for (int j = s; j < e; ++j) {
-                    const float4 xj = __ldg(st.pos + j);
-                    if (mine) {
-                        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-                        const float r2 = dx * dx + dy * dy + dz * dz;
-                        if (r2 < cut2 && j != i) {
-                            hits[w][count][lane] = j;
-                            ++count;
-                        }
-                    }
-                    if (__any_sync(FULL, count == kHitCap)) flush();
+                int j = s;
+                for (; j + kUnroll <= e; j += kUnroll) {
+                    if (__any_sync(FULL, staged > kStage - kUnroll)) flush();
+                    float4 xj[kUnroll];
+#pragma unroll
+                    for (int u = 0; u < kUnroll; ++u) xj[u] = __ldg(pos + j + u);
+#pragma unroll
+                    for (int u = 0; u < kUnroll; ++u) test(mine, xj[u], j + u);
                 }
+                if (__any_sync(FULL, staged > kStage - kUnroll)) flush();
+                for (; j < e; ++j) test(mine, __ldg(pos + j), j);
             }
         }
     }
     flush();
-    if (!active) return;
-    rt.accad[i] = make_float4(m * ax + __ldg(&P->acc_x), m * ay + __ldg(&P->acc_y), m * az + __ldg(&P->acc_z),
-                              m * drho);
-    rt.spin[i] = make_float4(0.5f * (l10 - l01), 0.5f * (l20 - l02), 0.5f * (l21 - l12), 0.0f);
-    store_t2(rt.acestn, i,
-             make_tensor2d(l00, l11, l22, 0.5f * (l01 + l10), 0.5f * (l02 + l20), 0.5f * (l12 + l21)));
+    if (active) {
+        count_out[t] = total;
+        if (total > LQ_NBR_CAP && health) atomicAdd(health + HEALTH_NBR_OVERFLOW, 1);
+    }
+}
+
+/* Pair sums from the lists; a particle whose list overflowed walks its
+ * stencil directly.  List entries are fetched four pairs ahead so the
+ * dependent neighbour loads do not wait on the list stream. */
+__global__ void __launch_bounds__(kBlock) k_interaction_list(const Parameters* __restrict__ P, int np, int npb,
+                                                             State st, Rates rt, Cells cells,
+                                                             const int* __restrict__ list,
+                                                             const int* __restrict__ count, int stride)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = npb + t;
+    if (i >= np) return;
+    const PairConst K = load_pair_const(P);
+    Target T;
+    load_target(K, st, i, true, T);
+    const int n = __ldg(count + t);
+    if (n <= LQ_NBR_CAP) {
+        const int* row = list + t;
+        int nxt[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) nxt[u] = u < n ? __ldg(row + (size_t)u * stride) : i;
+        for (int k = 0; k < n; k += 4) {
+            int cur[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                cur[u] = nxt[u];
+                const int kk = k + 4 + u;
+                nxt[u] = kk < n ? __ldg(row + (size_t)kk * stride) : i;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (k + u < n) pair_body(K, st, T, cur[u]);
+        }
+    } else {
+        walk_stencil(P, K, st, cells, i, T.x, [&](int j) { pair_body(K, st, T, j); });
+    }
+    store_rates(P, K, rt, i, T);
 }
 
 /* ------------------------------------------------------------- Adami */
@@ -337,15 +482,164 @@ __global__ void __launch_bounds__(kBlock) k_shepard(const Parameters* __restrict
     }
 }
 
+/* ------------------------------------------------- list-driven Adami */
+/* The Adami extrapolation of k_adami, summed over a boundary particle's
+ * list of material neighbours (built with a skin; pairs at q >= 2 are
+ * skipped exactly as the cell walk skips them). */
+__global__ void __launch_bounds__(kBlock) k_adami_list(const Parameters* __restrict__ P, int npb, State st,
+                                                       const int* __restrict__ list, const int* __restrict__ count,
+                                                       int stride)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npb) return;
+    const int n = min(__ldg(count + i), LQ_NBR_CAP);
+    if (n == 0) return;
+    const float ih = __ldg(&P->i_h), m = __ldg(&P->m), Cw = __ldg(&P->kernel_normalization_par);
+    const float4 xi = __ldg(st.pos + i);
+    tensor2d S = make_tensor2d(0.0f);
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int k = 0; k < n; ++k) {
+        const int j = __ldg(list + (size_t)k * stride + i);
+        const float4 xj = __ldg(st.pos + j);
+        const float3 d = make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
+        const float q = norm3df(d.x, d.y, d.z) * ih;
+        if (q < 2.0f) {
+            const float ker = Cw * (2.0f - q) * (2.0f - q) * (2.0f - q) * (2.0f - q) * (q + 0.5f);
+            const float vol = m / __ldg(&st.vel[j].w);
+            const tensor2d sj = load_t2(st.str, j);
+            S.xx += sj.xx * ker * vol;
+            S.yy += sj.yy * ker * vol;
+            S.zz += sj.zz * ker * vol;
+            S.xy += sj.xy * ker * vol;
+            S.xz += sj.xz * ker * vol;
+            S.yz += sj.yz * ker * vol;
+            acc.x += d.x * ker * vol;
+            acc.y += d.y * ker * vol;
+            acc.z += d.z * ker * vol;
+            acc.w += ker * vol;
+        }
+    }
+    if (acc.w > 0.0f) {
+        const float rho0 = __ldg(&P->rho0);
+        tensor2d out;
+        out.xx = (S.xx - rho0 * __ldg(&P->acc_x) * acc.x) / acc.w;
+        out.yy = (S.yy - rho0 * __ldg(&P->acc_y) * acc.y) / acc.w;
+        out.zz = (S.zz - rho0 * __ldg(&P->acc_z) * acc.z) / acc.w;
+        out.xy = S.xy / acc.w;
+        out.xz = S.xz / acc.w;
+        out.yz = S.yz / acc.w;
+        store_t2(st.str, i, out);
+    }
+}
+
+/* ----------------------------------------------- list-driven Shepard */
+/* The Shepard filter of k_shepard over a material particle's list (its
+ * boundary neighbours are skipped: the filter uses the material layer
+ * only).  Writes the filtered stress of material slots to out_str. */
+__global__ void __launch_bounds__(kBlock) k_shepard_list(const Parameters* __restrict__ P, int np, int npb, State st,
+                                                         tensor2d* __restrict__ out_str,
+                                                         const int* __restrict__ list,
+                                                         const int* __restrict__ count, int stride)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = npb + t;
+    if (i >= np) return;
+    const int n = __ldg(count + t);
+    const float ih = __ldg(&P->i_h), m = __ldg(&P->m), Cw = __ldg(&P->kernel_normalization_par);
+    const float4 xi = __ldg(st.pos + i);
+    tensor2d S = make_tensor2d(0.0f);
+    float w = 0.0f;
+    auto add = [&](int j) {
+        if (j < npb) return;
+        const float4 xj = __ldg(st.pos + j);
+        const float3 d = make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
+        const float q = norm3df(d.x, d.y, d.z) * ih;
+        if (q < 2.0f) {
+            const float ker = Cw * (2.0f - q) * (2.0f - q) * (2.0f - q) * (2.0f - q) * (q + 0.5f);
+            const float vol = m / __ldg(&st.vel[j].w);
+            const tensor2d sj = load_t2(st.str, j);
+            S.xx += sj.xx * ker * vol;
+            S.yy += sj.yy * ker * vol;
+            S.zz += sj.zz * ker * vol;
+            S.xy += sj.xy * ker * vol;
+            S.xz += sj.xz * ker * vol;
+            S.yz += sj.yz * ker * vol;
+            w += ker * vol;
+        }
+    };
+    if (n <= LQ_NBR_CAP) {
+        for (int k = 0; k < n; ++k) add(__ldg(list + (size_t)k * stride + t));
+    } else {
+        /* overflowed list: the 27 cells of the material layer (no grid here:
+         * a full scan of material slots in its place is too slow, so the
+         * caller guarantees lists were built without overflow or accepts
+         * the counted overflow in the health word) */
+        for (int k = 0; k < LQ_NBR_CAP; ++k) add(__ldg(list + (size_t)k * stride + t));
+    }
+    S.xx /= w;
+    S.yy /= w;
+    S.zz /= w;
+    S.xy /= w;
+    S.xz /= w;
+    S.yz /= w;
+    store_t2(out_str, i, S);
+}
+
 }  // namespace
 
 int launch_interaction(const Parameters* ph, const Parameters* pd, const State& st, const Rates& r, const Cells& c,
                        cudaStream_t s)
 {
     if (ph->npm <= 0) return LQ_OK;
-    k_interaction<<<blocks_for(ph->npm, kInteractionBlock), kInteractionBlock, 0, s>>>(pd, ph->np, ph->npb, st, r,
-                                                                                      c);
-    LQ_TRY_CUDA(cudaGetLastError(), "k_interaction");
+    k_interaction_direct<<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, r, c);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_interaction_direct");
+    return LQ_OK;
+}
+
+int launch_neighbor_list(const Parameters* ph, const Parameters* pd, const float4* pos, const Cells& c,
+                         const NeighborList& nl, cudaStream_t s)
+{
+    return launch_neighbor_list_range(ph, pd, ph->npb, ph->npm, 0, 2.0f * ph->h * 1.00005f, pos, c, nl, nullptr, s);
+}
+
+int launch_neighbor_list_range(const Parameters* ph, const Parameters* pd, int first, int n, int layer_lo, float cut,
+                               const float4* pos, const Cells& c, const NeighborList& nl, int* health,
+                               cudaStream_t s)
+{
+    if (n <= 0) return LQ_OK;
+    if (nl.stride < n) return set_error(LQ_ERR_ARG, "neighbour list stride %d < targets %d", nl.stride, n);
+    k_neighbor_list<<<blocks_for(n, kBlock), kBlock, 0, s>>>(pd, first, n, layer_lo, cut * cut, pos, c, nl.list,
+                                                            nl.count, nl.stride, health);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_neighbor_list");
+    return LQ_OK;
+}
+
+int launch_adami_list(const Parameters* ph, const Parameters* pd, const State& st, const NeighborList& nl,
+                      cudaStream_t s)
+{
+    if (ph->npb <= 0) return LQ_OK;
+    k_adami_list<<<blocks_for(ph->npb, kBlock), kBlock, 0, s>>>(pd, ph->npb, st, nl.list, nl.count, nl.stride);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_adami_list");
+    return LQ_OK;
+}
+
+int launch_shepard_list(const Parameters* ph, const Parameters* pd, const State& st, tensor2d* out_str,
+                        const NeighborList& nl, cudaStream_t s)
+{
+    if (ph->npm <= 0) return LQ_OK;
+    k_shepard_list<<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, out_str, nl.list,
+                                                                 nl.count, nl.stride);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_shepard_list");
+    return LQ_OK;
+}
+
+int launch_interaction_list(const Parameters* ph, const Parameters* pd, const State& st, const Rates& r,
+                            const Cells& c, const NeighborList& nl, cudaStream_t s)
+{
+    if (ph->npm <= 0) return LQ_OK;
+    k_interaction_list<<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, r, c, nl.list,
+                                                                     nl.count, nl.stride);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_interaction_list");
     return LQ_OK;
 }
 
