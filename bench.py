@@ -321,7 +321,7 @@ def bench_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": workload, "np": np_, "npm": npm, "npb": par.npb, "ncell": par.ncell,
-                       "form": "plain FP32, %s, Verlet lists (skin 0.1h)" % ("eager launches" if args.eager else "CUDA-graph step"),
+                       "form": "plain FP32, %s, Verlet lists (skin 0.05h)" % ("eager launches" if args.eager else "CUDA-graph step"),
                        "timed_window": "steps %d..%d of the run" % (s0, s1),
                        "l2": "state larger than L2 (3 x %.0f MB state buffers)" % (np_ * 96 / 1e6),
                        "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},

@@ -155,7 +155,7 @@ int lq_sim_health(void* sim, int* health4);
 /* Neighbour lists are kept across steps and rebuilt (search, sort, list
  * build) only when a particle's displacement since the last build plus a
  * bound on its next step's motion reaches half the skin; the lists hold
- * every pair within 2h + skin.  Default skin 0.1 h; setting it forces a
+ * every pair within 2h + skin.  Default skin 0.05 h; setting it forces a
  * rebuild before the next step.  lq_sim_rebuilds counts rebuilds so far. */
 int lq_sim_set_skin(void* sim, float skin_over_h);
 int lq_sim_rebuilds(void* sim, long long* count);

@@ -17,7 +17,9 @@ import numpy as np
 
 from .params import Parameters, PARAMETER_FIELDS, dp_cone, elastic_moduli  # noqa: F401
 
-_LIB_PATH = Path(__file__).resolve().parent / "liblqb200.so"
+# LOQUAT_B200_LIB selects another build of the same library (kernel variants
+# compared side by side); by default the in-tree build is used.
+_LIB_PATH = Path(os.environ.get("LOQUAT_B200_LIB") or Path(__file__).resolve().parent / "liblqb200.so")
 _lib = None
 
 LQ_OK, LQ_ERR_ARG, LQ_ERR_CUDA, LQ_ERR_ALLOC, LQ_ERR_IO, LQ_ERR_STATE, LQ_ERR_NOTFOUND = range(7)

@@ -47,9 +47,9 @@ def _stale(obj: Path, src: Path, hdr_mtime: float) -> bool:
     return m < src.stat().st_mtime or m < hdr_mtime
 
 
-def _compile(src: Path, ptxas_verbose: bool) -> tuple[Path, str]:
+def _compile(src: Path, ptxas_verbose: bool, extra=()) -> tuple[Path, str]:
     obj = BUILD / (src.name + ".o")
-    cmd = [NVCC, *ARCH, *COMMON, "-c", str(src), "-o", str(obj)]
+    cmd = [NVCC, *ARCH, *COMMON, *extra, "-c", str(src), "-o", str(obj)]
     if ptxas_verbose and src.suffix == ".cu":
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -58,16 +58,22 @@ def _compile(src: Path, ptxas_verbose: bool) -> tuple[Path, str]:
     return obj, r.stderr
 
 
-def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = True) -> Path:
-    """Compile and link the library; returns its path."""
-    BUILD.mkdir(exist_ok=True)
+def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = True, defines=(), out: Path | None = None,
+          build_dir: Path | None = None) -> Path:
+    """Compile and link the library; returns its path.  `defines` adds -D
+    options and `out`/`build_dir` place a variant build elsewhere."""
+    global BUILD, LIB
+    if out is not None:
+        BUILD, LIB = Path(build_dir or Path(out).parent / "_build"), Path(out)
+    BUILD.mkdir(parents=True, exist_ok=True)
+    extra = [f"-D{d}" for d in defines]
     hdr_mtime = max((h.stat().st_mtime for h in _headers()), default=0.0)
     srcs = _sources()
     todo = [s for s in srcs if force or ptxas_verbose or _stale(BUILD / (s.name + ".o"), s, hdr_mtime)]
     reports = []
     if todo:
         with cf.ThreadPoolExecutor(max_workers=min(8, len(todo))) as ex:
-            for obj, err in ex.map(lambda s: _compile(s, ptxas_verbose), todo):
+            for obj, err in ex.map(lambda s: _compile(s, ptxas_verbose, extra), todo):
                 if err.strip():
                     reports.append((obj.name, err))
     objs = [BUILD / (s.name + ".o") for s in srcs]
@@ -86,8 +92,11 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose-ptxas", action="store_true")
+    ap.add_argument("-D", dest="defines", action="append", default=[], help="preprocessor definition")
+    ap.add_argument("--out", type=Path, default=None, help="variant library path (objects beside it)")
     a = ap.parse_args(argv)
-    lib = build(force=a.force, ptxas_verbose=a.verbose_ptxas, quiet=False)
+    lib = build(force=a.force or bool(a.defines), ptxas_verbose=a.verbose_ptxas, quiet=False, defines=a.defines,
+                out=a.out)
     print(lib)
 
 

@@ -34,7 +34,7 @@ namespace {
 
 using lqb::State;
 
-constexpr float kDefaultSkinOverH = 0.1f;
+constexpr float kDefaultSkinOverH = 0.05f;
 
 struct LqSim {
     Parameters ph{};

@@ -216,6 +216,10 @@ __global__ void __launch_bounds__(kBlock) k_interaction_direct(const Parameters*
     store_rates(P, K, rt, i, T);
 }
 
+#ifndef LQ_PAIR_MIN_BLOCKS
+#define LQ_PAIR_MIN_BLOCKS 6   /* 128-thread blocks per SM: 75 registers, no spills (measured best of 1, 6, 8) */
+#endif
+
 constexpr int kListWarps = kBlock / 32;
 constexpr int kStage = 32;
 constexpr int kUnroll = 8;
@@ -312,10 +316,9 @@ __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __re
 /* Pair sums from the lists; a particle whose list overflowed walks its
  * stencil directly.  List entries are fetched four pairs ahead so the
  * dependent neighbour loads do not wait on the list stream. */
-__global__ void __launch_bounds__(kBlock) k_interaction_list(const Parameters* __restrict__ P, int np, int npb,
-                                                             State st, Rates rt, Cells cells,
-                                                             const int* __restrict__ list,
-                                                             const int* __restrict__ count, int stride)
+__global__ void __launch_bounds__(kBlock, LQ_PAIR_MIN_BLOCKS) k_interaction_list(
+    const Parameters* __restrict__ P, int np, int npb, State st, Rates rt, Cells cells, const int* __restrict__ list,
+    const int* __restrict__ count, int stride)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = npb + t;
@@ -325,17 +328,20 @@ __global__ void __launch_bounds__(kBlock) k_interaction_list(const Parameters* _
     load_target(K, st, i, true, T);
     const int n = __ldg(count + t);
     if (n <= LQ_NBR_CAP) {
-        const int* row = list + t;
+        /* entry k of this particle is at list[k * stride + t]; p walks
+         * four entries at a time, offsets within a group stay 32-bit */
+        const int* p = list + t;
+        const size_t step4 = 4 * (size_t)stride;
         int nxt[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) nxt[u] = u < n ? __ldg(row + (size_t)u * stride) : i;
+        for (int u = 0; u < 4; ++u) nxt[u] = u < n ? __ldg(p + u * stride) : i;
         for (int k = 0; k < n; k += 4) {
+            p += step4;
             int cur[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 cur[u] = nxt[u];
-                const int kk = k + 4 + u;
-                nxt[u] = kk < n ? __ldg(row + (size_t)kk * stride) : i;
+                nxt[u] = k + 4 + u < n ? __ldg(p + u * stride) : i;
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u)
