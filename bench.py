@@ -51,7 +51,8 @@ def parse_args(argv=None):
     ap.add_argument("--steps", type=int, default=250)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["cylinder", "column"], default="cylinder")
+    ap.add_argument("--config", choices=["cylinder", "column", "ensemble"], default="cylinder")
+    ap.add_argument("--scenarios", type=int, default=256, help="ensemble size (--config ensemble)")
     ap.add_argument("--dr", type=float, default=None, help="override the particle spacing")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -346,10 +347,74 @@ def bench_ours(args):
     return 0
 
 
+def bench_ensemble(args):
+    """Batched ensemble (one simulation holding every scenario, one graph
+    launch per step) against the same scenarios run one after another, each
+    as its own plain simulation.  Both timed with CUDA events on the
+    simulations' streams, after the same warm-up."""
+    import torch
+
+    import loquat_b200 as lq
+    from loquat_b200 import cases
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    comb, parts = cases.ensemble(n=args.scenarios, seed=4 + rank)
+    par = comb.par
+
+    def timed(sim, steps):
+        ext = torch.cuda.ExternalStream(sim.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sim.synchronize()
+        e0.record(ext)
+        sim.step(steps)
+        e1.record(ext)
+        sim.synchronize()
+        return e0.elapsed_time(e1)
+
+    sim = lq.Simulation(par, *comb.arrays())
+    sim.set_materials(comb.meta["materials"])
+    sim.set_frames(comb.meta["frames"])
+    sim.step(args.warmup)
+    rb0 = sim.rebuilds()
+    clocks = ClockSampler(gpu_uuid(torch, local)) if rank == 0 else None
+    ms_batch = timed(sim, args.steps)
+    clk = clocks.stop() if clocks else None
+    rebuilds = sim.rebuilds() - rb0
+    health = sim.health()
+    sim.close()
+    ms_seq = 0.0
+    for p in parts:
+        s = lq.Simulation(p.par, *p.arrays())
+        s.step(args.warmup)
+        ms_seq += timed(s, args.steps)
+        s.close()
+    npm = par.npm
+    v_batch = npm * args.steps / (ms_batch / 1e3)
+    v_seq = npm * args.steps / (ms_seq / 1e3)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "particle-steps/s", "value": v_batch, "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batch / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "ensemble of %d Drucker-Prager column collapses (counts log-uniform 5e3-2e5, "
+                                   "H/L 0.5-4, phi 20-40 deg, c 0-5 kPa, dr=2 mm, h=1.2dr)" % args.scenarios,
+                       "np": par.np, "npm": npm, "npb": par.npb, "ncell": par.ncell,
+                       "form": "batched: one simulation, per-scenario frames and materials, CUDA-graph step"},
+            "sequential": {"value": v_seq, "ms_per_step": ms_seq / args.steps,
+                           "form": "the same scenarios one after another, one plain simulation each"},
+            "batched_over_sequential": v_batch / v_seq,
+            "neighbour_list_rebuilds": rebuilds, "health": [int(x) for x in health], "clocks": clk,
+        }))
+    return 0
+
+
 def main(argv=None):
     args = parse_args(argv)
     if args.impl == "reference":
         return bench_reference(args)
+    if args.config == "ensemble":
+        return bench_ensemble(args)
     return bench_ours(args)
 
 

@@ -159,6 +159,22 @@ int lq_sim_health(void* sim, int* health4);
  * rebuild before the next step.  lq_sim_rebuilds counts rebuilds so far. */
 int lq_sim_set_skin(void* sim, float skin_over_h);
 int lq_sim_rebuilds(void* sim, long long* count);
+/* Per-object materials, for many independent scenarios in one simulation
+ * (each scenario's particles placed farther than 2h from the others):
+ * a material particle uses row (int)idep.x of the n x 5 host table (the
+ * five model parameters of Parameters.model_par_1..5; the constitutive
+ * model itself stays global).  Rows out of range are clamped.  n = 0
+ * returns to the global parameters.  No reference counterpart: the
+ * reference runs one scenario per process. */
+int lq_sim_set_materials(void* sim, int n, const float* table);
+/* Per-object grid frames, for the same use: each object keeps local
+ * coordinates and owns a block of grid rows in y.  rows is n x 2 ints,
+ * (first row, number of rows) for object ids 0..n-1; a particle's local y
+ * cell c maps to grid row first + c, and c outside [0, rows) counts as
+ * outside the lattice.  Blocks of objects that must not interact need at
+ * least one empty row between them.  Forces a search before the next step.
+ * No reference counterpart. */
+int lq_sim_set_frames(void* sim, int n, const int* rows);
 /* Own kernel launches of a step without a rebuild (plain) and of a step
  * with the Shepard pass; a rebuild adds lq_sim_rebuild_launches more. */
 int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard);

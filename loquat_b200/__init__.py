@@ -68,6 +68,8 @@ _SIGNATURES = {
     "lq_sim_launches_per_step": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "lq_sim_profile": (_I, [_VP, _I, _VP, _VP]),
     "lq_sim_set_skin": (_I, [_VP, _F]),
+    "lq_sim_set_materials": (_I, [_VP, _I, _VP]),
+    "lq_sim_set_frames": (_I, [_VP, _I, _VP]),
     "lq_sim_rebuilds": (_I, [_VP, ctypes.POINTER(_LL)]),
     "lq_sim_rebuild_launches": (_I, [_VP, ctypes.POINTER(_I)]),
     "lq_io_load_parameters": (_I, [ctypes.c_char_p, _VP]),
@@ -281,6 +283,17 @@ class Simulation:
 
     def set_skin(self, skin_over_h: float):
         check(lib().lq_sim_set_skin(self.handle, skin_over_h), "lq_sim_set_skin")
+
+    def set_materials(self, table):
+        """Per-object model parameters: row k (5 floats) applies to material
+        particles whose idep.x is k."""
+        t = np.ascontiguousarray(table, np.float32).reshape(-1, 5)
+        check(lib().lq_sim_set_materials(self.handle, t.shape[0], t.ctypes.data), "lq_sim_set_materials")
+
+    def set_frames(self, rows):
+        """Per-object grid rows: rows[k] = (first row, number of rows)."""
+        r = np.ascontiguousarray(rows, np.int32).reshape(-1, 2)
+        check(lib().lq_sim_set_frames(self.handle, r.shape[0], r.ctypes.data), "lq_sim_set_frames")
 
     def rebuilds(self) -> int:
         c = _LL()

@@ -238,3 +238,100 @@ def config_case(index: int, **kw) -> Case:
     if index == 1:
         return cylinder_collapse(**kw)
     raise ValueError(f"configuration {index} has no generator yet")
+
+
+def _column_parts(nsx, nsy, nsz, dr, layers, runout_cells, wall_top_cells):
+    """Soil block and Adami walls (floor, back wall, two side walls) of one
+    column-collapse scenario in local coordinates starting at 0."""
+    b = layers * dr
+    nwy = nsy + 2 * layers
+    nrx = nsx + runout_cells
+    soil = _lattice(nsx, nsy, nsz, dr, (b, b, b))
+    bnd = np.concatenate([
+        _lattice(nrx + layers, nwy, layers, dr, (0.0, 0.0, 0.0)),
+        _lattice(layers, nsy, wall_top_cells, dr, (0.0, b, b)),
+        _lattice(nrx + layers, layers, wall_top_cells, dr, (0.0, 0.0, b)),
+        _lattice(nrx + layers, layers, wall_top_cells, dr, (0.0, b + nsy * dr, b)),
+    ])
+    extent = ((nrx + layers) * dr, nwy * dr, b + nsz * dr)
+    return soil, bnd, extent
+
+
+def ensemble(n=256, seed=4, dr=0.002, hdr=1.2, count_range=(5.0e3, 2.0e5), aspect_range=(0.5, 4.0),
+             phi_range=(20.0, 40.0), cohesion_range=(0.0, 5.0e3), thickness_layers=10, layers=3,
+             runout_frac=0.5, rho0=2650.0, E=0.84e6, nu=0.3, cfl=0.1, alpha=0.25, shepard=30, jitter_frac=0.01):
+    """An ensemble of independent Drucker-Prager column collapses.
+
+    Scenario k has a soil count drawn log-uniform on count_range, aspect
+    ratio H/L uniform on aspect_range, friction angle uniform on phi_range
+    (degrees) and cohesion uniform on cohesion_range (Pa); all share dr, h,
+    density and elasticity, hence one time step.  Returns (combined, parts).
+    `parts` are the scenarios as standalone cases.  `combined` holds all of
+    them in one particle set for a single simulation: every particle of
+    scenario k (boundary and soil) has object id k + 1 and keeps its local
+    coordinates; meta["frames"] gives each object its own block of grid
+    rows (with an empty row between blocks, so no pair crosses scenarios)
+    and meta["materials"] its (K, G, k_phi, k_psi, k_c) -- for
+    Simulation.set_frames and Simulation.set_materials."""
+    rng = np.random.default_rng(seed)
+    K, G = elastic_moduli(E, nu)
+    lo, hi = np.log(count_range[0]), np.log(count_range[1])
+    parts = []
+    for k in range(n):
+        count = float(np.exp(rng.uniform(lo, hi)))
+        a = float(rng.uniform(*aspect_range))
+        phi = float(rng.uniform(*phi_range))
+        coh = float(rng.uniform(*cohesion_range))
+        nsy = thickness_layers
+        nsx = max(2, int(round(np.sqrt(count / (nsy * a)))))
+        nsz = max(2, int(round(a * nsx)))
+        runout = max(2, int(round(runout_frac * nsx)))
+        soil, bnd, extent = _column_parts(nsx, nsy, nsz, dr, layers, runout, int(round(1.1 * nsz)))
+        kphi, kpsi, kc = dp_cone(phi, 0.0, coh)
+        par_k = _base_parameters(dr, hdr, rho0, (extent[0], extent[1], 1.5 * extent[2]), E, nu, cfl, 1,
+                                 lambda K_, G_, a=(K, G, kphi, kpsi, kc): a, shepard, alpha, (0.0, 0.0, -9.81))
+        b = layers * dr
+        part = assemble(f"ensemble_{k}", par_k, bnd, soil, np.random.default_rng(int(rng.integers(1 << 30))),
+                        jitter_frac * dr, rho0, -9.81, b + nsz * dr, b, 1.0 - np.sin(np.radians(phi)),
+                        object_ids=(k + 1, k + 1),
+                        meta=dict(config="ensemble", scenario=k, phi=phi, cohesion=coh, aspect=nsz / nsx,
+                                  extent=extent, material=(K, G, kphi, kpsi, kc)))
+        parts.append(part)
+    two_h = 2.0 * hdr * dr
+    table = np.zeros((n + 1, 5), np.float32)
+    frames = np.zeros((n + 1, 2), np.int32)
+    row = 0
+    for k, p in enumerate(parts):
+        table[k + 1] = p.meta["material"]
+        rows = int(np.floor(p.meta["extent"][1] / two_h)) + 2
+        frames[k + 1] = (row, rows)
+        row += rows + 1
+    xsize = max(p.meta["extent"][0] for p in parts)
+    zsize = max(p.meta["extent"][2] for p in parts)
+    par = _base_parameters(dr, hdr, rho0, (xsize, row * two_h, 1.5 * zsize), E, nu, cfl, 1,
+                           lambda K_, G_: tuple(table[1]), shepard, alpha, (0.0, 0.0, -9.81))
+    nb = sum(p.par.npb for p in parts)
+    ns = sum(p.par.npm for p in parts)
+    arrays = [np.zeros((nb + ns, 4), np.float32), np.zeros((nb + ns, 4), np.float32),
+              np.zeros((nb + ns, 4), np.float32), np.zeros((nb + ns, 6), np.float32),
+              np.zeros((nb + ns, 6), np.float32)]
+    ob, om = 0, nb
+    slices = []
+    for p in parts:
+        pb, pm = p.par.npb, p.par.npm
+        for a_out, a_in in zip(arrays, p.arrays()):
+            a_out[ob:ob + pb] = a_in[:pb]
+            a_out[om:om + pm] = a_in[pb:]
+        slices.append(((ob, ob + pb), (om, om + pm)))
+        ob += pb
+        om += pm
+    from . import initialize_parameters
+
+    par.np, par.npb, par.npm = nb + ns, nb, ns
+    initialize_parameters(par)
+    par.dt = par.cfl * par.h / par.cs
+    assert par.cell_num_y >= row
+    combined = Case("ensemble", par, *arrays,
+                    meta=dict(config="ensemble", n=n, materials=table, frames=frames, slices=slices, np=nb + ns,
+                              npb=nb, npm=ns))
+    return combined, parts

@@ -38,7 +38,8 @@ inline int blocks_for(long long n, int b = kBlock) { return (int)((n + b - 1) / 
 __global__ void __launch_bounds__(kBlock) k_hash_count(const Parameters* __restrict__ P, int np, int npb,
                                                        const float4* __restrict__ pos, int* __restrict__ key,
                                                        int* __restrict__ rank, int* __restrict__ count,
-                                                       int* __restrict__ health)
+                                                       int* __restrict__ health, const float4* __restrict__ idep,
+                                                       Frames fr)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = i < np;
@@ -47,7 +48,14 @@ __global__ void __launch_bounds__(kBlock) k_hash_count(const Parameters* __restr
         const float ih = __ldg(&P->i_h);
         const int nx = __ldg(&P->cell_num_x), ny = __ldg(&P->cell_num_y), nz = __ldg(&P->cell_num_z);
         const float4 p = __ldg(pos + i);
-        const int cx = cell_axis(p.x, ih, nx), cy = cell_axis(p.y, ih, ny), cz = cell_axis(p.z, ih, nz);
+        int cy = cell_axis(p.y, ih, ny);
+        if (fr.rows) {
+            /* local cell, then the object's row block */
+            const float s = floorf(0.5f * p.y * ih);
+            const int local = (s >= 0.0f && s < 1.0e9f) ? (int)s : -1;
+            cy = local < 0 ? -1 : frame_row(fr, __ldg(&idep[i].x), local);
+        }
+        const int cx = cell_axis(p.x, ih, nx), cz = cell_axis(p.z, ih, nz);
         if (cx < 0 || cy < 0 || cz < 0) {
             k = __ldg(&P->ncell_delete);
             if (health) atomicAdd(health + (i < npb ? HEALTH_BND_OUT : HEALTH_MAT_OUT), 1);
@@ -170,7 +178,7 @@ int scan_scratch_bytes(int ncell, size_t* bytes)
 }
 
 int grid_search(const Parameters* ph, const Parameters* pd, const float4* pos, GridBuffers& g, bool bounds,
-                int* health, cudaStream_t s)
+                int* health, cudaStream_t s, const float4* idep, const Frames& fr)
 {
     const int np = ph->np, npb = ph->npb, ncell = ph->ncell;
     if (np < 0 || npb < 0 || npb > np || ncell < 1)
@@ -182,7 +190,8 @@ int grid_search(const Parameters* ph, const Parameters* pd, const float4* pos, G
         return set_error(LQ_ERR_ARG, "grid_search: Parameters cell counts are not initialised");
     LQ_TRY(fill_int(g.count, ncell + 1, 0, s));
     if (np > 0) {
-        k_hash_count<<<blocks_for(np), kBlock, 0, s>>>(pd, np, npb, pos, g.key, g.rank, g.count, health);
+        if (fr.rows && !idep) return set_error(LQ_ERR_ARG, "grid_search: frames need the idep array");
+        k_hash_count<<<blocks_for(np), kBlock, 0, s>>>(pd, np, npb, pos, g.key, g.rank, g.count, health, idep, fr);
         LQ_TRY_CUDA(cudaGetLastError(), "k_hash_count");
     }
     size_t bytes = g.scan_bytes;

@@ -29,7 +29,7 @@ inline int blocks_for(long long n, int b) { return (int)((n + b - 1) / b); }
  * v += dt/2 a; rho += dt/2 drho; x += dt/2 v_new; eps += dt/2 deps;
  * stress and plastic strain from the model at dt/2. */
 __global__ void __launch_bounds__(kBlock) k_predict(const Parameters* __restrict__ P, int np, int npb, State in,
-                                                    State out, State snap, bool do_snap, Rates rt)
+                                                    State out, State snap, bool do_snap, Rates rt, MaterialTable mt)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(kBlock) k_predict(const Parameters* __restrict
         return;
     }
     const float dt = __ldg(&P->dt);
-    const Material M = load_material(P);
+    const Material M = particle_material(load_material(P), mt, id.x);
     const float4 a = __ldg(rt.accad + i);
     const float4 w = __ldg(rt.spin + i);
     const tensor2d de = load_t2(rt.acestn, i);
@@ -107,7 +107,8 @@ struct VerletCheck {
 
 __global__ void __launch_bounds__(kBlock) k_correct(const Parameters* __restrict__ P, int np, int npb, State cur,
                                                     State ini, const int* __restrict__ ini_idx, State out, Rates rt,
-                                                    int* __restrict__ health, VerletCheck verlet, int first)
+                                                    int* __restrict__ health, VerletCheck verlet, int first,
+                                                    MaterialTable mt)
 {
     const int i = first + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
@@ -121,7 +122,6 @@ __global__ void __launch_bounds__(kBlock) k_correct(const Parameters* __restrict
     }
     const int k = ini_idx ? __ldg(ini_idx + i) : i;
     const float dt = __ldg(&P->dt);
-    const Material M = load_material(P);
     const float4 a = __ldg(rt.accad + i);
     const float4 w = __ldg(rt.spin + i);
     const tensor2d de = load_t2(rt.acestn, i);
@@ -132,6 +132,7 @@ __global__ void __launch_bounds__(kBlock) k_correct(const Parameters* __restrict
     const tensor2d e0 = load_t2_rw(ini.stn, k);
     const float4 xc = cur.pos[i];
     const float4 id = cur.idep[i];
+    const Material M = particle_material(load_material(P), mt, id.x);
 
     float4 v;
     v.x = v0.x + dt * a.x;
@@ -181,12 +182,12 @@ __global__ void __launch_bounds__(kBlock) k_correct(const Parameters* __restrict
 }  // namespace
 
 int launch_predict(const Parameters* ph, const Parameters* pd, const State& in, const State& out, const State* snap,
-                   const Rates& r, cudaStream_t s)
+                   const Rates& r, cudaStream_t s, const MaterialTable& mt)
 {
     if (ph->np <= 0) return LQ_OK;
     const bool do_snap = snap && snap->pos;
     State sn = do_snap ? *snap : State{nullptr, nullptr, nullptr, nullptr, nullptr};
-    k_predict<<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r);
+    k_predict<<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt);
     LQ_TRY_CUDA(cudaGetLastError(), "k_predict");
     return LQ_OK;
 }
@@ -196,18 +197,19 @@ int launch_correct(const Parameters* ph, const Parameters* pd, const State& cur,
 {
     if (ph->npm <= 0) return LQ_OK;
     k_correct<<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, ini_idx, cur, r, health,
-                                                             VerletCheck{nullptr, nullptr, 0.0f}, ph->npb);
+                                                             VerletCheck{nullptr, nullptr, 0.0f}, ph->npb,
+                                                             MaterialTable());
     LQ_TRY_CUDA(cudaGetLastError(), "k_correct");
     return LQ_OK;
 }
 
 int launch_correct_into(const Parameters* ph, const Parameters* pd, const State& cur, const State& ini,
                         const State& out, const Rates& r, int* health, const float4* xbuild, int* rebuild,
-                        float skin, cudaStream_t s)
+                        float skin, cudaStream_t s, const MaterialTable& mt)
 {
     if (ph->np <= 0) return LQ_OK;
     k_correct<<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health,
-                                                            VerletCheck{xbuild, rebuild, 0.5f * skin}, 0);
+                                                            VerletCheck{xbuild, rebuild, 0.5f * skin}, 0, mt);
     LQ_TRY_CUDA(cudaGetLastError(), "k_correct");
     return LQ_OK;
 }

@@ -51,6 +51,27 @@ __device__ __forceinline__ int stencil_axis(float x, float i_h)
     return (int)fminf(fmaxf(s, -2.0f), 1073741824.0f);
 }
 
+/* Grid row of a particle's local y cell under per-object frames: returns
+ * -1 when the local cell is outside its object's rows. */
+__device__ __forceinline__ int frame_row(const Frames& fr, float id, int cy_local)
+{
+    int k = (int)id;
+    k = k < 0 ? 0 : (k >= fr.n ? fr.n - 1 : k);
+    const int base = __ldg(fr.rows + 2 * k), rows = __ldg(fr.rows + 2 * k + 1);
+    return (cy_local >= 0 && cy_local < rows) ? base + cy_local : -1;
+}
+
+/* Stencil centre row under frames (clamped like stencil_axis). */
+__device__ __forceinline__ int frame_stencil_row(const Frames& fr, float id, int cy_local)
+{
+    int k = (int)id;
+    k = k < 0 ? 0 : (k >= fr.n ? fr.n - 1 : k);
+    const int base = __ldg(fr.rows + 2 * k), rows = __ldg(fr.rows + 2 * k + 1);
+    /* a stencil centred outside the object's rows touches none of them */
+    if (cy_local < -1 || cy_local > rows) return -2;
+    return base + cy_local;
+}
+
 /* The particles of the three cells (X, Y, zlo..zhi) of one layer are one
  * contiguous slot range because keys are z-fastest and the sort is by key.
  * Returns false when the range is empty. */
@@ -100,6 +121,22 @@ __device__ __forceinline__ Material load_material(const Parameters* P)
     m.p3 = __ldg(&P->model_par_3);
     m.p4 = __ldg(&P->model_par_4);
     m.p5 = __ldg(&P->model_par_5);
+    return m;
+}
+
+/* The material of a particle with object id `id` (see MaterialTable). */
+__device__ __forceinline__ Material particle_material(const Material& base, const MaterialTable& mt, float id)
+{
+    if (!mt.p) return base;
+    int k = (int)id;
+    k = k < 0 ? 0 : (k >= mt.n ? mt.n - 1 : k);
+    const float* r = mt.p + 5 * k;
+    Material m = base;
+    m.p1 = __ldg(r + 0);
+    m.p2 = __ldg(r + 1);
+    m.p3 = __ldg(r + 2);
+    m.p4 = __ldg(r + 3);
+    m.p5 = __ldg(r + 4);
     return m;
 }
 

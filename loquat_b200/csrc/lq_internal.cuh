@@ -55,6 +55,25 @@ struct Cells {
     const int* end;
 };
 
+/* Per-object constitutive parameters: when p is set, a material particle
+ * uses row (int)idep.x (clamped to [0, n)) of the n x 5 table p in place of
+ * model_par_1..5.  Lets one simulation hold many independent scenarios
+ * with their own materials. */
+struct MaterialTable {
+    const float* p = nullptr;
+    int n = 0;
+};
+
+/* Per-object cell frames: when rows is set, a particle with object id k
+ * ((int)idep.x, clamped to [0, n)) lies in its own block of grid rows: its
+ * local y cell c (0 <= c < rows[2k+1], else outside the lattice) maps to
+ * grid row rows[2k] + c.  Positions stay local to each object, so many
+ * independent scenarios share one grid without losing float precision. */
+struct Frames {
+    const int* rows = nullptr;
+    int n = 0;
+};
+
 /* Health counters written by the kernels (see lq_sim_health). */
 enum { HEALTH_NONFINITE = 0, HEALTH_MAT_OUT = 1, HEALTH_BND_OUT = 2, HEALTH_NBR_OVERFLOW = 3, HEALTH_WORDS = 4 };
 
@@ -80,7 +99,8 @@ int scan_scratch_bytes(int ncell, size_t* bytes);
  * particles by cell key.  Writes key, rank, count, start, part_idx,
  * part_cel, and beg/end when `bounds` is set.  `health` may be null. */
 int grid_search(const Parameters* par_host, const Parameters* par_dev, const float4* pos, GridBuffers& g,
-                bool bounds, int* health, cudaStream_t s);
+                bool bounds, int* health, cudaStream_t s, const float4* idep = nullptr,
+                const Frames& fr = Frames());
 
 int gather_float4(int n, const int* idx, const float4* in, float4* out, cudaStream_t s);
 int gather_tensor2d(int n, const int* idx, const tensor2d* in, tensor2d* out, cudaStream_t s);
@@ -104,7 +124,7 @@ int launch_interaction(const Parameters* par_host, const Parameters* par_dev, co
 int launch_neighbor_list(const Parameters* par_host, const Parameters* par_dev, const float4* pos, const Cells& c,
                          const NeighborList& nl, cudaStream_t s);
 int launch_interaction_list(const Parameters* par_host, const Parameters* par_dev, const State& st, const Rates& r,
-                            const Cells& c, const NeighborList& nl, cudaStream_t s);
+                            const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr = Frames());
 int launch_adami(const Parameters* par_host, const Parameters* par_dev, const State& st, const Cells& c,
                  cudaStream_t s);
 /* Shepard filter of material stress into out_str[npb, np).  When `full` is
@@ -115,7 +135,7 @@ int launch_shepard(const Parameters* par_host, const Parameters* par_dev, const 
 /* Predictor: out <- in advanced by dt/2 on material slots, boundary slots
  * copied when out != in; `snap` (may be all-null) receives a copy of `in`. */
 int launch_predict(const Parameters* par_host, const Parameters* par_dev, const State& in, const State& out,
-                   const State* snap, const Rates& r, cudaStream_t s);
+                   const State* snap, const Rates& r, cudaStream_t s, const MaterialTable& mt = MaterialTable());
 /* Corrector in place on `cur`; ini values read at ini_idx[i] (identity when
  * ini_idx is null).  Non-finite results are counted in health. */
 int launch_correct(const Parameters* par_host, const Parameters* par_dev, const State& cur, const State& ini,
@@ -126,7 +146,7 @@ int launch_correct(const Parameters* par_host, const Parameters* par_dev, const 
  * built at xbuild with this skin may not hold through the next step. */
 int launch_correct_into(const Parameters* par_host, const Parameters* par_dev, const State& cur, const State& ini,
                         const State& out, const Rates& r, int* health, const float4* xbuild, int* rebuild,
-                        float skin, cudaStream_t s);
+                        float skin, cudaStream_t s, const MaterialTable& mt = MaterialTable());
 
 /* List-driven Adami (boundary targets, material neighbours) and Shepard. */
 int launch_adami_list(const Parameters* par_host, const Parameters* par_dev, const State& st, const NeighborList& nl,
@@ -138,7 +158,7 @@ int launch_shepard_list(const Parameters* par_host, const Parameters* par_dev, c
  * counted in health[HEALTH_NBR_OVERFLOW]. */
 int launch_neighbor_list_range(const Parameters* par_host, const Parameters* par_dev, int first, int n, int layer_lo,
                                float cut, const float4* pos, const Cells& c, const NeighborList& nl, int* health,
-                               cudaStream_t s);
+                               cudaStream_t s, const float4* idep = nullptr, const Frames& fr = Frames());
 /* Fills n ints with v; adds v to one int. */
 int fill_int(int* p, int n, int v, cudaStream_t s);
 int add_int(int* p, int v, cudaStream_t s);

@@ -55,6 +55,8 @@ struct LqSim {
     int* rebuild = nullptr;            /* device flag: rebuild before the next step */
     int* rebuilds = nullptr;           /* device counter of rebuilds */
     int* host_flag = nullptr;          /* pinned mirror for the eager path */
+    lqb::MaterialTable mt;             /* per-object materials (optional) */
+    lqb::Frames fr;                    /* per-object grid rows (optional) */
     std::vector<void*> allocs;
     cudaGraphExec_t step_exec = nullptr;
     cudaGraphExec_t shep_exec = nullptr;
@@ -151,13 +153,15 @@ int enqueue_rebuild(LqSim* S, cudaStream_t s)
     const Parameters* ph = &S->ph;
     const Parameters* pd = S->pd;
     const lqb::Cells cells{S->g.start, nullptr, nullptr};
-    LQ_TRY(lqb::grid_search(ph, pd, S->S.pos, S->g, false, S->health, s));
+    LQ_TRY(lqb::grid_search(ph, pd, S->S.pos, S->g, false, S->health, s, S->S.idep, S->fr));
     LQ_TRY(lqb::gather_state(S->np, S->g.part_idx, S->S, S->T, s));
     k_copy_state<<<blocks(S->np), 256, 0, s>>>(S->np, S->T, S->S, S->xbuild);
     LQ_TRY_CUDA(cudaGetLastError(), "k_copy_state");
     const float cut = 2.0f * ph->h + S->skin;
-    LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, S->npb, S->npm, 0, cut, S->S.pos, cells, S->nlm, S->health, s));
-    LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, S->nlb, S->health, s));
+    LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, S->npb, S->npm, 0, cut, S->S.pos, cells, S->nlm, S->health, s,
+                                           S->S.idep, S->fr));
+    LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, S->nlb, S->health, s,
+                                           S->S.idep, S->fr));
     return LQ_OK;
 }
 
@@ -169,12 +173,13 @@ int enqueue_stages(LqSim* S, cudaStream_t s)
     const lqb::Cells cells{S->g.start, nullptr, nullptr};
     /* predictor stage (reference src/loquat.cu:343-368) */
     LQ_TRY(lqb::launch_adami_list(ph, pd, S->S, S->nlb, s));
-    LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S, S->R, cells, S->nlm, s));
-    LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s));
+    LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S, S->R, cells, S->nlm, s, S->fr));
+    LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt));
     /* corrector stage (reference src/loquat.cu:371-396) */
     LQ_TRY(lqb::launch_adami_list(ph, pd, S->S2, S->nlb, s));
-    LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S2, S->R, cells, S->nlm, s));
-    LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild, S->skin, s));
+    LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S2, S->R, cells, S->nlm, s, S->fr));
+    LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild, S->skin, s,
+                                    S->mt));
     return LQ_OK;
 }
 
@@ -540,6 +545,44 @@ extern "C" int lq_sim_set_skin(void* sim, float skin_over_h)
     return LQ_OK;
 }
 
+extern "C" int lq_sim_set_materials(void* sim, int n, const float* table)
+{
+    if (!sim || n < 0 || (n > 0 && !table)) return lqb::set_error(LQ_ERR_ARG, "lq_sim_set_materials: bad argument");
+    LqSim* S = static_cast<LqSim*>(sim);
+    LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "set materials");
+    float* d = nullptr;
+    if (n > 0) {
+        LQ_TRY(dev_alloc(S, (void**)&d, sizeof(float) * 5 * (size_t)n));
+        LQ_TRY_CUDA(cudaMemcpy(d, table, sizeof(float) * 5 * (size_t)n, cudaMemcpyHostToDevice), "material table");
+    }
+    S->mt.p = d;
+    S->mt.n = n;
+    LQ_TRY(build_graphs(S));
+    return LQ_OK;
+}
+
+extern "C" int lq_sim_set_frames(void* sim, int n, const int* rows)
+{
+    if (!sim || n < 0 || (n > 0 && !rows)) return lqb::set_error(LQ_ERR_ARG, "lq_sim_set_frames: bad argument");
+    LqSim* S = static_cast<LqSim*>(sim);
+    for (int k = 0; k < n; ++k) {
+        if (rows[2 * k] < 0 || rows[2 * k + 1] < 0 || rows[2 * k] + rows[2 * k + 1] > S->ph.cell_num_y)
+            return lqb::set_error(LQ_ERR_ARG, "lq_sim_set_frames: object %d rows [%d, +%d) outside cell_num_y=%d", k,
+                                  rows[2 * k], rows[2 * k + 1], S->ph.cell_num_y);
+    }
+    LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "set frames");
+    int* d = nullptr;
+    if (n > 0) {
+        LQ_TRY(dev_alloc(S, (void**)&d, sizeof(int) * 2 * (size_t)n));
+        LQ_TRY_CUDA(cudaMemcpy(d, rows, sizeof(int) * 2 * (size_t)n, cudaMemcpyHostToDevice), "frame table");
+    }
+    S->fr.rows = d;
+    S->fr.n = n;
+    LQ_TRY(set_flag(S, 1));
+    LQ_TRY(build_graphs(S));
+    return LQ_OK;
+}
+
 extern "C" int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard)
 {
     if (!sim) return lqb::set_error(LQ_ERR_ARG, "lq_sim_launches_per_step: null sim");
@@ -603,7 +646,7 @@ int profiled_step(LqSim* S, PhaseTimer& T)
     LQ_TRY(host_take_flag(S, &rebuild));
     if (rebuild) {
         LQ_TRY(T.mark(s, PH_SEARCH));
-        LQ_TRY(lqb::grid_search(ph, pd, S->S.pos, S->g, false, S->health, s));
+        LQ_TRY(lqb::grid_search(ph, pd, S->S.pos, S->g, false, S->health, s, S->S.idep, S->fr));
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_GATHER));
         LQ_TRY(lqb::gather_state(S->np, S->g.part_idx, S->S, S->T, s));
@@ -613,8 +656,9 @@ int profiled_step(LqSim* S, PhaseTimer& T)
         const float cut = 2.0f * ph->h + S->skin;
         LQ_TRY(T.mark(s, PH_LIST));
         LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, S->npb, S->npm, 0, cut, S->S.pos, cells, S->nlm, S->health,
-                                               s));
-        LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, S->nlb, S->health, s));
+                                               s, S->S.idep, S->fr));
+        LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, S->nlb, S->health, s,
+                                               S->S.idep, S->fr));
         LQ_TRY(T.close(s));
     }
     State* cur[2] = {&S->S, &S->S2};
@@ -623,14 +667,14 @@ int profiled_step(LqSim* S, PhaseTimer& T)
         LQ_TRY(lqb::launch_adami_list(ph, pd, *cur[stage], S->nlb, s));
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_INTERACTION));
-        LQ_TRY(lqb::launch_interaction_list(ph, pd, *cur[stage], S->R, cells, S->nlm, s));
+        LQ_TRY(lqb::launch_interaction_list(ph, pd, *cur[stage], S->R, cells, S->nlm, s, S->fr));
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_INTEGRATE));
         if (stage == 0)
-            LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s));
+            LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt));
         else
             LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild,
-                                            S->skin, s));
+                                            S->skin, s, S->mt));
         LQ_TRY(T.close(s));
     }
     return LQ_OK;

@@ -181,11 +181,14 @@ __device__ __forceinline__ void store_rates(const Parameters* __restrict__ P, co
  * then slot. */
 template <class F>
 __device__ __forceinline__ void walk_stencil(const Parameters* __restrict__ P, const PairConst& K, const State& st,
-                                             const Cells& cells, int i, const float4& xi, F&& f)
+                                             const Cells& cells, int i, const float4& xi, F&& f,
+                                             const Frames& fr = Frames())
 {
     const int nx = __ldg(&P->cell_num_x), ny = __ldg(&P->cell_num_y), nz = __ldg(&P->cell_num_z);
     const int L = __ldg(&P->ncell_one_layer);
-    const int cx = stencil_axis(xi.x, K.ih), cy = stencil_axis(xi.y, K.ih), cz = stencil_axis(xi.z, K.ih);
+    const int cx = stencil_axis(xi.x, K.ih), cz = stencil_axis(xi.z, K.ih);
+    int cy = stencil_axis(xi.y, K.ih);
+    if (fr.rows) cy = frame_stencil_row(fr, __ldg(&st.idep[i].x), cy);
     const int zlo = max(cz - 1, 0), zhi = min(cz + 1, nz - 1);
     if (zlo > zhi) return;
     for (int layer = 0; layer < 2; ++layer) {
@@ -238,7 +241,8 @@ __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __re
                                                           int layer_lo, float cut2, const float4* __restrict__ pos,
                                                           Cells cells, int* __restrict__ list,
                                                           int* __restrict__ count_out, int stride,
-                                                          int* __restrict__ health)
+                                                          int* __restrict__ health, const float4* __restrict__ idep,
+                                                          Frames fr)
 {
     __shared__ int stage[kListWarps][kStage][32];
     const unsigned FULL = 0xffffffffu;
@@ -274,6 +278,7 @@ __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __re
         cx = stencil_axis(xi.x, K.ih);
         cy = stencil_axis(xi.y, K.ih);
         cz = stencil_axis(xi.z, K.ih);
+        if (fr.rows) cy = frame_stencil_row(fr, __ldg(&idep[i].x), cy);
     }
     unsigned todo = __ballot_sync(FULL, active);
     while (todo) {
@@ -318,7 +323,7 @@ __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __re
  * dependent neighbour loads do not wait on the list stream. */
 __global__ void __launch_bounds__(kBlock, LQ_PAIR_MIN_BLOCKS) k_interaction_list(
     const Parameters* __restrict__ P, int np, int npb, State st, Rates rt, Cells cells, const int* __restrict__ list,
-    const int* __restrict__ count, int stride)
+    const int* __restrict__ count, int stride, Frames fr)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = npb + t;
@@ -348,7 +353,7 @@ __global__ void __launch_bounds__(kBlock, LQ_PAIR_MIN_BLOCKS) k_interaction_list
                 if (k + u < n) pair_body(K, st, T, cur[u]);
         }
     } else {
-        walk_stencil(P, K, st, cells, i, T.x, [&](int j) { pair_body(K, st, T, j); });
+        walk_stencil(P, K, st, cells, i, T.x, [&](int j) { pair_body(K, st, T, j); }, fr);
     }
     store_rates(P, K, rt, i, T);
 }
@@ -610,12 +615,13 @@ int launch_neighbor_list(const Parameters* ph, const Parameters* pd, const float
 
 int launch_neighbor_list_range(const Parameters* ph, const Parameters* pd, int first, int n, int layer_lo, float cut,
                                const float4* pos, const Cells& c, const NeighborList& nl, int* health,
-                               cudaStream_t s)
+                               cudaStream_t s, const float4* idep, const Frames& fr)
 {
+    if (fr.rows && !idep) return set_error(LQ_ERR_ARG, "neighbour list: frames need the idep array");
     if (n <= 0) return LQ_OK;
     if (nl.stride < n) return set_error(LQ_ERR_ARG, "neighbour list stride %d < targets %d", nl.stride, n);
     k_neighbor_list<<<blocks_for(n, kBlock), kBlock, 0, s>>>(pd, first, n, layer_lo, cut * cut, pos, c, nl.list,
-                                                            nl.count, nl.stride, health);
+                                                            nl.count, nl.stride, health, idep, fr);
     LQ_TRY_CUDA(cudaGetLastError(), "k_neighbor_list");
     return LQ_OK;
 }
@@ -640,11 +646,11 @@ int launch_shepard_list(const Parameters* ph, const Parameters* pd, const State&
 }
 
 int launch_interaction_list(const Parameters* ph, const Parameters* pd, const State& st, const Rates& r,
-                            const Cells& c, const NeighborList& nl, cudaStream_t s)
+                            const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr)
 {
     if (ph->npm <= 0) return LQ_OK;
     k_interaction_list<<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, r, c, nl.list,
-                                                                     nl.count, nl.stride);
+                                                                     nl.count, nl.stride, fr);
     LQ_TRY_CUDA(cudaGetLastError(), "k_interaction_list");
     return LQ_OK;
 }
