@@ -263,11 +263,8 @@ def bench_ours(args):
     torch.cuda.synchronize()
     clk = clocks.stop() if clocks else None
     s1, _ = sim.clock()
-    ms = start.elapsed_time(end)
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    from loquat_b200 import replicas
+    ms = replicas.max_over_ranks(start.elapsed_time(end), device="cuda")
     shep_steps = sum(1 for s in range(s0, s1) if par.stress_shepard_filter and s % par.stress_shepard_filter == 0
                      and s != 0)
     rebuilds = sim.rebuilds() - rb0
@@ -302,11 +299,7 @@ def bench_ours(args):
         sim.download(out)
         e1.record(ext)
         sim.synchronize()
-        ems = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([ems], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = replicas.max_over_ranks(e0.elapsed_time(e1), device="cuda")
         state_bytes = sum(a.nbytes for a in host)
         e2e = {"value": npm * args.steps * world / (ems / 1e3), "unit": "particle-steps/s",
                "h2d_bytes_per_step": state_bytes / args.steps,
@@ -357,10 +350,22 @@ def bench_ensemble(args):
     import loquat_b200 as lq
     from loquat_b200 import cases
 
+    from loquat_b200 import replicas
+
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
-    comb, parts = cases.ensemble(n=args.scenarios, seed=4 + rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    _, all_parts = cases.ensemble(n=args.scenarios, seed=4)
+    shares = replicas.partition([p.par.npm for p in all_parts], world)
+    parts = [all_parts[k] for k in shares[rank]]
+    comb = cases.combine(parts)
     par = comb.par
+    total_npm = sum(p.par.npm for p in all_parts)
 
     def timed(sim, steps):
         ext = torch.cuda.ExternalStream(sim.stream())
@@ -377,8 +382,11 @@ def bench_ensemble(args):
     sim.set_frames(comb.meta["frames"])
     sim.step(args.warmup)
     rb0 = sim.rebuilds()
+    sim.synchronize()
+    if dist:
+        dist.barrier()
     clocks = ClockSampler(gpu_uuid(torch, local)) if rank == 0 else None
-    ms_batch = timed(sim, args.steps)
+    ms_batch = replicas.max_over_ranks(timed(sim, args.steps), device="cuda")
     clk = clocks.stop() if clocks else None
     rebuilds = sim.rebuilds() - rb0
     health = sim.health()
@@ -389,23 +397,29 @@ def bench_ensemble(args):
         s.step(args.warmup)
         ms_seq += timed(s, args.steps)
         s.close()
-    npm = par.npm
+    ms_seq = replicas.max_over_ranks(ms_seq, device="cuda")
+    npm = total_npm
     v_batch = npm * args.steps / (ms_batch / 1e3)
     v_seq = npm * args.steps / (ms_seq / 1e3)
     if rank == 0:
         print(json.dumps({
             "metric": "particle-steps/s", "value": v_batch, "unit": "particle-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batch / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "ensemble of %d Drucker-Prager column collapses (counts log-uniform 5e3-2e5, "
                                    "H/L 0.5-4, phi 20-40 deg, c 0-5 kPa, dr=2 mm, h=1.2dr)" % args.scenarios,
-                       "np": par.np, "npm": npm, "npb": par.npb, "ncell": par.ncell,
+                       "npm": npm, "rank0_np": par.np, "rank0_ncell": par.ncell,
+                       "parallelism": "scenarios split over %d ranks by particle count" % world,
                        "form": "batched: one simulation, per-scenario frames and materials, CUDA-graph step"},
             "sequential": {"value": v_seq, "ms_per_step": ms_seq / args.steps,
                            "form": "the same scenarios one after another, one plain simulation each"},
             "batched_over_sequential": v_batch / v_seq,
             "neighbour_list_rebuilds": rebuilds, "health": [int(x) for x in health], "clocks": clk,
+            "partition": {"ranks": world, "imbalance": replicas.imbalance([p.par.npm for p in all_parts], shares)},
         }))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 

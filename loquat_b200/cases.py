@@ -297,19 +297,41 @@ def ensemble(n=256, seed=4, dr=0.002, hdr=1.2, count_range=(5.0e3, 2.0e5), aspec
                         meta=dict(config="ensemble", scenario=k, phi=phi, cohesion=coh, aspect=nsz / nsx,
                                   extent=extent, material=(K, G, kphi, kpsi, kc)))
         parts.append(part)
+    return combine(parts), parts
+
+
+def combine(parts):
+    """One particle set holding the given ensemble scenarios (cases from
+    ensemble(), all with the same dr, h and time step): boundary particles
+    of every scenario first, then soil; each scenario keeps its local
+    coordinates and object id.  meta["frames"] gives object k its own block
+    of grid rows with an empty row between blocks, meta["materials"] its
+    constitutive parameters, meta["slices"] each part's (boundary, soil)
+    slot ranges."""
+    if not parts:
+        raise ValueError("no scenarios")
+    p0 = parts[0].par
+    dr, hdr = float(p0.dr), float(p0.hdr)
+    n = max(int(p.idep[0, 0]) for p in parts)
     two_h = 2.0 * hdr * dr
     table = np.zeros((n + 1, 5), np.float32)
     frames = np.zeros((n + 1, 2), np.int32)
     row = 0
-    for k, p in enumerate(parts):
-        table[k + 1] = p.meta["material"]
+    for p in parts:
+        k = int(p.idep[0, 0])
+        table[k] = p.meta["material"]
         rows = int(np.floor(p.meta["extent"][1] / two_h)) + 2
-        frames[k + 1] = (row, rows)
+        frames[k] = (row, rows)
         row += rows + 1
     xsize = max(p.meta["extent"][0] for p in parts)
     zsize = max(p.meta["extent"][2] for p in parts)
-    par = _base_parameters(dr, hdr, rho0, (xsize, row * two_h, 1.5 * zsize), E, nu, cfl, 1,
-                           lambda K_, G_: tuple(table[1]), shepard, alpha, (0.0, 0.0, -9.81))
+    K, G = float(p0.model_par_1), float(p0.model_par_2)
+    E = 9.0 * K * G / (3.0 * K + G)
+    nu = (3.0 * K - 2.0 * G) / (2.0 * (3.0 * K + G))
+    par = _base_parameters(dr, hdr, float(p0.rho0), (xsize, row * two_h, 1.5 * zsize), E, nu, float(p0.cfl), 1,
+                           lambda K_, G_: tuple(table[int(parts[0].idep[0, 0])]), int(p0.stress_shepard_filter),
+                           float(p0.artificial_viscosity_alpha), (float(p0.acc_x), float(p0.acc_y), float(p0.acc_z)))
+    par.cs = p0.cs
     nb = sum(p.par.npb for p in parts)
     ns = sum(p.par.npm for p in parts)
     arrays = [np.zeros((nb + ns, 4), np.float32), np.zeros((nb + ns, 4), np.float32),
@@ -331,7 +353,7 @@ def ensemble(n=256, seed=4, dr=0.002, hdr=1.2, count_range=(5.0e3, 2.0e5), aspec
     initialize_parameters(par)
     par.dt = par.cfl * par.h / par.cs
     assert par.cell_num_y >= row
-    combined = Case("ensemble", par, *arrays,
-                    meta=dict(config="ensemble", n=n, materials=table, frames=frames, slices=slices, np=nb + ns,
-                              npb=nb, npm=ns))
-    return combined, parts
+    assert abs(par.dt - p0.dt) <= 1e-12 * p0.dt, "scenarios must share one time step"
+    return Case("ensemble", par, *arrays,
+                meta=dict(config="ensemble", n=len(parts), materials=table, frames=frames, slices=slices,
+                          np=nb + ns, npb=nb, npm=ns))
