@@ -56,10 +56,14 @@ def parse_args(argv=None):
     ap.add_argument("--dr", type=float, default=None, help="override the particle spacing")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--form", choices=["plain", "mixed"], default="mixed",
+                    help="plain FP32, or mixed precision (FP64 integrator accumulation and stress update, "
+                         "compensated interaction sums)")
     ap.add_argument("--profile-steps", type=int, default=10)
     ap.add_argument("--start-step", type=int, default=2500,
                     help="untimed steps run first so the timed window sits mid-run of the 5000-step collapse "
                          "(the particles move and the neighbour lists are rebuilt at a representative rate)")
+    ap.add_argument("--no-compare", action="store_true", help="skip timing the other precision form")
     ap.add_argument("--eager", action="store_true",
                     help="launch kernels one by one instead of replaying the step graph (for ncu, which cannot "
                          "profile kernels inside graphs with conditional nodes)")
@@ -241,7 +245,7 @@ def bench_ours(args):
     case = make_case(args, rank)
     par = case.par
     npm, np_ = par.npm, par.np
-    sim = lq.Simulation(par, *case.arrays(), graph=not args.eager)
+    sim = lq.Simulation(par, *case.arrays(), graph=not args.eager, mixed=args.form == "mixed")
     ext = torch.cuda.ExternalStream(sim.stream())
     plain, with_shep = sim.launches_per_step()
 
@@ -305,6 +309,28 @@ def bench_ours(args):
                "h2d_bytes_per_step": state_bytes / args.steps,
                "d2h_bytes_per_step": (state_bytes + 16 * args.steps) / args.steps}
 
+    # the other precision form on the same workload and window, for comparison
+    forms = {args.form: {"value": value, "ms_per_step": ms / args.steps}}
+    if not args.no_compare:
+        other = "plain" if args.form == "mixed" else "mixed"
+        sim.close()
+        osim = lq.Simulation(par, *case.arrays(), graph=not args.eager, mixed=other == "mixed")
+        if args.start_step > 0:
+            osim.step(args.start_step)
+        osim.step(args.warmup)
+        osim.synchronize()
+        if dist:
+            dist.barrier()
+        oext = torch.cuda.ExternalStream(osim.stream())
+        o0, o1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        o0.record(oext)
+        osim.step(args.steps)
+        o1.record(oext)
+        osim.synchronize()
+        oms = replicas.max_over_ranks(o0.elapsed_time(o1), device="cuda")
+        forms[other] = {"value": npm * args.steps * world / (oms / 1e3), "ms_per_step": oms / args.steps}
+        sim = osim
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu, _ = run_cpu_baseline(args)
@@ -313,9 +339,11 @@ def bench_ours(args):
         line = {
             "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.form == "plain" else "f32+f64", "data": "synthetic",
             "config": {"workload": workload, "np": np_, "npm": npm, "npb": par.npb, "ncell": par.ncell,
-                       "form": "plain FP32, %s, Verlet lists (skin 0.05h)" % ("eager launches" if args.eager else "CUDA-graph step"),
+                       "form": "%s, %s, Verlet lists (skin 0.05h)" % (
+                           "plain FP32" if args.form == "plain" else "mixed precision (FP64 integrator)",
+                           "eager launches" if args.eager else "CUDA-graph step"),
                        "timed_window": "steps %d..%d of the run" % (s0, s1),
                        "l2": "state larger than L2 (3 x %.0f MB state buffers)" % (np_ * 96 / 1e6),
                        "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
@@ -325,6 +353,7 @@ def bench_ours(args):
                          "bytes_per_launch": BYTES_INTERACTION_PER_PARTICLE * npm,
                          "ms_per_launch": t_int * 1e3},
             "phases_ms_per_step": {k: v[0] / max(args.profile_steps, 1) for k, v in prof.items()},
+            "forms": forms,
             "gpu_launches": launches,
             "neighbour_list_rebuilds": rebuilds,
             "health": [int(x) for x in health],

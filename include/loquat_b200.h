@@ -124,6 +124,10 @@ int lq_corrector(const void* par_host, const void* par_device,
 /* ---- whole-step driver (the hot loop of LoquatSph::RunSimulation,
  *      reference src/loquat.cu:322-409) ------------------------------------ */
 #define LQ_SIM_GRAPH   1   /* replay each step as one captured CUDA graph      */
+#define LQ_SIM_MIXED   2   /* mixed precision: FP64 position, velocity and
+                              density accumulation and FP64 stress updates in
+                              the integrator, compensated sums in the
+                              interaction; the neighbour kernels read FP32 */
 
 /* Creates a simulation from host arrays (np = par->np particles, boundary
  * first).  par must have been through lq_initialize_parameters.  The state
@@ -196,6 +200,11 @@ int lq_io_load_particles(const char* dat_path, int np,
 int lq_io_save_particles(const char* dat_path, int np,
                          const float* pospres, const float* velrhop, const float* idep,
                          const float* str, const float* stn);
+/* ParaView output (reference src/loquat_io.cu:372-548): one ASCII .vtu
+ * file per object id, <dir>/<id>_<output_number>.vtu. */
+int lq_io_save_vtu(const char* dir, int output_number, int np,
+                   const float* pospres, const float* velrhop, const float* idep,
+                   const float* str, const float* stn);
 
 #ifdef __cplusplus
 }

@@ -24,6 +24,7 @@ _lib = None
 
 LQ_OK, LQ_ERR_ARG, LQ_ERR_CUDA, LQ_ERR_ALLOC, LQ_ERR_IO, LQ_ERR_STATE, LQ_ERR_NOTFOUND = range(7)
 LQ_SIM_GRAPH = 1
+LQ_SIM_MIXED = 2
 
 
 class LoquatError(RuntimeError):
@@ -76,6 +77,7 @@ _SIGNATURES = {
     "lq_io_save_parameters": (_I, [ctypes.c_char_p, _VP]),
     "lq_io_load_particles": (_I, [ctypes.c_char_p, _I] + [_VP] * 5),
     "lq_io_save_particles": (_I, [ctypes.c_char_p, _I] + [_VP] * 5),
+    "lq_io_save_vtu": (_I, [ctypes.c_char_p, _I, _I] + [_VP] * 5),
 }
 
 
@@ -217,11 +219,12 @@ class Grid:
 class Simulation:
     """Whole-step driver (lq_sim_*): the hot loop of reference src/loquat.cu:322-409."""
 
-    def __init__(self, par: Parameters, pospres, velrhop, idep, str_, stn, graph: bool = True):
+    def __init__(self, par: Parameters, pospres, velrhop, idep, str_, stn, graph: bool = True, mixed: bool = False):
         arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (pospres, velrhop, idep, str_, stn)]
         h = _VP()
-        check(lib().lq_sim_create(ctypes.byref(par), *[a.ctypes.data for a in arrs],
-                                  LQ_SIM_GRAPH if graph else 0, ctypes.byref(h)), "lq_sim_create")
+        flags = (LQ_SIM_GRAPH if graph else 0) | (LQ_SIM_MIXED if mixed else 0)
+        check(lib().lq_sim_create(ctypes.byref(par), *[a.ctypes.data for a in arrs], flags, ctypes.byref(h)),
+              "lq_sim_create")
         self.handle = h
         self.np = par.np
         self.par = par.copy()
@@ -335,3 +338,9 @@ def save_particles(dat_path, pospres, velrhop, idep, str_, stn) -> None:
     arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (pospres, velrhop, idep, str_, stn)]
     check(lib().lq_io_save_particles(os.fsencode(str(dat_path)), arrs[0].shape[0], *[a.ctypes.data for a in arrs]),
           "lq_io_save_particles")
+
+
+def save_vtu(directory, output_number: int, pospres, velrhop, idep, str_, stn) -> None:
+    arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (pospres, velrhop, idep, str_, stn)]
+    check(lib().lq_io_save_vtu(os.fsencode(str(directory)), output_number, arrs[0].shape[0],
+                               *[a.ctypes.data for a in arrs]), "lq_io_save_vtu")

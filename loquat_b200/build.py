@@ -22,6 +22,8 @@ CSRC = PKG / "csrc"
 INCLUDE = ROOT / "include"
 BUILD = PKG / "_build"
 LIB = PKG / "liblqb200.so"
+APP_SRC = PKG / "app" / "loquat_main.cpp"
+APP = PKG / "bin" / "loquat"
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -82,10 +84,26 @@ def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = True, 
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    if out is None:
+        build_app(force=force)
     if not quiet or ptxas_verbose:
         for name, err in reports:
             print(f"== {name}\n{err}", file=sys.stderr)
     return LIB
+
+
+def build_app(force: bool = False) -> Path:
+    """The `loquat` command-line driver, linked against the library
+    (found beside it through an rpath of $ORIGIN/..)."""
+    APP.parent.mkdir(exist_ok=True)
+    if not force and APP.exists() and APP.stat().st_mtime >= max(APP_SRC.stat().st_mtime, LIB.stat().st_mtime):
+        return APP
+    cmd = [NVCC, *ARCH, "-O2", "-std=c++17", f"-I{INCLUDE}", str(APP_SRC), f"-L{PKG}", "-llqb200",
+           "-Xlinker", "-rpath,$ORIGIN/..", "-o", str(APP)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"driver build failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    return APP
 
 
 def main(argv=None):

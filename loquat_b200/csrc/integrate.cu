@@ -28,6 +28,7 @@ inline int blocks_for(long long n, int b) { return (int)((n + b - 1) / b); }
 /* Half step of the material slots (reference src/predictor_corrector.cu:169-218):
  * v += dt/2 a; rho += dt/2 drho; x += dt/2 v_new; eps += dt/2 deps;
  * stress and plastic strain from the model at dt/2. */
+template <bool kMixed>
 __global__ void __launch_bounds__(kBlock) k_predict(const Parameters* __restrict__ P, int np, int npb, State in,
                                                     State out, State snap, bool do_snap, Rates rt, MaterialTable mt)
 {
@@ -52,6 +53,10 @@ __global__ void __launch_bounds__(kBlock) k_predict(const Parameters* __restrict
             out.idep[i] = id;
             store_t2(out.str, i, s0);
             store_t2(out.stn, i, e0);
+            if (kMixed) {
+                out.xd[i] = in.xd[i];
+                out.vd[i] = in.vd[i];
+            }
         }
         return;
     }
@@ -61,6 +66,32 @@ __global__ void __launch_bounds__(kBlock) k_predict(const Parameters* __restrict
     const float4 w = __ldg(rt.spin + i);
     const tensor2d de = load_t2(rt.acestn, i);
 
+    if (kMixed) {
+        /* FP64 accumulation of velocity, density and position; FP64 stress update */
+        const double hdt = 0.5 * (double)dt;
+        double4 vd = in.vd[i], xd = in.xd[i];
+        vd.x += hdt * a.x; vd.y += hdt * a.y; vd.z += hdt * a.z; vd.w += hdt * a.w;
+        xd.x += hdt * vd.x; xd.y += hdt * vd.y; xd.z += hdt * vd.z;
+        T6d e = widen6(e0), dd = widen6(de);
+        e.xx += dd.xx * hdt; e.yy += dd.yy * hdt; e.zz += dd.zz * hdt;
+        e.xy += dd.xy * hdt; e.xz += dd.xz * hdt; e.yz += dd.yz * hdt;
+        double p = x0.w, ep = id.y;
+        T6d sd = widen6(s0);
+        if (M.model == 1) {
+            dp_update_d(M, hdt, w, dd, p, ep, sd);
+        } else {
+            hypo_update_d(M, hdt, dd, w, sd);
+            ep = sqrt(2.0 / 3.0 * contract6(e, e));
+        }
+        out.xd[i] = xd;
+        out.vd[i] = vd;
+        out.pos[i] = make_float4((float)xd.x, (float)xd.y, (float)xd.z, (float)p);
+        out.vel[i] = make_float4((float)vd.x, (float)vd.y, (float)vd.z, (float)vd.w);
+        out.idep[i] = make_float4(id.x, (float)ep, id.z, id.w);
+        store_t2(out.str, i, narrow6(sd));
+        store_t2(out.stn, i, narrow6(e));
+        return;
+    }
     float4 v = v0;
     v.x += 0.5f * dt * a.x;
     v.y += 0.5f * dt * a.y;
@@ -105,6 +136,7 @@ struct VerletCheck {
     float half_skin;
 };
 
+template <bool kMixed>
 __global__ void __launch_bounds__(kBlock) k_correct(const Parameters* __restrict__ P, int np, int npb, State cur,
                                                     State ini, const int* __restrict__ ini_idx, State out, Rates rt,
                                                     int* __restrict__ health, VerletCheck verlet, int first,
@@ -118,6 +150,10 @@ __global__ void __launch_bounds__(kBlock) k_correct(const Parameters* __restrict
         out.idep[i] = cur.idep[i];
         store_t2(out.str, i, load_t2_rw(cur.str, i));
         store_t2(out.stn, i, load_t2_rw(cur.stn, i));
+        if (kMixed) {
+            out.xd[i] = cur.xd[i];
+            out.vd[i] = cur.vd[i];
+        }
         return;
     }
     const int k = ini_idx ? __ldg(ini_idx + i) : i;
@@ -134,27 +170,56 @@ __global__ void __launch_bounds__(kBlock) k_correct(const Parameters* __restrict
     const float4 id = cur.idep[i];
     const Material M = particle_material(load_material(P), mt, id.x);
 
-    float4 v;
-    v.x = v0.x + dt * a.x;
-    v.y = v0.y + dt * a.y;
-    v.z = v0.z + dt * a.z;
-    v.w = v0.w + dt * a.w;
-    float4 x;
-    x.x = 0.5f * (v.x + v0.x) * dt + x0.x;
-    x.y = 0.5f * (v.y + v0.y) * dt + x0.y;
-    x.z = 0.5f * (v.z + v0.z) * dt + x0.z;
-    const tensor2d e = e0 + de * dt;
-
-    float p = xc.w;
-    float ep = ep0;
-    tensor2d s = s0;
-    if (M.model == 1) {
-        dp_update(M, dt, w, de, p, ep, s);
+    float4 v, x;
+    tensor2d s, e;
+    float ep;
+    if (kMixed) {
+        const double ddt = dt;
+        const double4 v0d = ini.vd[k], x0d = ini.xd[k];
+        double4 vd, xd;
+        vd.x = v0d.x + ddt * a.x; vd.y = v0d.y + ddt * a.y; vd.z = v0d.z + ddt * a.z; vd.w = v0d.w + ddt * a.w;
+        xd.x = 0.5 * (vd.x + v0d.x) * ddt + x0d.x;
+        xd.y = 0.5 * (vd.y + v0d.y) * ddt + x0d.y;
+        xd.z = 0.5 * (vd.z + v0d.z) * ddt + x0d.z;
+        xd.w = 0.0;
+        T6d ed = widen6(e0), dd = widen6(de);
+        ed.xx += dd.xx * ddt; ed.yy += dd.yy * ddt; ed.zz += dd.zz * ddt;
+        ed.xy += dd.xy * ddt; ed.xz += dd.xz * ddt; ed.yz += dd.yz * ddt;
+        double pd = xc.w, epd = ep0;
+        T6d sd = widen6(s0);
+        if (M.model == 1) {
+            dp_update_d(M, ddt, w, dd, pd, epd, sd);
+        } else {
+            hypo_update_d(M, ddt, dd, w, sd);
+            epd = sqrt(2.0 / 3.0 * contract6(ed, ed));
+        }
+        out.xd[i] = xd;
+        out.vd[i] = vd;
+        v = make_float4((float)vd.x, (float)vd.y, (float)vd.z, (float)vd.w);
+        x = make_float4((float)xd.x, (float)xd.y, (float)xd.z, (float)pd);
+        s = narrow6(sd);
+        e = narrow6(ed);
+        ep = (float)epd;
     } else {
-        hypo_update(M, dt, de, w, s);
-        ep = sqrtf(2.0f / 3.0f * J2(e));
+        v.x = v0.x + dt * a.x;
+        v.y = v0.y + dt * a.y;
+        v.z = v0.z + dt * a.z;
+        v.w = v0.w + dt * a.w;
+        x.x = 0.5f * (v.x + v0.x) * dt + x0.x;
+        x.y = 0.5f * (v.y + v0.y) * dt + x0.y;
+        x.z = 0.5f * (v.z + v0.z) * dt + x0.z;
+        e = e0 + de * dt;
+        float p = xc.w;
+        ep = ep0;
+        s = s0;
+        if (M.model == 1) {
+            dp_update(M, dt, w, de, p, ep, s);
+        } else {
+            hypo_update(M, dt, de, w, s);
+            ep = sqrtf(2.0f / 3.0f * J2(e));
+        }
+        x.w = p;
     }
-    x.w = p;
     out.pos[i] = x;
     out.vel[i] = v;
     out.idep[i] = make_float4(id.x, ep, id.z, id.w);
@@ -187,7 +252,11 @@ int launch_predict(const Parameters* ph, const Parameters* pd, const State& in, 
     if (ph->np <= 0) return LQ_OK;
     const bool do_snap = snap && snap->pos;
     State sn = do_snap ? *snap : State{nullptr, nullptr, nullptr, nullptr, nullptr};
-    k_predict<<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt);
+    if (in.xd && out.xd)
+        k_predict<true><<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt);
+    else
+        k_predict<false><<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r,
+                                                                       mt);
     LQ_TRY_CUDA(cudaGetLastError(), "k_predict");
     return LQ_OK;
 }
@@ -196,7 +265,7 @@ int launch_correct(const Parameters* ph, const Parameters* pd, const State& cur,
                    const int* ini_idx, const Rates& r, int* health, cudaStream_t s)
 {
     if (ph->npm <= 0) return LQ_OK;
-    k_correct<<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, ini_idx, cur, r, health,
+    k_correct<false><<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, ini_idx, cur, r, health,
                                                              VerletCheck{nullptr, nullptr, 0.0f}, ph->npb,
                                                              MaterialTable());
     LQ_TRY_CUDA(cudaGetLastError(), "k_correct");
@@ -208,8 +277,13 @@ int launch_correct_into(const Parameters* ph, const Parameters* pd, const State&
                         float skin, cudaStream_t s, const MaterialTable& mt)
 {
     if (ph->np <= 0) return LQ_OK;
-    k_correct<<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health,
-                                                            VerletCheck{xbuild, rebuild, 0.5f * skin}, 0, mt);
+    const VerletCheck vc{xbuild, rebuild, 0.5f * skin};
+    if (cur.xd && ini.xd && out.xd)
+        k_correct<true><<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r,
+                                                                      health, vc, 0, mt);
+    else
+        k_correct<false><<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r,
+                                                                       health, vc, 0, mt);
     LQ_TRY_CUDA(cudaGetLastError(), "k_correct");
     return LQ_OK;
 }

@@ -17,6 +17,7 @@
  * representation that reads back to the same float instead of 6 digits.
  * Errors return a status with a message; nothing exits the process.
  */
+#include <algorithm>
 #include <cerrno>
 #include <charconv>
 #include <cstdio>
@@ -347,4 +348,70 @@ extern "C" int lq_io_save_particles(const char* dat_path, int np, const float* p
     const bool ok = ferror(fp) == 0;
     fclose(fp);
     return ok ? LQ_OK : set_error(LQ_ERR_IO, "write error on %s", dat_path);
+}
+
+/* ParaView output (reference src/loquat_io.cu:372-548): one ASCII .vtu file
+ * per object id, "<dir>/<id>_<n>.vtu", objects in descending id order, each
+ * a piece of vertex cells with Pressure, Velocity, Density, PlasticStrain,
+ * Stress, Strain point data. */
+extern "C" int lq_io_save_vtu(const char* dir, int output_number, int np, const float* pos, const float* vel,
+                              const float* idep, const float* str, const float* stn)
+{
+    if (!dir || np < 0 || (np > 0 && (!pos || !vel || !idep || !str || !stn)))
+        return set_error(LQ_ERR_ARG, "lq_io_save_vtu: bad argument");
+    std::vector<int> order(np);
+    for (int i = 0; i < np; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return (int)idep[4 * (size_t)a] > (int)idep[4 * (size_t)b];
+    });
+    size_t k = 0;
+    char buf[64];
+    auto put = [&](FILE* fp, float v) {
+        auto r = std::to_chars(buf, buf + sizeof(buf), v);
+        *r.ptr++ = ' ';
+        fwrite(buf, 1, (size_t)(r.ptr - buf), fp);
+    };
+    while (k < order.size()) {
+        const int id = (int)idep[4 * (size_t)order[k]];
+        size_t e = k;
+        while (e < order.size() && (int)idep[4 * (size_t)order[e]] == id) ++e;
+        const size_t n = e - k;
+        std::string name = std::string(dir) + "/" + std::to_string(id) + "_" + std::to_string(output_number) + ".vtu";
+        FILE* fp = fopen(name.c_str(), "w");
+        if (!fp) return set_error(LQ_ERR_IO, "cannot write file %s", name.c_str());
+        fprintf(fp, "<?xml version=\"1.0\"?>\n<VTKFile type=\"UnstructuredGrid\" version=\"0.1\" "
+                    "byte_order=\"LittleEndian\">\n  <UnstructuredGrid GhostLevel=\"0\">\n"
+                    "    <Piece NumberOfPoints=\"%zu\" NumberOfCells=\"%zu\" Name=\"%d\">\n      <PointData>\n",
+                n, n, id);
+        auto arr = [&](const char* label, int comps, auto getter) {
+            if (comps > 1)
+                fprintf(fp, "        <DataArray type=\"Float32\" Name=\"%s\" NumberOfComponents=\"%d\">\n", label,
+                        comps);
+            else
+                fprintf(fp, "        <DataArray type=\"Float32\" Name=\"%s\">\n", label);
+            for (size_t q = k; q < e; ++q) getter((size_t)order[q], fp);
+            fprintf(fp, "</DataArray>\n");
+        };
+        arr("Pressure", 1, [&](size_t i, FILE* f) { put(f, pos[4 * i + 3]); });
+        arr("Velocity", 3, [&](size_t i, FILE* f) { for (int c = 0; c < 3; ++c) put(f, vel[4 * i + c]); });
+        arr("Density", 1, [&](size_t i, FILE* f) { put(f, vel[4 * i + 3]); });
+        arr("PlasticStrain", 1, [&](size_t i, FILE* f) { put(f, idep[4 * i + 1]); });
+        arr("Stress", 6, [&](size_t i, FILE* f) { for (int c = 0; c < 6; ++c) put(f, str[6 * i + c]); });
+        arr("Strain", 6, [&](size_t i, FILE* f) { for (int c = 0; c < 6; ++c) put(f, stn[6 * i + c]); });
+        fprintf(fp, "      </PointData>\n      <CellData>\n      </CellData>\n      <Points>\n");
+        arr("Points", 3, [&](size_t i, FILE* f) { for (int c = 0; c < 3; ++c) put(f, pos[4 * i + c]); });
+        fprintf(fp, "      </Points>\n      <Cells>\n");
+        fprintf(fp, "        <DataArray type=\"Int64\" Name=\"connectivity\" format=\"ascii\">\n");
+        for (size_t q = 0; q < n; ++q) fprintf(fp, "%zu ", q);
+        fprintf(fp, "</DataArray>\n        <DataArray type=\"Int64\" Name=\"offsets\" format=\"ascii\">\n");
+        for (size_t q = 0; q < n; ++q) fprintf(fp, "%zu ", q + 1);
+        fprintf(fp, "</DataArray>\n        <DataArray type=\"Int64\" Name=\"types\" format=\"ascii\">\n");
+        for (size_t q = 0; q < n; ++q) fputs("1 ", fp);
+        fprintf(fp, "</DataArray>\n      </Cells>\n    </Piece>\n  </UnstructuredGrid>\n</VTKFile>\n");
+        const bool ok = ferror(fp) == 0;
+        fclose(fp);
+        if (!ok) return set_error(LQ_ERR_IO, "write error on %s", name.c_str());
+        k = e;
+    }
+    return LQ_OK;
 }

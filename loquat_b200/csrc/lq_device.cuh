@@ -228,4 +228,104 @@ __device__ __forceinline__ void hypo_update(const Material& M, float dtp, const 
     }
 }
 
+/* ---------------------------------------------- FP64 stress updates */
+/* The same updates in double precision, for the mixed-precision form: the
+ * return map's plastic multiplier and the hypoplastic rate are formed and
+ * applied in FP64, and only the stored result is rounded to float. */
+struct T6d {
+    double xx, yy, zz, xy, xz, yz;
+};
+
+__device__ __forceinline__ T6d widen6(const tensor2d& t) { return T6d{t.xx, t.yy, t.zz, t.xy, t.xz, t.yz}; }
+
+__device__ __forceinline__ tensor2d narrow6(const T6d& t)
+{
+    return make_tensor2d((float)t.xx, (float)t.yy, (float)t.zz, (float)t.xy, (float)t.xz, (float)t.yz);
+}
+
+__device__ __forceinline__ double contract6(const T6d& a, const T6d& b)
+{
+    return a.xx * b.xx + a.yy * b.yy + a.zz * b.zz + 2.0 * (a.xy * b.xy + a.xz * b.xz + a.yz * b.yz);
+}
+
+__device__ __forceinline__ T6d jaumann_d(const float4& w4, const T6d& s)
+{
+    const double wx = w4.x, wy = w4.y, wz = w4.z;
+    T6d r;
+    r.xx = -2.0 * (wx * s.xy + wy * s.xz);
+    r.yy = 2.0 * (wx * s.xy - wz * s.yz);
+    r.zz = 2.0 * (wy * s.xz + wz * s.yz);
+    r.xy = wx * (s.xx - s.yy) - wz * s.xz - wy * s.yz;
+    r.xz = wy * (s.xx - s.zz) + wz * s.xy - wx * s.yz;
+    r.yz = wz * (s.yy - s.zz) + wx * s.xz + wy * s.xy;
+    return r;
+}
+
+__device__ __forceinline__ void dp_update_d(const Material& M, double dtp, const float4& w, const T6d& d, double& p,
+                                            double& ep, T6d& s)
+{
+    const double K = M.p1, G = M.p2, kphi = M.p3, kpsi = M.p4, kc = M.p5;
+    T6d r = jaumann_d(w, s);
+    const double ace = (K - 2.0 / 3.0 * G) * (d.xx + d.yy + d.zz);
+    r.xx += 2.0 * G * d.xx + ace;
+    r.yy += 2.0 * G * d.yy + ace;
+    r.zz += 2.0 * G * d.zz + ace;
+    r.xy += 2.0 * G * d.xy;
+    r.xz += 2.0 * G * d.xz;
+    r.yz += 2.0 * G * d.yz;
+    s.xx += r.xx * dtp; s.yy += r.yy * dtp; s.zz += r.zz * dtp;
+    s.xy += r.xy * dtp; s.xz += r.xz * dtp; s.yz += r.yz * dtp;
+    double sm = (s.xx + s.yy + s.zz) / 3.0;
+    s.xx -= sm; s.yy -= sm; s.zz -= sm;
+    const double tenf = (M.p3 == 0.0f) ? 0.0 : kc / kphi;
+    const double over = sm - tenf;
+    if (over >= 0.0) {
+        ep += over / K * (1.0 / 3.0) * sqrt(2.0);
+        sm = tenf;
+    }
+    const double tau = sqrt(0.5 * contract6(s, s));
+    const double f = tau + kphi * sm - kc;
+    if (f > 0.0) {
+        const double dl = f / (G + K * kphi * kpsi);
+        sm -= K * kpsi * dl;
+        const double ratio = tau < (double)1e-10f ? 1.0 : (kc - kphi * sm) / tau;
+        s.xx *= ratio; s.yy *= ratio; s.zz *= ratio;
+        s.xy *= ratio; s.xz *= ratio; s.yz *= ratio;
+        ep += dl * sqrt(1.0 / 3.0 + 2.0 / 9.0 * kpsi * kpsi);
+    }
+    s.xx += sm; s.yy += sm; s.zz += sm;
+    p = -sm;
+}
+
+__device__ __forceinline__ void hypo_update_d(const Material& M, double dtp, const T6d& d, const float4& w, T6d& s)
+{
+    const double c1 = M.p1, c2 = M.p2, c3 = M.p3, c4 = M.p4, coh = M.p5;
+    const T6d jau = jaumann_d(w, s);
+    T6d T = s;
+    if (M.p5 > 0.0f) {
+        T.xx -= coh; T.yy -= coh; T.zz -= coh;
+    }
+    double t1 = T.xx + T.yy + T.zz;
+    if (fabs(t1) < 4.0) {
+        t1 = -4.0;
+        T.xx = -1.0; T.yy = -1.0; T.zz = -2.0;
+        T.xy = 0.0; T.yz = 0.0;   /* T.xz kept, as the reference does */
+    }
+    const double d1 = d.xx + d.yy + d.zz;
+    const double td = contract6(T, d);
+    const double nd = sqrt(contract6(d, d));
+    const double a = c2 * d1 + c3 * td / t1, b = c4 * nd, c = c1 * t1;
+    const double third = t1 / 3.0;
+    s.xx += (jau.xx + d.xx * c + T.xx * a + (2.0 * T.xx - third) * b) * dtp;
+    s.yy += (jau.yy + d.yy * c + T.yy * a + (2.0 * T.yy - third) * b) * dtp;
+    s.zz += (jau.zz + d.zz * c + T.zz * a + (2.0 * T.zz - third) * b) * dtp;
+    s.xy += (jau.xy + d.xy * c + T.xy * a + 2.0 * T.xy * b) * dtp;
+    s.xz += (jau.xz + d.xz * c + T.xz * a + 2.0 * T.xz * b) * dtp;
+    s.yz += (jau.yz + d.yz * c + T.yz * a + 2.0 * T.yz * b) * dtp;
+    const double pres = (s.xx + s.yy + s.zz) / 3.0;
+    if (pres > coh) {
+        s.xx -= pres - coh; s.yy -= pres - coh; s.zz -= pres - coh;
+    }
+}
+
 }  // namespace lqb

@@ -37,6 +37,11 @@ struct State {
     float4* idep;    /* object id, plastic strain, -, -   */
     tensor2d* str;   /* Cauchy stress, tension positive   */
     tensor2d* stn;   /* total strain                      */
+    /* mixed-precision form only: FP64 copies that the integrator
+     * accumulates in (x, y, z, -) and (vx, vy, vz, density); the float
+     * fields above are their rounded copies read by the neighbour kernels */
+    double4* xd = nullptr;
+    double4* vd = nullptr;
 };
 
 /* Per-stage rates written by the interaction pass (reference src/loquat.h:74-77). */
@@ -124,7 +129,8 @@ int launch_interaction(const Parameters* par_host, const Parameters* par_dev, co
 int launch_neighbor_list(const Parameters* par_host, const Parameters* par_dev, const float4* pos, const Cells& c,
                          const NeighborList& nl, cudaStream_t s);
 int launch_interaction_list(const Parameters* par_host, const Parameters* par_dev, const State& st, const Rates& r,
-                            const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr = Frames());
+                            const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr = Frames(),
+                            bool compensated = false);
 int launch_adami(const Parameters* par_host, const Parameters* par_dev, const State& st, const Cells& c,
                  cudaStream_t s);
 /* Shepard filter of material stress into out_str[npb, np).  When `full` is

@@ -80,6 +80,10 @@ int alloc_state(LqSim* S, State& st)
     LQ_TRY(dev_alloc(S, (void**)&st.idep, n * sizeof(float4)));
     LQ_TRY(dev_alloc(S, (void**)&st.str, n * sizeof(tensor2d)));
     LQ_TRY(dev_alloc(S, (void**)&st.stn, n * sizeof(tensor2d)));
+    if (S->flags & LQ_SIM_MIXED) {
+        LQ_TRY(dev_alloc(S, (void**)&st.xd, n * sizeof(double4)));
+        LQ_TRY(dev_alloc(S, (void**)&st.vd, n * sizeof(double4)));
+    }
     return LQ_OK;
 }
 
@@ -119,6 +123,20 @@ __global__ void k_copy_state(int n, State in, State out, float4* __restrict__ xb
     b[0] = a[0];
     b[1] = a[1];
     b[2] = a[2];
+    if (in.xd) {
+        out.xd[i] = in.xd[i];
+        out.vd[i] = in.vd[i];
+    }
+}
+
+/* Widens the float state into the FP64 copies (mixed form, after upload). */
+__global__ void k_widen(int n, State st)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 x = st.pos[i], v = st.vel[i];
+    st.xd[i] = make_double4(x.x, x.y, x.z, 0.0);
+    st.vd[i] = make_double4(v.x, v.y, v.z, v.w);
 }
 
 __global__ void k_copy_t2(int first, int n, const tensor2d* __restrict__ in, tensor2d* __restrict__ out)
@@ -173,11 +191,11 @@ int enqueue_stages(LqSim* S, cudaStream_t s)
     const lqb::Cells cells{S->g.start, nullptr, nullptr};
     /* predictor stage (reference src/loquat.cu:343-368) */
     LQ_TRY(lqb::launch_adami_list(ph, pd, S->S, S->nlb, s));
-    LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S, S->R, cells, S->nlm, s, S->fr));
+    LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S, S->R, cells, S->nlm, s, S->fr, S->flags & LQ_SIM_MIXED));
     LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt));
     /* corrector stage (reference src/loquat.cu:371-396) */
     LQ_TRY(lqb::launch_adami_list(ph, pd, S->S2, S->nlb, s));
-    LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S2, S->R, cells, S->nlm, s, S->fr));
+    LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S2, S->R, cells, S->nlm, s, S->fr, S->flags & LQ_SIM_MIXED));
     LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild, S->skin, s,
                                     S->mt));
     return LQ_OK;
@@ -310,6 +328,14 @@ int upload(LqSim* S, const float* pos, const float* vel, const float* idep, cons
 
 int set_flag(LqSim* S, int v) { return lqb::fill_int(S->rebuild, 1, v, S->stream); }
 
+int widen(LqSim* S)
+{
+    if (!S->S.xd) return LQ_OK;
+    k_widen<<<blocks(S->np), 256, 0, S->stream>>>(S->np, S->S);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_widen");
+    return LQ_OK;
+}
+
 int build_graphs(LqSim* S)
 {
     if (S->step_exec) cudaGraphExecDestroy(S->step_exec);
@@ -389,6 +415,7 @@ int create(LqSim* S, const Parameters* par, const float* pos, const float* vel, 
     LQ_TRY_CUDA(cudaMemcpyAsync(S->pd, &S->ph, sizeof(Parameters), cudaMemcpyHostToDevice, S->stream),
                 "upload Parameters");
     LQ_TRY(upload(S, pos, vel, idep, str, stn, S->S));
+    LQ_TRY(widen(S));
     /* the first step searches and sorts (reference src/loquat.cu:297-298) */
     LQ_TRY(set_flag(S, 1));
     LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "sim create");
@@ -471,6 +498,7 @@ extern "C" int lq_sim_upload(void* sim, const float* pospres, const float* velrh
         return lqb::set_error(LQ_ERR_ARG, "lq_sim_upload: null argument");
     LqSim* S = static_cast<LqSim*>(sim);
     LQ_TRY(upload(S, pospres, velrhop, idep, str, stn, S->S));
+    LQ_TRY(widen(S));
     return set_flag(S, 1); /* new positions: search and rebuild the lists first */
 }
 
@@ -667,7 +695,8 @@ int profiled_step(LqSim* S, PhaseTimer& T)
         LQ_TRY(lqb::launch_adami_list(ph, pd, *cur[stage], S->nlb, s));
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_INTERACTION));
-        LQ_TRY(lqb::launch_interaction_list(ph, pd, *cur[stage], S->R, cells, S->nlm, s, S->fr));
+        LQ_TRY(lqb::launch_interaction_list(ph, pd, *cur[stage], S->R, cells, S->nlm, s, S->fr,
+                                            S->flags & LQ_SIM_MIXED));
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_INTEGRATE));
         if (stage == 0)

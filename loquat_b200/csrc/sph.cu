@@ -80,8 +80,19 @@ struct Target {
     float Sxx, Syy, Szz, Sxy, Sxz, Syz; /* sigma_i / rho_i^2 */
     float Rx, Ry, Rz;                   /* artificial stress of i */
     float drho, ax, ay, az;
+    float cdrho, cax, cay, caz;         /* compensation terms (mixed form) */
     float l00, l01, l02, l10, l11, l12, l20, l21, l22;
 };
+
+/* Compensated (Kahan) accumulation: sum + y with the lost low-order part
+ * carried in c. */
+__device__ __forceinline__ void kahan_add(float& sum, float& c, float y)
+{
+    const float yy = y - c;
+    const float t = sum + yy;
+    c = (t - sum) - yy;
+    sum = t;
+}
 
 __device__ __forceinline__ void load_target(const PairConst& K, const State& st, int i, bool active, Target& T)
 {
@@ -103,6 +114,7 @@ __device__ __forceinline__ void load_target(const PairConst& K, const State& st,
         T.Rz = si.zz > 0.f ? -K.eps * T.Szz : 0.f;
     }
     T.drho = T.ax = T.ay = T.az = 0.f;
+    T.cdrho = T.cax = T.cay = T.caz = 0.f;
     T.l00 = T.l01 = T.l02 = T.l10 = T.l11 = T.l12 = T.l20 = T.l21 = T.l22 = 0.f;
 }
 
@@ -114,7 +126,9 @@ __device__ __forceinline__ float sqrt_approx(float x)
 }
 
 /* One pair, without branches: a pair at q >= 2 gets a zero kernel gradient
- * and adds zero to every sum. */
+ * and adds zero to every sum.  kKahan compensates the density and
+ * momentum sums. */
+template <bool kKahan = false>
 __device__ __forceinline__ void pair_body(const PairConst& K, const State& st, Target& T, int j)
 {
     const float4 xj = __ldg(st.pos + j);
@@ -127,7 +141,10 @@ __device__ __forceinline__ void pair_body(const PairConst& K, const State& st, T
     const float fac = K.Cg * t * t * t;
     const float gx = fac * dx, gy = fac * dy, gz = fac * dz;
     const float vx = T.v.x - vj.x, vy = T.v.y - vj.y, vz = T.v.z - vj.z;
-    T.drho += vx * gx + vy * gy + vz * gz;
+    if (kKahan)
+        kahan_add(T.drho, T.cdrho, vx * gx + vy * gy + vz * gz);
+    else
+        T.drho += vx * gx + vy * gy + vz * gz;
     const float rinv = __fdividef(1.0f, vj.w);
     const float rj2 = rinv * rinv;
     const float Txx = T.Sxx + sj.xx * rj2, Tyy = T.Syy + sj.yy * rj2, Tzz = T.Szz + sj.zz * rj2;
@@ -154,9 +171,15 @@ __device__ __forceinline__ void pair_body(const PairConst& K, const State& st, T
         py += (T.Ry + Rjy) * f4 * gy;
         pz += (T.Rz + Rjz) * f4 * gz;
     }
-    T.ax += px;
-    T.ay += py;
-    T.az += pz;
+    if (kKahan) {
+        kahan_add(T.ax, T.cax, px);
+        kahan_add(T.ay, T.cay, py);
+        kahan_add(T.az, T.caz, pz);
+    } else {
+        T.ax += px;
+        T.ay += py;
+        T.az += pz;
+    }
     const float Vj = K.m * rinv;
     const float wx = Vj * vx, wy = Vj * vy, wz = Vj * vz;
     T.l00 -= wx * gx; T.l01 -= wx * gy; T.l02 -= wx * gz;
@@ -321,6 +344,7 @@ __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __re
 /* Pair sums from the lists; a particle whose list overflowed walks its
  * stencil directly.  List entries are fetched four pairs ahead so the
  * dependent neighbour loads do not wait on the list stream. */
+template <bool kKahan>
 __global__ void __launch_bounds__(kBlock, LQ_PAIR_MIN_BLOCKS) k_interaction_list(
     const Parameters* __restrict__ P, int np, int npb, State st, Rates rt, Cells cells, const int* __restrict__ list,
     const int* __restrict__ count, int stride, Frames fr)
@@ -350,10 +374,10 @@ __global__ void __launch_bounds__(kBlock, LQ_PAIR_MIN_BLOCKS) k_interaction_list
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                if (k + u < n) pair_body(K, st, T, cur[u]);
+                if (k + u < n) pair_body<kKahan>(K, st, T, cur[u]);
         }
     } else {
-        walk_stencil(P, K, st, cells, i, T.x, [&](int j) { pair_body(K, st, T, j); }, fr);
+        walk_stencil(P, K, st, cells, i, T.x, [&](int j) { pair_body<kKahan>(K, st, T, j); }, fr);
     }
     store_rates(P, K, rt, i, T);
 }
@@ -646,11 +670,16 @@ int launch_shepard_list(const Parameters* ph, const Parameters* pd, const State&
 }
 
 int launch_interaction_list(const Parameters* ph, const Parameters* pd, const State& st, const Rates& r,
-                            const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr)
+                            const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr,
+                            bool compensated)
 {
     if (ph->npm <= 0) return LQ_OK;
-    k_interaction_list<<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, r, c, nl.list,
-                                                                     nl.count, nl.stride, fr);
+    if (compensated)
+        k_interaction_list<true><<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, r, c,
+                                                                               nl.list, nl.count, nl.stride, fr);
+    else
+        k_interaction_list<false><<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, r, c,
+                                                                                nl.list, nl.count, nl.stride, fr);
     LQ_TRY_CUDA(cudaGetLastError(), "k_interaction_list");
     return LQ_OK;
 }

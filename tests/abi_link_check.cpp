@@ -40,6 +40,7 @@ int main()
         (const void*)&lq_sim_set_skin, (const void*)&lq_sim_set_materials, (const void*)&lq_sim_set_frames, (const void*)&lq_sim_rebuilds, (const void*)&lq_sim_rebuild_launches,
         (const void*)&lq_io_load_parameters,
         (const void*)&lq_io_save_parameters, (const void*)&lq_io_load_particles, (const void*)&lq_io_save_particles,
+        (const void*)&lq_io_save_vtu,
     };
     int n = 0;
     for (const void* f : fns) n += f != nullptr;

@@ -42,10 +42,11 @@ def field_errors(got, want, nb):
                 str=rel_l2(g[3][mat], w[3][mat]), pos=rel_l2(g[0][mat, :3], w[0][mat, :3]))
 
 
+@pytest.mark.parametrize("mixed", [False, True])
 @pytest.mark.parametrize("model", [1, 2])
-def test_native_sim_vs_oracle_1_10_100_steps(lq, orc, cuda, model):
+def test_native_sim_vs_oracle_1_10_100_steps(lq, orc, cuda, model, mixed):
     c = cases.small_column(model=model, velocity_noise=0.02, shepard=30, seed=21).with_ids()
-    sim = lq.Simulation(c.par, *c.arrays())
+    sim = lq.Simulation(c.par, *c.arrays(), mixed=mixed)
     osim = orc.OracleSim(c.par, *c.arrays())
     done = 0
     report = {}
@@ -56,8 +57,9 @@ def test_native_sim_vs_oracle_1_10_100_steps(lq, orc, cuda, model):
         e = field_errors(sim.download(), osim.get(), c.par.npb)
         report[n] = e
         for k, tol in TOL_SIM[n].items():
-            assert e[k] < tol, (model, n, k, report)
-    print("model", model, {n: {k: f"{v:.2e}" for k, v in e.items()} for n, e in report.items()})
+            assert e[k] < tol, (model, mixed, n, k, report)
+    print("model", model, "mixed" if mixed else "plain",
+          {n: {k: f"{v:.2e}" for k, v in e.items()} for n, e in report.items()})
     assert not sim.health().any()
 
 
@@ -148,3 +150,54 @@ def test_health_word_counts_escapes_and_non_finite_state(lq, cuda):
     assert h[1] >= 1                 # material particle outside the lattice
     assert h[0] >= 1                 # non-finite values detected
     assert h[2] == 0
+
+
+def shifted(case, dx):
+    """The case moved by dx in x (domain grown to match)."""
+    import loquat_b200 as lq
+
+    c = case.with_ids()
+    c.pospres[:, 0] += np.float32(dx)
+    c.par.domain_size_x += dx
+    lq.initialize_parameters(c.par)
+    c.par.dt = c.par.cfl * c.par.h / c.par.cs
+    return c
+
+
+def test_mixed_form_keeps_precision_far_from_the_origin(lq, orc, cuda):
+    """1 m from the origin a float position step of ~1e-7 m loses most of its
+    bits; the mixed form accumulates positions and velocities in FP64."""
+    c = shifted(cases.small_column(velocity_noise=0.02, shepard=30, seed=23), 1.0)
+    osim = orc.OracleSim(c.par, *c.arrays())
+    osim.step(100)
+    want = osim.get()
+    errs = {}
+    for mixed in (False, True):
+        sim = lq.Simulation(c.par, *c.arrays(), mixed=mixed)
+        sim.step(100)
+        errs[mixed] = field_errors(sim.download(), want, c.par.npb)
+    print("far from origin, 100 steps:", {("mixed" if m else "plain"): {k: f"{v:.2e}" for k, v in e.items()}
+                                           for m, e in errs.items()})
+    for k in ("vel", "str", "rho"):
+        assert errs[True][k] < 1e-3, (k, errs)
+    assert errs[True]["vel"] < errs[False]["vel"], errs
+
+
+def test_cylinder_at_full_domain_scale_vs_oracle(lq, orc, cuda):
+    """The bench workload's geometry scaled down in particle count but not in
+    coordinates: a small cylinder at the centre of a 1 m floor (dr = 2.949 mm,
+    h = 1.3 dr, phi = 30 deg), 100 steps.  The mixed form stays within 1e-3
+    of the FP64 oracle."""
+    c = cases.cylinder_collapse(radius=0.04, height=0.08, floor_radius_factor=12.5).with_ids()
+    osim = orc.OracleSim(c.par, *c.arrays())
+    osim.step(100)
+    want = osim.get()
+    errs = {}
+    for mixed in (False, True):
+        sim = lq.Simulation(c.par, *c.arrays(), mixed=mixed)
+        sim.step(100)
+        errs[mixed] = field_errors(sim.download(), want, c.par.npb)
+    print("cylinder at 0.5 m, 100 steps:", {("mixed" if m else "plain"): {k: f"{v:.2e}" for k, v in e.items()}
+                                             for m, e in errs.items()})
+    for k in ("vel", "str", "rho"):
+        assert errs[True][k] < 1e-3, (k, errs)
