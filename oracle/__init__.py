@@ -52,6 +52,9 @@ def lib():
         L.or_corrector.argtypes = [_VP, _I, _I] + [_VP] * 13
         L.or_dp_update.argtypes = [_VP, _D] + [_VP] * 5
         L.or_hypo_update.argtypes = [_VP, _D] + [_VP] * 3
+        L.or_sim_set_vw.argtypes = [_VP, _I, _VP]
+        L.or_vw_update.argtypes = [_VP, _D, _VP, _VP, _VP, _VP]
+        L.or_vw_rate.argtypes = [_VP, _VP, _D, _VP, _VP, _VP, _VP]
         _lib = L
     return _lib
 
@@ -171,6 +174,11 @@ class OracleSim:
         self.np = arrs[0].shape[0]
         self.h = lib().or_sim_create(ctypes.addressof(par), *map(_p, arrs), step0, time0)
 
+    def set_vw(self, rows):
+        """Model-3 (von Wolffersdorff) material rows, n x 10, by object id."""
+        self._vw = np.ascontiguousarray(rows, np.float32).reshape(-1, 10)
+        lib().or_sim_set_vw(self.h, self._vw.shape[0], _p(self._vw))
+
     def step(self, n: int = 1):
         lib().or_sim_step(self.h, n)
 
@@ -186,3 +194,19 @@ class OracleSim:
             self.h = None
 
     __del__ = close
+
+
+def vw_update(row, dt, d6, spin3, s6, e):
+    row = np.ascontiguousarray(row, np.float32)
+    d6, spin3, s6 = _d(d6, 6).ravel().copy(), _d(spin3, 3).ravel().copy(), _d(s6, 6).ravel().copy()
+    ee = np.array([e], np.float64)
+    n = lib().or_vw_update(_p(row), dt, _p(d6), _p(spin3), _p(s6), _p(ee))
+    return s6, float(ee[0]), n
+
+
+def vw_rate(row, s6, e, d6, spin3):
+    row = np.ascontiguousarray(row, np.float32)
+    s6, d6, spin3 = _d(s6, 6).ravel().copy(), _d(d6, 6).ravel().copy(), _d(spin3, 3).ravel().copy()
+    r, er = np.zeros(6), np.zeros(1)
+    lib().or_vw_rate(_p(row), _p(s6), e, _p(d6), _p(spin3), _p(r), _p(er))
+    return r, float(er[0])

@@ -434,15 +434,158 @@ void hypo_update(const OrParams& P, double dtp, const double* d, const double* w
         for (int k = 0; k < 3; ++k) s[k] -= (pres - coh);
 }
 
+/* -------------------------------------- von Wolffersdorff (model 3) */
+/* Not in the reference (its hypoplastic model is the four-parameter one
+ * above): the hypoplastic relation with a predefined limit-state surface of
+ * von Wolffersdorff (1996, Mech. Cohes.-Frict. Mater. 1:251-271), written
+ * from the published equations, tension positive (T < 0 in compression):
+ *   Tdot = fb fe / (That:That) [F^2 D + a^2 That (That:D) + fd a F (That + That*) |D|] + Jaumann
+ *   That = T / tr T, That* = That - I/3, |D| = sqrt(D:D)
+ *   a = sqrt3 (3 - sin phic) / (2 sqrt2 sin phic)
+ *   F = sqrt(tan^2 psi / 8 + (2 - tan^2 psi) / (2 + sqrt2 tan psi cos3theta)) - tan psi / (2 sqrt2)
+ *   tan psi = sqrt3 |That*|, cos3theta = -sqrt6 tr(That*^3) / (That*:That*)^{3/2}
+ *   e_x = e_x0 exp(-(-tr T / hs)^n) for x = i, c, d
+ *   fe = (ec / e)^beta, fd = ((e - ed) / (ec - ed))^alpha
+ *   fb = (hs / n) (ei0 / ec0)^beta (1 + ei) / ei (-tr T / hs)^(1 - n)
+ *        / (3 + a^2 - a sqrt3 ((ei0 - ed0) / (ec0 - ed0))^alpha)
+ *   edot = (1 + e) tr D
+ * A stress with tr T > -3 Pa (free surface, tension) is reset to -1 Pa
+ * isotropic before the rate is formed, as the four-parameter model resets
+ * near-zero stress.  The step is integrated by explicit sub-steps (Euler /
+ * Heun pair) whose relative stress difference is kept below `tol`.
+ * Table row: phic (deg), hs (Pa), n, ed0, ec0, ei0, alpha, beta, tol,
+ * max sub-steps. */
+struct VW {
+    double sphi, a, hs, n, ed0, ec0, ei0, alpha, beta, tol, fbden;
+    int maxsub;
+};
+
+VW vw_constants(const float* row)
+{
+    VW c;
+    const double phic = row[0] * 3.14159265358979323846 / 180.0;
+    c.sphi = std::sin(phic);
+    c.a = std::sqrt(3.0) * (3.0 - c.sphi) / (2.0 * std::sqrt(2.0) * c.sphi);
+    c.hs = row[1];
+    c.n = row[2];
+    c.ed0 = row[3];
+    c.ec0 = row[4];
+    c.ei0 = row[5];
+    c.alpha = row[6];
+    c.beta = row[7];
+    c.tol = row[8];
+    c.maxsub = (int)row[9];
+    c.fbden = 3.0 + c.a * c.a - c.a * std::sqrt(3.0) * std::pow((c.ei0 - c.ed0) / (c.ec0 - c.ed0), c.alpha);
+    return c;
+}
+
+/* tr(A^3) of a symmetric tensor (xx yy zz xy xz yz) */
+inline double trace_cube(const double* A)
+{
+    const double xx = A[0], yy = A[1], zz = A[2], xy = A[3], xz = A[4], yz = A[5];
+    return xx * xx * xx + yy * yy * yy + zz * zz * zz + 3.0 * (xy * xy * (xx + yy) + xz * xz * (xx + zz) +
+                                                                yz * yz * (yy + zz)) + 6.0 * xy * xz * yz;
+}
+
+void vw_rate(const VW& c, const double* T_in, double e, const double* d, const double* w, double* Tdot, double* edot)
+{
+    double T[6];
+    for (int k = 0; k < 6; ++k) T[k] = T_in[k];
+    double trT = T[0] + T[1] + T[2];
+    if (!(trT < -3.0)) {
+        for (int k = 0; k < 3; ++k) T[k] = -1.0;
+        for (int k = 3; k < 6; ++k) T[k] = 0.0;
+        trT = -3.0;
+    }
+    double Th[6], Ts[6];
+    for (int k = 0; k < 6; ++k) Th[k] = T[k] / trT;
+    for (int k = 0; k < 6; ++k) Ts[k] = Th[k];
+    for (int k = 0; k < 3; ++k) Ts[k] -= 1.0 / 3.0;
+    const double ThTh = contract(Th, Th);
+    const double TsTs = contract(Ts, Ts);
+    const double tpsi = std::sqrt(3.0 * TsTs);
+    double c3t = 1.0;
+    if (TsTs > 1e-30) c3t = -std::sqrt(6.0) * trace_cube(Ts) / std::pow(TsTs, 1.5);
+    c3t = std::fmax(-1.0, std::fmin(1.0, c3t));
+    const double F = std::sqrt(tpsi * tpsi / 8.0 + (2.0 - tpsi * tpsi) / (2.0 + std::sqrt(2.0) * tpsi * c3t)) -
+                     tpsi / (2.0 * std::sqrt(2.0));
+    const double pr = -trT / c.hs;
+    const double ex = std::exp(-std::pow(pr, c.n));
+    const double ei = c.ei0 * ex, ec = c.ec0 * ex, ed = c.ed0 * ex;
+    const double fe = std::pow(ec / e, c.beta);
+    const double fd = std::pow(std::fmax((e - ed) / (ec - ed), 0.0), c.alpha);
+    const double fb = (c.hs / c.n) * std::pow(c.ei0 / c.ec0, c.beta) * (1.0 + ei) / ei * std::pow(pr, 1.0 - c.n) /
+                      c.fbden;
+    const double ThD = contract(Th, d);
+    const double nD = std::sqrt(contract(d, d));
+    const double k0 = fb * fe / ThTh;
+    double jau[6];
+    jaumann(w, T_in, jau);
+    for (int k = 0; k < 6; ++k)
+        Tdot[k] = k0 * (F * F * d[k] + c.a * c.a * Th[k] * ThD + fd * c.a * F * (Th[k] + Ts[k]) * nD) + jau[k];
+    *edot = (1.0 + e) * (d[0] + d[1] + d[2]);
+}
+
+/* Adaptive explicit integration of the model over dt; returns sub-steps. */
+int vw_update(const VW& c, double dt, const double* d, const double* w, double* s, double& e)
+{
+    double t = 0.0, h = dt;
+    int steps = 0;
+    while (t < dt) {
+        h = std::fmin(h, dt - t);
+        if (steps >= c.maxsub - 1) h = dt - t;
+        double k1[6], k2[6], s1[6], s2[6], ke1, ke2;
+        vw_rate(c, s, e, d, w, k1, &ke1);
+        for (int k = 0; k < 6; ++k) s1[k] = s[k] + h * k1[k];
+        const double e1 = e + h * ke1;
+        vw_rate(c, s1, e1, d, w, k2, &ke2);
+        double num = 0.0, den = 0.0;
+        for (int k = 0; k < 6; ++k) {
+            s2[k] = s[k] + 0.5 * h * (k1[k] + k2[k]);
+            const double df = s2[k] - s1[k];
+            num += df * df * (k < 3 ? 1.0 : 2.0);
+            den += s2[k] * s2[k] * (k < 3 ? 1.0 : 2.0);
+        }
+        const double err = std::sqrt(num / std::fmax(den, 1e-30));
+        ++steps;
+        /* the last allowed sub-step is accepted whatever its error, so the
+         * whole interval is always integrated */
+        const bool last = steps >= c.maxsub - 1 || h <= dt * 1e-6;
+        if (err <= c.tol || last) {
+            for (int k = 0; k < 6; ++k) s[k] = s2[k];
+            e += 0.5 * h * (ke1 + ke2);
+            t += h;
+            const double g = err > 0.0 ? 0.9 * std::sqrt(c.tol / err) : 2.0;
+            h *= std::fmin(2.0, std::fmax(0.2, g));
+        } else {
+            h *= std::fmax(0.2, 0.9 * std::sqrt(c.tol / err));
+        }
+    }
+    return steps;
+}
+
 /* ---------------------------------------------- predictor / corrector */
 struct StateView {
     double *pos, *vel, *idep, *str, *stn;
 };
 
+/* Per-object material rows for model 3 (10 floats each). */
+struct VWTable {
+    const float* rows = nullptr;
+    int n = 0;
+};
+
+inline VW vw_for(const VWTable& t, double id)
+{
+    int k = (int)id;
+    k = k < 0 ? 0 : (k >= t.n ? t.n - 1 : k);
+    return vw_constants(t.rows + 10 * k);
+}
+
 /* reference src/predictor_corrector.cu:169-218 (material slots only; the
  * snapshot of all slots is taken by the caller) */
 void predictor(const OrParams& P, int np, int npb, StateView S, const double* accad, const double* spin,
-               const double* acestn)
+               const double* acestn, const VWTable& vwt = VWTable())
 {
     const double hdt = 0.5 * (double)P.dt;
 #pragma omp parallel for schedule(static)
@@ -461,6 +604,11 @@ void predictor(const OrParams& P, int np, int npb, StateView S, const double* ac
         const double* w = spin + 4 * (size_t)i;
         if (P.constitutive_model == 1) {
             dp_update(P, hdt, w, de, p, ep, s);
+        } else if (P.constitutive_model == 3) {
+            double ev = S.idep[4 * (size_t)i + 2];
+            vw_update(vw_for(vwt, S.idep[4 * (size_t)i]), hdt, de, w, s, ev);
+            S.idep[4 * (size_t)i + 2] = ev;
+            ep = std::sqrt(2.0 / 3.0 * contract(e, e));
         } else {
             hypo_update(P, hdt, de, w, s);
             ep = std::sqrt(2.0 / 3.0 * contract(e, e));
@@ -472,7 +620,7 @@ void predictor(const OrParams& P, int np, int npb, StateView S, const double* ac
 
 /* reference src/predictor_corrector.cu:256-307 */
 void corrector(const OrParams& P, int np, int npb, StateView S, StateView I, const double* accad,
-               const double* spin, const double* acestn)
+               const double* spin, const double* acestn, const VWTable& vwt = VWTable())
 {
     const double dt = (double)P.dt;
 #pragma omp parallel for schedule(static)
@@ -495,6 +643,11 @@ void corrector(const OrParams& P, int np, int npb, StateView S, StateView I, con
         const double* w = spin + 4 * (size_t)i;
         if (P.constitutive_model == 1) {
             dp_update(P, dt, w, de, p, ep, s);
+        } else if (P.constitutive_model == 3) {
+            double ev = I.idep[4 * (size_t)i + 2];
+            vw_update(vw_for(vwt, I.idep[4 * (size_t)i]), dt, de, w, s, ev);
+            S.idep[4 * (size_t)i + 2] = ev;
+            ep = std::sqrt(2.0 / 3.0 * contract(e, e));
         } else {
             hypo_update(P, dt, de, w, s);
             ep = std::sqrt(2.0 / 3.0 * contract(e, e));
@@ -514,6 +667,8 @@ struct OrSim {
     std::vector<double> pos, vel, idep, str, stn;
     std::vector<double> pos0, vel0, idep0, str0, stn0;
     std::vector<double> accad, spin, acestn, tmp;
+    std::vector<float> vw_rows;
+    VWTable vwt;
     Grid g;
 
     StateView cur() { return {pos.data(), vel.data(), idep.data(), str.data(), stn.data()}; }
@@ -558,12 +713,12 @@ struct OrSim {
         adami_stage();
         interaction_stage();
         pos0 = pos; vel0 = vel; idep0 = idep; str0 = str; stn0 = stn;
-        predictor(P, np, npb, cur(), accad.data(), spin.data(), acestn.data());
+        predictor(P, np, npb, cur(), accad.data(), spin.data(), acestn.data(), vwt);
         search();
         sort_all();
         adami_stage();
         interaction_stage();
-        corrector(P, np, npb, cur(), ini(), accad.data(), spin.data(), acestn.data());
+        corrector(P, np, npb, cur(), ini(), accad.data(), spin.data(), acestn.data(), vwt);
         const int N = P.stress_shepard_filter;
         if (N != 0 && step % N == 0 && step != 0) {
             search();
@@ -710,6 +865,29 @@ void* or_sim_create(const void* pv, const double* pos, const double* vel, const 
     s->search();
     s->sort_primary();
     return s;
+}
+
+/* Model-3 material rows (n x 10 floats, by object id). */
+int or_sim_set_vw(void* sv, int n, const float* rows)
+{
+    OrSim* s = (OrSim*)sv;
+    s->vw_rows.assign(rows, rows + 10 * (size_t)n);
+    s->vwt.rows = s->vw_rows.data();
+    s->vwt.n = n;
+    return 0;
+}
+
+/* One model-3 update of a single material point (unit tests). */
+int or_vw_update(const float* row, double dt, const double* d6, const double* spin3, double* s6, double* e)
+{
+    return vw_update(vw_constants(row), dt, d6, spin3, s6, *e);
+}
+
+int or_vw_rate(const float* row, const double* s6, double e, const double* d6, const double* spin3, double* rate6,
+               double* erate)
+{
+    vw_rate(vw_constants(row), s6, e, d6, spin3, rate6, erate);
+    return 0;
 }
 
 int or_sim_step(void* sv, int n)
