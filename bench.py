@@ -51,7 +51,9 @@ def parse_args(argv=None):
     ap.add_argument("--steps", type=int, default=250)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["cylinder", "column", "ensemble"], default="cylinder")
+    ap.add_argument("--config", choices=["cylinder", "column", "ensemble", "slope", "inclined"], default="cylinder",
+                    help="slope / inclined: the von Wolffersdorff workloads (2.856 M soil at dr 5 mm; 16.0 M at "
+                         "dr 2.5 mm)")
     ap.add_argument("--scenarios", type=int, default=256, help="ensemble size (--config ensemble)")
     ap.add_argument("--dr", type=float, default=None, help="override the particle spacing")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -60,14 +62,18 @@ def parse_args(argv=None):
                     help="plain FP32, or mixed precision (FP64 integrator accumulation and stress update, "
                          "compensated interaction sums)")
     ap.add_argument("--profile-steps", type=int, default=10)
-    ap.add_argument("--start-step", type=int, default=2500,
+    ap.add_argument("--start-step", type=int, default=None,
                     help="untimed steps run first so the timed window sits mid-run of the 5000-step collapse "
-                         "(the particles move and the neighbour lists are rebuilt at a representative rate)")
+                         "(the particles move and the neighbour lists are rebuilt at a representative rate); "
+                         "default 2500, 200 for the von Wolffersdorff workloads")
     ap.add_argument("--no-compare", action="store_true", help="skip timing the other precision form")
     ap.add_argument("--eager", action="store_true",
                     help="launch kernels one by one instead of replaying the step graph (for ncu, which cannot "
                          "profile kernels inside graphs with conditional nodes)")
-    return ap.parse_args(argv)
+    a = ap.parse_args(argv)
+    if a.start_step is None:
+        a.start_step = 200 if a.config in ("slope", "inclined") else 2500
+    return a
 
 
 def make_case(args, rank=0):
@@ -77,6 +83,10 @@ def make_case(args, rank=0):
         kw = {} if args.dr is None else {"dr": args.dr}
         return cases.cylinder_collapse(seed=1 + rank, **kw)
     kw = {} if args.dr is None else {"dr": args.dr}
+    if args.config == "slope":
+        return cases.slope_failure(seed=1 + rank, **kw)
+    if args.config == "inclined":
+        return cases.inclined_block(seed=1 + rank, **kw)
     return cases.column_collapse(seed=1 + rank, **kw)
 
 
@@ -89,6 +99,9 @@ def cpu_sample_case(args):
         s = (1.0e5 / 1.96e6) ** (1.0 / 3.0)
         return cases.cylinder_collapse(radius=0.2 * s, height=0.4 * s, seed=1), "cylinder R=%.4f m H=%.4f m" % (
             0.2 * s, 0.4 * s)
+    if args.config in ("slope", "inclined"):
+        s = (1.0e5 / 2.856e6) ** (1.0 / 3.0)
+        return cases.slope_failure(dr=0.005 / s, seed=1), "slope failure at dr=%.2f mm (~100 k soil)" % (5.0 / s)
     return cases.column_collapse(seed=1), "column collapse 50k"
 
 
@@ -178,6 +191,8 @@ def run_cpu_baseline(args, steps=5, warmup=1):
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
     sim = oracle.OracleSim(case.par, *case.arrays())
+    if "hypoplastic" in case.meta:
+        sim.set_vw(case.meta["hypoplastic"])
     sim.step(warmup)
     t0 = time.perf_counter()
     sim.step(steps)
@@ -199,6 +214,8 @@ def bench_reference(args):
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
     sim = oracle.OracleSim(case.par, *case.arrays())
+    if "hypoplastic" in case.meta:
+        sim.set_vw(case.meta["hypoplastic"])
     sim.step(args.warmup)
     t0 = time.perf_counter()
     sim.step(args.steps)
@@ -223,6 +240,12 @@ def workload_name(args):
     if args.config == "cylinder":
         return "cylinder collapse R=0.2 m H=0.4 m dr=%.3f mm h=1.3dr DP phi=30 (plain FP32)" % (
             1e3 * (args.dr or 0.002949))
+    if args.config == "slope":
+        return ("von Wolffersdorff slope failure 2.0x0.6x0.35 m at 45 deg dr=%.1f mm h=1.2dr e0=0.70 "
+                "(FP64 sub-stepping, tol 1e-4)" % (1e3 * (args.dr or 0.005)))
+    if args.config == "inclined":
+        return ("von Wolffersdorff 1.0x1.0x0.25 m block on a 30 deg plane dr=%.1f mm h=1.2dr e0=0.65 "
+                "(FP64 sub-stepping, tol 1e-4)" % (1e3 * (args.dr or 0.0025)))
     return "column collapse 0.2x0.1x0.02 m dr=2 mm h=1.2dr DP phi=19.8 (plain FP32)"
 
 
@@ -246,6 +269,8 @@ def bench_ours(args):
     par = case.par
     npm, np_ = par.npm, par.np
     sim = lq.Simulation(par, *case.arrays(), graph=not args.eager, mixed=args.form == "mixed")
+    if "hypoplastic" in case.meta:
+        sim.set_hypoplastic(case.meta["hypoplastic"])
     ext = torch.cuda.ExternalStream(sim.stream())
     plain, with_shep = sim.launches_per_step()
 
@@ -315,6 +340,8 @@ def bench_ours(args):
         other = "plain" if args.form == "mixed" else "mixed"
         sim.close()
         osim = lq.Simulation(par, *case.arrays(), graph=not args.eager, mixed=other == "mixed")
+        if "hypoplastic" in case.meta:
+            osim.set_hypoplastic(case.meta["hypoplastic"])
         if args.start_step > 0:
             osim.step(args.start_step)
         osim.step(args.warmup)

@@ -171,6 +171,15 @@ int lq_sim_rebuilds(void* sim, long long* count);
  * returns to the global parameters.  No reference counterpart: the
  * reference runs one scenario per process. */
 int lq_sim_set_materials(void* sim, int n, const float* table);
+/* Constitutive model 3 (von Wolffersdorff hypoplasticity with a limit-state
+ * surface, integrated in FP64 with adaptive explicit sub-steps; no reference
+ * counterpart).  table is n x 10 floats per object id (row (int)idep.x,
+ * clamped): phi_c in degrees, h_s in Pa, n, e_d0, e_c0, e_i0, alpha, beta,
+ * the relative sub-step tolerance and the maximum number of sub-steps.  The
+ * void ratio of each particle lives in idep.z.  Required before the first
+ * step when Parameters.constitutive_model is 3; rows are checked
+ * (0 < phi_c < 90, 0 < e_d0 < e_c0 < e_i0, ...). */
+int lq_sim_set_hypoplastic(void* sim, int n, const float* table);
 /* Per-object grid frames, for the same use: each object keeps local
  * coordinates and owns a block of grid rows in y.  rows is n x 2 ints,
  * (first row, number of rows) for object ids 0..n-1; a particle's local y

@@ -70,6 +70,7 @@ _SIGNATURES = {
     "lq_sim_profile": (_I, [_VP, _I, _VP, _VP]),
     "lq_sim_set_skin": (_I, [_VP, _F]),
     "lq_sim_set_materials": (_I, [_VP, _I, _VP]),
+    "lq_sim_set_hypoplastic": (_I, [_VP, _I, _VP]),
     "lq_sim_set_frames": (_I, [_VP, _I, _VP]),
     "lq_sim_rebuilds": (_I, [_VP, ctypes.POINTER(_LL)]),
     "lq_sim_rebuild_launches": (_I, [_VP, ctypes.POINTER(_I)]),
@@ -292,6 +293,13 @@ class Simulation:
         particles whose idep.x is k."""
         t = np.ascontiguousarray(table, np.float32).reshape(-1, 5)
         check(lib().lq_sim_set_materials(self.handle, t.shape[0], t.ctypes.data), "lq_sim_set_materials")
+
+    def set_hypoplastic(self, table):
+        """Constitutive model 3 rows (10 floats per object id): phi_c (deg),
+        h_s, n, e_d0, e_c0, e_i0, alpha, beta, sub-step tolerance, maximum
+        sub-steps.  The void ratio is carried in idep.z."""
+        t = np.ascontiguousarray(table, np.float32).reshape(-1, 10)
+        check(lib().lq_sim_set_hypoplastic(self.handle, t.shape[0], t.ctypes.data), "lq_sim_set_hypoplastic")
 
     def set_frames(self, rows):
         """Per-object grid rows: rows[k] = (first row, number of rows)."""

@@ -27,7 +27,7 @@ class Case:
     par: Parameters
     pospres: np.ndarray   # (np, 4) x, y, z, pressure
     velrhop: np.ndarray   # (np, 4) vx, vy, vz, density
-    idep: np.ndarray      # (np, 4) object id, plastic strain, 0, 0
+    idep: np.ndarray      # (np, 4) object id, plastic strain, void ratio (model 3), free
     str_: np.ndarray      # (np, 6) stress, tension positive
     stn: np.ndarray       # (np, 6) strain
     meta: dict = field(default_factory=dict)
@@ -42,13 +42,12 @@ class Case:
     def with_ids(self) -> "Case":
         """Copy whose idep.w holds each particle's original index (exact in
         float below 2**24), so particles can be matched after re-sorting;
-        no kernel reads idep.z or idep.w."""
+        no kernel reads idep.w (idep.z is the void ratio of model 3)."""
         idep = self.idep.copy()
         n = idep.shape[0]
-        idep[:, 3] = np.arange(n, dtype=np.float64).astype(np.float32)
         if n >= 1 << 24:
-            idep[:, 2] = (np.arange(n) >> 24).astype(np.float32)
-            idep[:, 3] = (np.arange(n) & ((1 << 24) - 1)).astype(np.float32)
+            raise ValueError("with_ids: particle indices from 2**24 on are not exact in idep.w")
+        idep[:, 3] = np.arange(n, dtype=np.float64).astype(np.float32)
         return Case(self.name, self.par.copy(), self.pospres.copy(), self.velrhop.copy(), idep,
                     self.str_.copy(), self.stn.copy(), dict(self.meta))
 
@@ -191,14 +190,17 @@ def cylinder_collapse(dr=0.002949, radius=0.2, height=0.4, floor_radius_factor=2
 def small_column(nsx=16, nsy=6, nsz=12, dr=0.002, layers=3, hdr=1.2, model=1, seed=3, jitter_frac=0.01,
                  velocity_noise=0.0, shepard=5, hypo_pars=(-300.0, -500.0, -300.0, -200.0, 0.0),
                  E=0.84e6, nu=0.3, phi=19.8, cohesion=0.0, rho0=2650.0, alpha=0.25, front_wall=False,
-                 name="small_column") -> Case:
+                 e0=0.70, vw=None, name="small_column") -> Case:
     """A few-thousand-particle column for parity tests.  `velocity_noise`
     (m/s) adds a seeded random velocity to the soil so every term of the
     interaction pass is exercised from the first step.  model 2 uses the
     four-parameter hypoplastic law with `hypo_pars` = (c1, c2, c3, c4, cohesion);
     in that form the ||D|| term only dissipates for c4 < 0 (T is compressive),
     and a positive c4 makes the explicit update blow up within tens of steps.
-    `front_wall` closes the box at the soil's free face (a confined block)."""
+    `front_wall` closes the box at the soil's free face (a confined block).
+    model 3 (von Wolffersdorff) uses the row `vw` (vw_row() by default),
+    initial void ratio e0 in idep.z and density rho0 as given; the row is
+    returned in meta["hypoplastic"] for Simulation.set_hypoplastic."""
     b = layers * dr
     nrx = nsx + (0 if front_wall else 10)
     soil = _lattice(nsx, nsy, nsz, dr, (b, b, b))
@@ -217,27 +219,161 @@ def small_column(nsx=16, nsy=6, nsz=12, dr=0.002, layers=3, hdr=1.2, model=1, se
     if model == 1:
         kphi, kpsi, kc = dp_cone(phi, 0.0, cohesion)
         pars = lambda K, G: (K, G, kphi, kpsi, kc)  # noqa: E731
-    else:
+    elif model == 2:
         pars = lambda K, G: tuple(hypo_pars)  # noqa: E731
+    else:
+        pars = lambda K, G: (0.0, 0.0, 0.0, 0.0, 0.0)  # noqa: E731
     par = _base_parameters(dr, hdr, rho0, domain, E, nu, 0.1, model, pars, shepard, alpha, (0.0, 0.0, -9.81))
     K0 = 1.0 - math.sin(math.radians(phi))
     rng = np.random.default_rng(seed)
     c = assemble(name, par, bnd, soil, rng, jitter_frac * dr, rho0, -9.81, b + nsz * dr, b, K0,
                  meta=dict(config="small", dr=dr, top=b + nsz * dr))
+    if model == 3:
+        c.idep[c.par.npb:, 2] = e0
+        row = vw_row() if vw is None else np.asarray(vw, np.float32)
+        c.meta["hypoplastic"] = np.stack([row, row])
     if velocity_noise > 0:
         nb = c.par.npb
         c.velrhop[nb:, :3] = rng.uniform(-velocity_noise, velocity_noise, size=(c.par.npm, 3)).astype(np.float32)
     return c
 
 
+# ------------------------------------------------ von Wolffersdorff sand
+# Sand of the slope and inclined-plane workloads: phi_c (deg), h_s (Pa), n,
+# e_d0, e_c0, e_i0, alpha, beta.
+VW_SAND = (30.0, 2.6e9, 0.27, 0.61, 0.98, 1.10, 0.18, 1.0)
+
+
+def vw_row(sand=VW_SAND, tol=1e-4, max_substeps=64) -> np.ndarray:
+    """One row of the model-3 table (Simulation.set_hypoplastic)."""
+    return np.array(list(sand) + [tol, max_substeps], np.float32)
+
+
+def vw_modulus(p, e, sand=VW_SAND) -> float:
+    """Isotropic tangent stiffness of the von Wolffersdorff model at mean
+    pressure p (Pa, compression positive) and void ratio e: for T = -p I and
+    D = eps I the rate is 3 fb fe (1 + a^2/3) eps I, plus the |D| term for
+    loading; returns fb fe (1 + a^2 + fd a), an upper bound of the
+    constrained modulus used to size the sound speed."""
+    phic, hs, n, ed0, ec0, ei0, alpha, beta = sand
+    sp = math.sin(math.radians(phic))
+    a = math.sqrt(3.0) * (3.0 - sp) / (2.0 * math.sqrt(2.0) * sp)
+    pr = 3.0 * max(p, 1.0) / hs
+    x = math.exp(-pr ** n)
+    ei, ec, ed = ei0 * x, ec0 * x, ed0 * x
+    den = 3.0 + a * a - a * math.sqrt(3.0) * ((ei0 - ed0) / (ec0 - ed0)) ** alpha
+    fb = (hs / n) * (ei0 / ec0) ** beta * (1.0 + ei) / ei * pr ** (1.0 - n) / den
+    fe = (ec / e) ** beta
+    fd = max((e - ed) / (ec - ed), 0.0) ** alpha
+    return fb * fe * (1.0 + a * a + fd * a)
+
+
+def _vw_parameters(dr, hdr, rho, domain, p_max, e0, sand, cfl, shepard, alpha, gravity):
+    """Parameters of a model-3 case: cs from the tangent stiffness at twice
+    the largest initial mean pressure (the explicit step must resolve the
+    stiffest soil, at the base)."""
+    M = vw_modulus(2.0 * p_max, e0, sand)
+    E = 3.0 * M * (1.0 - 2.0 * 0.3)   # K = M at nu = 0.3 in elastic_moduli
+    return _base_parameters(dr, hdr, rho, domain, E, 0.3, cfl, 3, lambda K, G: (0.0,) * 5, shepard, alpha,
+                            gravity)
+
+
+def slope_failure(dr=0.005, length=2.0, height=0.6, width=0.35, angle=45.0, runout=1.0, layers=3, hdr=1.2,
+                  e0=0.70, rho_s=2650.0, sand=VW_SAND, tol=1e-4, max_substeps=64, cfl=0.1, alpha=0.25,
+                  shepard=30, seed=1, jitter_frac=0.01, name="slope_failure") -> Case:
+    """Sand slope failure with the von Wolffersdorff model: a trapezoid of
+    soil `length` long and `height` high whose free face drops at `angle`
+    towards +x, `width` thick between two side walls, against a back wall at
+    x = 0, on a floor that runs `runout` beyond the toe.  Density
+    rho_s / (1 + e0); geostatic stress from the local surface with
+    K0 = 1 - sin(phi_c); void ratio e0 in idep.z.  At the defaults (2.0 x 0.6
+    x 0.35 m at dr = 5 mm) the soil holds 2.856 M particles: the stated
+    geometry at that spacing, not a 4.2 M count."""
+    b = layers * dr
+    rho = rho_s / (1.0 + e0)
+    nsx, nsy, nsz = round(length / dr), round(width / dr), round(height / dr)
+    t = math.tan(math.radians(angle))
+    block = _lattice(nsx, nsy, nsz, dr, (0.0, 0.0, 0.0))
+    top = np.minimum(height, (length - block[:, 0]) * t)
+    soil = block[block[:, 2] < top] + np.array([b, b, b])
+    nrx = nsx + round(runout / dr)
+    nwy = nsy + 2 * layers
+    nwz = round(1.1 * height / dr)
+    bnd = np.concatenate([
+        _lattice(nrx + layers, nwy, layers, dr, (0.0, 0.0, 0.0)),               # floor
+        _lattice(layers, nsy, nwz, dr, (0.0, b, b)),                            # back wall
+        _lattice(nrx + layers, layers, nwz, dr, (0.0, 0.0, b)),                 # side walls
+        _lattice(nrx + layers, layers, nwz, dr, (0.0, b + nsy * dr, b)),
+    ])
+    domain = ((nrx + layers) * dr, nwy * dr, b + 1.5 * height)
+    p_max = rho * 9.81 * height * (1.0 + 2.0 * (1.0 - math.sin(math.radians(sand[0])))) / 3.0
+    par = _vw_parameters(dr, hdr, rho, domain, p_max, e0, sand, cfl, shepard, alpha, (0.0, 0.0, -9.81))
+    K0 = 1.0 - math.sin(math.radians(sand[0]))
+    surface = lambda x: b + np.minimum(height, (length - (x[:, 0] - b)) * t)  # noqa: E731
+    c = assemble(name, par, bnd, soil, np.random.default_rng(seed), jitter_frac * dr, rho, -9.81, surface, b, K0,
+                 meta=dict(config="slope", dr=dr, length=length, height=height, angle=angle, e0=e0))
+    c.idep[c.par.npb:, 2] = e0
+    row = vw_row(sand, tol, max_substeps)
+    c.meta["hypoplastic"] = np.stack([row, row])
+    return c
+
+
+def inclined_block(dr=0.0025, length=1.0, width=1.0, height=0.25, angle=30.0, runout=1.0, upslope=0.1, layers=3,
+                   hdr=1.2, e0=0.65, rho_s=2650.0, sand=VW_SAND, tol=1e-4, max_substeps=64, cfl=0.1, alpha=0.25,
+                   shepard=30, seed=1, jitter_frac=0.01, name="inclined_block") -> Case:
+    """Soil block on an inclined plane with the von Wolffersdorff model.  The
+    frame is the plane's: z is normal to it and gravity is rotated,
+    g = 9.81 (sin angle, 0, -cos angle), so the block runs out towards +x.
+    The block (length x width x height) starts `upslope` from the plane's
+    upper end, between two side walls, with `runout` of plane below it.
+    Initial stress is the infinite-slope state: sigma_zz = rho g_z (top - z),
+    sigma_xx = sigma_yy = K0 sigma_zz, sigma_xz = rho g_x (top - z).  At
+    dr = 2.5 mm the block holds 16.0 M particles (1.0 x 1.0 x 0.25 m at
+    4 mm would hold 3.9 M)."""
+    b = layers * dr
+    rho = rho_s / (1.0 + e0)
+    th = math.radians(angle)
+    gx, gz = 9.81 * math.sin(th), -9.81 * math.cos(th)
+    nsx, nsy, nsz = round(length / dr), round(width / dr), round(height / dr)
+    nup = round(upslope / dr)
+    nrx = nup + nsx + round(runout / dr)
+    nwy = nsy + 2 * layers
+    nwz = round(1.2 * height / dr)
+    soil = _lattice(nsx, nsy, nsz, dr, (nup * dr, b, b))
+    bnd = np.concatenate([
+        _lattice(nrx, nwy, layers, dr, (0.0, 0.0, 0.0)),                        # plane
+        _lattice(nrx, layers, nwz, dr, (0.0, 0.0, b)),                          # side walls
+        _lattice(nrx, layers, nwz, dr, (0.0, b + nsy * dr, b)),
+    ])
+    domain = (nrx * dr, nwy * dr, b + 2.0 * height)
+    K0 = 1.0 - math.sin(math.radians(sand[0]))
+    p_max = rho * abs(gz) * height * (1.0 + 2.0 * K0) / 3.0
+    par = _vw_parameters(dr, hdr, rho, domain, p_max, e0, sand, cfl, shepard, alpha, (gx, 0.0, gz))
+    c = assemble(name, par, bnd, soil, np.random.default_rng(seed), jitter_frac * dr, rho, gz, b + height, b, K0,
+                 meta=dict(config="inclined", dr=dr, angle=angle, e0=e0))
+    nb = c.par.npb
+    depth = np.maximum(b + height - c.pospres[nb:, 2].astype(np.float64), 0.0)
+    c.str_[nb:, 4] = (rho * gx * depth).astype(np.float32)
+    c.idep[nb:, 2] = e0
+    row = vw_row(sand, tol, max_substeps)
+    c.meta["hypoplastic"] = np.stack([row, row])
+    return c
+
+
 def config_case(index: int, **kw) -> Case:
     """Case of one of the benchmark configurations (0-based):
-    0 column collapse 50k, 1 cylinder collapse ~1.96M (plain FP32 form)."""
+    0 column collapse 50k, 1 cylinder collapse ~1.96M (plain FP32 form),
+    2 von Wolffersdorff slope failure 2.856M, 4 von Wolffersdorff block on
+    a 30 degree plane 16.0M (3 is the ensemble(), a set of cases)."""
     if index == 0:
         return column_collapse(**kw)
     if index == 1:
         return cylinder_collapse(**kw)
-    raise ValueError(f"configuration {index} has no generator yet")
+    if index == 2:
+        return slope_failure(**kw)
+    if index == 4:
+        return inclined_block(**kw)
+    raise ValueError(f"configuration {index} has no single-case generator")
 
 
 def _column_parts(nsx, nsy, nsz, dr, layers, runout_cells, wall_top_cells):

@@ -22,15 +22,22 @@ namespace lqb {
 namespace {
 
 constexpr int kBlock = 128;
+/* resident blocks per SM asked of the model-3 instantiations: 4 caps them at
+ * 128 registers (a few spilled bytes), measured faster than 1 (168 registers)
+ * and 6 (80) on the 2.85 M-particle slope */
+#ifndef LQ_VW_MIN_BLOCKS
+#define LQ_VW_MIN_BLOCKS 4
+#endif
 
 inline int blocks_for(long long n, int b) { return (int)((n + b - 1) / b); }
 
 /* Half step of the material slots (reference src/predictor_corrector.cu:169-218):
  * v += dt/2 a; rho += dt/2 drho; x += dt/2 v_new; eps += dt/2 deps;
  * stress and plastic strain from the model at dt/2. */
-template <bool kMixed>
-__global__ void __launch_bounds__(kBlock) k_predict(const Parameters* __restrict__ P, int np, int npb, State in,
-                                                    State out, State snap, bool do_snap, Rates rt, MaterialTable mt)
+template <bool kMixed, bool kVW>
+__global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_predict(const Parameters* __restrict__ P, int np, int npb, State in,
+                                                    State out, State snap, bool do_snap, Rates rt, MaterialTable mt,
+                                                    MaterialTable vw)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
@@ -75,10 +82,13 @@ __global__ void __launch_bounds__(kBlock) k_predict(const Parameters* __restrict
         T6d e = widen6(e0), dd = widen6(de);
         e.xx += dd.xx * hdt; e.yy += dd.yy * hdt; e.zz += dd.zz * hdt;
         e.xy += dd.xy * hdt; e.xz += dd.xz * hdt; e.yz += dd.yz * hdt;
-        double p = x0.w, ep = id.y;
+        double p = x0.w, ep = id.y, ev = id.z;
         T6d sd = widen6(s0);
-        if (M.model == 1) {
+        if (!kVW && M.model == 1) {
             dp_update_d(M, hdt, w, dd, p, ep, sd);
+        } else if (kVW) {
+            vw_update_d(vw_const(vw, id.x), hdt, dd, w, sd, ev);
+            ep = sqrt(2.0 / 3.0 * contract6(e, e));
         } else {
             hypo_update_d(M, hdt, dd, w, sd);
             ep = sqrt(2.0 / 3.0 * contract6(e, e));
@@ -87,7 +97,7 @@ __global__ void __launch_bounds__(kBlock) k_predict(const Parameters* __restrict
         out.vd[i] = vd;
         out.pos[i] = make_float4((float)xd.x, (float)xd.y, (float)xd.z, (float)p);
         out.vel[i] = make_float4((float)vd.x, (float)vd.y, (float)vd.z, (float)vd.w);
-        out.idep[i] = make_float4(id.x, (float)ep, id.z, id.w);
+        out.idep[i] = make_float4(id.x, (float)ep, (float)ev, id.w);
         store_t2(out.str, i, narrow6(sd));
         store_t2(out.stn, i, narrow6(e));
         return;
@@ -104,10 +114,18 @@ __global__ void __launch_bounds__(kBlock) k_predict(const Parameters* __restrict
     const tensor2d e = e0 + de * (0.5f * dt);
 
     float p = x0.w;
-    float ep = id.y;
+    float ep = id.y, ev = id.z;
     tensor2d s = s0;
-    if (M.model == 1) {
+    if (!kVW && M.model == 1) {
         dp_update(M, 0.5f * dt, w, de, p, ep, s);
+    } else if (kVW) {
+        /* the adaptive sub-stepping runs in FP64 in both forms */
+        T6d sd = widen6(s0);
+        double evd = ev;
+        vw_update_d(vw_const(vw, id.x), 0.5 * (double)dt, widen6(de), w, sd, evd);
+        s = narrow6(sd);
+        ev = (float)evd;
+        ep = sqrtf(2.0f / 3.0f * J2(e));
     } else {
         hypo_update(M, 0.5f * dt, de, w, s);
         ep = sqrtf(2.0f / 3.0f * J2(e));
@@ -115,7 +133,7 @@ __global__ void __launch_bounds__(kBlock) k_predict(const Parameters* __restrict
     x.w = p;
     out.pos[i] = x;
     out.vel[i] = v;
-    out.idep[i] = make_float4(id.x, ep, id.z, id.w);
+    out.idep[i] = make_float4(id.x, ep, ev, id.w);
     store_t2(out.str, i, s);
     store_t2(out.stn, i, e);
 }
@@ -136,11 +154,11 @@ struct VerletCheck {
     float half_skin;
 };
 
-template <bool kMixed>
-__global__ void __launch_bounds__(kBlock) k_correct(const Parameters* __restrict__ P, int np, int npb, State cur,
+template <bool kMixed, bool kVW>
+__global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(const Parameters* __restrict__ P, int np, int npb, State cur,
                                                     State ini, const int* __restrict__ ini_idx, State out, Rates rt,
                                                     int* __restrict__ health, VerletCheck verlet, int first,
-                                                    MaterialTable mt)
+                                                    MaterialTable mt, MaterialTable vw)
 {
     const int i = first + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
@@ -163,7 +181,8 @@ __global__ void __launch_bounds__(kBlock) k_correct(const Parameters* __restrict
     const tensor2d de = load_t2(rt.acestn, i);
     const float4 x0 = ini.pos[k];
     const float4 v0 = ini.vel[k];
-    const float ep0 = ini.idep[k].y;
+    const float4 id0 = ini.idep[k];
+    const float ep0 = id0.y;
     const tensor2d s0 = load_t2_rw(ini.str, k);
     const tensor2d e0 = load_t2_rw(ini.stn, k);
     const float4 xc = cur.pos[i];
@@ -172,7 +191,7 @@ __global__ void __launch_bounds__(kBlock) k_correct(const Parameters* __restrict
 
     float4 v, x;
     tensor2d s, e;
-    float ep;
+    float ep, ev = id.z;
     if (kMixed) {
         const double ddt = dt;
         const double4 v0d = ini.vd[k], x0d = ini.xd[k];
@@ -187,8 +206,13 @@ __global__ void __launch_bounds__(kBlock) k_correct(const Parameters* __restrict
         ed.xy += dd.xy * ddt; ed.xz += dd.xz * ddt; ed.yz += dd.yz * ddt;
         double pd = xc.w, epd = ep0;
         T6d sd = widen6(s0);
-        if (M.model == 1) {
+        if (!kVW && M.model == 1) {
             dp_update_d(M, ddt, w, dd, pd, epd, sd);
+        } else if (kVW) {
+            double evd = id0.z;
+            vw_update_d(vw_const(vw, id.x), ddt, dd, w, sd, evd);
+            ev = (float)evd;
+            epd = sqrt(2.0 / 3.0 * contract6(ed, ed));
         } else {
             hypo_update_d(M, ddt, dd, w, sd);
             epd = sqrt(2.0 / 3.0 * contract6(ed, ed));
@@ -212,8 +236,15 @@ __global__ void __launch_bounds__(kBlock) k_correct(const Parameters* __restrict
         float p = xc.w;
         ep = ep0;
         s = s0;
-        if (M.model == 1) {
+        if (!kVW && M.model == 1) {
             dp_update(M, dt, w, de, p, ep, s);
+        } else if (kVW) {
+            T6d sd = widen6(s0);
+            double evd = id0.z;
+            vw_update_d(vw_const(vw, id.x), (double)dt, widen6(de), w, sd, evd);
+            s = narrow6(sd);
+            ev = (float)evd;
+            ep = sqrtf(2.0f / 3.0f * J2(e));
         } else {
             hypo_update(M, dt, de, w, s);
             ep = sqrtf(2.0f / 3.0f * J2(e));
@@ -222,7 +253,7 @@ __global__ void __launch_bounds__(kBlock) k_correct(const Parameters* __restrict
     }
     out.pos[i] = x;
     out.vel[i] = v;
-    out.idep[i] = make_float4(id.x, ep, id.z, id.w);
+    out.idep[i] = make_float4(id.x, ep, ev, id.w);
     store_t2(out.str, i, s);
     store_t2(out.stn, i, e);
     if (health) {
@@ -247,16 +278,24 @@ __global__ void __launch_bounds__(kBlock) k_correct(const Parameters* __restrict
 }  // namespace
 
 int launch_predict(const Parameters* ph, const Parameters* pd, const State& in, const State& out, const State* snap,
-                   const Rates& r, cudaStream_t s, const MaterialTable& mt)
+                   const Rates& r, cudaStream_t s, const MaterialTable& mt, const MaterialTable& vw)
 {
     if (ph->np <= 0) return LQ_OK;
+    if (ph->constitutive_model == 3 && (!vw.p || vw.n <= 0))
+        return set_error(LQ_ERR_ARG, "predictor: constitutive model 3 needs a von Wolffersdorff table");
     const bool do_snap = snap && snap->pos;
     State sn = do_snap ? *snap : State{nullptr, nullptr, nullptr, nullptr, nullptr};
-    if (in.xd && out.xd)
-        k_predict<true><<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt);
-    else
-        k_predict<false><<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r,
-                                                                       mt);
+    /* model 3 gets its own instantiation: its FP64 sub-stepping needs far
+     * more registers than the other models' kernels */
+    const bool vwm = ph->constitutive_model == 3;
+    const int nb = blocks_for(ph->np, kBlock);
+    if (in.xd && out.xd) {
+        if (vwm) k_predict<true, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw);
+        else k_predict<true, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw);
+    } else {
+        if (vwm) k_predict<false, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw);
+        else k_predict<false, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw);
+    }
     LQ_TRY_CUDA(cudaGetLastError(), "k_predict");
     return LQ_OK;
 }
@@ -265,25 +304,32 @@ int launch_correct(const Parameters* ph, const Parameters* pd, const State& cur,
                    const int* ini_idx, const Rates& r, int* health, cudaStream_t s)
 {
     if (ph->npm <= 0) return LQ_OK;
-    k_correct<false><<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, ini_idx, cur, r, health,
+    if (ph->constitutive_model == 3)
+        return set_error(LQ_ERR_ARG, "corrector: constitutive model 3 needs a von Wolffersdorff table");
+    k_correct<false, false><<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, ini_idx, cur, r, health,
                                                              VerletCheck{nullptr, nullptr, 0.0f}, ph->npb,
-                                                             MaterialTable());
+                                                             MaterialTable(), MaterialTable());
     LQ_TRY_CUDA(cudaGetLastError(), "k_correct");
     return LQ_OK;
 }
 
 int launch_correct_into(const Parameters* ph, const Parameters* pd, const State& cur, const State& ini,
                         const State& out, const Rates& r, int* health, const float4* xbuild, int* rebuild,
-                        float skin, cudaStream_t s, const MaterialTable& mt)
+                        float skin, cudaStream_t s, const MaterialTable& mt, const MaterialTable& vw)
 {
     if (ph->np <= 0) return LQ_OK;
+    if (ph->constitutive_model == 3 && (!vw.p || vw.n <= 0))
+        return set_error(LQ_ERR_ARG, "corrector: constitutive model 3 needs a von Wolffersdorff table");
     const VerletCheck vc{xbuild, rebuild, 0.5f * skin};
-    if (cur.xd && ini.xd && out.xd)
-        k_correct<true><<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r,
-                                                                      health, vc, 0, mt);
-    else
-        k_correct<false><<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r,
-                                                                       health, vc, 0, mt);
+    const bool vwm = ph->constitutive_model == 3;
+    const int nb = blocks_for(ph->np, kBlock);
+    if (cur.xd && ini.xd && out.xd) {
+        if (vwm) k_correct<true, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw);
+        else k_correct<true, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw);
+    } else {
+        if (vwm) k_correct<false, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw);
+        else k_correct<false, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw);
+    }
     LQ_TRY_CUDA(cudaGetLastError(), "k_correct");
     return LQ_OK;
 }

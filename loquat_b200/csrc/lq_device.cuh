@@ -328,4 +328,151 @@ __device__ __forceinline__ void hypo_update_d(const Material& M, double dtp, con
     }
 }
 
+/* ------------------------------------ von Wolffersdorff (model 3) */
+/* Hypoplasticity with a predefined limit-state surface (von Wolffersdorff
+ * 1996), tension positive, integrated in FP64 by explicit sub-steps (Euler /
+ * Heun pair with the relative stress difference kept below tol); not in the
+ * reference.  Row: phic (deg), hs, n, ed0, ec0, ei0, alpha, beta, tol,
+ * max sub-steps.  Equations:
+ *   Tdot = fb fe / (That:That) [F^2 D + a^2 That (That:D) + fd a F (That + That*) |D|] + Jaumann
+ *   with That = T/trT, a = sqrt3 (3 - sin phic) / (2 sqrt2 sin phic),
+ *   F from tan psi = sqrt3 |That*| and cos3theta, e_x = e_x0 exp(-(-trT/hs)^n),
+ *   fe = (ec/e)^beta, fd = ((e-ed)/(ec-ed))^alpha, edot = (1+e) tr D.
+ * Stresses with tr T > -3 Pa are replaced by -1 Pa isotropic before the
+ * rate is formed; where tan psi exceeds sqrt2 (F undefined: a tensile
+ * principal direction) the deviator of That is scaled back to
+ * tan psi = sqrt2 (1 - 1e-3) at the same mean stress. */
+struct VWConst {
+    double a, a2, fbk, lnhs, ihs, n, ed0, ec0, lnec0, ei0, alpha, beta, tol;
+    int maxsub;
+};
+
+/* Row constants; the powers of constants are formed once here:
+ * fbk = (hs / n) (ei0 / ec0)^beta / (3 + a^2 - a sqrt3 ((ei0 - ed0) / (ec0 - ed0))^alpha). */
+__device__ __forceinline__ VWConst vw_const(const MaterialTable& mt, float id)
+{
+    int k = (int)id;
+    k = k < 0 ? 0 : (k >= mt.n ? mt.n - 1 : k);
+    const float* r = mt.p + 10 * k;
+    VWConst c;
+    const double phic = (double)__ldg(r) * 3.14159265358979323846 / 180.0;
+    const double sphi = sin(phic);
+    const double hs = __ldg(r + 1);
+    c.a = sqrt(3.0) * (3.0 - sphi) / (2.0 * sqrt(2.0) * sphi);
+    c.a2 = c.a * c.a;
+    c.n = __ldg(r + 2);
+    c.ed0 = __ldg(r + 3);
+    c.ec0 = __ldg(r + 4);
+    c.ei0 = __ldg(r + 5);
+    c.alpha = __ldg(r + 6);
+    c.beta = __ldg(r + 7);
+    c.tol = __ldg(r + 8);
+    c.maxsub = (int)__ldg(r + 9);
+    c.lnhs = log(hs);
+    c.ihs = 1.0 / hs;
+    c.lnec0 = log(c.ec0);
+    const double den = 3.0 + c.a2 - c.a * sqrt(3.0) * pow((c.ei0 - c.ed0) / (c.ec0 - c.ed0), c.alpha);
+    c.fbk = (hs / c.n) * pow(c.ei0 / c.ec0, c.beta) / den;
+    return c;
+}
+
+__device__ __forceinline__ double trace_cube6(const T6d& A)
+{
+    return A.xx * A.xx * A.xx + A.yy * A.yy * A.yy + A.zz * A.zz * A.zz +
+           3.0 * (A.xy * A.xy * (A.xx + A.yy) + A.xz * A.xz * (A.xx + A.zz) + A.yz * A.yz * (A.yy + A.zz)) +
+           6.0 * A.xy * A.xz * A.yz;
+}
+
+/* The rate with the state-dependent powers through shared logarithms:
+ * pr = -trT/hs, pr^n = exp(n ln pr), pr^(1-n) = pr / pr^n, ex = exp(-pr^n),
+ * fe = exp(beta (ln ec0 - pr^n - ln e)), fd = exp(alpha ln((e - ed) / (ec - ed))). */
+static __device__ __noinline__ void vw_rate_d(const VWConst& c, const T6d& Tin, double e, const T6d& d,
+                                              const float4& w, T6d& R, double& edot)
+{
+    T6d T = Tin;
+    double trT = T.xx + T.yy + T.zz;
+    if (!(trT < -3.0)) {
+        T = T6d{-1.0, -1.0, -1.0, 0.0, 0.0, 0.0};
+        trT = -3.0;
+    }
+    const double it = 1.0 / trT;
+    T6d Th{T.xx * it, T.yy * it, T.zz * it, T.xy * it, T.xz * it, T.yz * it};
+    T6d Ts{Th.xx - 1.0 / 3.0, Th.yy - 1.0 / 3.0, Th.zz - 1.0 / 3.0, Th.xy, Th.xz, Th.yz};
+    double TsTs = contract6(Ts, Ts);
+    double tpsi = sqrt(3.0 * TsTs);
+    const double lim = sqrt(2.0) * (1.0 - 1e-3);
+    if (tpsi > lim) {
+        const double f = lim / tpsi;
+        Ts = T6d{Ts.xx * f, Ts.yy * f, Ts.zz * f, Ts.xy * f, Ts.xz * f, Ts.yz * f};
+        Th = T6d{Ts.xx + 1.0 / 3.0, Ts.yy + 1.0 / 3.0, Ts.zz + 1.0 / 3.0, Ts.xy, Ts.xz, Ts.yz};
+        TsTs *= f * f;
+        tpsi = lim;
+    }
+    const double ThTh = contract6(Th, Th);
+    double c3t = 1.0;
+    if (TsTs > 1e-30) c3t = -sqrt(6.0) * trace_cube6(Ts) / (TsTs * sqrt(TsTs));
+    c3t = fmax(-1.0, fmin(1.0, c3t));
+    const double F = sqrt(fmax(tpsi * tpsi / 8.0 + (2.0 - tpsi * tpsi) / (2.0 + sqrt(2.0) * tpsi * c3t), 0.0)) -
+                     tpsi / (2.0 * sqrt(2.0));
+    const double lnpr = log(-trT) - c.lnhs;
+    const double prn = exp(c.n * lnpr);
+    const double ex = exp(-prn);
+    const double ei = c.ei0 * ex, ec = c.ec0 * ex, ed = c.ed0 * ex;
+    const double fe = exp(c.beta * (c.lnec0 - prn - log(e)));
+    const double q = (e - ed) / (ec - ed);
+    const double fd = q > 0.0 ? exp(c.alpha * log(q)) : (c.alpha == 0.0 ? 1.0 : 0.0);
+    const double fb = c.fbk * (1.0 + 1.0 / ei) * (-trT * c.ihs) / prn;
+    const double ThD = contract6(Th, d);
+    const double nD = sqrt(contract6(d, d));
+    const double k0 = fb * fe / ThTh;
+    const double F2 = F * F, nf = fd * c.a * F * nD;
+    const T6d J = jaumann_d(w, Tin);
+    R.xx = k0 * (F2 * d.xx + c.a2 * Th.xx * ThD + nf * (Th.xx + Ts.xx)) + J.xx;
+    R.yy = k0 * (F2 * d.yy + c.a2 * Th.yy * ThD + nf * (Th.yy + Ts.yy)) + J.yy;
+    R.zz = k0 * (F2 * d.zz + c.a2 * Th.zz * ThD + nf * (Th.zz + Ts.zz)) + J.zz;
+    R.xy = k0 * (F2 * d.xy + c.a2 * Th.xy * ThD + nf * (Th.xy + Ts.xy)) + J.xy;
+    R.xz = k0 * (F2 * d.xz + c.a2 * Th.xz * ThD + nf * (Th.xz + Ts.xz)) + J.xz;
+    R.yz = k0 * (F2 * d.yz + c.a2 * Th.yz * ThD + nf * (Th.yz + Ts.yz)) + J.yz;
+    edot = (1.0 + e) * (d.xx + d.yy + d.zz);
+}
+
+/* Adaptive explicit integration over dt; returns the number of sub-steps. */
+static __device__ __noinline__ int vw_update_d(const VWConst& c, double dt, const T6d& d, const float4& w, T6d& s, double& e)
+{
+    double t = 0.0, h = dt;
+    int steps = 0;
+    T6d k1;
+    double ke1;
+    bool fresh = false;   /* k1 holds the rate at (s, e): kept across a rejected trial */
+    while (t < dt) {
+        h = fmin(h, dt - t);
+        if (steps >= c.maxsub - 1) h = dt - t;
+        T6d k2, s1;
+        double ke2;
+        if (!fresh) vw_rate_d(c, s, e, d, w, k1, ke1);
+        fresh = true;
+        s1 = T6d{s.xx + h * k1.xx, s.yy + h * k1.yy, s.zz + h * k1.zz, s.xy + h * k1.xy, s.xz + h * k1.xz,
+                 s.yz + h * k1.yz};
+        vw_rate_d(c, s1, e + h * ke1, d, w, k2, ke2);
+        const T6d s2{s.xx + 0.5 * h * (k1.xx + k2.xx), s.yy + 0.5 * h * (k1.yy + k2.yy),
+                     s.zz + 0.5 * h * (k1.zz + k2.zz), s.xy + 0.5 * h * (k1.xy + k2.xy),
+                     s.xz + 0.5 * h * (k1.xz + k2.xz), s.yz + 0.5 * h * (k1.yz + k2.yz)};
+        const T6d df{s2.xx - s1.xx, s2.yy - s1.yy, s2.zz - s1.zz, s2.xy - s1.xy, s2.xz - s1.xz, s2.yz - s1.yz};
+        const double err = sqrt(contract6(df, df) / fmax(contract6(s2, s2), 1e-30));
+        ++steps;
+        const bool last = steps >= c.maxsub - 1 || h <= dt * 1e-6;
+        if (err <= c.tol || last) {
+            s = s2;
+            e += 0.5 * h * (ke1 + ke2);
+            t += h;
+            fresh = false;
+            const double g = err > 0.0 ? 0.9 * sqrt(c.tol / err) : 2.0;
+            h *= fmin(2.0, fmax(0.2, g));
+        } else {
+            h *= fmax(0.2, 0.9 * sqrt(c.tol / err));
+        }
+    }
+    return steps;
+}
+
 }  // namespace lqb

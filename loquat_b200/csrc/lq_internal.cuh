@@ -141,7 +141,8 @@ int launch_shepard(const Parameters* par_host, const Parameters* par_dev, const 
 /* Predictor: out <- in advanced by dt/2 on material slots, boundary slots
  * copied when out != in; `snap` (may be all-null) receives a copy of `in`. */
 int launch_predict(const Parameters* par_host, const Parameters* par_dev, const State& in, const State& out,
-                   const State* snap, const Rates& r, cudaStream_t s, const MaterialTable& mt = MaterialTable());
+                   const State* snap, const Rates& r, cudaStream_t s, const MaterialTable& mt = MaterialTable(),
+                   const MaterialTable& vw = MaterialTable());
 /* Corrector in place on `cur`; ini values read at ini_idx[i] (identity when
  * ini_idx is null).  Non-finite results are counted in health. */
 int launch_correct(const Parameters* par_host, const Parameters* par_dev, const State& cur, const State& ini,
@@ -152,7 +153,8 @@ int launch_correct(const Parameters* par_host, const Parameters* par_dev, const 
  * built at xbuild with this skin may not hold through the next step. */
 int launch_correct_into(const Parameters* par_host, const Parameters* par_dev, const State& cur, const State& ini,
                         const State& out, const Rates& r, int* health, const float4* xbuild, int* rebuild,
-                        float skin, cudaStream_t s, const MaterialTable& mt = MaterialTable());
+                        float skin, cudaStream_t s, const MaterialTable& mt = MaterialTable(),
+                        const MaterialTable& vw = MaterialTable());
 
 /* List-driven Adami (boundary targets, material neighbours) and Shepard. */
 int launch_adami_list(const Parameters* par_host, const Parameters* par_dev, const State& st, const NeighborList& nl,

@@ -56,6 +56,7 @@ struct LqSim {
     int* rebuilds = nullptr;           /* device counter of rebuilds */
     int* host_flag = nullptr;          /* pinned mirror for the eager path */
     lqb::MaterialTable mt;             /* per-object materials (optional) */
+    lqb::MaterialTable vw;             /* von Wolffersdorff rows (model 3) */
     lqb::Frames fr;                    /* per-object grid rows (optional) */
     std::vector<void*> allocs;
     cudaGraphExec_t step_exec = nullptr;
@@ -192,12 +193,12 @@ int enqueue_stages(LqSim* S, cudaStream_t s)
     /* predictor stage (reference src/loquat.cu:343-368) */
     LQ_TRY(lqb::launch_adami_list(ph, pd, S->S, S->nlb, s));
     LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S, S->R, cells, S->nlm, s, S->fr, S->flags & LQ_SIM_MIXED));
-    LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt));
+    LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt, S->vw));
     /* corrector stage (reference src/loquat.cu:371-396) */
     LQ_TRY(lqb::launch_adami_list(ph, pd, S->S2, S->nlb, s));
     LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S2, S->R, cells, S->nlm, s, S->fr, S->flags & LQ_SIM_MIXED));
     LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild, S->skin, s,
-                                    S->mt));
+                                    S->mt, S->vw));
     return LQ_OK;
 }
 
@@ -343,6 +344,8 @@ int build_graphs(LqSim* S)
     S->step_exec = S->shep_exec = nullptr;
     S->conditional = false;
     if (!(S->flags & LQ_SIM_GRAPH)) return LQ_OK;
+    /* model 3 steps need the von Wolffersdorff table; capture once it is set */
+    if (S->ph.constitutive_model == 3 && S->vw.n == 0) return LQ_OK;
     if (capture_step(S) == LQ_OK) {
         S->conditional = true;
     } else {
@@ -368,8 +371,8 @@ int create(LqSim* S, const Parameters* par, const float* pos, const float* vel, 
         return lqb::set_error(LQ_ERR_ARG, "lq_sim_create: Parameters not initialised (call lq_initialize_parameters)");
     if (!(S->ph.cs > 0.0f) || !(S->ph.cfl > 0.0f))
         return lqb::set_error(LQ_ERR_ARG, "lq_sim_create: cs and cfl must be positive");
-    if (S->ph.constitutive_model != 1 && S->ph.constitutive_model != 2)
-        return lqb::set_error(LQ_ERR_ARG, "lq_sim_create: constitutive_model must be 1 or 2");
+    if (S->ph.constitutive_model < 1 || S->ph.constitutive_model > 3)
+        return lqb::set_error(LQ_ERR_ARG, "lq_sim_create: constitutive_model must be 1, 2 or 3");
     S->ph.dt = S->ph.cfl * S->ph.h / S->ph.cs; /* reference src/loquat.cu:333 */
     S->time = (double)S->ph.time;
     S->skin = kDefaultSkinOverH * S->ph.h;
@@ -456,6 +459,8 @@ extern "C" int lq_sim_step(void* sim, int nsteps)
 {
     if (!sim || nsteps < 0) return lqb::set_error(LQ_ERR_ARG, "lq_sim_step: bad argument");
     LqSim* S = static_cast<LqSim*>(sim);
+    if (S->ph.constitutive_model == 3 && S->vw.n == 0)
+        return lqb::set_error(LQ_ERR_ARG, "lq_sim_step: constitutive model 3 needs lq_sim_set_hypoplastic first");
     const int N = S->ph.stress_shepard_filter;
     for (int k = 0; k < nsteps; ++k) {
         S->ph.time = (float)S->time;
@@ -589,6 +594,31 @@ extern "C" int lq_sim_set_materials(void* sim, int n, const float* table)
     return LQ_OK;
 }
 
+extern "C" int lq_sim_set_hypoplastic(void* sim, int n, const float* table)
+{
+    if (!sim || n < 1 || !table) return lqb::set_error(LQ_ERR_ARG, "lq_sim_set_hypoplastic: bad argument");
+    for (int k = 0; k < n; ++k) {
+        const float* r = table + 10 * (size_t)k;
+        const bool ok = r[0] > 0.0f && r[0] < 90.0f && r[1] > 0.0f && r[2] > 0.0f && r[2] < 1.0f && r[3] > 0.0f &&
+                        r[3] < r[4] && r[4] < r[5] && r[6] >= 0.0f && r[7] >= 0.0f && r[8] > 0.0f && r[8] < 1.0f &&
+                        r[9] >= 1.0f && r[9] <= 100000.0f;
+        if (!ok)
+            return lqb::set_error(LQ_ERR_ARG,
+                                  "lq_sim_set_hypoplastic: row %d needs 0 < phic < 90, hs > 0, 0 < n < 1, "
+                                  "0 < ed0 < ec0 < ei0, alpha, beta >= 0, 0 < tol < 1, 1 <= max_substeps <= 1e5",
+                                  k);
+    }
+    LqSim* S = static_cast<LqSim*>(sim);
+    LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "set hypoplastic");
+    float* d = nullptr;
+    LQ_TRY(dev_alloc(S, (void**)&d, sizeof(float) * 10 * (size_t)n));
+    LQ_TRY_CUDA(cudaMemcpy(d, table, sizeof(float) * 10 * (size_t)n, cudaMemcpyHostToDevice), "hypoplastic table");
+    S->vw.p = d;
+    S->vw.n = n;
+    LQ_TRY(build_graphs(S));
+    return LQ_OK;
+}
+
 extern "C" int lq_sim_set_frames(void* sim, int n, const int* rows)
 {
     if (!sim || n < 0 || (n > 0 && !rows)) return lqb::set_error(LQ_ERR_ARG, "lq_sim_set_frames: bad argument");
@@ -700,10 +730,10 @@ int profiled_step(LqSim* S, PhaseTimer& T)
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_INTEGRATE));
         if (stage == 0)
-            LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt));
+            LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt, S->vw));
         else
             LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild,
-                                            S->skin, s, S->mt));
+                                            S->skin, s, S->mt, S->vw));
         LQ_TRY(T.close(s));
     }
     return LQ_OK;

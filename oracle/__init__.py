@@ -180,7 +180,8 @@ class OracleSim:
         lib().or_sim_set_vw(self.h, self._vw.shape[0], _p(self._vw))
 
     def step(self, n: int = 1):
-        lib().or_sim_step(self.h, n)
+        if lib().or_sim_step(self.h, n) != 0:
+            raise RuntimeError("OracleSim.step: constitutive model 3 needs set_vw first")
 
     def get(self):
         n = self.np

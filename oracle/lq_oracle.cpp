@@ -451,7 +451,9 @@ void hypo_update(const OrParams& P, double dtp, const double* d, const double* w
  *   edot = (1 + e) tr D
  * A stress with tr T > -3 Pa (free surface, tension) is reset to -1 Pa
  * isotropic before the rate is formed, as the four-parameter model resets
- * near-zero stress.  The step is integrated by explicit sub-steps (Euler /
+ * near-zero stress; a stress with tan psi beyond sqrt2 (where F is not
+ * defined: a tensile principal direction) has its deviator scaled back to
+ * tan psi = sqrt2 (1 - 1e-3) at the same mean stress.  The step is integrated by explicit sub-steps (Euler /
  * Heun pair) whose relative stress difference is kept below `tol`.
  * Table row: phic (deg), hs (Pa), n, ed0, ec0, ei0, alpha, beta, tol,
  * max sub-steps. */
@@ -501,14 +503,26 @@ void vw_rate(const VW& c, const double* T_in, double e, const double* d, const d
     for (int k = 0; k < 6; ++k) Th[k] = T[k] / trT;
     for (int k = 0; k < 6; ++k) Ts[k] = Th[k];
     for (int k = 0; k < 3; ++k) Ts[k] -= 1.0 / 3.0;
+    double TsTs = contract(Ts, Ts);
+    double tpsi = std::sqrt(3.0 * TsTs);
+    /* F is undefined from tan psi = sqrt2 on (states with tension): the
+     * deviator is scaled back inside, keeping the mean stress */
+    const double lim = std::sqrt(2.0) * (1.0 - 1e-3);
+    if (tpsi > lim) {
+        const double f = lim / tpsi;
+        for (int k = 0; k < 6; ++k) Ts[k] *= f;
+        for (int k = 0; k < 6; ++k) Th[k] = Ts[k];
+        for (int k = 0; k < 3; ++k) Th[k] += 1.0 / 3.0;
+        TsTs *= f * f;
+        tpsi = lim;
+    }
     const double ThTh = contract(Th, Th);
-    const double TsTs = contract(Ts, Ts);
-    const double tpsi = std::sqrt(3.0 * TsTs);
     double c3t = 1.0;
     if (TsTs > 1e-30) c3t = -std::sqrt(6.0) * trace_cube(Ts) / std::pow(TsTs, 1.5);
     c3t = std::fmax(-1.0, std::fmin(1.0, c3t));
-    const double F = std::sqrt(tpsi * tpsi / 8.0 + (2.0 - tpsi * tpsi) / (2.0 + std::sqrt(2.0) * tpsi * c3t)) -
-                     tpsi / (2.0 * std::sqrt(2.0));
+    const double F =
+        std::sqrt(std::fmax(tpsi * tpsi / 8.0 + (2.0 - tpsi * tpsi) / (2.0 + std::sqrt(2.0) * tpsi * c3t), 0.0)) -
+        tpsi / (2.0 * std::sqrt(2.0));
     const double pr = -trT / c.hs;
     const double ex = std::exp(-std::pow(pr, c.n));
     const double ei = c.ei0 * ex, ec = c.ec0 * ex, ed = c.ed0 * ex;
@@ -893,6 +907,7 @@ int or_vw_rate(const float* row, const double* s6, double e, const double* d6, c
 int or_sim_step(void* sv, int n)
 {
     OrSim* s = (OrSim*)sv;
+    if (s->P.constitutive_model == 3 && s->vwt.n == 0) return -1; /* model 3 needs or_sim_set_vw */
     for (int k = 0; k < n; ++k) s->one_step();
     return 0;
 }

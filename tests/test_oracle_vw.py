@@ -86,3 +86,34 @@ def test_triaxial_compression_reaches_the_critical_state(orc):
     ec = ROW[4] * math.exp(-(3 * p / ROW[1]) ** ROW[2])
     assert abs(e - ec) < 0.01 * ec, (e, ec)
     assert abs(2 * dr / da + 1) < 0.02               # volumetric / axial strain rate -> 0
+
+
+def test_states_outside_the_limit_surface_give_finite_rates(orc):
+    """Near-zero and tensile stresses (free surface) must not produce NaN:
+    tr T >= -3 Pa is reset, tan psi beyond sqrt2 is scaled back inside."""
+    d = np.array([1e-3, -2e-3, -4e-3, 5e-4, 1e-4, -3e-4])
+    for s in ([-2.94, -1.95, 1.65, -1.0, -3.09, 0.55],      # tr T = -3.24 Pa, tan psi = 3.1
+              [-5e3, 2e3, 1e3, 0, 0, 0],                      # tension in two directions
+              [1.0, 1.0, 1.0, 0, 0, 0],                       # all tension
+              [-1e4, 0.0, 0.0, 0, 0, 0]):                     # uniaxial: tan psi = sqrt2 exactly
+        r, er = orc.vw_rate(ROW, np.array(s, float), 0.7, d, np.array([0.1, 0.0, -0.2]))
+        assert np.isfinite(r).all() and math.isfinite(er), s
+        t, e, n = orc.vw_update(ROW, 1e-3, d, np.zeros(3), np.array(s, float), 0.7)
+        assert np.isfinite(t).all() and math.isfinite(e), s
+
+
+def test_projection_is_continuous_at_the_limit_surface(orc):
+    """Just inside and just outside tan psi = sqrt2 (1 - 1e-3) the rate is the same."""
+    d = np.array([-1e-3, 5e-4, 5e-4, 0, 0, 0.0])
+    lim = math.sqrt(2.0) * (1 - 1e-3)
+    p = 1e4
+    # axisymmetric compression state with tan psi = x: That* = diag(2, -1, -1) x / (3 sqrt2)
+    def state(x):
+        ts = np.array([2, -1, -1]) * x / (3 * math.sqrt(2))
+        th = ts + 1.0 / 3.0
+        return np.concatenate([-3 * p * th, np.zeros(3)])
+    a, _ = orc.vw_rate(ROW, state(lim * (1 - 1e-9)), 0.7, d, np.zeros(3))
+    b, _ = orc.vw_rate(ROW, state(lim * (1 + 1e-9)), 0.7, d, np.zeros(3))
+    c, _ = orc.vw_rate(ROW, state(lim * 1.5), 0.7, d, np.zeros(3))
+    assert np.allclose(a, b, rtol=1e-6)
+    assert np.allclose(b, c, rtol=1e-6)    # the scaled-back state is the same
