@@ -6,7 +6,8 @@
 Workload (default): 3D cylinder collapse, R = 0.2 m, H = 0.4 m,
 dr = 2.949 mm (about 1.96 M soil particles) on a 3-layer Adami floor,
 Drucker-Prager phi = 30 deg, E = 5 MPa, nu = 0.3, rho = 2000 kg/m^3,
-Wendland C2 with h = 1.3 dr, plain FP32 form.  Seeded synthetic input.
+Wendland C2 with h = 1.3 dr, mixed-precision form (the plain FP32 form is
+timed in the same run).  Seeded synthetic input.
 One step = predictor + corrector stages (search, gather, Adami,
 interaction, integration) plus the Shepard pass every 30 steps.
 
@@ -41,8 +42,14 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 BYTES_INTERACTION_PER_PARTICLE = 112   # 56 B read (pos, velrhop, str) + 56 B written (accad, spin, acestn)
-FLOPS_PER_PAIR = 80                    # counted from the interaction kernel's pair body
-FLOPS_PER_CANDIDATE = 8                # distance test
+# FP32 operations per list entry of the pair kernel (k_interaction_rec's
+# pair body with artificial viscosity on and artificial stress off, an FMA
+# counted as 2, MUFU sqrt / reciprocal as 1): distance and kernel gradient
+# 18, density rate 6, momentum 21, viscosity 19, velocity difference and
+# gradient 24, momentum sums 3, neighbour volume 2 (93); the compensated sums
+# of the mixed form add 12.
+FLOPS_PER_ENTRY = {"plain": 93, "mixed": 105}
+FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9 / 1e12   # TFLOP/s: SMs x FP32 lanes x FMA x max SM clock
 
 
 def parse_args(argv=None):
@@ -113,14 +120,16 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def traffic_from_profiles(workload: str):
-    """DRAM bytes per interaction launch from the committed ncu summary, if any."""
+def traffic_from_profiles(workload: str, form: str):
+    """ncu figures of the pair kernel for this workload and form from the
+    committed summary (profiles/interaction_traffic.json), if any:
+    {"traffic": DRAM bytes per launch, ...}."""
     f = ROOT / "profiles" / "interaction_traffic.json"
     if not f.exists():
         return None
     try:
         d = json.loads(f.read_text())
-        return d.get(workload)
+        return d.get(f"{workload} [{form}]")
     except Exception:
         return None
 
@@ -238,15 +247,14 @@ def bench_reference(args):
 
 def workload_name(args):
     if args.config == "cylinder":
-        return "cylinder collapse R=0.2 m H=0.4 m dr=%.3f mm h=1.3dr DP phi=30 (plain FP32)" % (
-            1e3 * (args.dr or 0.002949))
+        return "cylinder collapse R=0.2 m H=0.4 m dr=%.3f mm h=1.3dr DP phi=30" % (1e3 * (args.dr or 0.002949))
     if args.config == "slope":
         return ("von Wolffersdorff slope failure 2.0x0.6x0.35 m at 45 deg dr=%.1f mm h=1.2dr e0=0.70 "
                 "(FP64 sub-stepping, tol 1e-4)" % (1e3 * (args.dr or 0.005)))
     if args.config == "inclined":
         return ("von Wolffersdorff 1.0x1.0x0.25 m block on a 30 deg plane dr=%.1f mm h=1.2dr e0=0.65 "
                 "(FP64 sub-stepping, tol 1e-4)" % (1e3 * (args.dr or 0.0025)))
-    return "column collapse 0.2x0.1x0.02 m dr=2 mm h=1.2dr DP phi=19.8 (plain FP32)"
+    return "column collapse 0.2x0.1x0.02 m dr=2 mm h=1.2dr DP phi=19.8"
 
 
 def bench_ours(args):
@@ -308,7 +316,11 @@ def bench_ours(args):
     peak, peak_kind = measured_peaks()
     achieved_gbs = BYTES_INTERACTION_PER_PARTICLE * npm / t_int / 1e9 if t_int > 0 else None
     workload = workload_name(args)
-    traffic = traffic_from_profiles(workload)
+    ncu = traffic_from_profiles(workload, args.form)
+    traffic = ncu.get("traffic") if ncu else None
+    entries, _ = sim.neighbor_entries()
+    flops = FLOPS_PER_ENTRY[args.form] * entries
+    achieved_tf = flops / t_int / 1e12 if t_int > 0 else None
 
     e2e = None
     if not args.no_e2e:
@@ -376,9 +388,15 @@ def bench_ours(args):
                        "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                          "frac": (achieved_gbs / peak) if achieved_gbs else None, "traffic": traffic,
-                         "kernel": "k_interaction_list", "peak_kind": peak_kind,
+                         "kernel": "k_interaction_rec", "peak_kind": peak_kind,
                          "bytes_per_launch": BYTES_INTERACTION_PER_PARTICLE * npm,
-                         "ms_per_launch": t_int * 1e3},
+                         "ms_per_launch": t_int * 1e3,
+                         "ncu": ncu},
+            "roofline_fp32": {"achieved": achieved_tf, "peak": FP32_PEAK_NOMINAL, "unit": "TFLOP/s",
+                              "frac": (achieved_tf / FP32_PEAK_NOMINAL) if achieved_tf else None,
+                              "peak_kind": "nominal (no measured FP32 peak)",
+                              "flops_per_launch": flops, "list_entries": entries,
+                              "flops_per_entry": FLOPS_PER_ENTRY[args.form]},
             "phases_ms_per_step": {k: v[0] / max(args.profile_steps, 1) for k, v in prof.items()},
             "forms": forms,
             "gpu_launches": launches,

@@ -192,6 +192,10 @@ int lq_sim_set_frames(void* sim, int n, const int* rows);
  * with the Shepard pass; a rebuild adds lq_sim_rebuild_launches more. */
 int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard);
 int lq_sim_rebuild_launches(void* sim, int* launches);
+/* Entries in the current neighbour lists of material and of boundary
+ * particles (pairs within 2h + skin at the last build), for work
+ * accounting; synchronises the simulation's stream. */
+int lq_sim_neighbor_entries(void* sim, long long* material, long long* boundary);
 /* Advances nsteps steps launching kernels one by one with CUDA events
  * around each phase, then synchronises and returns the summed device time
  * per phase in phase_ms[7]: search, gather, Adami, interaction pairs,

@@ -74,6 +74,7 @@ _SIGNATURES = {
     "lq_sim_set_frames": (_I, [_VP, _I, _VP]),
     "lq_sim_rebuilds": (_I, [_VP, ctypes.POINTER(_LL)]),
     "lq_sim_rebuild_launches": (_I, [_VP, ctypes.POINTER(_I)]),
+    "lq_sim_neighbor_entries": (_I, [_VP, ctypes.POINTER(_LL), ctypes.POINTER(_LL)]),
     "lq_io_load_parameters": (_I, [ctypes.c_char_p, _VP]),
     "lq_io_save_parameters": (_I, [ctypes.c_char_p, _VP]),
     "lq_io_load_particles": (_I, [ctypes.c_char_p, _I] + [_VP] * 5),
@@ -315,6 +316,13 @@ class Simulation:
         c = _I()
         check(lib().lq_sim_rebuild_launches(self.handle, ctypes.byref(c)), "lq_sim_rebuild_launches")
         return c.value
+
+    def neighbor_entries(self):
+        """(material, boundary) entries in the current neighbour lists."""
+        a, b = _LL(), _LL()
+        check(lib().lq_sim_neighbor_entries(self.handle, ctypes.byref(a), ctypes.byref(b)),
+              "lq_sim_neighbor_entries")
+        return a.value, b.value
 
     def launches_per_step(self):
         a, b = _I(), _I()

@@ -57,6 +57,7 @@ struct LqSim {
     int* host_flag = nullptr;          /* pinned mirror for the eager path */
     lqb::MaterialTable mt;             /* per-object materials (optional) */
     lqb::MaterialTable vw;             /* von Wolffersdorff rows (model 3) */
+    float* rec = nullptr;              /* scaled neighbour stress, np x 6 floats */
     lqb::Frames fr;                    /* per-object grid rows (optional) */
     std::vector<void*> allocs;
     cudaGraphExec_t step_exec = nullptr;
@@ -192,11 +193,13 @@ int enqueue_stages(LqSim* S, cudaStream_t s)
     const lqb::Cells cells{S->g.start, nullptr, nullptr};
     /* predictor stage (reference src/loquat.cu:343-368) */
     LQ_TRY(lqb::launch_adami_list(ph, pd, S->S, S->nlb, s));
-    LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S, S->R, cells, S->nlm, s, S->fr, S->flags & LQ_SIM_MIXED));
+    LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S, S->R, cells, S->nlm, s, S->fr, S->flags & LQ_SIM_MIXED,
+                                        S->rec));
     LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt, S->vw));
     /* corrector stage (reference src/loquat.cu:371-396) */
     LQ_TRY(lqb::launch_adami_list(ph, pd, S->S2, S->nlb, s));
-    LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S2, S->R, cells, S->nlm, s, S->fr, S->flags & LQ_SIM_MIXED));
+    LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S2, S->R, cells, S->nlm, s, S->fr, S->flags & LQ_SIM_MIXED,
+                                        S->rec));
     LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild, S->skin, s,
                                     S->mt, S->vw));
     return LQ_OK;
@@ -385,6 +388,9 @@ int create(LqSim* S, const Parameters* par, const float* pos, const float* vel, 
     LQ_TRY(alloc_state(S, S->T));
     const size_t n = (size_t)S->np;
     LQ_TRY(dev_alloc(S, (void**)&S->xbuild, n * sizeof(float4)));
+#ifndef LQ_NO_NBR_RECORD
+    LQ_TRY(dev_alloc(S, (void**)&S->rec, n * 6 * sizeof(float)));   /* cudaMalloc: 256-byte aligned */
+#endif
     LQ_TRY(dev_alloc(S, (void**)&S->R.accad, n * sizeof(float4)));
     LQ_TRY(dev_alloc(S, (void**)&S->R.spin, n * sizeof(float4)));
     LQ_TRY(dev_alloc(S, (void**)&S->R.acestn, n * sizeof(tensor2d)));
@@ -646,12 +652,31 @@ extern "C" int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard
     if (!sim) return lqb::set_error(LQ_ERR_ARG, "lq_sim_launches_per_step: null sim");
     LqSim* S = static_cast<LqSim*>(sim);
     /* own kernels of a step without a rebuild: decide (graph only), Adami
-     * (when npb > 0), interaction and integrator per stage; a Shepard pass
+     * (when npb > 0), record packing (when used), interaction and
+     * integrator per stage; a Shepard pass
      * adds the filter and its copy */
-    const int stage = (S->npb > 0 ? 1 : 0) + 1 + 1;
+    const int stage = (S->npb > 0 ? 1 : 0) + (S->rec ? 2 : 1) + 1;
     const int decide = S->conditional ? 1 : 0;
     if (plain) *plain = decide + 2 * stage;
     if (with_shepard) *with_shepard = decide + 2 * stage + (S->npm > 0 ? 2 : 0);
+    return LQ_OK;
+}
+
+extern "C" int lq_sim_neighbor_entries(void* sim, long long* material, long long* boundary)
+{
+    if (!sim || !material || !boundary) return lqb::set_error(LQ_ERR_ARG, "lq_sim_neighbor_entries: null argument");
+    LqSim* S = static_cast<LqSim*>(sim);
+    LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "neighbor entries");
+    auto total = [](const int* d, int n, long long* out) -> int {
+        std::vector<int> h((size_t)(n > 0 ? n : 0));
+        if (n > 0) LQ_TRY_CUDA(cudaMemcpy(h.data(), d, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost), "counts");
+        long long t = 0;
+        for (int c : h) t += c < LQ_NBR_CAP ? c : LQ_NBR_CAP;
+        *out = t;
+        return LQ_OK;
+    };
+    LQ_TRY(total(S->nlm.count, S->npm, material));
+    LQ_TRY(total(S->nlb.count, S->npb, boundary));
     return LQ_OK;
 }
 
@@ -726,7 +751,7 @@ int profiled_step(LqSim* S, PhaseTimer& T)
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_INTERACTION));
         LQ_TRY(lqb::launch_interaction_list(ph, pd, *cur[stage], S->R, cells, S->nlm, s, S->fr,
-                                            S->flags & LQ_SIM_MIXED));
+                                            S->flags & LQ_SIM_MIXED, S->rec));
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_INTEGRATE));
         if (stage == 0)

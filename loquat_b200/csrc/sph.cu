@@ -11,6 +11,7 @@
  * same runs and their loads hit L1.
  */
 #include <climits>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 
@@ -181,6 +182,74 @@ __device__ __forceinline__ void pair_body(const PairConst& K, const State& st, T
         T.az += pz;
     }
     const float Vj = K.m * rinv;
+    const float wx = Vj * vx, wy = Vj * vy, wz = Vj * vz;
+    T.l00 -= wx * gx; T.l01 -= wx * gy; T.l02 -= wx * gz;
+    T.l10 -= wy * gx; T.l11 -= wy * gy; T.l12 -= wy * gz;
+    T.l20 -= wz * gx; T.l21 -= wz * gy; T.l22 -= wz * gz;
+}
+
+/* Scaled neighbour stress for the list pair kernel: sigma / rho^2 in two
+ * dense arrays, s4[j] = (xx, yy, zz, xy) and s2[j] = (xz, yz).  A warp's
+ * gathered neighbours sit close together in memory, so the L1 cost of a
+ * gather follows the cache lines each load instruction touches: the
+ * 24-byte stress read as three float2 loads touches its lines three times,
+ * the dense pair once (14 lines per 32 contiguous neighbours for pos,
+ * velrhop, s4 and s2, against 26).  1 / rho is formed as the state-array
+ * pair body forms it. */
+template <bool kKahan = false>
+__device__ __forceinline__ void pair_body_rec(const PairConst& K, const State& st, const float4* __restrict__ s4,
+                                              const float2* __restrict__ s2, Target& T, int j)
+{
+    const float4 xj = __ldg(st.pos + j);
+    const float4 vj = __ldg(st.vel + j);
+    const float4 sa = __ldg(s4 + j);
+    const float2 sb = __ldg(s2 + j);
+    const float a[8] = {xj.x, xj.y, xj.z, 0.0f, vj.x, vj.y, vj.z, vj.w};
+    const float b[6] = {sa.x, sa.y, sa.z, sa.w, sb.x, sb.y};
+    const float dx = T.x.x - a[0], dy = T.x.y - a[1], dz = T.x.z - a[2];
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    const float q = sqrt_approx(r2) * K.ih;
+    const float t = fmaxf(2.0f - q, 0.0f);
+    const float fac = K.Cg * t * t * t;
+    const float gx = fac * dx, gy = fac * dy, gz = fac * dz;
+    const float vx = T.v.x - a[4], vy = T.v.y - a[5], vz = T.v.z - a[6];
+    if (kKahan)
+        kahan_add(T.drho, T.cdrho, vx * gx + vy * gy + vz * gz);
+    else
+        T.drho += vx * gx + vy * gy + vz * gz;
+    const float Txx = T.Sxx + b[0], Tyy = T.Syy + b[1], Tzz = T.Szz + b[2];
+    const float Txy = T.Sxy + b[3], Txz = T.Sxz + b[4], Tyz = T.Syz + b[5];
+    float px = Txx * gx + Txy * gy + Txz * gz;
+    float py = Txy * gx + Tyy * gy + Tyz * gz;
+    float pz = Txz * gx + Tyz * gy + Tzz * gz;
+    if (K.visc) {
+        const float vr = fminf(vx * dx + vy * dy + vz * dz, 0.0f);
+        const float pi = __fdividef(-K.avc * K.h * vr, (r2 + K.eta) * (0.5f * (T.v.w + a[7])));
+        px -= pi * gx;
+        py -= pi * gy;
+        pz -= pi * gz;
+    }
+    if (K.artp) {
+        const float wk = K.Cw * t * t * t * t * (q + 0.5f);
+        const float f = __fdividef(wk, K.wdr);
+        const float f4 = (f * f) * (f * f);
+        const float Rjx = b[0] > 0.f ? -K.eps * b[0] : 0.f;
+        const float Rjy = b[1] > 0.f ? -K.eps * b[1] : 0.f;
+        const float Rjz = b[2] > 0.f ? -K.eps * b[2] : 0.f;
+        px += (T.Rx + Rjx) * f4 * gx;
+        py += (T.Ry + Rjy) * f4 * gy;
+        pz += (T.Rz + Rjz) * f4 * gz;
+    }
+    if (kKahan) {
+        kahan_add(T.ax, T.cax, px);
+        kahan_add(T.ay, T.cay, py);
+        kahan_add(T.az, T.caz, pz);
+    } else {
+        T.ax += px;
+        T.ay += py;
+        T.az += pz;
+    }
+    const float Vj = K.m * __fdividef(1.0f, a[7]);
     const float wx = Vj * vx, wy = Vj * vy, wz = Vj * vz;
     T.l00 -= wx * gx; T.l01 -= wx * gy; T.l02 -= wx * gz;
     T.l10 -= wy * gx; T.l11 -= wy * gy; T.l12 -= wy * gz;
@@ -375,6 +444,57 @@ __global__ void __launch_bounds__(kBlock, LQ_PAIR_MIN_BLOCKS) k_interaction_list
 #pragma unroll
             for (int u = 0; u < 4; ++u)
                 if (k + u < n) pair_body<kKahan>(K, st, T, cur[u]);
+        }
+    } else {
+        walk_stencil(P, K, st, cells, i, T.x, [&](int j) { pair_body<kKahan>(K, st, T, j); }, fr);
+    }
+    store_rates(P, K, rt, i, T);
+}
+
+__global__ void __launch_bounds__(kBlock) k_pack_stress(int np, State st, float4* __restrict__ s4,
+                                                        float2* __restrict__ s2)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    const float rho = __ldg(&st.vel[i].w);
+    const tensor2d s = load_t2(st.str, i);
+    const float rinv = __fdividef(1.0f, rho);
+    const float rj2 = rinv * rinv;
+    s4[i] = make_float4(s.xx * rj2, s.yy * rj2, s.zz * rj2, s.xy * rj2);
+    s2[i] = make_float2(s.xz * rj2, s.yz * rj2);
+}
+
+/* k_interaction_list with the neighbour stress from the scaled arrays (same sums, same order). */
+template <bool kKahan>
+__global__ void __launch_bounds__(kBlock, LQ_PAIR_MIN_BLOCKS) k_interaction_rec(
+    const Parameters* __restrict__ P, int np, int npb, State st, Rates rt, Cells cells, const int* __restrict__ list,
+    const int* __restrict__ count, int stride, Frames fr, const float4* __restrict__ s4,
+    const float2* __restrict__ s2)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = npb + t;
+    if (i >= np) return;
+    const PairConst K = load_pair_const(P);
+    Target T;
+    load_target(K, st, i, true, T);
+    const int n = __ldg(count + t);
+    if (n <= LQ_NBR_CAP) {
+        const int* p = list + t;
+        const size_t step4 = 4 * (size_t)stride;
+        int nxt[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) nxt[u] = u < n ? __ldg(p + u * stride) : i;
+        for (int k = 0; k < n; k += 4) {
+            p += step4;
+            int cur[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                cur[u] = nxt[u];
+                nxt[u] = k + 4 + u < n ? __ldg(p + u * stride) : i;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (k + u < n) pair_body_rec<kKahan>(K, st, s4, s2, T, cur[u]);
         }
     } else {
         walk_stencil(P, K, st, cells, i, T.x, [&](int j) { pair_body<kKahan>(K, st, T, j); }, fr);
@@ -671,9 +791,27 @@ int launch_shepard_list(const Parameters* ph, const Parameters* pd, const State&
 
 int launch_interaction_list(const Parameters* ph, const Parameters* pd, const State& st, const Rates& r,
                             const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr,
-                            bool compensated)
+                            bool compensated, float* rec)
 {
     if (ph->npm <= 0) return LQ_OK;
+    if (rec) {
+        if (reinterpret_cast<uintptr_t>(rec) % 16 != 0)
+            return set_error(LQ_ERR_ARG, "interaction: scaled-stress arrays must be 16-byte aligned");
+        float4* s4 = reinterpret_cast<float4*>(rec);
+        float2* s2 = reinterpret_cast<float2*>(rec + 4 * (size_t)ph->np);
+        k_pack_stress<<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(ph->np, st, s4, s2);
+        LQ_TRY_CUDA(cudaGetLastError(), "k_pack_stress");
+        if (compensated)
+            k_interaction_rec<true><<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, r, c,
+                                                                                  nl.list, nl.count, nl.stride, fr,
+                                                                                  s4, s2);
+        else
+            k_interaction_rec<false><<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, r, c,
+                                                                                   nl.list, nl.count, nl.stride, fr,
+                                                                                   s4, s2);
+        LQ_TRY_CUDA(cudaGetLastError(), "k_interaction_rec");
+        return LQ_OK;
+    }
     if (compensated)
         k_interaction_list<true><<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, r, c,
                                                                                nl.list, nl.count, nl.stride, fr);
