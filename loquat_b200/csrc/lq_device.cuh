@@ -386,8 +386,8 @@ __device__ __forceinline__ double trace_cube6(const T6d& A)
 /* The rate with the state-dependent powers through shared logarithms:
  * pr = -trT/hs, pr^n = exp(n ln pr), pr^(1-n) = pr / pr^n, ex = exp(-pr^n),
  * fe = exp(beta (ln ec0 - pr^n - ln e)), fd = exp(alpha ln((e - ed) / (ec - ed))). */
-static __device__ __noinline__ void vw_rate_d(const VWConst& c, const T6d& Tin, double e, const T6d& d,
-                                              const float4& w, T6d& R, double& edot)
+__device__ __forceinline__ void vw_rate_d(const VWConst& c, const T6d& Tin, double e, const T6d& d,
+                                          const float4& w, T6d& R, double& edot)
 {
     T6d T = Tin;
     double trT = T.xx + T.yy + T.zz;
@@ -436,41 +436,54 @@ static __device__ __noinline__ void vw_rate_d(const VWConst& c, const T6d& Tin, 
     edot = (1.0 + e) * (d.xx + d.yy + d.zz);
 }
 
-/* Adaptive explicit integration over dt; returns the number of sub-steps. */
-static __device__ __noinline__ int vw_update_d(const VWConst& c, double dt, const T6d& d, const float4& w, T6d& s, double& e)
+/* Adaptive explicit integration over dt; returns the number of sub-steps.
+ * The loop has one rate evaluation site (inlined once): each pass evaluates
+ * either the first rate of a trial at (s, e) or the second at the Euler
+ * point (s1, e1); a rejected trial keeps its first rate. */
+__device__ __forceinline__ int vw_update_d(const VWConst& c, double dt, const T6d& d, const float4& w, T6d& s,
+                                           double& e)
 {
     double t = 0.0, h = dt;
     int steps = 0;
-    T6d k1;
-    double ke1;
-    bool fresh = false;   /* k1 holds the rate at (s, e): kept across a rejected trial */
+    T6d k1{}, s1{}, x = s;
+    double ke1 = 0.0, xe = e;
+    bool have_k1 = false;
     while (t < dt) {
-        h = fmin(h, dt - t);
-        if (steps >= c.maxsub - 1) h = dt - t;
-        T6d k2, s1;
-        double ke2;
-        if (!fresh) vw_rate_d(c, s, e, d, w, k1, ke1);
-        fresh = true;
-        s1 = T6d{s.xx + h * k1.xx, s.yy + h * k1.yy, s.zz + h * k1.zz, s.xy + h * k1.xy, s.xz + h * k1.xz,
-                 s.yz + h * k1.yz};
-        vw_rate_d(c, s1, e + h * ke1, d, w, k2, ke2);
-        const T6d s2{s.xx + 0.5 * h * (k1.xx + k2.xx), s.yy + 0.5 * h * (k1.yy + k2.yy),
-                     s.zz + 0.5 * h * (k1.zz + k2.zz), s.xy + 0.5 * h * (k1.xy + k2.xy),
-                     s.xz + 0.5 * h * (k1.xz + k2.xz), s.yz + 0.5 * h * (k1.yz + k2.yz)};
-        const T6d df{s2.xx - s1.xx, s2.yy - s1.yy, s2.zz - s1.zz, s2.xy - s1.xy, s2.xz - s1.xz, s2.yz - s1.yz};
-        const double err = sqrt(contract6(df, df) / fmax(contract6(s2, s2), 1e-30));
-        ++steps;
-        const bool last = steps >= c.maxsub - 1 || h <= dt * 1e-6;
-        if (err <= c.tol || last) {
-            s = s2;
-            e += 0.5 * h * (ke1 + ke2);
-            t += h;
-            fresh = false;
-            const double g = err > 0.0 ? 0.9 * sqrt(c.tol / err) : 2.0;
-            h *= fmin(2.0, fmax(0.2, g));
+        T6d r;
+        double re;
+        vw_rate_d(c, x, xe, d, w, r, re);
+        if (!have_k1) {
+            k1 = r;
+            ke1 = re;
+            have_k1 = true;
         } else {
+            const T6d s2{s.xx + 0.5 * h * (k1.xx + r.xx), s.yy + 0.5 * h * (k1.yy + r.yy),
+                         s.zz + 0.5 * h * (k1.zz + r.zz), s.xy + 0.5 * h * (k1.xy + r.xy),
+                         s.xz + 0.5 * h * (k1.xz + r.xz), s.yz + 0.5 * h * (k1.yz + r.yz)};
+            const T6d df{s2.xx - s1.xx, s2.yy - s1.yy, s2.zz - s1.zz, s2.xy - s1.xy, s2.xz - s1.xz, s2.yz - s1.yz};
+            const double err = sqrt(contract6(df, df) / fmax(contract6(s2, s2), 1e-30));
+            ++steps;
+            const bool last = steps >= c.maxsub - 1 || h <= dt * 1e-6;
+            if (err <= c.tol || last) {
+                s = s2;
+                e += 0.5 * h * (ke1 + re);
+                t += h;
+                const double g = err > 0.0 ? 0.9 * sqrt(c.tol / err) : 2.0;
+                h *= fmin(2.0, fmax(0.2, g));
+                have_k1 = false;
+                x = s;
+                xe = e;
+                continue;
+            }
             h *= fmax(0.2, 0.9 * sqrt(c.tol / err));
         }
+        /* trial from (s, e) with the first rate k1 */
+        h = fmin(h, dt - t);
+        if (steps >= c.maxsub - 1) h = dt - t;
+        s1 = T6d{s.xx + h * k1.xx, s.yy + h * k1.yy, s.zz + h * k1.zz, s.xy + h * k1.xy, s.xz + h * k1.xz,
+                 s.yz + h * k1.yz};
+        x = s1;
+        xe = e + h * ke1;
     }
     return steps;
 }
