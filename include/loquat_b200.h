@@ -208,6 +208,14 @@ int lq_sim_profile(void* sim, int nsteps, double* phase_ms, int* phase_launches)
 /* ---- XML / .dat formats (reference src/loquat_io.cu:69-370) ------------ */
 int lq_io_load_parameters(const char* xml_path, void* par_host);
 int lq_io_save_parameters(const char* xml_path, const void* par_host);
+/* Constitutive model 3 in the parameter file (extension keys with no
+ * reference counterpart): vw-phi-c, vw-hs, vw-n, vw-ed0, vw-ec0, vw-ei0,
+ * vw-alpha, vw-beta, vw-tolerance (float), vw-max-substeps (int) and
+ * vw-initial-void-ratio (float, for soil particles whose idep.z is 0; the
+ * 22-column particle file does not carry idep.z).  vw_row receives the
+ * 10-float row of lq_sim_set_hypoplastic. */
+int lq_io_load_hypoplastic(const char* xml_path, float* vw_row, float* e0);
+int lq_io_save_parameters_vw(const char* xml_path, const void* par_host, const float* vw_row, float e0);
 int lq_io_load_particles(const char* dat_path, int np,
                          float* pospres, float* velrhop, float* idep, float* str, float* stn);
 int lq_io_save_particles(const char* dat_path, int np,

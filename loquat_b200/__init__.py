@@ -77,6 +77,8 @@ _SIGNATURES = {
     "lq_sim_neighbor_entries": (_I, [_VP, ctypes.POINTER(_LL), ctypes.POINTER(_LL)]),
     "lq_io_load_parameters": (_I, [ctypes.c_char_p, _VP]),
     "lq_io_save_parameters": (_I, [ctypes.c_char_p, _VP]),
+    "lq_io_load_hypoplastic": (_I, [ctypes.c_char_p, _VP, ctypes.POINTER(_F)]),
+    "lq_io_save_parameters_vw": (_I, [ctypes.c_char_p, _VP, _VP, _F]),
     "lq_io_load_particles": (_I, [ctypes.c_char_p, _I] + [_VP] * 5),
     "lq_io_save_particles": (_I, [ctypes.c_char_p, _I] + [_VP] * 5),
     "lq_io_save_vtu": (_I, [ctypes.c_char_p, _I, _I] + [_VP] * 5),
@@ -338,8 +340,24 @@ def load_parameters(xml_path) -> Parameters:
     return p
 
 
-def save_parameters(xml_path, par: Parameters) -> None:
-    check(lib().lq_io_save_parameters(os.fsencode(str(xml_path)), ctypes.byref(par)), "lq_io_save_parameters")
+def save_parameters(xml_path, par: Parameters, hypoplastic=None) -> None:
+    """Writes the parameter file; `hypoplastic` = (10-float row, initial void
+    ratio) adds the model-3 keys."""
+    if hypoplastic is None:
+        check(lib().lq_io_save_parameters(os.fsencode(str(xml_path)), ctypes.byref(par)), "lq_io_save_parameters")
+        return
+    row = np.ascontiguousarray(hypoplastic[0], np.float32).reshape(10)
+    check(lib().lq_io_save_parameters_vw(os.fsencode(str(xml_path)), ctypes.byref(par), row.ctypes.data,
+                                         float(hypoplastic[1])), "lq_io_save_parameters_vw")
+
+
+def load_hypoplastic(xml_path):
+    """(10-float model-3 row, initial void ratio) from a parameter file."""
+    row = np.zeros(10, np.float32)
+    e0 = _F()
+    check(lib().lq_io_load_hypoplastic(os.fsencode(str(xml_path)), row.ctypes.data, ctypes.byref(e0)),
+          "lq_io_load_hypoplastic")
+    return row, e0.value
 
 
 def load_particles(dat_path, np_: int):

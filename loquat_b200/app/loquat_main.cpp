@@ -48,10 +48,15 @@ struct Host {
     }
 };
 
-void save(const std::string& dir, Parameters& par, Host& h)
+/* vw: the model-3 row when constitutive-model is 3 (its keys are written
+ * with the parameters), else null */
+void save(const std::string& dir, Parameters& par, Host& h, const float* vw, float e0)
 {
     const std::string xml = dir + "/output_" + std::to_string(par.output_number) + ".xml";
-    LQ_CALL(lq_io_save_parameters(xml.c_str(), &par));
+    if (vw)
+        LQ_CALL(lq_io_save_parameters_vw(xml.c_str(), &par, vw, e0));
+    else
+        LQ_CALL(lq_io_save_parameters(xml.c_str(), &par));
     if (par.output_format == 2) {
         LQ_CALL(lq_io_save_vtu(dir.c_str(), par.output_number, par.np, h.pos.data(), h.vel.data(), h.idep.data(),
                                h.str.data(), h.stn.data()));
@@ -105,13 +110,24 @@ int main(int argc, char** argv)
     h.resize(par.np);
     LQ_CALL(lq_io_load_particles((project + ".dat").c_str(), par.np, h.pos.data(), h.vel.data(), h.idep.data(),
                                  h.str.data(), h.stn.data()));
+    /* constitutive model 3: material row and initial void ratio from the
+     * parameter file's extension keys; the particle file has no void ratio */
+    float vw_row[10] = {0};
+    float e0 = 0.0f;
+    const bool vw = par.constitutive_model == 3;
+    if (vw) {
+        LQ_CALL(lq_io_load_hypoplastic((project + ".xml").c_str(), vw_row, &e0));
+        for (int i = par.npb; i < par.np; ++i)
+            if (h.idep[4 * (size_t)i + 2] == 0.0f) h.idep[4 * (size_t)i + 2] = e0;
+    }
     const std::string dir = project;
     mkdir(dir.c_str(), 0755);
 
     void* sim = nullptr;
     LQ_CALL(lq_sim_create(&par, h.pos.data(), h.vel.data(), h.idep.data(), h.str.data(), h.stn.data(), flags, &sim));
+    if (vw) LQ_CALL(lq_sim_set_hypoplastic(sim, 1, vw_row));
     LQ_CALL(lq_update_time_step(&par));
-    save(dir, par, h);
+    save(dir, par, h, vw ? vw_row : nullptr, e0);
 
     const double dt = par.dt;
     double time = par.time;
@@ -147,7 +163,7 @@ int main(int argc, char** argv)
             par.output_number++;
             LQ_CALL(lq_sim_download(sim, h.pos.data(), h.vel.data(), h.idep.data(), h.str.data(), h.stn.data()));
             const auto s0 = std::chrono::steady_clock::now();
-            save(dir, par, h);
+            save(dir, par, h, vw ? vw_row : nullptr, e0);
             saving += std::chrono::duration<double>(std::chrono::steady_clock::now() - s0).count();
             printf("----------Save-----------\nTime = %0.5f | Step = %lld | FPS = %0.5f\n", par.time, step - 1, fps);
             printf("Number of particles: %d | Number of cells: %d\n", par.np, par.ncell);

@@ -216,10 +216,19 @@ extern "C" int lq_io_load_parameters(const char* xml_path, void* par_host)
     return LQ_OK;
 }
 
-extern "C" int lq_io_save_parameters(const char* xml_path, const void* par_host)
+namespace {
+
+/* Keys of constitutive model 3 (von Wolffersdorff), an extension with no
+ * counterpart in the reference's parameter file: the 10-float material row
+ * of lq_sim_set_hypoplastic and the initial void ratio. */
+const char* const kVwKeys[9] = {"vw-phi-c", "vw-hs", "vw-n", "vw-ed0", "vw-ec0", "vw-ei0", "vw-alpha", "vw-beta",
+                                "vw-tolerance"};
+const char* const kVwMaxSub = "vw-max-substeps";
+const char* const kVwE0 = "vw-initial-void-ratio";
+
+/* Writes the parameter file; `vw` (10 floats) and e0 add the model-3 keys. */
+int write_parameters(const char* xml_path, const Parameters& p, const float* vw, float e0)
 {
-    if (!xml_path || !par_host) return set_error(LQ_ERR_ARG, "lq_io_save_parameters: null argument");
-    const Parameters& p = *static_cast<const Parameters*>(par_host);
     FILE* fp = fopen(xml_path, "w");
     if (!fp) return set_error(LQ_ERR_IO, "cannot write file %s", xml_path);
     auto I = [&](const char* k, int v) { fprintf(fp, "  <%s type=\"int\">%d</%s>\n", k, v, k); };
@@ -270,10 +279,47 @@ extern "C" int lq_io_save_parameters(const char* xml_path, const void* par_host)
     I("artificial-pressure", p.artificial_pressure);
     if (p.artificial_pressure == 1) F("artificial-pressure-coefficient", p.artificial_pressure_coefficient);
     I("output-format", p.output_format);
+    if (vw) {
+        for (int k = 0; k < 9; ++k) F(kVwKeys[k], vw[k]);
+        I(kVwMaxSub, (int)vw[9]);
+        F(kVwE0, e0);
+    }
     fprintf(fp, "</parameters>\n");
     const bool ok = ferror(fp) == 0;
     fclose(fp);
     return ok ? LQ_OK : set_error(LQ_ERR_IO, "write error on %s", xml_path);
+}
+
+}  // namespace
+
+extern "C" int lq_io_save_parameters(const char* xml_path, const void* par_host)
+{
+    if (!xml_path || !par_host) return set_error(LQ_ERR_ARG, "lq_io_save_parameters: null argument");
+    return write_parameters(xml_path, *static_cast<const Parameters*>(par_host), nullptr, 0.0f);
+}
+
+extern "C" int lq_io_save_parameters_vw(const char* xml_path, const void* par_host, const float* vw_row, float e0)
+{
+    if (!xml_path || !par_host || !vw_row) return set_error(LQ_ERR_ARG, "lq_io_save_parameters_vw: null argument");
+    return write_parameters(xml_path, *static_cast<const Parameters*>(par_host), vw_row, e0);
+}
+
+extern "C" int lq_io_load_hypoplastic(const char* xml_path, float* vw_row, float* e0)
+{
+    if (!xml_path || !vw_row || !e0) return set_error(LQ_ERR_ARG, "lq_io_load_hypoplastic: null argument");
+    std::string text;
+    if (!read_file(xml_path, text)) return set_error(LQ_ERR_IO, "cannot load the parameter file %s", xml_path);
+    std::map<std::string, XmlValue> kv;
+    LQ_TRY(parse_parameters_xml(text, kv));
+    Reader r{kv};
+    float row[10];
+    for (int k = 0; k < 9; ++k) row[k] = r.get_float(kVwKeys[k]);
+    row[9] = (float)r.get_int(kVwMaxSub);
+    const float v = r.get_float(kVwE0);
+    if (r.status != LQ_OK) return r.status;
+    memcpy(vw_row, row, sizeof(row));
+    *e0 = v;
+    return LQ_OK;
 }
 
 extern "C" int lq_io_load_particles(const char* dat_path, int np, float* pos, float* vel, float* idep, float* str,

@@ -39,7 +39,7 @@ int main()
         (const void*)&lq_sim_health, (const void*)&lq_sim_launches_per_step, (const void*)&lq_sim_profile,
         (const void*)&lq_sim_set_skin, (const void*)&lq_sim_set_materials, (const void*)&lq_sim_set_hypoplastic, (const void*)&lq_sim_set_frames, (const void*)&lq_sim_rebuilds, (const void*)&lq_sim_rebuild_launches, (const void*)&lq_sim_neighbor_entries,
         (const void*)&lq_io_load_parameters,
-        (const void*)&lq_io_save_parameters, (const void*)&lq_io_load_particles, (const void*)&lq_io_save_particles,
+        (const void*)&lq_io_save_parameters, (const void*)&lq_io_load_hypoplastic, (const void*)&lq_io_save_parameters_vw, (const void*)&lq_io_load_particles, (const void*)&lq_io_save_particles,
         (const void*)&lq_io_save_vtu,
     };
     int n = 0;

@@ -199,6 +199,31 @@ def test_xml_reader_errors(lq, tmp_path):
     assert "DP-kpsi" in str(e.value)
 
 
+def test_xml_model_3_extension_keys_round_trip(lq, tmp_path):
+    from loquat_b200 import cases
+
+    c = cases.small_column(model=3)
+    row = cases.vw_row(tol=2e-4, max_substeps=48)
+    f = tmp_path / "vw.xml"
+    lq.save_parameters(f, c.par, hypoplastic=(row, 0.70))
+    text = f.read_text()
+    assert '<constitutive-model type="int">3</constitutive-model>' in text
+    assert '<vw-max-substeps type="int">48</vw-max-substeps>' in text
+    q = lq.load_parameters(f)
+    assert q.constitutive_model == 3 and q.np == c.par.np
+    f2 = tmp_path / "vw2.xml"
+    lq.save_parameters(f2, q, hypoplastic=lq.load_hypoplastic(f))
+    assert f2.read_text() == text
+    got, e0 = lq.load_hypoplastic(f)
+    assert np.array_equal(got, row) and e0 == np.float32(0.70)
+    # a model-3 file without the keys names the first missing one
+    g = tmp_path / "plain.xml"
+    lq.save_parameters(g, c.par)
+    with pytest.raises(lq.LoquatError) as e:
+        lq.load_hypoplastic(g)
+    assert e.value.status == lq.LQ_ERR_NOTFOUND and "vw-phi-c" in str(e.value)
+
+
 def test_dat_round_trip_and_errors(lq, tmp_path):
     rng = np.random.default_rng(0)
     n = 257

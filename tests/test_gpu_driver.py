@@ -77,3 +77,38 @@ def test_driver_vtu_outputs(lq, cuda, tmp_path):
     assert f'NumberOfPoints="{c.par.npm}"' in text
     for name in ("Pressure", "Velocity", "Density", "PlasticStrain", "Stress", "Strain", "connectivity"):
         assert f'Name="{name}"' in text
+
+
+def test_driver_runs_model_3_from_the_parameter_file(lq, cuda, tmp_path):
+    """constitutive-model 3 with the vw-* keys: the driver sets the table and
+    the initial void ratio, and its final state equals the library's run."""
+    if not APP.exists():
+        pytest.fail("driver not built: python -m loquat_b200.build")
+    c = cases.small_column(model=3, velocity_noise=0.02, shepard=5, seed=33)
+    par = c.par
+    every = 4
+    par.output_format = 1
+    par.output_frequency = every * par.dt * 0.999
+    par.time_max = 3 * every * par.dt * 0.9999
+    row = c.meta["hypoplastic"][1]
+    proj = tmp_path / "vw"
+    lq.save_parameters(str(proj) + ".xml", par, hypoplastic=(row, 0.70))
+    idep = c.idep.copy()
+    idep[:, 2] = 0.0                          # the particle file carries no void ratio
+    lq.save_particles(str(proj) + ".dat", c.pospres, c.velrhop, idep, c.str_, c.stn)
+    out = run(proj)
+    d = Path(str(proj))
+    last = max(int(p.stem) for p in d.glob("*.dat"))
+    got = lq.load_particles(d / f"{last}.dat", par.np)
+    assert lq.load_hypoplastic(d / f"output_{last}.xml")[1] == np.float32(0.70)
+    import re
+
+    s = [int(m) for m in re.findall(r"Step = (\d+)", out)][-1]
+    sim = lq.Simulation(c.par, *c.arrays())
+    sim.set_hypoplastic(c.meta["hypoplastic"])
+    sim.step(s + 1)
+    want = sim.download()
+    for k, (a, b) in enumerate(zip(got, want)):
+        if k == 2:
+            a, b = a[:, :2], b[:, :2]
+        assert np.array_equal(a, b), k
