@@ -128,10 +128,10 @@ int launch_interaction(const Parameters* par_host, const Parameters* par_dev, co
                        const Cells& c, cudaStream_t s);
 int launch_neighbor_list(const Parameters* par_host, const Parameters* par_dev, const float4* pos, const Cells& c,
                          const NeighborList& nl, cudaStream_t s);
-/* With `rec` (np x 6 floats, 16-byte aligned) the neighbour stress is
- * first scaled by 1/rho^2 into two dense arrays (np float4, then np float2)
- * that the pair kernel gathers; without it the pair kernel reads the 24-byte
- * stress records. */
+/* With `rec` (np x 13 floats, 16-byte aligned) the neighbour data are first
+ * packed into dense arrays (position and density, velocity and sigma/rho^2;
+ * 52 bytes per particle) that the pair kernel gathers; without it the pair
+ * kernel reads the state arrays. */
 int launch_interaction_list(const Parameters* par_host, const Parameters* par_dev, const State& st, const Rates& r,
                             const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr = Frames(),
                             bool compensated = false, float* rec = nullptr);

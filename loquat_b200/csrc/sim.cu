@@ -57,7 +57,7 @@ struct LqSim {
     int* host_flag = nullptr;          /* pinned mirror for the eager path */
     lqb::MaterialTable mt;             /* per-object materials (optional) */
     lqb::MaterialTable vw;             /* von Wolffersdorff rows (model 3) */
-    float* rec = nullptr;              /* scaled neighbour stress, np x 6 floats */
+    float* rec = nullptr;              /* packed neighbour data, np x 13 floats */
     lqb::Frames fr;                    /* per-object grid rows (optional) */
     std::vector<void*> allocs;
     cudaGraphExec_t step_exec = nullptr;
@@ -389,7 +389,7 @@ int create(LqSim* S, const Parameters* par, const float* pos, const float* vel, 
     const size_t n = (size_t)S->np;
     LQ_TRY(dev_alloc(S, (void**)&S->xbuild, n * sizeof(float4)));
 #ifndef LQ_NO_NBR_RECORD
-    LQ_TRY(dev_alloc(S, (void**)&S->rec, n * 6 * sizeof(float)));   /* cudaMalloc: 256-byte aligned */
+    LQ_TRY(dev_alloc(S, (void**)&S->rec, n * 13 * sizeof(float)));   /* cudaMalloc: 256-byte aligned */
 #endif
     LQ_TRY(dev_alloc(S, (void**)&S->R.accad, n * sizeof(float4)));
     LQ_TRY(dev_alloc(S, (void**)&S->R.spin, n * sizeof(float4)));

@@ -188,24 +188,32 @@ __device__ __forceinline__ void pair_body(const PairConst& K, const State& st, T
     T.l20 -= wz * gx; T.l21 -= wz * gy; T.l22 -= wz * gz;
 }
 
-/* Scaled neighbour stress for the list pair kernel: sigma / rho^2 in two
- * dense arrays, s4[j] = (xx, yy, zz, xy) and s2[j] = (xz, yz).  A warp's
- * gathered neighbours sit close together in memory, so the L1 cost of a
- * gather follows the cache lines each load instruction touches: the
- * 24-byte stress read as three float2 loads touches its lines three times,
- * the dense pair once (14 lines per 32 contiguous neighbours for pos,
- * velrhop, s4 and s2, against 26).  1 / rho is formed as the state-array
- * pair body forms it. */
+/* Packed neighbour data for the list pair kernel: four dense arrays over
+ * all slots, 52 bytes per particle,
+ *   nb.xr[j] = (x, y, z, rho), nb.vs[j] = (vx, vy, vz, sxx),
+ *   nb.s3[j] = (syy, szz, sxy, sxz), nb.s1[j] = syz,
+ * with s = sigma / rho^2.  The pair kernel is bound by the L1 data pipe: a
+ * warp's gathered neighbours sit close together in memory and the pipe's
+ * work follows the bytes each load instruction gathers, so the 13 floats a
+ * pair needs are gathered without the pressure word of pospres and without
+ * the 24-byte stress records (read as three 8-byte loads).  1 / rho is
+ * formed as the state-array pair body forms it. */
+struct NbrArrays {
+    float4* xr;
+    float4* vs;
+    float4* s3;
+    float* s1;
+};
+
 template <bool kKahan = false>
-__device__ __forceinline__ void pair_body_rec(const PairConst& K, const State& st, const float4* __restrict__ s4,
-                                              const float2* __restrict__ s2, Target& T, int j)
+__device__ __forceinline__ void pair_body_rec(const PairConst& K, const NbrArrays& nb, Target& T, int j)
 {
-    const float4 xj = __ldg(st.pos + j);
-    const float4 vj = __ldg(st.vel + j);
-    const float4 sa = __ldg(s4 + j);
-    const float2 sb = __ldg(s2 + j);
-    const float a[8] = {xj.x, xj.y, xj.z, 0.0f, vj.x, vj.y, vj.z, vj.w};
-    const float b[6] = {sa.x, sa.y, sa.z, sa.w, sb.x, sb.y};
+    const float4 xr = __ldg(nb.xr + j);
+    const float4 vs = __ldg(nb.vs + j);
+    const float4 s3 = __ldg(nb.s3 + j);
+    const float s1 = __ldg(nb.s1 + j);
+    const float a[8] = {xr.x, xr.y, xr.z, 0.0f, vs.x, vs.y, vs.z, xr.w};
+    const float b[6] = {vs.w, s3.x, s3.y, s3.z, s3.w, s1};
     const float dx = T.x.x - a[0], dy = T.x.y - a[1], dz = T.x.z - a[2];
     const float r2 = dx * dx + dy * dy + dz * dz;
     const float q = sqrt_approx(r2) * K.ih;
@@ -451,25 +459,26 @@ __global__ void __launch_bounds__(kBlock, LQ_PAIR_MIN_BLOCKS) k_interaction_list
     store_rates(P, K, rt, i, T);
 }
 
-__global__ void __launch_bounds__(kBlock) k_pack_stress(int np, State st, float4* __restrict__ s4,
-                                                        float2* __restrict__ s2)
+__global__ void __launch_bounds__(kBlock) k_pack_neighbors(int np, State st, NbrArrays nb)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
-    const float rho = __ldg(&st.vel[i].w);
+    const float4 x = __ldg(st.pos + i);
+    const float4 v = __ldg(st.vel + i);
     const tensor2d s = load_t2(st.str, i);
-    const float rinv = __fdividef(1.0f, rho);
+    const float rinv = __fdividef(1.0f, v.w);
     const float rj2 = rinv * rinv;
-    s4[i] = make_float4(s.xx * rj2, s.yy * rj2, s.zz * rj2, s.xy * rj2);
-    s2[i] = make_float2(s.xz * rj2, s.yz * rj2);
+    nb.xr[i] = make_float4(x.x, x.y, x.z, v.w);
+    nb.vs[i] = make_float4(v.x, v.y, v.z, s.xx * rj2);
+    nb.s3[i] = make_float4(s.yy * rj2, s.zz * rj2, s.xy * rj2, s.xz * rj2);
+    nb.s1[i] = s.yz * rj2;
 }
 
-/* k_interaction_list with the neighbour stress from the scaled arrays (same sums, same order). */
+/* k_interaction_list over the packed neighbour arrays (same sums, same order). */
 template <bool kKahan>
 __global__ void __launch_bounds__(kBlock, LQ_PAIR_MIN_BLOCKS) k_interaction_rec(
     const Parameters* __restrict__ P, int np, int npb, State st, Rates rt, Cells cells, const int* __restrict__ list,
-    const int* __restrict__ count, int stride, Frames fr, const float4* __restrict__ s4,
-    const float2* __restrict__ s2)
+    const int* __restrict__ count, int stride, Frames fr, NbrArrays nb)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = npb + t;
@@ -494,7 +503,7 @@ __global__ void __launch_bounds__(kBlock, LQ_PAIR_MIN_BLOCKS) k_interaction_rec(
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                if (k + u < n) pair_body_rec<kKahan>(K, st, s4, s2, T, cur[u]);
+                if (k + u < n) pair_body_rec<kKahan>(K, nb, T, cur[u]);
         }
     } else {
         walk_stencil(P, K, st, cells, i, T.x, [&](int j) { pair_body<kKahan>(K, st, T, j); }, fr);
@@ -796,19 +805,20 @@ int launch_interaction_list(const Parameters* ph, const Parameters* pd, const St
     if (ph->npm <= 0) return LQ_OK;
     if (rec) {
         if (reinterpret_cast<uintptr_t>(rec) % 16 != 0)
-            return set_error(LQ_ERR_ARG, "interaction: scaled-stress arrays must be 16-byte aligned");
-        float4* s4 = reinterpret_cast<float4*>(rec);
-        float2* s2 = reinterpret_cast<float2*>(rec + 4 * (size_t)ph->np);
-        k_pack_stress<<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(ph->np, st, s4, s2);
-        LQ_TRY_CUDA(cudaGetLastError(), "k_pack_stress");
+            return set_error(LQ_ERR_ARG, "interaction: packed neighbour arrays must be 16-byte aligned");
+        const size_t n = (size_t)ph->np;
+        NbrArrays nb{reinterpret_cast<float4*>(rec), reinterpret_cast<float4*>(rec) + n,
+                     reinterpret_cast<float4*>(rec) + 2 * n, rec + 12 * n};
+        k_pack_neighbors<<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(ph->np, st, nb);
+        LQ_TRY_CUDA(cudaGetLastError(), "k_pack_neighbors");
         if (compensated)
             k_interaction_rec<true><<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, r, c,
                                                                                   nl.list, nl.count, nl.stride, fr,
-                                                                                  s4, s2);
+                                                                                  nb);
         else
             k_interaction_rec<false><<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, r, c,
                                                                                    nl.list, nl.count, nl.stride, fr,
-                                                                                   s4, s2);
+                                                                                   nb);
         LQ_TRY_CUDA(cudaGetLastError(), "k_interaction_rec");
         return LQ_OK;
     }
