@@ -201,3 +201,37 @@ def test_cylinder_at_full_domain_scale_vs_oracle(lq, orc, cuda):
                                              for m, e in errs.items()})
     for k in ("vel", "str", "rho"):
         assert errs[True][k] < 1e-3, (k, errs)
+
+
+def subset(lq, case, keep_boundary, keep_material):
+    """The case restricted to the first `keep_boundary` boundary and first
+    `keep_material` material particles (counts updated)."""
+    from loquat_b200.cases import Case
+
+    nb = case.par.npb
+    idx = np.concatenate([np.arange(min(keep_boundary, nb)),
+                          nb + np.arange(min(keep_material, case.par.npm))]).astype(np.int64)
+    par = case.par.copy()
+    par.npb = int(min(keep_boundary, nb))
+    par.npm = int(min(keep_material, case.par.npm))
+    par.np = par.npb + par.npm
+    lq.initialize_parameters(par)
+    par.dt = par.cfl * par.h / par.cs
+    return Case(case.name, par, *[a[idx].copy() for a in case.arrays()], dict(case.meta))
+
+
+@pytest.mark.parametrize("nb,nm", [(0, 10 ** 9), (10 ** 9, 0), (0, 1), (10 ** 9, 1), (5, 33)],
+                         ids=["material-only", "boundary-only", "one-particle", "one-material", "ragged"])
+def test_degenerate_particle_sets_step_like_the_oracle(lq, orc, cuda, nb, nm):
+    """Material only (no Adami pass), boundary only (no interaction or
+    integration), a lone particle, and counts that fill no warp."""
+    c = subset(lq, cases.small_column(velocity_noise=0.02, shepard=4, seed=41), nb, nm).with_ids()
+    sim = lq.Simulation(c.par, *c.arrays())
+    osim = orc.OracleSim(c.par, *c.arrays())
+    sim.step(9)
+    osim.step(9)
+    got, want = by_id(sim.download()), by_id(osim.get())
+    for k in range(5):
+        assert np.all(np.isfinite(got[k]))
+        assert rel_l2(got[k], want[k]) < 1e-4, (k, rel_l2(got[k], want[k]))
+    assert not sim.health().any()
