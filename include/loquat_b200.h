@@ -192,6 +192,17 @@ int lq_sim_set_frames(void* sim, int n, const int* rows);
  * with the Shepard pass; a rebuild adds lq_sim_rebuild_launches more. */
 int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard);
 int lq_sim_rebuild_launches(void* sim, int* launches);
+/* Checkpoints of a simulation: the state (with the FP64 copies of the
+ * mixed form), step, time, skin and the per-object tables, in a binary file
+ * of this library's own format.  Saving forces a neighbour search before the
+ * simulation's next step, so a simulation loaded from the file with the same
+ * precision form and the run that continues take bit-identical steps.
+ * lq_sim_load_checkpoint creates the simulation (flags as for
+ * lq_sim_create; LQ_SIM_MIXED must match the saved form).  The reference
+ * restarts from its output XML and particle file instead, which round to
+ * float text and drop the void ratio. */
+int lq_sim_save_checkpoint(void* sim, const char* path);
+int lq_sim_load_checkpoint(const char* path, int flags, void** sim);
 /* Entries in the current neighbour lists of material and of boundary
  * particles (pairs within 2h + skin at the last build), for work
  * accounting; synchronises the simulation's stream. */

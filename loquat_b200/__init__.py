@@ -74,6 +74,8 @@ _SIGNATURES = {
     "lq_sim_set_frames": (_I, [_VP, _I, _VP]),
     "lq_sim_rebuilds": (_I, [_VP, ctypes.POINTER(_LL)]),
     "lq_sim_rebuild_launches": (_I, [_VP, ctypes.POINTER(_I)]),
+    "lq_sim_save_checkpoint": (_I, [_VP, ctypes.c_char_p]),
+    "lq_sim_load_checkpoint": (_I, [ctypes.c_char_p, _I, ctypes.POINTER(_VP)]),
     "lq_sim_neighbor_entries": (_I, [_VP, ctypes.POINTER(_LL), ctypes.POINTER(_LL)]),
     "lq_io_load_parameters": (_I, [ctypes.c_char_p, _VP]),
     "lq_io_save_parameters": (_I, [ctypes.c_char_p, _VP]),
@@ -233,6 +235,21 @@ class Simulation:
         self.np = par.np
         self.par = par.copy()
 
+    @classmethod
+    def load_checkpoint(cls, path, graph: bool = True, mixed: bool = False) -> "Simulation":
+        """A simulation restored from lq_sim_save_checkpoint's file (`mixed`
+        must match the saved form)."""
+        h = _VP()
+        flags = (LQ_SIM_GRAPH if graph else 0) | (LQ_SIM_MIXED if mixed else 0)
+        check(lib().lq_sim_load_checkpoint(os.fsencode(str(path)), flags, ctypes.byref(h)), "lq_sim_load_checkpoint")
+        self = cls.__new__(cls)
+        self.handle = h
+        with open(path, "rb") as f:
+            f.seek(48)           # magic, version, flags, step, time, skin, three counts
+            self.par = Parameters.from_bytes(f.read(ctypes.sizeof(Parameters)))
+        self.np = self.par.np
+        return self
+
     def close(self):
         if getattr(self, "handle", None):
             lib().lq_sim_destroy(self.handle)
@@ -318,6 +335,11 @@ class Simulation:
         c = _I()
         check(lib().lq_sim_rebuild_launches(self.handle, ctypes.byref(c)), "lq_sim_rebuild_launches")
         return c.value
+
+    def save_checkpoint(self, path):
+        """Binary checkpoint (state, FP64 copies, step, time, tables); the
+        run that continues and a run loaded from the file step identically."""
+        check(lib().lq_sim_save_checkpoint(self.handle, os.fsencode(str(path))), "lq_sim_save_checkpoint")
 
     def neighbor_entries(self):
         """(material, boundary) entries in the current neighbour lists."""

@@ -25,6 +25,8 @@
  * reads the flag before each step, which gives the same sequence of
  * rebuilds.  dt = cfl h / cs is constant, as in the reference.
  */
+#include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <vector>
 
@@ -59,6 +61,8 @@ struct LqSim {
     lqb::MaterialTable vw;             /* von Wolffersdorff rows (model 3) */
     float* rec = nullptr;              /* packed neighbour data, np x 13 floats */
     lqb::Frames fr;                    /* per-object grid rows (optional) */
+    std::vector<float> mt_host, vw_host; /* host copies of the tables, for checkpoints */
+    std::vector<int> fr_host;
     std::vector<void*> allocs;
     cudaGraphExec_t step_exec = nullptr;
     cudaGraphExec_t shep_exec = nullptr;
@@ -596,6 +600,7 @@ extern "C" int lq_sim_set_materials(void* sim, int n, const float* table)
     }
     S->mt.p = d;
     S->mt.n = n;
+    S->mt_host.assign(table, table + 5 * (size_t)n);
     LQ_TRY(build_graphs(S));
     return LQ_OK;
 }
@@ -621,6 +626,7 @@ extern "C" int lq_sim_set_hypoplastic(void* sim, int n, const float* table)
     LQ_TRY_CUDA(cudaMemcpy(d, table, sizeof(float) * 10 * (size_t)n, cudaMemcpyHostToDevice), "hypoplastic table");
     S->vw.p = d;
     S->vw.n = n;
+    S->vw_host.assign(table, table + 10 * (size_t)n);
     LQ_TRY(build_graphs(S));
     return LQ_OK;
 }
@@ -642,6 +648,7 @@ extern "C" int lq_sim_set_frames(void* sim, int n, const int* rows)
     }
     S->fr.rows = d;
     S->fr.n = n;
+    S->fr_host.assign(rows, rows + 2 * (size_t)n);
     LQ_TRY(set_flag(S, 1));
     LQ_TRY(build_graphs(S));
     return LQ_OK;
@@ -659,6 +666,200 @@ extern "C" int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard
     const int decide = S->conditional ? 1 : 0;
     if (plain) *plain = decide + 2 * stage;
     if (with_shepard) *with_shepard = decide + 2 * stage + (S->npm > 0 ? 2 : 0);
+    return LQ_OK;
+}
+
+/* ------------------------------------------------------------ checkpoints */
+/* Binary checkpoint, little-endian as written by this library:
+ *   "LQB200CK" | u32 version | u32 flags | i64 step | f64 time | f32 skin |
+ *   i32 np, npb, npm | Parameters (208 B) |
+ *   pospres, velrhop, idep (np x 16 B) | str, stn (np x 24 B) |
+ *   [mixed form: x and v+rho in FP64, np x 32 B each] |
+ *   i32 n + n x 5 f32 materials | i32 n + n x 10 f32 model-3 rows | i32 n + n x 2 i32 frames */
+namespace {
+
+constexpr char kCkMagic[8] = {'L', 'Q', 'B', '2', '0', '0', 'C', 'K'};
+constexpr uint32_t kCkVersion = 1;
+
+struct CkWriter {
+    FILE* f;
+    bool ok = true;
+    void put(const void* p, size_t n)
+    {
+        if (ok && n) ok = fwrite(p, 1, n, f) == n;
+    }
+    template <class T> void val(const T& v) { put(&v, sizeof(T)); }
+};
+
+struct CkReader {
+    const std::vector<char>& b;
+    size_t at = 0;
+    bool ok = true;
+    const char* take(size_t n)
+    {
+        if (!ok || b.size() - at < n) {
+            ok = false;
+            return nullptr;
+        }
+        const char* p = b.data() + at;
+        at += n;
+        return p;
+    }
+    template <class T> T val()
+    {
+        T v{};
+        if (const char* p = take(sizeof(T))) memcpy(&v, p, sizeof(T));
+        return v;
+    }
+};
+
+}  // namespace
+
+extern "C" int lq_sim_save_checkpoint(void* sim, const char* path)
+{
+    if (!sim || !path) return lqb::set_error(LQ_ERR_ARG, "lq_sim_save_checkpoint: null argument");
+    LqSim* S = static_cast<LqSim*>(sim);
+    const size_t n = (size_t)S->np;
+    std::vector<float> pos(4 * n), vel(4 * n), idep(4 * n), str(6 * n), stn(6 * n);
+    std::vector<double> xd, vd;
+    LQ_TRY(lq_sim_download(sim, pos.data(), vel.data(), idep.data(), str.data(), stn.data()));
+    if (S->S.xd) {
+        xd.resize(4 * n);
+        vd.resize(4 * n);
+        LQ_TRY_CUDA(cudaMemcpyAsync(xd.data(), S->S.xd, n * sizeof(double4), cudaMemcpyDeviceToHost, S->stream),
+                    "checkpoint x");
+        LQ_TRY_CUDA(cudaMemcpyAsync(vd.data(), S->S.vd, n * sizeof(double4), cudaMemcpyDeviceToHost, S->stream),
+                    "checkpoint v");
+        LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "checkpoint read");
+    }
+    FILE* f = fopen(path, "wb");
+    if (!f) return lqb::set_error(LQ_ERR_IO, "cannot write checkpoint %s", path);
+    CkWriter w{f};
+    w.put(kCkMagic, sizeof(kCkMagic));
+    w.val(kCkVersion);
+    w.val((uint32_t)S->flags);
+    w.val((int64_t)S->step);
+    w.val(S->time);
+    w.val(S->skin);
+    w.val((int32_t)S->np);
+    w.val((int32_t)S->npb);
+    w.val((int32_t)S->npm);
+    w.put(&S->ph, sizeof(Parameters));
+    for (auto* a : {&pos, &vel, &idep, &str, &stn}) w.put(a->data(), a->size() * sizeof(float));
+    if (!xd.empty()) {
+        w.put(xd.data(), xd.size() * sizeof(double));
+        w.put(vd.data(), vd.size() * sizeof(double));
+    }
+    w.val((int32_t)S->mt.n);
+    w.put(S->mt_host.data(), S->mt_host.size() * sizeof(float));
+    w.val((int32_t)S->vw.n);
+    w.put(S->vw_host.data(), S->vw_host.size() * sizeof(float));
+    w.val((int32_t)S->fr.n);
+    w.put(S->fr_host.data(), S->fr_host.size() * sizeof(int));
+    const bool ok = w.ok && fclose(f) == 0;
+    if (!ok) return lqb::set_error(LQ_ERR_IO, "write error on checkpoint %s", path);
+    /* the run that continues searches before its next step, as a run
+     * restarted from this file does, so both take identical steps */
+    return set_flag(S, 1);
+}
+
+extern "C" int lq_sim_load_checkpoint(const char* path, int flags, void** sim)
+{
+    if (!path || !sim) return lqb::set_error(LQ_ERR_ARG, "lq_sim_load_checkpoint: null argument");
+    *sim = nullptr;
+    std::vector<char> buf;
+    {
+        FILE* f = fopen(path, "rb");
+        if (!f) return lqb::set_error(LQ_ERR_IO, "cannot open checkpoint %s", path);
+        char chunk[1 << 16];
+        size_t got;
+        while ((got = fread(chunk, 1, sizeof(chunk), f)) > 0) buf.insert(buf.end(), chunk, chunk + got);
+        fclose(f);
+    }
+    CkReader r{buf};
+    const char* magic = r.take(sizeof(kCkMagic));
+    if (!magic || memcmp(magic, kCkMagic, sizeof(kCkMagic)) != 0)
+        return lqb::set_error(LQ_ERR_IO, "%s is not a LOQUAT-B200 checkpoint", path);
+    const uint32_t version = r.val<uint32_t>();
+    if (r.ok && version != kCkVersion)
+        return lqb::set_error(LQ_ERR_IO, "%s: checkpoint version %u, this library reads %u", path, version,
+                              kCkVersion);
+    const uint32_t saved_flags = r.val<uint32_t>();
+    const long long step = r.val<int64_t>();
+    const double time = r.val<double>();
+    const float skin = r.val<float>();
+    const int np = r.val<int32_t>(), npb = r.val<int32_t>(), npm = r.val<int32_t>();
+    Parameters par;
+    const char* pp = r.take(sizeof(Parameters));
+    if (!r.ok || np <= 0 || npb < 0 || npm < 0 || npb + npm != np)
+        return lqb::set_error(LQ_ERR_IO, "%s: truncated or inconsistent checkpoint header", path);
+    memcpy(&par, pp, sizeof(par));
+    if (par.np != np || par.npb != npb || par.npm != npm)
+        return lqb::set_error(LQ_ERR_IO, "%s: particle counts disagree with its Parameters", path);
+    if ((saved_flags & LQ_SIM_MIXED) != ((uint32_t)flags & LQ_SIM_MIXED))
+        return lqb::set_error(LQ_ERR_ARG, "%s was written by the %s form; load it with the same LQ_SIM_MIXED flag",
+                              path, (saved_flags & LQ_SIM_MIXED) ? "mixed-precision" : "plain FP32");
+    const size_t n = (size_t)np;
+    const float* arr[5];
+    const size_t width[5] = {4, 4, 4, 6, 6};
+    for (int k = 0; k < 5; ++k) arr[k] = reinterpret_cast<const float*>(r.take(width[k] * n * sizeof(float)));
+    const char* xd = nullptr;
+    const char* vd = nullptr;
+    if (saved_flags & LQ_SIM_MIXED) {
+        xd = r.take(n * sizeof(double4));
+        vd = r.take(n * sizeof(double4));
+    }
+    std::vector<float> mt, vw;
+    std::vector<int> fr;
+    const int nmt = r.val<int32_t>();
+    if (r.ok && nmt > 0)
+        if (const char* p = r.take(5 * (size_t)nmt * sizeof(float)))
+            mt.assign(reinterpret_cast<const float*>(p), reinterpret_cast<const float*>(p) + 5 * (size_t)nmt);
+    const int nvw = r.val<int32_t>();
+    if (r.ok && nvw > 0)
+        if (const char* p = r.take(10 * (size_t)nvw * sizeof(float)))
+            vw.assign(reinterpret_cast<const float*>(p), reinterpret_cast<const float*>(p) + 10 * (size_t)nvw);
+    const int nfr = r.val<int32_t>();
+    if (r.ok && nfr > 0)
+        if (const char* p = r.take(2 * (size_t)nfr * sizeof(int)))
+            fr.assign(reinterpret_cast<const int*>(p), reinterpret_cast<const int*>(p) + 2 * (size_t)nfr);
+    if (!r.ok || nmt < 0 || nvw < 0 || nfr < 0 || r.at != buf.size())
+        return lqb::set_error(LQ_ERR_IO, "%s: truncated or malformed checkpoint", path);
+
+    /* aligned copies of the state arrays (the file offsets are not) */
+    std::vector<float> a[5];
+    for (int k = 0; k < 5; ++k) a[k].assign(arr[k], arr[k] + width[k] * n);
+    void* out = nullptr;
+    LQ_TRY(lq_sim_create(&par, a[0].data(), a[1].data(), a[2].data(), a[3].data(), a[4].data(), flags, &out));
+    LqSim* S = static_cast<LqSim*>(out);
+    auto fail = [&](int st) {
+        lq_sim_destroy(out);
+        return st;
+    };
+    if (xd) {
+        std::vector<double> hx(4 * n), hv(4 * n);
+        memcpy(hx.data(), xd, n * sizeof(double4));
+        memcpy(hv.data(), vd, n * sizeof(double4));
+        cudaError_t e = cudaMemcpyAsync(S->S.xd, hx.data(), n * sizeof(double4), cudaMemcpyHostToDevice, S->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(S->S.vd, hv.data(), n * sizeof(double4), cudaMemcpyHostToDevice, S->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
+        if (e != cudaSuccess)
+            return fail(lqb::set_error(LQ_ERR_CUDA, "checkpoint FP64 state: %s", cudaGetErrorString(e)));
+    }
+    S->step = step;
+    S->time = time;
+    S->ph.time = (float)time;
+    int st = LQ_OK;
+    if (st == LQ_OK && nmt > 0) st = lq_sim_set_materials(out, nmt, mt.data());
+    if (st == LQ_OK && nvw > 0) st = lq_sim_set_hypoplastic(out, nvw, vw.data());
+    if (st == LQ_OK && nfr > 0) st = lq_sim_set_frames(out, nfr, fr.data());
+    if (st == LQ_OK && skin != S->skin) {
+        S->skin = skin;            /* as saved, not through skin / h */
+        st = build_graphs(S);
+    }
+    if (st != LQ_OK) return fail(st);
+    *sim = out;
     return LQ_OK;
 }
 

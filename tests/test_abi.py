@@ -254,3 +254,32 @@ def test_null_arguments_are_rejected_without_a_gpu(lq):
     assert L.lq_sim_step(None, 1) == lq.LQ_ERR_ARG
     assert b"bad argument" in L.lq_last_error()
     assert L.lq_status_string(lq.LQ_ERR_IO) == b"I/O error"
+
+
+def test_checkpoint_reader_rejects_foreign_and_truncated_files(lq, tmp_path):
+    """Checked before any device work, so this runs without a GPU."""
+    import ctypes
+    import struct
+
+    from loquat_b200 import cases
+
+    def load(path):
+        h = ctypes.c_void_p()
+        return lq.lib().lq_sim_load_checkpoint(str(path).encode(), 0, ctypes.byref(h)), h
+
+    f = tmp_path / "x.lqck"
+    f.write_bytes(b"not a checkpoint at all")
+    st, h = load(f)
+    assert st == lq.LQ_ERR_IO and "not a LOQUAT-B200 checkpoint" in lq.lib().lq_last_error().decode()
+    assert not h.value
+    c = cases.small_column(seed=1)
+    par = c.par
+    head = b"LQB200CK" + struct.pack("<IIqdfiii", 1, 0, 5, 0.5, 0.0, par.np, par.npb, par.npm) + par.to_bytes()
+    f.write_bytes(head + b"\0" * 100)                       # arrays cut short
+    st, _ = load(f)
+    assert st == lq.LQ_ERR_IO and "truncated" in lq.lib().lq_last_error().decode()
+    f.write_bytes(b"LQB200CK" + struct.pack("<I", 7))       # unknown version
+    st, _ = load(f)
+    assert st == lq.LQ_ERR_IO and "version 7" in lq.lib().lq_last_error().decode()
+    st, _ = load(tmp_path / "missing.lqck")
+    assert st == lq.LQ_ERR_IO
