@@ -192,6 +192,12 @@ int lq_sim_set_frames(void* sim, int n, const int* rows);
  * with the Shepard pass; a rebuild adds lq_sim_rebuild_launches more. */
 int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard);
 int lq_sim_rebuild_launches(void* sim, int* launches);
+/* Bounds violations counted so far in this process by a library built with
+ * -D LQ_CHECKED (loquat_b200/liblqb200_checked.so): its list and grid
+ * kernels check every index they gather or scatter through and skip and
+ * count a bad one instead of accessing memory.  -1 from the product
+ * library, which has no checks.  Synchronises the device. */
+int lq_debug_bounds_violations(long long* count);
 /* Checkpoints of a simulation: the state (with the FP64 copies of the
  * mixed form), step, time, skin and the per-object tables, in a binary file
  * of this library's own format.  Saving forces a neighbour search before the

@@ -74,6 +74,7 @@ _SIGNATURES = {
     "lq_sim_set_frames": (_I, [_VP, _I, _VP]),
     "lq_sim_rebuilds": (_I, [_VP, ctypes.POINTER(_LL)]),
     "lq_sim_rebuild_launches": (_I, [_VP, ctypes.POINTER(_I)]),
+    "lq_debug_bounds_violations": (_I, [ctypes.POINTER(_LL)]),
     "lq_sim_save_checkpoint": (_I, [_VP, ctypes.c_char_p]),
     "lq_sim_load_checkpoint": (_I, [ctypes.c_char_p, _I, ctypes.POINTER(_VP)]),
     "lq_sim_neighbor_entries": (_I, [_VP, ctypes.POINTER(_LL), ctypes.POINTER(_LL)]),
@@ -400,3 +401,11 @@ def save_vtu(directory, output_number: int, pospres, velrhop, idep, str_, stn) -
     arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (pospres, velrhop, idep, str_, stn)]
     check(lib().lq_io_save_vtu(os.fsencode(str(directory)), output_number, arrs[0].shape[0],
                                *[a.ctypes.data for a in arrs]), "lq_io_save_vtu")
+
+
+def bounds_violations() -> int:
+    """Index-bounds violations counted by a bounds-checked build of the
+    library (loaded through LOQUAT_B200_LIB); -1 for the product build."""
+    c = _LL()
+    check(lib().lq_debug_bounds_violations(ctypes.byref(c)), "lq_debug_bounds_violations")
+    return c.value

@@ -49,8 +49,8 @@ def _stale(obj: Path, src: Path, hdr_mtime: float) -> bool:
     return m < src.stat().st_mtime or m < hdr_mtime
 
 
-def _compile(src: Path, ptxas_verbose: bool, extra=()) -> tuple[Path, str]:
-    obj = BUILD / (src.name + ".o")
+def _compile(src: Path, ptxas_verbose: bool, extra=(), build_dir: Path = BUILD) -> tuple[Path, str]:
+    obj = build_dir / (src.name + ".o")
     cmd = [NVCC, *ARCH, *COMMON, *extra, "-c", str(src), "-o", str(obj)]
     if ptxas_verbose and src.suffix == ".cu":
         cmd += ["-Xptxas", "-v"]
@@ -64,23 +64,23 @@ def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = True, 
           build_dir: Path | None = None) -> Path:
     """Compile and link the library; returns its path.  `defines` adds -D
     options and `out`/`build_dir` place a variant build elsewhere."""
-    global BUILD, LIB
+    bdir, lib = BUILD, LIB
     if out is not None:
-        BUILD, LIB = Path(build_dir or Path(out).parent / "_build"), Path(out)
-    BUILD.mkdir(parents=True, exist_ok=True)
+        bdir, lib = Path(build_dir or Path(out).parent / "_build"), Path(out)
+    bdir.mkdir(parents=True, exist_ok=True)
     extra = [f"-D{d}" for d in defines]
     hdr_mtime = max((h.stat().st_mtime for h in _headers()), default=0.0)
     srcs = _sources()
-    todo = [s for s in srcs if force or ptxas_verbose or _stale(BUILD / (s.name + ".o"), s, hdr_mtime)]
+    todo = [s for s in srcs if force or ptxas_verbose or _stale(bdir / (s.name + ".o"), s, hdr_mtime)]
     reports = []
     if todo:
         with cf.ThreadPoolExecutor(max_workers=min(8, len(todo))) as ex:
-            for obj, err in ex.map(lambda s: _compile(s, ptxas_verbose, extra), todo):
+            for obj, err in ex.map(lambda s: _compile(s, ptxas_verbose, extra, bdir), todo):
                 if err.strip():
                     reports.append((obj.name, err))
-    objs = [BUILD / (s.name + ".o") for s in srcs]
-    if force or todo or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
-        cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-cudart", "static"]
+    objs = [bdir / (s.name + ".o") for s in srcs]
+    if force or todo or not lib.exists() or lib.stat().st_mtime < max(o.stat().st_mtime for o in objs):
+        cmd = [NVCC, *ARCH, "-shared", "-o", str(lib), *map(str, objs), "-cudart", "static"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
@@ -89,7 +89,19 @@ def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = True, 
     if not quiet or ptxas_verbose:
         for name, err in reports:
             print(f"== {name}\n{err}", file=sys.stderr)
-    return LIB
+    return lib
+
+
+CHECKED_LIB = PKG / "liblqb200_checked.so"
+
+
+def build_checked(force: bool = False) -> Path:
+    """The bounds-checked variant (-D LQ_CHECKED): every index the list and
+    grid kernels gather or scatter through is checked before the access and
+    a violation is counted (lq_debug_bounds_violations) instead of made.
+    It stands in for a device memory checker.  Loaded in place of the
+    product library by setting LOQUAT_B200_LIB to its path."""
+    return build(force=force, defines=["LQ_CHECKED"], out=CHECKED_LIB, build_dir=PKG / "_build_checked")
 
 
 def build_app(force: bool = False) -> Path:

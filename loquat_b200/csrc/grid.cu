@@ -91,6 +91,7 @@ __global__ void __launch_bounds__(kBlock) k_scatter(int np, const int* __restric
     if (i >= np) return;
     const int k = key[i];
     const int d = __ldg(start + k) + rank[i];
+    if (!lq_in_range(d, np)) return;
     part_idx[d] = i;
     part_cel[d] = k;
 }
@@ -126,7 +127,9 @@ __global__ void __launch_bounds__(kBlock) k_gather_f4(int n, const int* __restri
                                                       float4* __restrict__ out)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = __ldg(in + __ldg(idx + i));
+    if (i >= n) return;
+    const int j = __ldg(idx + i);
+    if (lq_in_range(j, n)) out[i] = __ldg(in + j);
 }
 
 /* tensor2d as three float2 words: consecutive threads write consecutive words. */
@@ -137,7 +140,8 @@ __global__ void __launch_bounds__(kBlock) k_gather_t2(int n, const int* __restri
     if (t >= 3LL * n) return;
     const int i = (int)(t / 3);
     const int w = (int)(t - 3LL * i);
-    out[t] = __ldg(in + 3LL * __ldg(idx + i) + w);
+    const int j = __ldg(idx + i);
+    if (lq_in_range(j, n)) out[t] = __ldg(in + 3LL * j + w);
 }
 
 __global__ void __launch_bounds__(kBlock) k_gather_state(int n, const int* __restrict__ idx, State in, State out)
@@ -145,6 +149,7 @@ __global__ void __launch_bounds__(kBlock) k_gather_state(int n, const int* __res
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int j = __ldg(idx + i);
+    if (!lq_in_range(j, n)) return;
     out.pos[i] = __ldg(in.pos + j);
     out.vel[i] = __ldg(in.vel + j);
     out.idep[i] = __ldg(in.idep + j);
@@ -227,6 +232,18 @@ int gather_tensor2d(int n, const int* idx, const tensor2d* in, tensor2d* out, cu
     k_gather_t2<<<blocks_for(3LL * n), kBlock, 0, s>>>(n, idx, reinterpret_cast<const float2*>(in),
                                                         reinterpret_cast<float2*>(out));
     LQ_TRY_CUDA(cudaGetLastError(), "k_gather_t2");
+    return LQ_OK;
+}
+
+/* This translation unit's count of bounds violations (always 0 without
+ * LQ_CHECKED). */
+int bounds_count_grid(unsigned long long* v)
+{
+#ifdef LQ_CHECKED
+    LQ_TRY_CUDA(cudaMemcpyFromSymbol(v, lq_bounds_count, sizeof(*v)), "bounds counter");
+#else
+    *v = 0;
+#endif
     return LQ_OK;
 }
 

@@ -10,6 +10,23 @@
 
 namespace lqb {
 
+/* Bounds-checked builds (-D LQ_CHECKED): the list and grid kernels check
+ * every index they gather or scatter through before the access; a
+ * violation is counted in this translation unit's counter and the access is
+ * skipped.  This stands in for a device memory checker.  In the product
+ * build the check is a constant true and compiles away. */
+#ifdef LQ_CHECKED
+static __device__ unsigned long long lq_bounds_count;
+__device__ __forceinline__ bool lq_in_range(long long j, long long n)
+{
+    if (j >= 0 && j < n) return true;
+    atomicAdd(&lq_bounds_count, 1ull);
+    return false;
+}
+#else
+__device__ __forceinline__ constexpr bool lq_in_range(long long, long long) { return true; }
+#endif
+
 /* 8-byte accesses of a 24-byte tensor2d (the widest aligned access). */
 __device__ __forceinline__ tensor2d load_t2(const tensor2d* p, int i)
 {

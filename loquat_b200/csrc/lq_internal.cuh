@@ -99,6 +99,10 @@ struct GridBuffers {
 
 /* Sizes the scan scratch for n_cells + 1 entries. */
 int scan_scratch_bytes(int ncell, size_t* bytes);
+/* Bounds violations counted by the grid and the neighbour kernels of a
+ * bounds-checked build (-D LQ_CHECKED); 0 otherwise. */
+int bounds_count_grid(unsigned long long* v);
+int bounds_count_sph(unsigned long long* v);
 
 /* Hash, count, scan, scatter and in-cell ordering: a stable sort of the
  * particles by cell key.  Writes key, rank, count, start, part_idx,

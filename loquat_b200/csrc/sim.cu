@@ -30,6 +30,8 @@
 #include <cstring>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "lq_internal.cuh"
 
 namespace {
@@ -472,6 +474,10 @@ extern "C" int lq_sim_step(void* sim, int nsteps)
     if (S->ph.constitutive_model == 3 && S->vw.n == 0)
         return lqb::set_error(LQ_ERR_ARG, "lq_sim_step: constitutive model 3 needs lq_sim_set_hypoplastic first");
     const int N = S->ph.stress_shepard_filter;
+    nvtxRangePushA(S->step_exec ? "lq/steps (graph)" : "lq/steps (eager)");
+    struct PopRange {
+        ~PopRange() { nvtxRangePop(); }
+    } pop_range;
     for (int k = 0; k < nsteps; ++k) {
         S->ph.time = (float)S->time;
         if (S->step_exec) {
@@ -899,6 +905,11 @@ namespace {
  * (reference include/types.h:158-173, src/loquat.cu:345-395) with the
  * search and the list build split out. */
 enum { PH_SEARCH = 0, PH_GATHER, PH_ADAMI, PH_INTERACTION, PH_INTEGRATE, PH_SHEPARD, PH_LIST, PH_COUNT };
+/* NVTX range names of the phases (host ranges around each phase's
+ * launches; a tool such as ncu can select kernels by them with
+ * --nvtx --nvtx-include "lq/interaction/") */
+const char* const kPhaseNames[PH_COUNT] = {"lq/search", "lq/gather", "lq/adami", "lq/interaction",
+                                           "lq/integrate", "lq/shepard", "lq/list"};
 
 struct PhaseTimer {
     std::vector<cudaEvent_t> ev;
@@ -908,12 +919,14 @@ struct PhaseTimer {
     {
         if (used + 2 > (int)ev.size()) return lqb::set_error(LQ_ERR_ARG, "profile: event pool exhausted");
         phase.push_back(ph);
+        nvtxRangePushA(kPhaseNames[ph]);
         LQ_TRY_CUDA(cudaEventRecord(ev[used], s), "profile event");
         used += 1;
         return LQ_OK;
     }
     int close(cudaStream_t s)
     {
+        nvtxRangePop();
         LQ_TRY_CUDA(cudaEventRecord(ev[used], s), "profile event");
         used += 1;
         return LQ_OK;

@@ -353,6 +353,7 @@ __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __re
     const PairConst K = load_pair_const(P);
     const int nx = __ldg(&P->cell_num_x), ny = __ldg(&P->cell_num_y), nz = __ldg(&P->cell_num_z);
     const int L = __ldg(&P->ncell_one_layer);
+    const int np_all = __ldg(&P->np);
     const float4 xi = active ? __ldg(pos + i) : make_float4(0.f, 0.f, 0.f, 0.f);
     int* my_stage = &stage[w][0][lane];
 
@@ -397,6 +398,7 @@ __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __re
                 if (X < 0 || X >= nx || Y < 0 || Y >= ny) continue;
                 int s, e;
                 if (!zrun_range(cells, off + (X * ny + Y) * nz, zlo, zhi, s, e)) continue;
+                if (!lq_in_range(s, np_all) || !lq_in_range(e - 1, np_all)) continue;
                 int j = s;
                 for (; j + kUnroll <= e; j += kUnroll) {
                     if (__any_sync(FULL, staged > kStage - kUnroll)) flush();
@@ -451,7 +453,7 @@ __global__ void __launch_bounds__(kBlock, LQ_PAIR_MIN_BLOCKS) k_interaction_list
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                if (k + u < n) pair_body<kKahan>(K, st, T, cur[u]);
+                if (k + u < n && lq_in_range(cur[u], np)) pair_body<kKahan>(K, st, T, cur[u]);
         }
     } else {
         walk_stencil(P, K, st, cells, i, T.x, [&](int j) { pair_body<kKahan>(K, st, T, j); }, fr);
@@ -503,7 +505,7 @@ __global__ void __launch_bounds__(kBlock, LQ_PAIR_MIN_BLOCKS) k_interaction_rec(
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                if (k + u < n) pair_body_rec<kKahan>(K, nb, T, cur[u]);
+                if (k + u < n && lq_in_range(cur[u], np)) pair_body_rec<kKahan>(K, nb, T, cur[u]);
         }
     } else {
         walk_stencil(P, K, st, cells, i, T.x, [&](int j) { pair_body<kKahan>(K, st, T, j); }, fr);
@@ -662,8 +664,10 @@ __global__ void __launch_bounds__(kBlock) k_adami_list(const Parameters* __restr
     const float4 xi = __ldg(st.pos + i);
     tensor2d S = make_tensor2d(0.0f);
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int np_all = __ldg(&P->np);
     for (int k = 0; k < n; ++k) {
         const int j = __ldg(list + (size_t)k * stride + i);
+        if (!lq_in_range(j, np_all)) continue;
         const float4 xj = __ldg(st.pos + j);
         const float3 d = make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
         const float q = norm3df(d.x, d.y, d.z) * ih;
@@ -714,7 +718,7 @@ __global__ void __launch_bounds__(kBlock) k_shepard_list(const Parameters* __res
     tensor2d S = make_tensor2d(0.0f);
     float w = 0.0f;
     auto add = [&](int j) {
-        if (j < npb) return;
+        if (j < npb || !lq_in_range(j, np)) return;
         const float4 xj = __ldg(st.pos + j);
         const float3 d = make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
         const float q = norm3df(d.x, d.y, d.z) * ih;
@@ -750,6 +754,18 @@ __global__ void __launch_bounds__(kBlock) k_shepard_list(const Parameters* __res
 }
 
 }  // namespace
+
+/* This translation unit's count of bounds violations (always 0 without
+ * LQ_CHECKED). */
+int bounds_count_sph(unsigned long long* v)
+{
+#ifdef LQ_CHECKED
+    LQ_TRY_CUDA(cudaMemcpyFromSymbol(v, lq_bounds_count, sizeof(*v)), "bounds counter");
+#else
+    *v = 0;
+#endif
+    return LQ_OK;
+}
 
 int launch_interaction(const Parameters* ph, const Parameters* pd, const State& st, const Rates& r, const Cells& c,
                        cudaStream_t s)
@@ -955,4 +971,19 @@ void StressRegularization(Parameters* par_host, Parameters* par_device, float4* 
     check_or_die(lq_stress_regularization(par_host, par_device, (const float*)pospres, (const float*)velrhop,
                                           (float*)str, (float*)tensor2d_cache, cell_beg, cell_end, nullptr),
                  "StressRegularization");
+}
+
+extern "C" int lq_debug_bounds_violations(long long* count)
+{
+    if (!count) return lqb::set_error(LQ_ERR_ARG, "lq_debug_bounds_violations: null argument");
+#ifdef LQ_CHECKED
+    LQ_TRY_CUDA(cudaDeviceSynchronize(), "bounds counter");
+    unsigned long long a = 0, b = 0;
+    LQ_TRY(lqb::bounds_count_sph(&a));
+    LQ_TRY(lqb::bounds_count_grid(&b));
+    *count = (long long)(a + b);
+#else
+    *count = -1;
+#endif
+    return LQ_OK;
 }

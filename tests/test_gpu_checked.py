@@ -1,0 +1,60 @@
+"""The bounds-checked build (-D LQ_CHECKED, loquat_b200/liblqb200_checked.so)
+stands in for a device memory checker: its list and grid kernels check every
+index they gather or scatter through.  Runs of the native driver (both
+precision forms, Shepard passes and list rebuilds, a batched ensemble with
+frames, the von Wolffersdorff model) must
+count no violation.  Each run is a child process that loads the checked
+library in place of the product one."""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+ROOT = Path(__file__).resolve().parents[1]
+CHECKED = ROOT / "loquat_b200" / "liblqb200_checked.so"
+
+SCRIPT = r"""
+import numpy as np
+import loquat_b200 as lq
+from loquat_b200 import cases
+c = cases.small_column(velocity_noise=0.3, shepard=7, seed=61)
+for mixed in (False, True):
+    s = lq.Simulation(c.par, *c.arrays(), mixed=mixed)
+    s.step(60)
+    assert s.rebuilds() >= 2
+    assert not s.health().any()
+comb, _ = cases.ensemble(n=4, count_range=(1.5e3, 4.0e3), seed=13, shepard=7)
+s = lq.Simulation(comb.par, *comb.arrays())
+s.set_materials(comb.meta["materials"])
+s.set_frames(comb.meta["frames"])
+s.step(30)
+v = cases.small_column(model=3, velocity_noise=0.05, shepard=7, seed=62)
+s = lq.Simulation(v.par, *v.arrays(), mixed=True)
+s.set_hypoplastic(v.meta["hypoplastic"])
+s.step(20)
+print("VIOLATIONS", lq.bounds_violations())
+"""
+
+
+def run_child(lib):
+    env = dict(os.environ, LOQUAT_B200_LIB=str(lib), PYTHONPATH=str(ROOT))
+    r = subprocess.run([sys.executable, "-c", SCRIPT], capture_output=True, text=True, env=env, timeout=600,
+                       cwd=ROOT)
+    assert r.returncode == 0, r.stdout + r.stderr
+    line = [l for l in r.stdout.splitlines() if l.startswith("VIOLATIONS")][-1]
+    return int(line.split()[1])
+
+
+def test_checked_build_counts_no_bounds_violation(cuda):
+    if not CHECKED.exists():
+        pytest.fail("checked library not built: python -c 'import __graft_entry__ as g; g.build()'")
+    assert run_child(CHECKED) == 0
+
+
+def test_product_build_reports_no_checks(cuda):
+    assert run_child(ROOT / "loquat_b200" / "liblqb200.so") == -1
