@@ -128,6 +128,19 @@ int lq_corrector(const void* par_host, const void* par_device,
                               density accumulation and FP64 stress updates in
                               the integrator, compensated sums in the
                               interaction; the neighbour kernels read FP32 */
+/* Features the reference reads from its parameter file but never applies
+ * (density-shepard-filter, src/loquat_io.cu:180; dynamic-time-step,
+ * src/loquat.cu:325-333).  Off unless asked for here, so a case behaves as
+ * in the reference whatever its file says. */
+#define LQ_SIM_DENSITY_FILTER 4  /* every density_shepard_filter steps (> 0),
+                                    after the stress filter: rho_i =
+                                    sum m W / sum (m/rho_j) W over the material
+                                    layer, self included */
+#define LQ_SIM_DYNAMIC_DT     8  /* after each step, dt = cfl min(h / (cs +
+                                    v_max), sqrt(h / a_max)) over the material
+                                    particles (never above cfl h / cs); the
+                                    time then lives on the device and
+                                    lq_sim_clock synchronises to read it */
 
 /* Creates a simulation from host arrays (np = par->np particles, boundary
  * first).  par must have been through lq_initialize_parameters.  The state
@@ -204,7 +217,7 @@ int lq_debug_bounds_violations(long long* count);
  * simulation's next step, so a simulation loaded from the file with the same
  * precision form and the run that continues take bit-identical steps.
  * lq_sim_load_checkpoint creates the simulation (flags as for
- * lq_sim_create; LQ_SIM_MIXED must match the saved form).  The reference
+ * lq_sim_create; every flag but LQ_SIM_GRAPH must match the saved run's).  The reference
  * restarts from its output XML and particle file instead, which round to
  * float text and drop the void ratio. */
 int lq_sim_save_checkpoint(void* sim, const char* path);

@@ -25,6 +25,8 @@ _lib = None
 LQ_OK, LQ_ERR_ARG, LQ_ERR_CUDA, LQ_ERR_ALLOC, LQ_ERR_IO, LQ_ERR_STATE, LQ_ERR_NOTFOUND = range(7)
 LQ_SIM_GRAPH = 1
 LQ_SIM_MIXED = 2
+LQ_SIM_DENSITY_FILTER = 4
+LQ_SIM_DYNAMIC_DT = 8
 
 
 class LoquatError(RuntimeError):
@@ -223,13 +225,22 @@ class Grid:
         check(lib().lq_grid_sort_tensor2d(self.handle, n, ptr(data), ptr(cache), stream), "lq_grid_sort_tensor2d")
 
 
+def _sim_flags(graph, mixed, density_filter, dynamic_dt) -> int:
+    return ((LQ_SIM_GRAPH if graph else 0) | (LQ_SIM_MIXED if mixed else 0)
+            | (LQ_SIM_DENSITY_FILTER if density_filter else 0) | (LQ_SIM_DYNAMIC_DT if dynamic_dt else 0))
+
+
 class Simulation:
     """Whole-step driver (lq_sim_*): the hot loop of reference src/loquat.cu:322-409."""
 
-    def __init__(self, par: Parameters, pospres, velrhop, idep, str_, stn, graph: bool = True, mixed: bool = False):
+    def __init__(self, par: Parameters, pospres, velrhop, idep, str_, stn, graph: bool = True, mixed: bool = False,
+                 density_filter: bool = False, dynamic_dt: bool = False):
+        """density_filter / dynamic_dt switch on the density Shepard filter
+        (every par.density_shepard_filter steps) and the dynamic time step,
+        which the reference declares but never applies."""
         arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (pospres, velrhop, idep, str_, stn)]
         h = _VP()
-        flags = (LQ_SIM_GRAPH if graph else 0) | (LQ_SIM_MIXED if mixed else 0)
+        flags = _sim_flags(graph, mixed, density_filter, dynamic_dt)
         check(lib().lq_sim_create(ctypes.byref(par), *[a.ctypes.data for a in arrs], flags, ctypes.byref(h)),
               "lq_sim_create")
         self.handle = h
@@ -237,11 +248,12 @@ class Simulation:
         self.par = par.copy()
 
     @classmethod
-    def load_checkpoint(cls, path, graph: bool = True, mixed: bool = False) -> "Simulation":
-        """A simulation restored from lq_sim_save_checkpoint's file (`mixed`
-        must match the saved form)."""
+    def load_checkpoint(cls, path, graph: bool = True, mixed: bool = False, density_filter: bool = False,
+                        dynamic_dt: bool = False) -> "Simulation":
+        """A simulation restored from lq_sim_save_checkpoint's file (every
+        option but `graph` must match the saved run's)."""
         h = _VP()
-        flags = (LQ_SIM_GRAPH if graph else 0) | (LQ_SIM_MIXED if mixed else 0)
+        flags = _sim_flags(graph, mixed, density_filter, dynamic_dt)
         check(lib().lq_sim_load_checkpoint(os.fsencode(str(path)), flags, ctypes.byref(h)), "lq_sim_load_checkpoint")
         self = cls.__new__(cls)
         self.handle = h

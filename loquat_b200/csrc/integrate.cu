@@ -152,6 +152,7 @@ struct VerletCheck {
     const float4* xbuild;
     int* rebuild;
     float half_skin;
+    float dt_bound;   /* the largest step the next one can take */
 };
 
 template <bool kMixed, bool kVW>
@@ -270,7 +271,8 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(
         const float accel = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
         /* next step: the predictor half step and the corrector full step
          * move a particle by at most dt |v| + dt^2 |a| each; 2x covers both */
-        const float ahead = 2.0f * dt * (speed + dt * accel);
+        const float dtb = verlet.dt_bound;
+        const float ahead = 2.0f * dtb * (speed + dtb * accel);
         if (!(moved + ahead < verlet.half_skin)) atomicOr(verlet.rebuild, 1);
     }
 }
@@ -307,7 +309,7 @@ int launch_correct(const Parameters* ph, const Parameters* pd, const State& cur,
     if (ph->constitutive_model == 3)
         return set_error(LQ_ERR_ARG, "corrector: constitutive model 3 needs a von Wolffersdorff table");
     k_correct<false, false><<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, ini_idx, cur, r, health,
-                                                             VerletCheck{nullptr, nullptr, 0.0f}, ph->npb,
+                                                             VerletCheck{nullptr, nullptr, 0.0f, 0.0f}, ph->npb,
                                                              MaterialTable(), MaterialTable());
     LQ_TRY_CUDA(cudaGetLastError(), "k_correct");
     return LQ_OK;
@@ -320,7 +322,8 @@ int launch_correct_into(const Parameters* ph, const Parameters* pd, const State&
     if (ph->np <= 0) return LQ_OK;
     if (ph->constitutive_model == 3 && (!vw.p || vw.n <= 0))
         return set_error(LQ_ERR_ARG, "corrector: constitutive model 3 needs a von Wolffersdorff table");
-    const VerletCheck vc{xbuild, rebuild, 0.5f * skin};
+    /* a dynamic step never exceeds the fixed one, cfl h / cs (ph->dt) */
+    const VerletCheck vc{xbuild, rebuild, 0.5f * skin, ph->dt};
     const bool vwm = ph->constitutive_model == 3;
     const int nb = blocks_for(ph->np, kBlock);
     if (cur.xd && ini.xd && out.xd) {

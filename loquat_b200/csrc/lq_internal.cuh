@@ -169,6 +169,10 @@ int launch_adami_list(const Parameters* par_host, const Parameters* par_dev, con
                       cudaStream_t s);
 int launch_shepard_list(const Parameters* par_host, const Parameters* par_dev, const State& st, tensor2d* out_str,
                         const NeighborList& nl, cudaStream_t s);
+/* Density Shepard filter of material slots into rho_out[npb, np) over the
+ * material lists. */
+int launch_density_filter_list(const Parameters* par_host, const Parameters* par_dev, const State& st,
+                               float* rho_out, const NeighborList& nl, cudaStream_t s);
 /* Neighbour lists of targets [first, first + n) from grid layers
  * layer_lo..1 with cut-off radius `cut` (2h plus skin); list overflows are
  * counted in health[HEALTH_NBR_OVERFLOW]. */

@@ -62,6 +62,9 @@ struct LqSim {
     lqb::MaterialTable mt;             /* per-object materials (optional) */
     lqb::MaterialTable vw;             /* von Wolffersdorff rows (model 3) */
     float* rec = nullptr;              /* packed neighbour data, np x 13 floats */
+    float* rho_f = nullptr;            /* density filter output (LQ_SIM_DENSITY_FILTER) */
+    unsigned* vmax2 = nullptr;         /* max |v|^2, |a|^2 bits (LQ_SIM_DYNAMIC_DT) */
+    double* dtime = nullptr;           /* device-side time (LQ_SIM_DYNAMIC_DT) */
     lqb::Frames fr;                    /* per-object grid rows (optional) */
     std::vector<float> mt_host, vw_host; /* host copies of the tables, for checkpoints */
     std::vector<int> fr_host;
@@ -171,6 +174,55 @@ __global__ void k_decide(cudaGraphConditionalHandle h, int* flag, int* count)
 
 inline int blocks(int n) { return (n + 255) / 256; }
 
+/* Density filter result into the state (and the FP64 copy of the mixed form). */
+__global__ void k_set_density(int npb, int npm, const float* __restrict__ rho, float4* __restrict__ vel,
+                              double4* __restrict__ vd)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= npm) return;
+    const int i = npb + t;
+    const float r = rho[i];
+    vel[i].w = r;
+    if (vd) vd[i].w = (double)r;
+}
+
+/* Largest |v|^2 and |a|^2 over the material particles: non-negative floats
+ * order like their bit patterns, so an unsigned atomicMax reduces them. */
+__global__ void k_dt_max(int npb, int npm, const float4* __restrict__ vel, const float4* __restrict__ accad,
+                         unsigned* __restrict__ m2)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    float v2 = 0.0f, a2 = 0.0f;
+    if (t < npm) {
+        const float4 v = vel[npb + t], a = accad[npb + t];
+        v2 = v.x * v.x + v.y * v.y + v.z * v.z;
+        a2 = a.x * a.x + a.y * a.y + a.z * a.z;
+        if (!(v2 >= 0.0f)) v2 = 0.0f;   /* non-finite values are the health word's business */
+        if (!(a2 >= 0.0f)) a2 = 0.0f;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        v2 = fmaxf(v2, __shfl_xor_sync(0xffffffffu, v2, o));
+        a2 = fmaxf(a2, __shfl_xor_sync(0xffffffffu, a2, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(m2, __float_as_uint(v2));
+        atomicMax(m2 + 1, __float_as_uint(a2));
+    }
+}
+
+/* time += the step just taken; dt of the next step from the maxima;
+ * maxima cleared for the next reduction. */
+__global__ void k_dt_update(Parameters* P, unsigned* m2, double* time)
+{
+    const float v = sqrtf(__uint_as_float(m2[0])), a = sqrtf(__uint_as_float(m2[1]));
+    *time += (double)P->dt;
+    float dt = P->h / (P->cs + v);
+    if (a > 0.0f) dt = fminf(dt, sqrtf(P->h / a));
+    P->dt = P->cfl * dt;
+    m2[0] = 0u;
+    m2[1] = 0u;
+}
+
 /* ------------------------------------------------------------ sequences */
 
 /* Search, sort and list build; leaves the state in S with fresh lists. */
@@ -191,6 +243,31 @@ int enqueue_rebuild(LqSim* S, cudaStream_t s)
     return LQ_OK;
 }
 
+/* Dynamic time step (LQ_SIM_DYNAMIC_DT): the next step's dt into the
+ * device Parameters, the time advanced on the device. */
+int enqueue_dynamic_dt(LqSim* S, cudaStream_t s)
+{
+    if (!(S->flags & LQ_SIM_DYNAMIC_DT)) return LQ_OK;
+    if (S->npm > 0) {
+        k_dt_max<<<blocks(S->npm), 256, 0, s>>>(S->npb, S->npm, S->S.vel, S->R.accad, S->vmax2);
+        LQ_TRY_CUDA(cudaGetLastError(), "k_dt_max");
+    }
+    k_dt_update<<<1, 1, 0, s>>>(S->pd, S->vmax2, S->dtime);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_dt_update");
+    return LQ_OK;
+}
+
+/* Density Shepard filter (LQ_SIM_DENSITY_FILTER) on the lists. */
+int enqueue_density_filter(LqSim* S, cudaStream_t s)
+{
+    LQ_TRY(lqb::launch_density_filter_list(&S->ph, S->pd, S->S, S->rho_f, S->nlm, s));
+    if (S->npm > 0) {
+        k_set_density<<<blocks(S->npm), 256, 0, s>>>(S->npb, S->npm, S->rho_f, S->S.vel, S->S.vd);
+        LQ_TRY_CUDA(cudaGetLastError(), "k_set_density");
+    }
+    return LQ_OK;
+}
+
 /* The two stages of a step on the current lists. */
 int enqueue_stages(LqSim* S, cudaStream_t s)
 {
@@ -208,7 +285,7 @@ int enqueue_stages(LqSim* S, cudaStream_t s)
                                         S->rec));
     LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild, S->skin, s,
                                     S->mt, S->vw));
-    return LQ_OK;
+    return enqueue_dynamic_dt(S, s);
 }
 
 /* Shepard stress filter (reference src/loquat.cu:400-409) on the lists. */
@@ -394,6 +471,11 @@ int create(LqSim* S, const Parameters* par, const float* pos, const float* vel, 
     LQ_TRY(alloc_state(S, S->T));
     const size_t n = (size_t)S->np;
     LQ_TRY(dev_alloc(S, (void**)&S->xbuild, n * sizeof(float4)));
+    if (S->flags & LQ_SIM_DENSITY_FILTER) LQ_TRY(dev_alloc(S, (void**)&S->rho_f, n * sizeof(float)));
+    if (S->flags & LQ_SIM_DYNAMIC_DT) {
+        LQ_TRY(dev_alloc(S, (void**)&S->vmax2, 2 * sizeof(unsigned)));
+        LQ_TRY(dev_alloc(S, (void**)&S->dtime, sizeof(double)));
+    }
 #ifndef LQ_NO_NBR_RECORD
     LQ_TRY(dev_alloc(S, (void**)&S->rec, n * 13 * sizeof(float)));   /* cudaMalloc: 256-byte aligned */
 #endif
@@ -431,6 +513,11 @@ int create(LqSim* S, const Parameters* par, const float* pos, const float* vel, 
                 "upload Parameters");
     LQ_TRY(upload(S, pos, vel, idep, str, stn, S->S));
     LQ_TRY(widen(S));
+    if (S->flags & LQ_SIM_DYNAMIC_DT) {
+        LQ_TRY_CUDA(cudaMemsetAsync(S->vmax2, 0, 2 * sizeof(unsigned), S->stream), "dt maxima");
+        LQ_TRY_CUDA(cudaMemcpyAsync(S->dtime, &S->time, sizeof(double), cudaMemcpyHostToDevice, S->stream),
+                    "device time");
+    }
     /* the first step searches and sorts (reference src/loquat.cu:297-298) */
     LQ_TRY(set_flag(S, 1));
     LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "sim create");
@@ -492,7 +579,10 @@ extern "C" int lq_sim_step(void* sim, int nsteps)
                 LQ_TRY(enqueue_shepard(S, S->stream));
             }
         }
-        S->time += (double)S->ph.dt;
+        const int Nd = S->ph.density_shepard_filter;
+        if ((S->flags & LQ_SIM_DENSITY_FILTER) && Nd > 0 && S->step % Nd == 0 && S->step != 0)
+            LQ_TRY(enqueue_density_filter(S, S->stream));
+        S->time += (double)S->ph.dt;   /* the fixed step; the device keeps the time of dynamic steps */
         S->step++;
     }
     return LQ_OK;
@@ -555,7 +645,14 @@ extern "C" int lq_sim_clock(void* sim, long long* step, double* time)
     if (!sim) return lqb::set_error(LQ_ERR_ARG, "lq_sim_clock: null sim");
     LqSim* S = static_cast<LqSim*>(sim);
     if (step) *step = S->step;
-    if (time) *time = S->time;
+    if (time) {
+        *time = S->time;
+        if (S->flags & LQ_SIM_DYNAMIC_DT) {
+            LQ_TRY_CUDA(cudaMemcpyAsync(time, S->dtime, sizeof(double), cudaMemcpyDeviceToHost, S->stream),
+                        "device time");
+            LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "device time");
+        }
+    }
     return LQ_OK;
 }
 
@@ -670,8 +767,9 @@ extern "C" int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard
      * adds the filter and its copy */
     const int stage = (S->npb > 0 ? 1 : 0) + (S->rec ? 2 : 1) + 1;
     const int decide = S->conditional ? 1 : 0;
-    if (plain) *plain = decide + 2 * stage;
-    if (with_shepard) *with_shepard = decide + 2 * stage + (S->npm > 0 ? 2 : 0);
+    const int dyn = (S->flags & LQ_SIM_DYNAMIC_DT) ? (S->npm > 0 ? 2 : 1) : 0;
+    if (plain) *plain = decide + 2 * stage + dyn;
+    if (with_shepard) *with_shepard = decide + 2 * stage + dyn + (S->npm > 0 ? 2 : 0);
     return LQ_OK;
 }
 
@@ -738,6 +836,16 @@ extern "C" int lq_sim_save_checkpoint(void* sim, const char* path)
                     "checkpoint v");
         LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "checkpoint read");
     }
+    Parameters par = S->ph;
+    double time = S->time;
+    if (S->flags & LQ_SIM_DYNAMIC_DT) {
+        /* the next step's dt and the time live on the device */
+        LQ_TRY_CUDA(cudaMemcpyAsync(&par.dt, &S->pd->dt, sizeof(float), cudaMemcpyDeviceToHost, S->stream),
+                    "checkpoint dt");
+        LQ_TRY_CUDA(cudaMemcpyAsync(&time, S->dtime, sizeof(double), cudaMemcpyDeviceToHost, S->stream),
+                    "checkpoint time");
+        LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "checkpoint dt");
+    }
     FILE* f = fopen(path, "wb");
     if (!f) return lqb::set_error(LQ_ERR_IO, "cannot write checkpoint %s", path);
     CkWriter w{f};
@@ -745,12 +853,12 @@ extern "C" int lq_sim_save_checkpoint(void* sim, const char* path)
     w.val(kCkVersion);
     w.val((uint32_t)S->flags);
     w.val((int64_t)S->step);
-    w.val(S->time);
+    w.val(time);
     w.val(S->skin);
     w.val((int32_t)S->np);
     w.val((int32_t)S->npb);
     w.val((int32_t)S->npm);
-    w.put(&S->ph, sizeof(Parameters));
+    w.put(&par, sizeof(Parameters));
     for (auto* a : {&pos, &vel, &idep, &str, &stn}) w.put(a->data(), a->size() * sizeof(float));
     if (!xd.empty()) {
         w.put(xd.data(), xd.size() * sizeof(double));
@@ -805,6 +913,10 @@ extern "C" int lq_sim_load_checkpoint(const char* path, int flags, void** sim)
     if ((saved_flags & LQ_SIM_MIXED) != ((uint32_t)flags & LQ_SIM_MIXED))
         return lqb::set_error(LQ_ERR_ARG, "%s was written by the %s form; load it with the same LQ_SIM_MIXED flag",
                               path, (saved_flags & LQ_SIM_MIXED) ? "mixed-precision" : "plain FP32");
+    const uint32_t ext = LQ_SIM_DENSITY_FILTER | LQ_SIM_DYNAMIC_DT;
+    if ((saved_flags & ext) != ((uint32_t)flags & ext))
+        return lqb::set_error(LQ_ERR_ARG, "%s: load it with the LQ_SIM_DENSITY_FILTER / LQ_SIM_DYNAMIC_DT flags it "
+                              "was saved with (%u)", path, saved_flags & ext);
     const size_t n = (size_t)np;
     const float* arr[5];
     const size_t width[5] = {4, 4, 4, 6, 6};
@@ -856,6 +968,15 @@ extern "C" int lq_sim_load_checkpoint(const char* path, int flags, void** sim)
     S->step = step;
     S->time = time;
     S->ph.time = (float)time;
+    if (flags & LQ_SIM_DYNAMIC_DT) {
+        /* the saved next-step dt (create set the fixed one) and the time */
+        cudaError_t e = cudaMemcpyAsync(&S->pd->dt, &par.dt, sizeof(float), cudaMemcpyHostToDevice, S->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(S->dtime, &S->time, sizeof(double), cudaMemcpyHostToDevice, S->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
+        if (e != cudaSuccess)
+            return fail(lqb::set_error(LQ_ERR_CUDA, "checkpoint dt: %s", cudaGetErrorString(e)));
+    }
     int st = LQ_OK;
     if (st == LQ_OK && nmt > 0) st = lq_sim_set_materials(out, nmt, mt.data());
     if (st == LQ_OK && nvw > 0) st = lq_sim_set_hypoplastic(out, nvw, vw.data());
@@ -970,9 +1091,11 @@ int profiled_step(LqSim* S, PhaseTimer& T)
         LQ_TRY(T.mark(s, PH_INTEGRATE));
         if (stage == 0)
             LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt, S->vw));
-        else
+        else {
             LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild,
                                             S->skin, s, S->mt, S->vw));
+            LQ_TRY(enqueue_dynamic_dt(S, s));
+        }
         LQ_TRY(T.close(s));
     }
     return LQ_OK;
@@ -995,6 +1118,12 @@ extern "C" int lq_sim_profile(void* sim, int nsteps, double* phase_ms, int* phas
         if (st == LQ_OK && N != 0 && S->step % N == 0 && S->step != 0) {
             st = T.mark(S->stream, PH_SHEPARD);
             if (st == LQ_OK) st = enqueue_shepard(S, S->stream);
+            if (st == LQ_OK) st = T.close(S->stream);
+        }
+        const int Nd = S->ph.density_shepard_filter;
+        if (st == LQ_OK && (S->flags & LQ_SIM_DENSITY_FILTER) && Nd > 0 && S->step % Nd == 0 && S->step != 0) {
+            st = T.mark(S->stream, PH_SHEPARD);
+            if (st == LQ_OK) st = enqueue_density_filter(S, S->stream);
             if (st == LQ_OK) st = T.close(S->stream);
         }
         S->time += (double)S->ph.dt;

@@ -753,7 +753,47 @@ __global__ void __launch_bounds__(kBlock) k_shepard_list(const Parameters* __res
     store_t2(out_str, i, S);
 }
 
+/* Density Shepard filter over a material particle's list (boundary
+ * neighbours skipped; the list holds the particle itself, at q = 0):
+ * rho~_i = sum m W / sum (m / rho_j) W. */
+__global__ void __launch_bounds__(kBlock) k_density_filter_list(const Parameters* __restrict__ P, int np, int npb,
+                                                                State st, float* __restrict__ rho_out,
+                                                                const int* __restrict__ list,
+                                                                const int* __restrict__ count, int stride)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = npb + t;
+    if (i >= np) return;
+    const int n = min(__ldg(count + t), LQ_NBR_CAP);
+    const float ih = __ldg(&P->i_h), m = __ldg(&P->m), Cw = __ldg(&P->kernel_normalization_par);
+    const float4 xi = __ldg(st.pos + i);
+    float num = 0.0f, den = 0.0f;
+    for (int k = 0; k < n; ++k) {
+        const int j = __ldg(list + (size_t)k * stride + t);
+        if (j < npb || !lq_in_range(j, np)) continue;
+        const float4 xj = __ldg(st.pos + j);
+        const float3 d = make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
+        const float q = norm3df(d.x, d.y, d.z) * ih;
+        if (q < 2.0f) {
+            const float ker = Cw * (2.0f - q) * (2.0f - q) * (2.0f - q) * (2.0f - q) * (q + 0.5f);
+            num += m * ker;
+            den += ker * (m / __ldg(&st.vel[j].w));
+        }
+    }
+    rho_out[i] = num / den;
+}
+
 }  // namespace
+
+int launch_density_filter_list(const Parameters* ph, const Parameters* pd, const State& st, float* rho_out,
+                               const NeighborList& nl, cudaStream_t s)
+{
+    if (ph->npm <= 0) return LQ_OK;
+    k_density_filter_list<<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, rho_out, nl.list,
+                                                                        nl.count, nl.stride);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_density_filter_list");
+    return LQ_OK;
+}
 
 /* This translation unit's count of bounds violations (always 0 without
  * LQ_CHECKED). */

@@ -53,6 +53,9 @@ def lib():
         L.or_dp_update.argtypes = [_VP, _D] + [_VP] * 5
         L.or_hypo_update.argtypes = [_VP, _D] + [_VP] * 3
         L.or_sim_set_vw.argtypes = [_VP, _I, _VP]
+        L.or_sim_set_extensions.argtypes = [_VP, _I, _I]
+        L.or_sim_time.restype = ctypes.c_double
+        L.or_sim_time.argtypes = [_VP]
         L.or_vw_update.argtypes = [_VP, _D, _VP, _VP, _VP, _VP]
         L.or_vw_rate.argtypes = [_VP, _VP, _D, _VP, _VP, _VP, _VP]
         _lib = L
@@ -178,6 +181,14 @@ class OracleSim:
         """Model-3 (von Wolffersdorff) material rows, n x 10, by object id."""
         self._vw = np.ascontiguousarray(rows, np.float32).reshape(-1, 10)
         lib().or_sim_set_vw(self.h, self._vw.shape[0], _p(self._vw))
+
+    def set_extensions(self, density_filter: bool = False, dynamic_dt: bool = False):
+        """Features the reference declares but does not apply: the density
+        Shepard filter and the dynamic time step."""
+        lib().or_sim_set_extensions(self.h, int(density_filter), int(dynamic_dt))
+
+    def time(self) -> float:
+        return lib().or_sim_time(self.h)
 
     def step(self, n: int = 1):
         if lib().or_sim_step(self.h, n) != 0:

@@ -345,6 +345,55 @@ void shepard(const OrParams& P, int np, int npb, const double* pos, const double
     }
 }
 
+/* Density Shepard filter (not applied by the reference, whose parameter
+ * density-shepard-filter is read but unused, src/loquat_io.cu:180): for a
+ * material particle, rho~_i = sum_j m W_ij / sum_j (m / rho_j) W_ij over the
+ * material layer, self included -- the stress filter's neighbour set and
+ * weights applied to the density. */
+void shepard_density(const OrParams& P, int np, int npb, const double* pos, const double* vel, double* rho_out,
+                     const int* beg, const int* end, bool float_cells)
+{
+    const double ih = P.i_h, m = P.m;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int i = npb; i < np; ++i) {
+        const double* xi = pos + 4 * (size_t)i;
+        double num = 0, w = 0;
+        int cx, cy, cz;
+        stencil_centre(P, xi, float_cells, cx, cy, cz);
+        for_stencil(P, cx, cy, cz, P.ncell_one_layer, beg, end, [&](int j) {
+            const double* xj = pos + 4 * (size_t)j;
+            double d[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
+            double q = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) * ih;
+            if (q < 2.0) {
+                const double wk = wendland(P, q);
+                num += m * wk;
+                w += wk * (m / vel[4 * (size_t)j + 3]);
+            }
+        });
+        rho_out[i] = num / w;
+    }
+}
+
+/* Dynamic time step (the reference reads dynamic-time-step but always uses
+ * cfl h / cs, src/loquat.cu:325-333): from the material particles' largest
+ * speed and acceleration at the end of a step,
+ *   dt = cfl min(h / (cs + v_max), sqrt(h / a_max)),
+ * never above the fixed cfl h / cs. */
+double dynamic_dt(const OrParams& P, int np, int npb, const double* vel, const double* accad)
+{
+    double v2 = 0, a2 = 0;
+    for (int i = npb; i < np; ++i) {
+        const double* v = vel + 4 * (size_t)i;
+        const double* a = accad + 4 * (size_t)i;
+        v2 = std::fmax(v2, v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        a2 = std::fmax(a2, a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    }
+    const double h = P.h, cs = P.cs;
+    double dt = h / (cs + std::sqrt(v2));
+    if (a2 > 0) dt = std::fmin(dt, std::sqrt(h / std::sqrt(a2)));
+    return (double)P.cfl * dt;
+}
+
 /* ------------------------------------------- constitutive models (a9, a10) */
 inline double contract(const double* a, const double* b)
 {
@@ -684,6 +733,9 @@ struct OrSim {
     std::vector<float> vw_rows;
     VWTable vwt;
     Grid g;
+    bool density_filter = false;   /* extensions, off as in the reference */
+    bool dynamic = false;
+    double dt_next = 0.0;
 
     StateView cur() { return {pos.data(), vel.data(), idep.data(), str.data(), stn.data()}; }
     StateView ini() { return {pos0.data(), vel0.data(), idep0.data(), str0.data(), stn0.data()}; }
@@ -721,6 +773,7 @@ struct OrSim {
     void one_step()
     {
         P.dt = P.cfl * P.h / P.cs;
+        if (dynamic && dt_next > 0.0) P.dt = (float)dt_next;
         P.time = (float)time;
         search();
         sort_primary();
@@ -741,8 +794,17 @@ struct OrSim {
             shepard(P, np, npb, pos.data(), vel.data(), str.data(), out.data(), g.beg.data(), g.end.data(), false);
             for (size_t k = (size_t)npb * 6; k < out.size(); ++k) str[k] = out[k];
         }
+        const int Nd = P.density_shepard_filter;
+        if (density_filter && Nd > 0 && step % Nd == 0 && step != 0) {
+            search();
+            sort_primary();
+            std::vector<double> rho(np);
+            shepard_density(P, np, npb, pos.data(), vel.data(), rho.data(), g.beg.data(), g.end.data(), false);
+            for (int i = npb; i < np; ++i) vel[4 * (size_t)i + 3] = rho[i];
+        }
         time += (double)P.dt;
         step++;
+        if (dynamic) dt_next = dynamic_dt(P, np, npb, vel.data(), accad.data());
     }
 };
 
@@ -903,6 +965,18 @@ int or_vw_rate(const float* row, const double* s6, double e, const double* d6, c
     vw_rate(vw_constants(row), s6, e, d6, spin3, rate6, erate);
     return 0;
 }
+
+/* Extensions with no reference behaviour: the density Shepard filter every
+ * density_shepard_filter steps, and the dynamic time step. */
+int or_sim_set_extensions(void* sv, int density_filter, int dynamic_dt)
+{
+    OrSim* s = (OrSim*)sv;
+    s->density_filter = density_filter != 0;
+    s->dynamic = dynamic_dt != 0;
+    return 0;
+}
+
+double or_sim_time(void* sv) { return ((OrSim*)sv)->time; }
 
 int or_sim_step(void* sv, int n)
 {

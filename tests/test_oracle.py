@@ -255,3 +255,29 @@ def test_oracle_sim_confined_block_stays_geostatic(orc):
     want = -c.par.rho0 * 9.81 * depth[deep]
     got = s[nb:, 2][deep]
     assert np.median(np.abs(got - want) / np.abs(want)) < 0.15
+
+
+def test_oracle_extensions_density_filter_and_dynamic_step(orc):
+    """Density filter: a uniform density is a fixed point and noise is
+    smoothed; dynamic step: never above cfl h / cs, equal to it at rest."""
+    import numpy as np
+    from loquat_b200 import cases
+
+    c = cases.small_column(velocity_noise=0.0, shepard=0, seed=5)
+    c.par.density_shepard_filter = 1
+    o = orc.OracleSim(c.par, *c.arrays())
+    o.set_extensions(density_filter=True, dynamic_dt=True)
+    o.step(2)
+    nb = c.par.npb
+    rho = o.get()[1][nb:, 3]
+    assert np.allclose(rho, c.par.rho0, rtol=2e-3)
+    fixed = c.par.cfl * c.par.h / c.par.cs
+    assert o.time() <= 2 * fixed * (1 + 1e-7)
+    noisy = c.velrhop.copy()
+    rng = np.random.default_rng(3)
+    noisy[nb:, 3] *= 1 + rng.uniform(-1e-2, 1e-2, c.par.npm)
+    p = orc.OracleSim(c.par, c.pospres, noisy, c.idep, c.str_, c.stn)
+    p.set_extensions(density_filter=True)
+    p.step(2)
+    after = p.get()[1][nb:, 3]
+    assert np.std(after) < 0.6 * np.std(noisy[nb:, 3])
