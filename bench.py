@@ -74,6 +74,9 @@ def parse_args(argv=None):
                          "(the particles move and the neighbour lists are rebuilt at a representative rate); "
                          "default 2500, 200 for the von Wolffersdorff workloads")
     ap.add_argument("--no-compare", action="store_true", help="skip timing the other precision form")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default pair-kernel shape and list skin instead of lq_sim_autotune's choice")
+    ap.add_argument("--tune-steps", type=int, default=40, help="timed steps per autotuner trial")
     ap.add_argument("--eager", action="store_true",
                     help="launch kernels one by one instead of replaying the step graph (for ncu, which cannot "
                          "profile kernels inside graphs with conditional nodes)")
@@ -284,6 +287,12 @@ def bench_ours(args):
 
     if args.start_step > 0:
         sim.step(args.start_step)
+    tuned = None
+    if not args.no_autotune:
+        # the project's autotuner: pair-kernel launch shape and list skin by
+        # timing, the state left as it was (outside the timed region)
+        shape, skin = sim.autotune(args.tune_steps)
+        tuned = {"pair_shape": shape, "skin_over_h": skin, "steps_per_trial": args.tune_steps}
     sim.step(args.warmup)
     sim.synchronize()
     rb0 = sim.rebuilds()
@@ -356,6 +365,9 @@ def bench_ours(args):
             osim.set_hypoplastic(case.meta["hypoplastic"])
         if args.start_step > 0:
             osim.step(args.start_step)
+        if tuned:
+            osim.set_pair_shape(tuned["pair_shape"])
+            osim.set_skin(tuned["skin_over_h"])
         osim.step(args.warmup)
         osim.synchronize()
         if dist:
@@ -380,7 +392,8 @@ def bench_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.form == "plain" else "f32+f64", "data": "synthetic",
             "config": {"workload": workload, "np": np_, "npm": npm, "npb": par.npb, "ncell": par.ncell,
-                       "form": "%s, %s, Verlet lists (skin 0.05h)" % (
+                       "autotuned": tuned,
+                       "form": "%s, %s, Verlet lists" % (
                            "plain FP32" if args.form == "plain" else "mixed precision (FP64 integrator)",
                            "eager launches" if args.eager else "CUDA-graph step"),
                        "timed_window": "steps %d..%d of the run" % (s0, s1),
@@ -451,10 +464,15 @@ def bench_ensemble(args):
         sim.synchronize()
         return e0.elapsed_time(e1)
 
-    sim = lq.Simulation(par, *comb.arrays())
-    sim.set_materials(comb.meta["materials"])
-    sim.set_frames(comb.meta["frames"])
-    sim.step(args.warmup)
+    def batched(mixed):
+        sim = lq.Simulation(par, *comb.arrays(), mixed=mixed)
+        sim.set_materials(comb.meta["materials"])
+        sim.set_frames(comb.meta["frames"])
+        sim.step(args.warmup)
+        return sim
+
+    # the batched ensemble in the chosen form (the line's value), then in the other
+    sim = batched(args.form == "mixed")
     rb0 = sim.rebuilds()
     sim.synchronize()
     if dist:
@@ -464,6 +482,13 @@ def bench_ensemble(args):
     clk = clocks.stop() if clocks else None
     rebuilds = sim.rebuilds() - rb0
     health = sim.health()
+    plain_launches, _ = sim.launches_per_step()
+    sim.close()
+    other = "plain" if args.form == "mixed" else "mixed"
+    sim = batched(other == "mixed")
+    if dist:
+        dist.barrier()
+    ms_other = replicas.max_over_ranks(timed(sim, args.steps), device="cuda")
     sim.close()
     ms_seq = 0.0
     for p in parts:
@@ -474,20 +499,26 @@ def bench_ensemble(args):
     ms_seq = replicas.max_over_ranks(ms_seq, device="cuda")
     npm = total_npm
     v_batch = npm * args.steps / (ms_batch / 1e3)
+    v_other = npm * args.steps / (ms_other / 1e3)
     v_seq = npm * args.steps / (ms_seq / 1e3)
     if rank == 0:
         print(json.dumps({
             "metric": "particle-steps/s", "value": v_batch, "unit": "particle-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batch / args.steps,
-            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32" if args.form == "plain" else "f32+f64", "data": "synthetic",
             "config": {"workload": "ensemble of %d Drucker-Prager column collapses (counts log-uniform 5e3-2e5, "
                                    "H/L 0.5-4, phi 20-40 deg, c 0-5 kPa, dr=2 mm, h=1.2dr)" % args.scenarios,
                        "npm": npm, "rank0_np": par.np, "rank0_ncell": par.ncell,
                        "parallelism": "scenarios split over %d ranks by particle count" % world,
-                       "form": "batched: one simulation, per-scenario frames and materials, CUDA-graph step"},
+                       "form": "batched (%s): one simulation, per-scenario frames and materials, CUDA-graph step"
+                               % ("mixed precision" if args.form == "mixed" else "plain FP32")},
+            "forms": {args.form: {"value": v_batch, "ms_per_step": ms_batch / args.steps},
+                      other: {"value": v_other, "ms_per_step": ms_other / args.steps}},
             "sequential": {"value": v_seq, "ms_per_step": ms_seq / args.steps,
-                           "form": "the same scenarios one after another, one plain simulation each"},
+                           "form": "the same scenarios one after another, one plain FP32 simulation each"},
             "batched_over_sequential": v_batch / v_seq,
+            "gpu_launches_per_step": plain_launches,
             "neighbour_list_rebuilds": rebuilds, "health": [int(x) for x in health], "clocks": clk,
             "partition": {"ranks": world, "imbalance": replicas.imbalance([p.par.npm for p in all_parts], shares)},
         }))

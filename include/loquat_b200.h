@@ -205,6 +205,18 @@ int lq_sim_set_frames(void* sim, int n, const int* rows);
  * with the Shepard pass; a rebuild adds lq_sim_rebuild_launches more. */
 int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard);
 int lq_sim_rebuild_launches(void* sim, int* launches);
+/* Launch shape of the pair kernel (threads per block x resident blocks per
+ * SM, which caps its registers): 0 = 128 x 6 (default), 1 = 64 x 12,
+ * 2 = 256 x 3, 3 = 128 x 5, 4 = 128 x 7.  Results do not depend on it. */
+int lq_sim_set_pair_shape(void* sim, int shape);
+/* Autotuner: times `steps` steps (after two untimed ones) for each pair
+ * kernel shape at the current skin, then for skins of 0.02, 0.05, 0.1 and
+ * 0.2 h with the fastest shape, and keeps the fastest pair.  Every trial
+ * starts from a device copy of the state taken at the call, and the state,
+ * step, time and health word are put back afterwards, so tuning does not
+ * advance the simulation (it rebuilds its lists before the next step).
+ * Allocates the state copy for the duration of the call. */
+int lq_sim_autotune(void* sim, int steps, int* shape, float* skin_over_h);
 /* Bounds violations counted so far in this process by a library built with
  * -D LQ_CHECKED (loquat_b200/liblqb200_checked.so): its list and grid
  * kernels check every index they gather or scatter through and skip and

@@ -76,6 +76,8 @@ _SIGNATURES = {
     "lq_sim_set_frames": (_I, [_VP, _I, _VP]),
     "lq_sim_rebuilds": (_I, [_VP, ctypes.POINTER(_LL)]),
     "lq_sim_rebuild_launches": (_I, [_VP, ctypes.POINTER(_I)]),
+    "lq_sim_set_pair_shape": (_I, [_VP, _I]),
+    "lq_sim_autotune": (_I, [_VP, _I, ctypes.POINTER(_I), ctypes.POINTER(_F)]),
     "lq_debug_bounds_violations": (_I, [ctypes.POINTER(_LL)]),
     "lq_sim_save_checkpoint": (_I, [_VP, ctypes.c_char_p]),
     "lq_sim_load_checkpoint": (_I, [ctypes.c_char_p, _I, ctypes.POINTER(_VP)]),
@@ -348,6 +350,16 @@ class Simulation:
         c = _I()
         check(lib().lq_sim_rebuild_launches(self.handle, ctypes.byref(c)), "lq_sim_rebuild_launches")
         return c.value
+
+    def set_pair_shape(self, shape: int):
+        check(lib().lq_sim_set_pair_shape(self.handle, shape), "lq_sim_set_pair_shape")
+
+    def autotune(self, steps: int = 20):
+        """Chooses the pair kernel's launch shape and the list skin by timing
+        (state left as it was); returns (shape, skin / h)."""
+        sh, sk = _I(), _F()
+        check(lib().lq_sim_autotune(self.handle, steps, ctypes.byref(sh), ctypes.byref(sk)), "lq_sim_autotune")
+        return sh.value, sk.value
 
     def save_checkpoint(self, path):
         """Binary checkpoint (state, FP64 copies, step, time, tables); the

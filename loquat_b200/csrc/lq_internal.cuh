@@ -138,7 +138,11 @@ int launch_neighbor_list(const Parameters* par_host, const Parameters* par_dev, 
  * kernel reads the state arrays. */
 int launch_interaction_list(const Parameters* par_host, const Parameters* par_dev, const State& st, const Rates& r,
                             const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr = Frames(),
-                            bool compensated = false, float* rec = nullptr);
+                            bool compensated = false, float* rec = nullptr, int shape = 0);
+/* Launch shapes of the packed pair kernel: {threads per block, resident
+ * blocks per SM}. */
+constexpr int kPairShapeCount = 5;
+extern const int kPairShapes[kPairShapeCount][2];
 int launch_adami(const Parameters* par_host, const Parameters* par_dev, const State& st, const Cells& c,
                  cudaStream_t s);
 /* Shepard filter of material stress into out_str[npb, np).  When `full` is

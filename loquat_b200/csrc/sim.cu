@@ -28,6 +28,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <utility>
 #include <vector>
 
 #include <nvtx3/nvToolsExt.h>
@@ -63,6 +64,7 @@ struct LqSim {
     lqb::MaterialTable vw;             /* von Wolffersdorff rows (model 3) */
     float* rec = nullptr;              /* packed neighbour data, np x 13 floats */
     float* rho_f = nullptr;            /* density filter output (LQ_SIM_DENSITY_FILTER) */
+    int pair_shape = 0;                /* launch shape of the pair kernel (lqb::kPairShapes) */
     unsigned* vmax2 = nullptr;         /* max |v|^2, |a|^2 bits (LQ_SIM_DYNAMIC_DT) */
     double* dtime = nullptr;           /* device-side time (LQ_SIM_DYNAMIC_DT) */
     lqb::Frames fr;                    /* per-object grid rows (optional) */
@@ -277,12 +279,12 @@ int enqueue_stages(LqSim* S, cudaStream_t s)
     /* predictor stage (reference src/loquat.cu:343-368) */
     LQ_TRY(lqb::launch_adami_list(ph, pd, S->S, S->nlb, s));
     LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S, S->R, cells, S->nlm, s, S->fr, S->flags & LQ_SIM_MIXED,
-                                        S->rec));
+                                        S->rec, S->pair_shape));
     LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt, S->vw));
     /* corrector stage (reference src/loquat.cu:371-396) */
     LQ_TRY(lqb::launch_adami_list(ph, pd, S->S2, S->nlb, s));
     LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S2, S->R, cells, S->nlm, s, S->fr, S->flags & LQ_SIM_MIXED,
-                                        S->rec));
+                                        S->rec, S->pair_shape));
     LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild, S->skin, s,
                                     S->mt, S->vw));
     return enqueue_dynamic_dt(S, s);
@@ -773,6 +775,143 @@ extern "C" int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard
     return LQ_OK;
 }
 
+/* ------------------------------------------------------------- autotuning */
+extern "C" int lq_sim_set_pair_shape(void* sim, int shape)
+{
+    if (!sim || shape < 0 || shape >= lqb::kPairShapeCount)
+        return lqb::set_error(LQ_ERR_ARG, "lq_sim_set_pair_shape: shape must be in [0, %d)", lqb::kPairShapeCount);
+    LqSim* S = static_cast<LqSim*>(sim);
+    LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "set pair shape");
+    S->pair_shape = shape;
+    return build_graphs(S);
+}
+
+namespace {
+
+/* A device copy of everything a trial step changes, so that tuning leaves
+ * the simulation where it was. */
+struct Snapshot {
+    std::vector<std::pair<void*, size_t>> items;   /* (live buffer, bytes) */
+    std::vector<void*> copies;
+    long long step = 0;
+    double time = 0.0;
+    float skin = 0.0f;
+    int shape = 0;
+    ~Snapshot()
+    {
+        for (void* p : copies) cudaFree(p);
+    }
+    int take(LqSim* S)
+    {
+        const size_t n = (size_t)S->np;
+        items = {{S->S.pos, n * sizeof(float4)},  {S->S.vel, n * sizeof(float4)},
+                 {S->S.idep, n * sizeof(float4)}, {S->S.str, n * sizeof(tensor2d)},
+                 {S->S.stn, n * sizeof(tensor2d)}, {S->health, sizeof(int) * lqb::HEALTH_WORDS},
+                 {S->rebuilds, sizeof(int)},      {S->pd, sizeof(Parameters)}};
+        if (S->S.xd) {
+            items.push_back({S->S.xd, n * sizeof(double4)});
+            items.push_back({S->S.vd, n * sizeof(double4)});
+        }
+        if (S->dtime) items.push_back({S->dtime, sizeof(double)});
+        for (auto& it : items) {
+            void* c = nullptr;
+            cudaError_t e = cudaMalloc(&c, it.second);
+            if (e != cudaSuccess)
+                return lqb::set_error(LQ_ERR_ALLOC, "autotune: no room for a state copy (%zu bytes): %s", it.second,
+                                      cudaGetErrorString(e));
+            copies.push_back(c);
+            LQ_TRY_CUDA(cudaMemcpyAsync(c, it.first, it.second, cudaMemcpyDeviceToDevice, S->stream), "snapshot");
+        }
+        step = S->step;
+        time = S->time;
+        skin = S->skin;
+        shape = S->pair_shape;
+        return LQ_OK;
+    }
+    int restore(LqSim* S)
+    {
+        for (size_t k = 0; k < items.size(); ++k)
+            LQ_TRY_CUDA(cudaMemcpyAsync(items[k].first, copies[k], items[k].second, cudaMemcpyDeviceToDevice,
+                                        S->stream),
+                        "restore");
+        S->step = step;
+        S->time = time;
+        return set_flag(S, 1); /* lists are rebuilt before the next step */
+    }
+};
+
+int cuda_ok(cudaError_t e, const char* what) { return e == cudaSuccess ? LQ_OK : lqb::cuda_status(e, what); }
+
+/* ms per step of `steps` steps after two untimed ones. */
+int time_steps(LqSim* S, int steps, float* ms)
+{
+    cudaEvent_t a, b;
+    LQ_TRY_CUDA(cudaEventCreate(&a), "event");
+    LQ_TRY_CUDA(cudaEventCreate(&b), "event");
+    int st = lq_sim_step(S, 2);
+    if (st == LQ_OK) st = cuda_ok(cudaEventRecord(a, S->stream), "event");
+    if (st == LQ_OK) st = lq_sim_step(S, steps);
+    if (st == LQ_OK) st = cuda_ok(cudaEventRecord(b, S->stream), "event");
+    if (st == LQ_OK) st = cuda_ok(cudaEventSynchronize(b), "event");
+    if (st == LQ_OK) st = cuda_ok(cudaEventElapsedTime(ms, a, b), "event");
+    if (st == LQ_OK) *ms /= (float)steps;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return st;
+}
+
+}  // namespace
+
+extern "C" int lq_sim_autotune(void* sim, int steps, int* shape_out, float* skin_over_h_out)
+{
+    if (!sim || steps < 1) return lqb::set_error(LQ_ERR_ARG, "lq_sim_autotune: bad argument");
+    LqSim* S = static_cast<LqSim*>(sim);
+    if (S->ph.constitutive_model == 3 && S->vw.n == 0)
+        return lqb::set_error(LQ_ERR_ARG, "lq_sim_autotune: set the model-3 table first");
+    Snapshot snap;
+    LQ_TRY(snap.take(S));
+    const float h = S->ph.h;
+    int best_shape = S->pair_shape;
+    float best_skin = S->skin, best_ms = 3.4e38f;
+    float best_factor = S->skin / h;   /* skin / h as the caller would pass it to lq_sim_set_skin */
+    float factor = best_factor;
+    auto trial = [&](int shape, float skin) -> int {
+        LQ_TRY(snap.restore(S));
+        S->pair_shape = shape;
+        S->skin = skin;
+        LQ_TRY(build_graphs(S));
+        float ms = 0.0f;
+        LQ_TRY(time_steps(S, steps, &ms));
+        if (ms < best_ms) {
+            best_ms = ms;
+            best_shape = shape;
+            best_skin = skin;
+            best_factor = factor;
+        }
+        return LQ_OK;
+    };
+    /* launch shapes at the current skin, then skins with the best shape */
+    int st = LQ_OK;
+    for (int k = 0; k < lqb::kPairShapeCount && st == LQ_OK; ++k) st = trial(k, snap.skin);
+    const float skins[] = {0.02f, 0.05f, 0.1f, 0.2f};
+    const int shape = best_shape;
+    for (float f : skins) {
+        factor = f;
+        if (st == LQ_OK && f * h != snap.skin) st = trial(shape, f * h);
+    }
+    /* back to the state before tuning, with the chosen configuration */
+    int st2 = snap.restore(S);
+    S->pair_shape = st == LQ_OK ? best_shape : snap.shape;
+    S->skin = st == LQ_OK ? best_skin : snap.skin;
+    if (st2 == LQ_OK) st2 = build_graphs(S);
+    if (st2 == LQ_OK) st2 = cuda_ok(cudaStreamSynchronize(S->stream), "autotune");
+    if (st != LQ_OK) return st;
+    if (st2 != LQ_OK) return st2;
+    if (shape_out) *shape_out = S->pair_shape;
+    if (skin_over_h_out) *skin_over_h_out = best_factor;
+    return LQ_OK;
+}
+
 /* ------------------------------------------------------------ checkpoints */
 /* Binary checkpoint, little-endian as written by this library:
  *   "LQB200CK" | u32 version | u32 flags | i64 step | f64 time | f32 skin |
@@ -1086,7 +1225,7 @@ int profiled_step(LqSim* S, PhaseTimer& T)
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_INTERACTION));
         LQ_TRY(lqb::launch_interaction_list(ph, pd, *cur[stage], S->R, cells, S->nlm, s, S->fr,
-                                            S->flags & LQ_SIM_MIXED, S->rec));
+                                            S->flags & LQ_SIM_MIXED, S->rec, S->pair_shape));
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_INTEGRATE));
         if (stage == 0)

@@ -476,9 +476,13 @@ __global__ void __launch_bounds__(kBlock) k_pack_neighbors(int np, State st, Nbr
     nb.s1[i] = s.yz * rj2;
 }
 
-/* k_interaction_list over the packed neighbour arrays (same sums, same order). */
-template <bool kKahan>
-__global__ void __launch_bounds__(kBlock, LQ_PAIR_MIN_BLOCKS) k_interaction_rec(
+/* k_interaction_list over the packed neighbour arrays (same sums, same
+ * order).  kThreads x kMinBlocks is the launch shape: the block size and
+ * the resident blocks per SM the register allocation is capped for; the
+ * shapes of kPairShapes are compiled and one is chosen per simulation
+ * (lq_sim_autotune times them). */
+template <bool kKahan, int kThreads, int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_interaction_rec(
     const Parameters* __restrict__ P, int np, int npb, State st, Rates rt, Cells cells, const int* __restrict__ list,
     const int* __restrict__ count, int stride, Frames fr, NbrArrays nb)
 {
@@ -795,6 +799,10 @@ int launch_density_filter_list(const Parameters* ph, const Parameters* pd, const
     return LQ_OK;
 }
 
+/* Launch shapes of the pair kernel: threads per block x resident blocks
+ * per SM (the register cap).  Shape 0 is the default. */
+const int kPairShapes[kPairShapeCount][2] = {{kBlock, LQ_PAIR_MIN_BLOCKS}, {64, 12}, {256, 3}, {128, 5}, {128, 7}};
+
 /* This translation unit's count of bounds violations (always 0 without
  * LQ_CHECKED). */
 int bounds_count_sph(unsigned long long* v)
@@ -856,7 +864,7 @@ int launch_shepard_list(const Parameters* ph, const Parameters* pd, const State&
 
 int launch_interaction_list(const Parameters* ph, const Parameters* pd, const State& st, const Rates& r,
                             const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr,
-                            bool compensated, float* rec)
+                            bool compensated, float* rec, int shape)
 {
     if (ph->npm <= 0) return LQ_OK;
     if (rec) {
@@ -867,14 +875,19 @@ int launch_interaction_list(const Parameters* ph, const Parameters* pd, const St
                      reinterpret_cast<float4*>(rec) + 2 * n, rec + 12 * n};
         k_pack_neighbors<<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(ph->np, st, nb);
         LQ_TRY_CUDA(cudaGetLastError(), "k_pack_neighbors");
-        if (compensated)
-            k_interaction_rec<true><<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, r, c,
-                                                                                  nl.list, nl.count, nl.stride, fr,
-                                                                                  nb);
-        else
-            k_interaction_rec<false><<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, r, c,
-                                                                                   nl.list, nl.count, nl.stride, fr,
-                                                                                   nb);
+#define LQ_PAIR_LAUNCH(T, B)                                                                                \
+    (compensated ? k_interaction_rec<true, T, B><<<blocks_for(ph->npm, T), T, 0, s>>>(                      \
+                       pd, ph->np, ph->npb, st, r, c, nl.list, nl.count, nl.stride, fr, nb)                   \
+                 : k_interaction_rec<false, T, B><<<blocks_for(ph->npm, T), T, 0, s>>>(                     \
+                       pd, ph->np, ph->npb, st, r, c, nl.list, nl.count, nl.stride, fr, nb))
+        switch (shape) {
+            case 1: LQ_PAIR_LAUNCH(64, 12); break;
+            case 2: LQ_PAIR_LAUNCH(256, 3); break;
+            case 3: LQ_PAIR_LAUNCH(128, 5); break;
+            case 4: LQ_PAIR_LAUNCH(128, 7); break;
+            default: LQ_PAIR_LAUNCH(kBlock, LQ_PAIR_MIN_BLOCKS); break;
+        }
+#undef LQ_PAIR_LAUNCH
         LQ_TRY_CUDA(cudaGetLastError(), "k_interaction_rec");
         return LQ_OK;
     }
