@@ -77,6 +77,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default pair-kernel shape and list skin instead of lq_sim_autotune's choice")
     ap.add_argument("--tune-steps", type=int, default=40, help="timed steps per autotuner trial")
+    ap.add_argument("--pair-shape", type=int, default=None,
+                    help="fix the pair kernel's launch shape (lq_sim_set_pair_shape) instead of autotuning")
     ap.add_argument("--eager", action="store_true",
                     help="launch kernels one by one instead of replaying the step graph (for ncu, which cannot "
                          "profile kernels inside graphs with conditional nodes)")
@@ -288,7 +290,10 @@ def bench_ours(args):
     if args.start_step > 0:
         sim.step(args.start_step)
     tuned = None
-    if not args.no_autotune:
+    if args.pair_shape is not None:
+        sim.set_pair_shape(args.pair_shape)
+        tuned = {"pair_shape": args.pair_shape, "skin_over_h": 0.05, "steps_per_trial": 0}
+    elif not args.no_autotune:
         # the project's autotuner: pair-kernel launch shape and list skin by
         # timing, the state left as it was (outside the timed region)
         shape, skin = sim.autotune(args.tune_steps)
