@@ -84,11 +84,22 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_predict(
         e.xy += dd.xy * hdt; e.xz += dd.xz * hdt; e.yz += dd.yz * hdt;
         double p = x0.w, ep = id.y, ev = id.z;
         T6d sd = widen6(s0);
-        if (!kVW && M.model == 1) {
+        if (kVW) {
+            /* the kinematics are stored before the sub-stepping, whose FP64
+             * registers then need not share the SM with them */
+            out.xd[i] = xd;
+            out.vd[i] = vd;
+            out.pos[i] = make_float4((float)xd.x, (float)xd.y, (float)xd.z, x0.w);
+            out.vel[i] = make_float4((float)vd.x, (float)vd.y, (float)vd.z, (float)vd.w);
+            store_t2(out.stn, i, narrow6(e));
+            const float epf = (float)sqrt(2.0 / 3.0 * contract6(e, e));
+            vw_update_d(vw_const(vw, id.x), hdt, de, w, sd, ev);
+            out.idep[i] = make_float4(id.x, epf, (float)ev, id.w);
+            store_t2(out.str, i, narrow6(sd));
+            return;
+        }
+        if (M.model == 1) {
             dp_update_d(M, hdt, w, dd, p, ep, sd);
-        } else if (kVW) {
-            vw_update_d(vw_const(vw, id.x), hdt, dd, w, sd, ev);
-            ep = sqrt(2.0 / 3.0 * contract6(e, e));
         } else {
             hypo_update_d(M, hdt, dd, w, sd);
             ep = sqrt(2.0 / 3.0 * contract6(e, e));
@@ -116,16 +127,22 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_predict(
     float p = x0.w;
     float ep = id.y, ev = id.z;
     tensor2d s = s0;
-    if (!kVW && M.model == 1) {
-        dp_update(M, 0.5f * dt, w, de, p, ep, s);
-    } else if (kVW) {
-        /* the adaptive sub-stepping runs in FP64 in both forms */
+    if (kVW) {
+        /* the adaptive sub-stepping runs in FP64 in both forms; the
+         * kinematics are stored first */
+        out.pos[i] = x;
+        out.vel[i] = v;
+        store_t2(out.stn, i, e);
+        const float epf = sqrtf(2.0f / 3.0f * J2(e));
         T6d sd = widen6(s0);
         double evd = ev;
-        vw_update_d(vw_const(vw, id.x), 0.5 * (double)dt, widen6(de), w, sd, evd);
-        s = narrow6(sd);
-        ev = (float)evd;
-        ep = sqrtf(2.0f / 3.0f * J2(e));
+        vw_update_d(vw_const(vw, id.x), 0.5 * (double)dt, de, w, sd, evd);
+        out.idep[i] = make_float4(id.x, epf, (float)evd, id.w);
+        store_t2(out.str, i, narrow6(sd));
+        return;
+    }
+    if (M.model == 1) {
+        dp_update(M, 0.5f * dt, w, de, p, ep, s);
     } else {
         hypo_update(M, 0.5f * dt, de, w, s);
         ep = sqrtf(2.0f / 3.0f * J2(e));
@@ -190,6 +207,70 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(
     const float4 id = cur.idep[i];
     const Material M = particle_material(load_material(P), mt, id.x);
 
+    if (kVW) {
+        /* model 3: the kinematics, the health of the kinematics and the
+         * Verlet check come before the FP64 sub-stepping, so that its
+         * registers need not share the SM with them */
+        float4 v, x;
+        tensor2d e;
+        float ep;
+        if (kMixed) {
+            const double ddt = dt;
+            const double4 v0d = ini.vd[k], x0d = ini.xd[k];
+            double4 vd, xd;
+            vd.x = v0d.x + ddt * a.x; vd.y = v0d.y + ddt * a.y; vd.z = v0d.z + ddt * a.z; vd.w = v0d.w + ddt * a.w;
+            xd.x = 0.5 * (vd.x + v0d.x) * ddt + x0d.x;
+            xd.y = 0.5 * (vd.y + v0d.y) * ddt + x0d.y;
+            xd.z = 0.5 * (vd.z + v0d.z) * ddt + x0d.z;
+            xd.w = 0.0;
+            T6d ed = widen6(e0);
+            const T6d dd = widen6(de);
+            ed.xx += dd.xx * ddt; ed.yy += dd.yy * ddt; ed.zz += dd.zz * ddt;
+            ed.xy += dd.xy * ddt; ed.xz += dd.xz * ddt; ed.yz += dd.yz * ddt;
+            out.xd[i] = xd;
+            out.vd[i] = vd;
+            v = make_float4((float)vd.x, (float)vd.y, (float)vd.z, (float)vd.w);
+            x = make_float4((float)xd.x, (float)xd.y, (float)xd.z, xc.w);
+            e = narrow6(ed);
+            ep = (float)sqrt(2.0 / 3.0 * contract6(ed, ed));
+        } else {
+            v.x = v0.x + dt * a.x;
+            v.y = v0.y + dt * a.y;
+            v.z = v0.z + dt * a.z;
+            v.w = v0.w + dt * a.w;
+            x.x = 0.5f * (v.x + v0.x) * dt + x0.x;
+            x.y = 0.5f * (v.y + v0.y) * dt + x0.y;
+            x.z = 0.5f * (v.z + v0.z) * dt + x0.z;
+            x.w = xc.w;
+            e = e0 + de * dt;
+            ep = sqrtf(2.0f / 3.0f * J2(e));
+        }
+        out.pos[i] = x;
+        out.vel[i] = v;
+        store_t2(out.stn, i, e);
+        const bool bad = !(isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(v.x) && isfinite(v.y) &&
+                           isfinite(v.z) && isfinite(v.w));
+        if (verlet.xbuild) {
+            const float4 xb = __ldg(verlet.xbuild + i);
+            const float dx = x.x - xb.x, dy = x.y - xb.y, dz = x.z - xb.z;
+            const float moved = sqrtf(dx * dx + dy * dy + dz * dz);
+            const float speed = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
+            const float accel = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
+            const float dtb = verlet.dt_bound;
+            const float ahead = 2.0f * dtb * (speed + dtb * accel);
+            if (!(moved + ahead < verlet.half_skin)) atomicOr(verlet.rebuild, 1);
+        }
+        T6d sd = widen6(s0);
+        double evd = id0.z;
+        vw_update_d(vw_const(vw, id.x), (double)dt, de, w, sd, evd);
+        const tensor2d s = narrow6(sd);
+        out.idep[i] = make_float4(id.x, ep, (float)evd, id.w);
+        store_t2(out.str, i, s);
+        if (health && (bad || !(isfinite(s.xx) && isfinite(s.yy) && isfinite(s.zz) && isfinite(s.xy) &&
+                                isfinite(s.xz) && isfinite(s.yz))))
+            atomicAdd(health + HEALTH_NONFINITE, 1);
+        return;
+    }
     float4 v, x;
     tensor2d s, e;
     float ep, ev = id.z;
@@ -207,13 +288,8 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(
         ed.xy += dd.xy * ddt; ed.xz += dd.xz * ddt; ed.yz += dd.yz * ddt;
         double pd = xc.w, epd = ep0;
         T6d sd = widen6(s0);
-        if (!kVW && M.model == 1) {
+        if (M.model == 1) {
             dp_update_d(M, ddt, w, dd, pd, epd, sd);
-        } else if (kVW) {
-            double evd = id0.z;
-            vw_update_d(vw_const(vw, id.x), ddt, dd, w, sd, evd);
-            ev = (float)evd;
-            epd = sqrt(2.0 / 3.0 * contract6(ed, ed));
         } else {
             hypo_update_d(M, ddt, dd, w, sd);
             epd = sqrt(2.0 / 3.0 * contract6(ed, ed));
@@ -237,15 +313,8 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(
         float p = xc.w;
         ep = ep0;
         s = s0;
-        if (!kVW && M.model == 1) {
+        if (M.model == 1) {
             dp_update(M, dt, w, de, p, ep, s);
-        } else if (kVW) {
-            T6d sd = widen6(s0);
-            double evd = id0.z;
-            vw_update_d(vw_const(vw, id.x), (double)dt, widen6(de), w, sd, evd);
-            s = narrow6(sd);
-            ev = (float)evd;
-            ep = sqrtf(2.0f / 3.0f * J2(e));
         } else {
             hypo_update(M, dt, de, w, s);
             ep = sqrtf(2.0f / 3.0f * J2(e));

@@ -402,32 +402,39 @@ __device__ __forceinline__ double trace_cube6(const T6d& A)
 
 /* The rate with the state-dependent powers through shared logarithms:
  * pr = -trT/hs, pr^n = exp(n ln pr), pr^(1-n) = pr / pr^n, ex = exp(-pr^n),
- * fe = exp(beta (ln ec0 - pr^n - ln e)), fd = exp(alpha ln((e - ed) / (ec - ed))). */
-__device__ __forceinline__ void vw_rate_d(const VWConst& c, const T6d& Tin, double e, const T6d& d,
+ * fe = exp(beta (ln ec0 - pr^n - ln e)), fd = exp(alpha ln((e - ed) / (ec - ed))).
+ * The stretching d stays in float (it is read as float) and the deviator
+ * That* is formed from That where needed, to spare registers. */
+__device__ __forceinline__ void vw_rate_d(const VWConst& c, const T6d& Tin, double e, const tensor2d& d,
                                           const float4& w, T6d& R, double& edot)
 {
-    T6d T = Tin;
-    double trT = T.xx + T.yy + T.zz;
+    T6d Th = Tin;
+    double trT = Th.xx + Th.yy + Th.zz;
     if (!(trT < -3.0)) {
-        T = T6d{-1.0, -1.0, -1.0, 0.0, 0.0, 0.0};
+        Th = T6d{-1.0, -1.0, -1.0, 0.0, 0.0, 0.0};
         trT = -3.0;
     }
     const double it = 1.0 / trT;
-    T6d Th{T.xx * it, T.yy * it, T.zz * it, T.xy * it, T.xz * it, T.yz * it};
-    T6d Ts{Th.xx - 1.0 / 3.0, Th.yy - 1.0 / 3.0, Th.zz - 1.0 / 3.0, Th.xy, Th.xz, Th.yz};
-    double TsTs = contract6(Ts, Ts);
+    Th = T6d{Th.xx * it, Th.yy * it, Th.zz * it, Th.xy * it, Th.xz * it, Th.yz * it};
+    const double third = 1.0 / 3.0;
+    /* That* = That - I/3: the off-diagonal parts are That's */
+    double sxx = Th.xx - third, syy = Th.yy - third, szz = Th.zz - third;
+    double TsTs = sxx * sxx + syy * syy + szz * szz + 2.0 * (Th.xy * Th.xy + Th.xz * Th.xz + Th.yz * Th.yz);
     double tpsi = sqrt(3.0 * TsTs);
     const double lim = sqrt(2.0) * (1.0 - 1e-3);
     if (tpsi > lim) {
         const double f = lim / tpsi;
-        Ts = T6d{Ts.xx * f, Ts.yy * f, Ts.zz * f, Ts.xy * f, Ts.xz * f, Ts.yz * f};
-        Th = T6d{Ts.xx + 1.0 / 3.0, Ts.yy + 1.0 / 3.0, Ts.zz + 1.0 / 3.0, Ts.xy, Ts.xz, Ts.yz};
+        sxx *= f; syy *= f; szz *= f;
+        Th = T6d{sxx + third, syy + third, szz + third, Th.xy * f, Th.xz * f, Th.yz * f};
         TsTs *= f * f;
         tpsi = lim;
     }
     const double ThTh = contract6(Th, Th);
     double c3t = 1.0;
-    if (TsTs > 1e-30) c3t = -sqrt(6.0) * trace_cube6(Ts) / (TsTs * sqrt(TsTs));
+    if (TsTs > 1e-30) {
+        const T6d Ts{sxx, syy, szz, Th.xy, Th.xz, Th.yz};
+        c3t = -sqrt(6.0) * trace_cube6(Ts) / (TsTs * sqrt(TsTs));
+    }
     c3t = fmax(-1.0, fmin(1.0, c3t));
     const double F = sqrt(fmax(tpsi * tpsi / 8.0 + (2.0 - tpsi * tpsi) / (2.0 + sqrt(2.0) * tpsi * c3t), 0.0)) -
                      tpsi / (2.0 * sqrt(2.0));
@@ -439,30 +446,33 @@ __device__ __forceinline__ void vw_rate_d(const VWConst& c, const T6d& Tin, doub
     const double q = (e - ed) / (ec - ed);
     const double fd = q > 0.0 ? exp(c.alpha * log(q)) : (c.alpha == 0.0 ? 1.0 : 0.0);
     const double fb = c.fbk * (1.0 + 1.0 / ei) * (-trT * c.ihs) / prn;
-    const double ThD = contract6(Th, d);
-    const double nD = sqrt(contract6(d, d));
+    const double dxx = d.xx, dyy = d.yy, dzz = d.zz, dxy = d.xy, dxz = d.xz, dyz = d.yz;
+    const double ThD = Th.xx * dxx + Th.yy * dyy + Th.zz * dzz + 2.0 * (Th.xy * dxy + Th.xz * dxz + Th.yz * dyz);
+    const double nD = sqrt(dxx * dxx + dyy * dyy + dzz * dzz + 2.0 * (dxy * dxy + dxz * dxz + dyz * dyz));
     const double k0 = fb * fe / ThTh;
     const double F2 = F * F, nf = fd * c.a * F * nD;
     const T6d J = jaumann_d(w, Tin);
-    R.xx = k0 * (F2 * d.xx + c.a2 * Th.xx * ThD + nf * (Th.xx + Ts.xx)) + J.xx;
-    R.yy = k0 * (F2 * d.yy + c.a2 * Th.yy * ThD + nf * (Th.yy + Ts.yy)) + J.yy;
-    R.zz = k0 * (F2 * d.zz + c.a2 * Th.zz * ThD + nf * (Th.zz + Ts.zz)) + J.zz;
-    R.xy = k0 * (F2 * d.xy + c.a2 * Th.xy * ThD + nf * (Th.xy + Ts.xy)) + J.xy;
-    R.xz = k0 * (F2 * d.xz + c.a2 * Th.xz * ThD + nf * (Th.xz + Ts.xz)) + J.xz;
-    R.yz = k0 * (F2 * d.yz + c.a2 * Th.yz * ThD + nf * (Th.yz + Ts.yz)) + J.yz;
-    edot = (1.0 + e) * (d.xx + d.yy + d.zz);
+    R.xx = k0 * (F2 * dxx + c.a2 * Th.xx * ThD + nf * (Th.xx + sxx)) + J.xx;
+    R.yy = k0 * (F2 * dyy + c.a2 * Th.yy * ThD + nf * (Th.yy + syy)) + J.yy;
+    R.zz = k0 * (F2 * dzz + c.a2 * Th.zz * ThD + nf * (Th.zz + szz)) + J.zz;
+    R.xy = k0 * (F2 * dxy + c.a2 * Th.xy * ThD + nf * (2.0 * Th.xy)) + J.xy;
+    R.xz = k0 * (F2 * dxz + c.a2 * Th.xz * ThD + nf * (2.0 * Th.xz)) + J.xz;
+    R.yz = k0 * (F2 * dyz + c.a2 * Th.yz * ThD + nf * (2.0 * Th.yz)) + J.yz;
+    edot = (1.0 + e) * (dxx + dyy + dzz);
 }
 
 /* Adaptive explicit integration over dt; returns the number of sub-steps.
  * The loop has one rate evaluation site (inlined once): each pass evaluates
- * either the first rate of a trial at (s, e) or the second at the Euler
- * point (s1, e1); a rejected trial keeps its first rate. */
-__device__ __forceinline__ int vw_update_d(const VWConst& c, double dt, const T6d& d, const float4& w, T6d& s,
+ * either the first rate k1 of a trial at (s, e) or the second, k2, at the
+ * Euler point s + h k1.  The Heun result is s + h/2 (k1 + k2) and its
+ * difference from the Euler point, h/2 (k2 - k1), is the error estimate; a
+ * rejected trial keeps its k1. */
+__device__ __forceinline__ int vw_update_d(const VWConst& c, double dt, const tensor2d& d, const float4& w, T6d& s,
                                            double& e)
 {
     double t = 0.0, h = dt;
     int steps = 0;
-    T6d k1{}, s1{}, x = s;
+    T6d k1{}, x = s;
     double ke1 = 0.0, xe = e;
     bool have_k1 = false;
     while (t < dt) {
@@ -474,16 +484,17 @@ __device__ __forceinline__ int vw_update_d(const VWConst& c, double dt, const T6
             ke1 = re;
             have_k1 = true;
         } else {
-            const T6d s2{s.xx + 0.5 * h * (k1.xx + r.xx), s.yy + 0.5 * h * (k1.yy + r.yy),
-                         s.zz + 0.5 * h * (k1.zz + r.zz), s.xy + 0.5 * h * (k1.xy + r.xy),
-                         s.xz + 0.5 * h * (k1.xz + r.xz), s.yz + 0.5 * h * (k1.yz + r.yz)};
-            const T6d df{s2.xx - s1.xx, s2.yy - s1.yy, s2.zz - s1.zz, s2.xy - s1.xy, s2.xz - s1.xz, s2.yz - s1.yz};
+            const double hh = 0.5 * h;
+            const T6d s2{s.xx + hh * (k1.xx + r.xx), s.yy + hh * (k1.yy + r.yy), s.zz + hh * (k1.zz + r.zz),
+                         s.xy + hh * (k1.xy + r.xy), s.xz + hh * (k1.xz + r.xz), s.yz + hh * (k1.yz + r.yz)};
+            const T6d df{hh * (r.xx - k1.xx), hh * (r.yy - k1.yy), hh * (r.zz - k1.zz),
+                         hh * (r.xy - k1.xy), hh * (r.xz - k1.xz), hh * (r.yz - k1.yz)};
             const double err = sqrt(contract6(df, df) / fmax(contract6(s2, s2), 1e-30));
             ++steps;
             const bool last = steps >= c.maxsub - 1 || h <= dt * 1e-6;
             if (err <= c.tol || last) {
                 s = s2;
-                e += 0.5 * h * (ke1 + re);
+                e += hh * (ke1 + re);
                 t += h;
                 const double g = err > 0.0 ? 0.9 * sqrt(c.tol / err) : 2.0;
                 h *= fmin(2.0, fmax(0.2, g));
@@ -497,9 +508,8 @@ __device__ __forceinline__ int vw_update_d(const VWConst& c, double dt, const T6
         /* trial from (s, e) with the first rate k1 */
         h = fmin(h, dt - t);
         if (steps >= c.maxsub - 1) h = dt - t;
-        s1 = T6d{s.xx + h * k1.xx, s.yy + h * k1.yy, s.zz + h * k1.zz, s.xy + h * k1.xy, s.xz + h * k1.xz,
-                 s.yz + h * k1.yz};
-        x = s1;
+        x = T6d{s.xx + h * k1.xx, s.yy + h * k1.yy, s.zz + h * k1.zz, s.xy + h * k1.xy, s.xz + h * k1.xz,
+                s.yz + h * k1.yz};
         xe = e + h * ke1;
     }
     return steps;

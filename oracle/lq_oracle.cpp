@@ -605,7 +605,7 @@ int vw_update(const VW& c, double dt, const double* d, const double* w, double* 
         double num = 0.0, den = 0.0;
         for (int k = 0; k < 6; ++k) {
             s2[k] = s[k] + 0.5 * h * (k1[k] + k2[k]);
-            const double df = s2[k] - s1[k];
+            const double df = 0.5 * h * (k2[k] - k1[k]);   /* Heun minus Euler */
             num += df * df * (k < 3 ? 1.0 : 2.0);
             den += s2[k] * s2[k] * (k < 3 ? 1.0 : 2.0);
         }
