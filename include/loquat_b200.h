@@ -205,9 +205,12 @@ int lq_sim_set_frames(void* sim, int n, const int* rows);
  * with the Shepard pass; a rebuild adds lq_sim_rebuild_launches more. */
 int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard);
 int lq_sim_rebuild_launches(void* sim, int* launches);
-/* Launch shape of the pair kernel (threads per block x resident blocks per
- * SM, which caps its registers): 0 = 128 x 6 (default), 1 = 64 x 12,
- * 2 = 256 x 3, 3 = 128 x 5, 4 = 128 x 7.  Results do not depend on it. */
+/* Launch shape of the pair kernel.  0-4: one thread per target, threads
+ * per block x resident blocks per SM (which caps its registers): 0 = 128 x 6
+ * (default), 1 = 64 x 12, 2 = 256 x 3, 3 = 128 x 5, 4 = 128 x 7; these give
+ * bit-identical results.  5, 6: warp-cooperative, 8 or 32 lanes share a
+ * target's list and combine their sums with shuffle reductions (for small
+ * cases); the summation order differs, so results agree to rounding. */
 int lq_sim_set_pair_shape(void* sim, int shape);
 /* Autotuner: times `steps` steps (after two untimed ones) for each pair
  * kernel shape at the current skin, then for skins of 0.02, 0.05, 0.1 and

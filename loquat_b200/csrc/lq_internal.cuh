@@ -140,8 +140,9 @@ int launch_interaction_list(const Parameters* par_host, const Parameters* par_de
                             const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr = Frames(),
                             bool compensated = false, float* rec = nullptr, int shape = 0);
 /* Launch shapes of the packed pair kernel: {threads per block, resident
- * blocks per SM}. */
-constexpr int kPairShapeCount = 5;
+ * blocks per SM}, or {128, -G} for the warp-cooperative form with G lanes
+ * per target. */
+constexpr int kPairShapeCount = 7;
 extern const int kPairShapes[kPairShapeCount][2];
 int launch_adami(const Parameters* par_host, const Parameters* par_dev, const State& st, const Cells& c,
                  cudaStream_t s);

@@ -517,6 +517,61 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_interaction_rec(
     store_rates(P, K, rt, i, T);
 }
 
+/* Warp-cooperative form: a group of G lanes (G = 8 or 32) shares one
+ * target, lane g taking list entries g, g + G, ...; the group's partial sums
+ * are combined with shuffle reductions.  With few targets (a small case) a
+ * thread per target leaves most of the GPU idle and each thread's chain of
+ * dependent gathers long; groups give G times the parallelism.  In the
+ * compensated form each lane keeps its Kahan pair and the reduction adds
+ * sum - compensation. */
+template <int G>
+__device__ __forceinline__ float group_sum(float v)
+{
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, G);
+    return v;
+}
+
+template <bool kKahan, int G>
+__global__ void __launch_bounds__(128) k_interaction_group(const Parameters* __restrict__ P, int np, int npb,
+                                                           State st, Rates rt, Cells cells,
+                                                           const int* __restrict__ list,
+                                                           const int* __restrict__ count, int stride, Frames fr,
+                                                           NbrArrays nb)
+{
+    const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const int g = threadIdx.x % G;
+    const int t = gid;
+    const int i = npb + t;
+    const bool active = i < np;      /* whole groups leave together: no early return before the shuffles */
+    const PairConst K = load_pair_const(P);
+    Target T;
+    load_target(K, st, active ? i : npb, active, T);
+    const int n = active ? __ldg(count + t) : 0;
+    if (n <= LQ_NBR_CAP) {
+        for (int k = g; k < n; k += G) {
+            const int j = __ldg(list + (size_t)k * stride + t);
+            if (lq_in_range(j, np)) pair_body_rec<kKahan>(K, nb, T, j);
+        }
+    } else if (g == 0) {
+        walk_stencil(P, K, st, cells, i, T.x, [&](int j) { pair_body<kKahan>(K, st, T, j); }, fr);
+    }
+    if (kKahan) {
+        T.drho -= T.cdrho;
+        T.ax -= T.cax;
+        T.ay -= T.cay;
+        T.az -= T.caz;
+    }
+    T.drho = group_sum<G>(T.drho);
+    T.ax = group_sum<G>(T.ax);
+    T.ay = group_sum<G>(T.ay);
+    T.az = group_sum<G>(T.az);
+    T.l00 = group_sum<G>(T.l00); T.l01 = group_sum<G>(T.l01); T.l02 = group_sum<G>(T.l02);
+    T.l10 = group_sum<G>(T.l10); T.l11 = group_sum<G>(T.l11); T.l12 = group_sum<G>(T.l12);
+    T.l20 = group_sum<G>(T.l20); T.l21 = group_sum<G>(T.l21); T.l22 = group_sum<G>(T.l22);
+    if (active && g == 0) store_rates(P, K, rt, i, T);
+}
+
 /* ------------------------------------------------------------- Adami */
 /* Per-cell visiting order and the float expressions follow the reference
  * kernel (src/adami_boundary.cu:27-123) so both produce the same sums. */
@@ -800,8 +855,10 @@ int launch_density_filter_list(const Parameters* ph, const Parameters* pd, const
 }
 
 /* Launch shapes of the pair kernel: threads per block x resident blocks
- * per SM (the register cap).  Shape 0 is the default. */
-const int kPairShapes[kPairShapeCount][2] = {{kBlock, LQ_PAIR_MIN_BLOCKS}, {64, 12}, {256, 3}, {128, 5}, {128, 7}};
+ * per SM (the register cap); a negative second entry -G marks the
+ * warp-cooperative form with G lanes per target.  Shape 0 is the default. */
+const int kPairShapes[kPairShapeCount][2] = {{kBlock, LQ_PAIR_MIN_BLOCKS}, {64, 12}, {256, 3}, {128, 5},
+                                             {128, 7}, {128, -8}, {128, -32}};
 
 /* This translation unit's count of bounds violations (always 0 without
  * LQ_CHECKED). */
@@ -885,6 +942,28 @@ int launch_interaction_list(const Parameters* ph, const Parameters* pd, const St
             case 2: LQ_PAIR_LAUNCH(256, 3); break;
             case 3: LQ_PAIR_LAUNCH(128, 5); break;
             case 4: LQ_PAIR_LAUNCH(128, 7); break;
+            case 5:
+            case 6: {
+                const int G = shape == 5 ? 8 : 32;
+                const int nthreads = ph->npm * G;
+                const int grid = (nthreads + 127) / 128;
+                if (G == 8) {
+                    if (compensated)
+                        k_interaction_group<true, 8><<<grid, 128, 0, s>>>(pd, ph->np, ph->npb, st, r, c, nl.list,
+                                                                          nl.count, nl.stride, fr, nb);
+                    else
+                        k_interaction_group<false, 8><<<grid, 128, 0, s>>>(pd, ph->np, ph->npb, st, r, c, nl.list,
+                                                                           nl.count, nl.stride, fr, nb);
+                } else {
+                    if (compensated)
+                        k_interaction_group<true, 32><<<grid, 128, 0, s>>>(pd, ph->np, ph->npb, st, r, c, nl.list,
+                                                                           nl.count, nl.stride, fr, nb);
+                    else
+                        k_interaction_group<false, 32><<<grid, 128, 0, s>>>(pd, ph->np, ph->npb, st, r, c, nl.list,
+                                                                            nl.count, nl.stride, fr, nb);
+                }
+                break;
+            }
             default: LQ_PAIR_LAUNCH(kBlock, LQ_PAIR_MIN_BLOCKS); break;
         }
 #undef LQ_PAIR_LAUNCH
