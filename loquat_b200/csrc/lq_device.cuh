@@ -4,6 +4,8 @@
  */
 #pragma once
 
+#include <cstdio>
+
 #include <cuda_runtime.h>
 #include <types.h>
 #include "lq_internal.cuh"
@@ -17,12 +19,15 @@ namespace lqb {
  * build the check is a constant true and compiles away. */
 #ifdef LQ_CHECKED
 static __device__ unsigned long long lq_bounds_count;
-__device__ __forceinline__ bool lq_in_range(long long j, long long n)
+__device__ __forceinline__ bool lq_in_range_at(long long j, long long n, int line)
 {
     if (j >= 0 && j < n) return true;
-    atomicAdd(&lq_bounds_count, 1ull);
+    /* the first few violations name their source line */
+    if (atomicAdd(&lq_bounds_count, 1ull) < 4ull)
+        printf("LQ_CHECKED: bounds violation at line %d: index %lld, limit %lld\n", line, j, n);
     return false;
 }
+#define lq_in_range(j, n) lq_in_range_at((long long)(j), (long long)(n), __LINE__)
 #else
 __device__ __forceinline__ constexpr bool lq_in_range(long long, long long) { return true; }
 #endif

@@ -138,7 +138,14 @@ int launch_neighbor_list(const Parameters* par_host, const Parameters* par_dev, 
  * kernel reads the state arrays. */
 int launch_interaction_list(const Parameters* par_host, const Parameters* par_dev, const State& st, const Rates& r,
                             const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr = Frames(),
-                            bool compensated = false, float* rec = nullptr, int shape = 0);
+                            bool compensated = false, float* rec = nullptr, int shape = 0, bool pack = true);
+/* The packed neighbour arrays of slots [first, np) from the state. */
+int launch_pack_neighbors(const Parameters* par_host, const State& st, float* rec, int first, cudaStream_t s);
+/* Adami over the boundary lists reading the packed arrays (material slots
+ * packed), writing the boundary stress into the state and the packed
+ * arrays. */
+int launch_adami_packed(const Parameters* par_host, const Parameters* par_dev, const State& st,
+                        const NeighborList& nl, float* rec, cudaStream_t s);
 /* Launch shapes of the packed pair kernel: {threads per block, resident
  * blocks per SM}, or {128, -G} for the warp-cooperative form with G lanes
  * per target. */

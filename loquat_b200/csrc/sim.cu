@@ -242,6 +242,9 @@ int enqueue_rebuild(LqSim* S, cudaStream_t s)
                                            S->S.idep, S->fr));
     LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, S->nlb, S->health, s,
                                            S->S.idep, S->fr));
+    /* every slot's packed neighbour data (the boundary slots keep theirs
+     * until the next build) */
+    if (S->rec) LQ_TRY(lqb::launch_pack_neighbors(ph, S->S, S->rec, 0, s));
     return LQ_OK;
 }
 
@@ -270,6 +273,17 @@ int enqueue_density_filter(LqSim* S, cudaStream_t s)
     return LQ_OK;
 }
 
+/* Adami for a stage.  With the packed neighbour arrays, the material slots
+ * are packed first, Adami reads them and writes the boundary slots' packed
+ * stress itself (boundary positions and velocities are packed at each list
+ * build and do not change in between), so the pair kernel needs no pack. */
+int enqueue_adami_pack(LqSim* S, const State& st, cudaStream_t s)
+{
+    if (!S->rec) return lqb::launch_adami_list(&S->ph, S->pd, st, S->nlb, s);
+    LQ_TRY(lqb::launch_pack_neighbors(&S->ph, st, S->rec, S->npb, s));
+    return lqb::launch_adami_packed(&S->ph, S->pd, st, S->nlb, S->rec, s);
+}
+
 /* The two stages of a step on the current lists. */
 int enqueue_stages(LqSim* S, cudaStream_t s)
 {
@@ -277,14 +291,14 @@ int enqueue_stages(LqSim* S, cudaStream_t s)
     const Parameters* pd = S->pd;
     const lqb::Cells cells{S->g.start, nullptr, nullptr};
     /* predictor stage (reference src/loquat.cu:343-368) */
-    LQ_TRY(lqb::launch_adami_list(ph, pd, S->S, S->nlb, s));
+    LQ_TRY(enqueue_adami_pack(S, S->S, s));
     LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S, S->R, cells, S->nlm, s, S->fr, S->flags & LQ_SIM_MIXED,
-                                        S->rec, S->pair_shape));
+                                        S->rec, S->pair_shape, false));
     LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt, S->vw));
     /* corrector stage (reference src/loquat.cu:371-396) */
-    LQ_TRY(lqb::launch_adami_list(ph, pd, S->S2, S->nlb, s));
+    LQ_TRY(enqueue_adami_pack(S, S->S2, s));
     LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S2, S->R, cells, S->nlm, s, S->fr, S->flags & LQ_SIM_MIXED,
-                                        S->rec, S->pair_shape));
+                                        S->rec, S->pair_shape, false));
     LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild, S->skin, s,
                                     S->mt, S->vw));
     return enqueue_dynamic_dt(S, s);
@@ -1152,8 +1166,9 @@ extern "C" int lq_sim_rebuild_launches(void* sim, int* launches)
     if (!sim || !launches) return lqb::set_error(LQ_ERR_ARG, "lq_sim_rebuild_launches: null argument");
     LqSim* S = static_cast<LqSim*>(sim);
     /* count reset, hash, scatter, cell order (the scan is a library
-     * kernel), gather, copy, material list, boundary list (when npb > 0) */
-    *launches = 4 + 1 + 1 + 1 + (S->npb > 0 ? 1 : 0);
+     * kernel), gather, copy, material list, boundary list (when npb > 0),
+     * full pack of the neighbour data */
+    *launches = 4 + 1 + 1 + 1 + (S->npb > 0 ? 1 : 0) + (S->rec ? 1 : 0);
     return LQ_OK;
 }
 
@@ -1216,16 +1231,17 @@ int profiled_step(LqSim* S, PhaseTimer& T)
                                                s, S->S.idep, S->fr));
         LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, S->nlb, S->health, s,
                                                S->S.idep, S->fr));
+        if (S->rec) LQ_TRY(lqb::launch_pack_neighbors(ph, S->S, S->rec, 0, s));
         LQ_TRY(T.close(s));
     }
     State* cur[2] = {&S->S, &S->S2};
     for (int stage = 0; stage < 2; ++stage) {
         LQ_TRY(T.mark(s, PH_ADAMI));
-        LQ_TRY(lqb::launch_adami_list(ph, pd, *cur[stage], S->nlb, s));
+        LQ_TRY(enqueue_adami_pack(S, *cur[stage], s));
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_INTERACTION));
         LQ_TRY(lqb::launch_interaction_list(ph, pd, *cur[stage], S->R, cells, S->nlm, s, S->fr,
-                                            S->flags & LQ_SIM_MIXED, S->rec, S->pair_shape));
+                                            S->flags & LQ_SIM_MIXED, S->rec, S->pair_shape, false));
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_INTEGRATE));
         if (stage == 0)

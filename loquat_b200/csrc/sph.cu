@@ -461,9 +461,9 @@ __global__ void __launch_bounds__(kBlock, LQ_PAIR_MIN_BLOCKS) k_interaction_list
     store_rates(P, K, rt, i, T);
 }
 
-__global__ void __launch_bounds__(kBlock) k_pack_neighbors(int np, State st, NbrArrays nb)
+__global__ void __launch_bounds__(kBlock) k_pack_neighbors(int first, int np, State st, NbrArrays nb)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = first + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
     const float4 x = __ldg(st.pos + i);
     const float4 v = __ldg(st.vel + i);
@@ -759,6 +759,69 @@ __global__ void __launch_bounds__(kBlock) k_adami_list(const Parameters* __restr
     }
 }
 
+/* k_adami_list reading the material neighbours from the packed arrays
+ * (sigma_j V_j W = s_j rho_j m W with s = sigma / rho^2), and writing the
+ * boundary particle's new stress both into the state and, scaled, into the
+ * packed arrays, which then need no pack of the boundary slots before the
+ * pair kernel.  Targets without neighbours keep both as they were. */
+__global__ void __launch_bounds__(kBlock) k_adami_packed(const Parameters* __restrict__ P, int npb, State st,
+                                                         const int* __restrict__ list,
+                                                         const int* __restrict__ count, int stride, NbrArrays nb)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npb) return;
+    const int n = min(__ldg(count + i), LQ_NBR_CAP);
+    if (n == 0) return;
+    const int np_all = __ldg(&P->np);
+    const float ih = __ldg(&P->i_h), m = __ldg(&P->m), Cw = __ldg(&P->kernel_normalization_par);
+    const float4 xi = __ldg(st.pos + i);
+    tensor2d S = make_tensor2d(0.0f);
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int k = 0; k < n; ++k) {
+        const int j = __ldg(list + (size_t)k * stride + i);
+        if (!lq_in_range(j, np_all)) continue;
+        const float4 xr = __ldg(nb.xr + j);
+        const float3 d = make_float3(xi.x - xr.x, xi.y - xr.y, xi.z - xr.z);
+        const float q = norm3df(d.x, d.y, d.z) * ih;
+        if (q < 2.0f) {
+            const float ker = Cw * (2.0f - q) * (2.0f - q) * (2.0f - q) * (2.0f - q) * (q + 0.5f);
+            const float vol = m / xr.w;
+            const float cs = m * xr.w * ker;
+            const float4 vs = __ldg(nb.vs + j);
+            const float4 s3 = __ldg(nb.s3 + j);
+            const float s1 = __ldg(nb.s1 + j);
+            S.xx += vs.w * cs;
+            S.yy += s3.x * cs;
+            S.zz += s3.y * cs;
+            S.xy += s3.z * cs;
+            S.xz += s3.w * cs;
+            S.yz += s1 * cs;
+            acc.x += d.x * ker * vol;
+            acc.y += d.y * ker * vol;
+            acc.z += d.z * ker * vol;
+            acc.w += ker * vol;
+        }
+    }
+    if (acc.w > 0.0f) {
+        const float rho0 = __ldg(&P->rho0);
+        tensor2d out;
+        out.xx = (S.xx - rho0 * __ldg(&P->acc_x) * acc.x) / acc.w;
+        out.yy = (S.yy - rho0 * __ldg(&P->acc_y) * acc.y) / acc.w;
+        out.zz = (S.zz - rho0 * __ldg(&P->acc_z) * acc.z) / acc.w;
+        out.xy = S.xy / acc.w;
+        out.xz = S.xz / acc.w;
+        out.yz = S.yz / acc.w;
+        store_t2(st.str, i, out);
+        /* as k_pack_neighbors scales it */
+        const float rinv = __fdividef(1.0f, __ldg(&st.vel[i].w));
+        const float ri2 = rinv * rinv;
+        const float4 v = __ldg(st.vel + i);
+        nb.vs[i] = make_float4(v.x, v.y, v.z, out.xx * ri2);
+        nb.s3[i] = make_float4(out.yy * ri2, out.zz * ri2, out.xy * ri2, out.xz * ri2);
+        nb.s1[i] = out.yz * ri2;
+    }
+}
+
 /* ----------------------------------------------- list-driven Shepard */
 /* The Shepard filter of k_shepard over a material particle's list (its
  * boundary neighbours are skipped: the filter uses the material layer
@@ -900,6 +963,32 @@ int launch_neighbor_list_range(const Parameters* ph, const Parameters* pd, int f
     return LQ_OK;
 }
 
+static NbrArrays nbr_arrays(float* rec, int np)
+{
+    const size_t n = (size_t)np;
+    return NbrArrays{reinterpret_cast<float4*>(rec), reinterpret_cast<float4*>(rec) + n,
+                     reinterpret_cast<float4*>(rec) + 2 * n, rec + 12 * n};
+}
+
+int launch_pack_neighbors(const Parameters* ph, const State& st, float* rec, int first, cudaStream_t s)
+{
+    const int n = ph->np - first;
+    if (n <= 0) return LQ_OK;
+    k_pack_neighbors<<<blocks_for(n, kBlock), kBlock, 0, s>>>(first, ph->np, st, nbr_arrays(rec, ph->np));
+    LQ_TRY_CUDA(cudaGetLastError(), "k_pack_neighbors");
+    return LQ_OK;
+}
+
+int launch_adami_packed(const Parameters* ph, const Parameters* pd, const State& st, const NeighborList& nl,
+                        float* rec, cudaStream_t s)
+{
+    if (ph->npb <= 0) return LQ_OK;
+    k_adami_packed<<<blocks_for(ph->npb, kBlock), kBlock, 0, s>>>(pd, ph->npb, st, nl.list, nl.count, nl.stride,
+                                                                 nbr_arrays(rec, ph->np));
+    LQ_TRY_CUDA(cudaGetLastError(), "k_adami_packed");
+    return LQ_OK;
+}
+
 int launch_adami_list(const Parameters* ph, const Parameters* pd, const State& st, const NeighborList& nl,
                       cudaStream_t s)
 {
@@ -921,7 +1010,7 @@ int launch_shepard_list(const Parameters* ph, const Parameters* pd, const State&
 
 int launch_interaction_list(const Parameters* ph, const Parameters* pd, const State& st, const Rates& r,
                             const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr,
-                            bool compensated, float* rec, int shape)
+                            bool compensated, float* rec, int shape, bool pack)
 {
     if (ph->npm <= 0) return LQ_OK;
     if (rec) {
@@ -930,8 +1019,10 @@ int launch_interaction_list(const Parameters* ph, const Parameters* pd, const St
         const size_t n = (size_t)ph->np;
         NbrArrays nb{reinterpret_cast<float4*>(rec), reinterpret_cast<float4*>(rec) + n,
                      reinterpret_cast<float4*>(rec) + 2 * n, rec + 12 * n};
-        k_pack_neighbors<<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(ph->np, st, nb);
-        LQ_TRY_CUDA(cudaGetLastError(), "k_pack_neighbors");
+        if (pack) {
+            k_pack_neighbors<<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(0, ph->np, st, nb);
+            LQ_TRY_CUDA(cudaGetLastError(), "k_pack_neighbors");
+        }
 #define LQ_PAIR_LAUNCH(T, B)                                                                                \
     (compensated ? k_interaction_rec<true, T, B><<<blocks_for(ph->npm, T), T, 0, s>>>(                      \
                        pd, ph->np, ph->npb, st, r, c, nl.list, nl.count, nl.stride, fr, nb)                   \

@@ -47,7 +47,10 @@ def run_child(lib):
                        cwd=ROOT)
     assert r.returncode == 0, r.stdout + r.stderr
     line = [l for l in r.stdout.splitlines() if l.startswith("VIOLATIONS")][-1]
-    return int(line.split()[1])
+    n = int(line.split()[1])
+    if n > 0:
+        print("\n".join(l for l in r.stdout.splitlines() if "LQ_CHECKED" in l))
+    return n
 
 
 def test_checked_build_counts_no_bounds_violation(cuda):
