@@ -476,6 +476,22 @@ __global__ void __launch_bounds__(kBlock) k_pack_neighbors(int first, int np, St
     nb.s1[i] = s.yz * rj2;
 }
 
+/* A list entry: each 128-byte row of a list is read once per launch, so it
+ * bypasses L1 (no allocation) and leaves L1 to the neighbour data that the
+ * targets of a block share. */
+__device__ __forceinline__ int ld_list(const int* p)
+{
+#if defined(LQ_LIST_LDG)
+    return __ldg(p);
+#elif defined(LQ_LIST_CS)
+    return __ldcs(p);
+#else
+    int v;
+    asm("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+#endif
+}
+
 /* k_interaction_list over the packed neighbour arrays (same sums, same
  * order).  kThreads x kMinBlocks is the launch shape: the block size and
  * the resident blocks per SM the register allocation is capped for; the
@@ -498,14 +514,14 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_interaction_rec(
         const size_t step4 = 4 * (size_t)stride;
         int nxt[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) nxt[u] = u < n ? __ldg(p + u * stride) : i;
+        for (int u = 0; u < 4; ++u) nxt[u] = u < n ? ld_list(p + u * stride) : i;
         for (int k = 0; k < n; k += 4) {
             p += step4;
             int cur[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 cur[u] = nxt[u];
-                nxt[u] = k + 4 + u < n ? __ldg(p + u * stride) : i;
+                nxt[u] = k + 4 + u < n ? ld_list(p + u * stride) : i;
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u)
