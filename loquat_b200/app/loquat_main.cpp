@@ -2,7 +2,14 @@
  * loquat: command-line driver over the LOQUAT-B200 library, the counterpart
  * of the reference's executable (reference src/main.cpp, src/loquat.cu:216-476).
  *
- *   loquat <project> [gpu] [--mixed] [--no-graph]
+ *   loquat <project> [gpu] [--mixed] [--no-graph] [--density-filter] [--dynamic-dt]
+ *
+ * --density-filter and --dynamic-dt switch on features the reference reads
+ * from its parameter file but never applies (LQ_SIM_DENSITY_FILTER,
+ * LQ_SIM_DYNAMIC_DT).  With --dynamic-dt the steps have no fixed length, so
+ * the loop steps one at a time and reads the simulated time back from the
+ * device, saving once the time since the last output exceeds
+ * output-frequency.
  *
  * Reads <project>.xml and <project>.dat, writes output_<n>.xml and <n>.dat
  * (output-format 1) or <id>_<n>.vtu files (output-format 2) into the folder
@@ -79,6 +86,8 @@ int main(int argc, char** argv)
     for (int a = 1; a < argc; ++a) {
         if (!strcmp(argv[a], "--mixed")) flags |= LQ_SIM_MIXED;
         else if (!strcmp(argv[a], "--no-graph")) flags &= ~LQ_SIM_GRAPH;
+        else if (!strcmp(argv[a], "--density-filter")) flags |= LQ_SIM_DENSITY_FILTER;
+        else if (!strcmp(argv[a], "--dynamic-dt")) flags |= LQ_SIM_DYNAMIC_DT;
         else if (project.empty()) project = argv[a];
         else device = atoi(argv[a]);
     }
@@ -136,7 +145,31 @@ int main(int argc, char** argv)
     const auto t_start = std::chrono::steady_clock::now();
     auto t_interval = t_start;
     double saving = 0.0;
-    while (time < (double)par.time_max) {
+    const bool dynamic = (flags & LQ_SIM_DYNAMIC_DT) != 0;
+    double last_output = time;
+    while (dynamic && time < (double)par.time_max) {
+        LQ_CALL(lq_sim_step(sim, 1));
+        ++step;
+        long long st = 0;
+        LQ_CALL(lq_sim_clock(sim, &st, &time));
+        if (time - last_output > (double)par.output_frequency || time >= (double)par.time_max) {
+            const auto now = std::chrono::steady_clock::now();
+            const double interval = std::chrono::duration<double>(now - t_interval).count();
+            const double fps = (double)(step - step_interval) / interval;
+            par.time = (float)time;
+            par.output_number++;
+            LQ_CALL(lq_sim_download(sim, h.pos.data(), h.vel.data(), h.idep.data(), h.str.data(), h.stn.data()));
+            const auto s0 = std::chrono::steady_clock::now();
+            save(dir, par, h, vw ? vw_row : nullptr, e0);
+            saving += std::chrono::duration<double>(std::chrono::steady_clock::now() - s0).count();
+            printf("----------Save-----------\nTime = %0.5f | Step = %lld | FPS = %0.5f\n", par.time, step - 1, fps);
+            printf("Save file: %s/output_%d.xml\n\n", dir.c_str(), par.output_number);
+            last_output = time;
+            step_interval = step;
+            t_interval = std::chrono::steady_clock::now();
+        }
+    }
+    while (!dynamic && time < (double)par.time_max) {
         /* steps until the reference's loop would save (output_time > freq is
          * checked after a step and before time advances) or stop */
         long long k = 0;

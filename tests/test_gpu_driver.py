@@ -112,3 +112,40 @@ def test_driver_runs_model_3_from_the_parameter_file(lq, cuda, tmp_path):
         if k == 2:
             a, b = a[:, :2], b[:, :2]
         assert np.array_equal(a, b), k
+
+
+def test_driver_with_the_opt_in_extensions(lq, cuda, tmp_path):
+    """--density-filter --dynamic-dt: the steps take their length from the
+    device, the loop reads the time back, and the last output equals the
+    library's run with the same options and the same number of steps."""
+    if not APP.exists():
+        pytest.fail("driver not built: python -m loquat_b200.build")
+    c = cases.small_column(velocity_noise=0.3, shepard=5, seed=35)
+    par = c.par
+    par.density_shepard_filter = 4
+    par.output_format = 1
+    par.output_frequency = 5 * par.dt
+    par.time_max = 12 * par.dt
+    proj = tmp_path / "ext"
+    lq.save_parameters(str(proj) + ".xml", par)
+    lq.save_particles(str(proj) + ".dat", *c.arrays())
+    r = subprocess.run([str(APP), str(proj), "--density-filter", "--dynamic-dt"], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    import re
+
+    steps = [int(m) for m in re.findall(r"Step = (\d+)", r.stdout)]
+    assert len(steps) >= 2
+    d = Path(str(proj))
+    last = max(int(p.stem) for p in d.glob("*.dat"))
+    got = lq.load_particles(d / f"{last}.dat", par.np)
+    t_file = lq.load_parameters(d / f"output_{last}.xml").time
+    sim = lq.Simulation(c.par, *c.arrays(), density_filter=True, dynamic_dt=True)
+    sim.step(steps[-1] + 1)
+    want = sim.download()
+    for k, (a, b) in enumerate(zip(got, want)):
+        if k == 2:
+            a, b = a[:, :2], b[:, :2]
+        assert np.array_equal(a, b), k
+    assert t_file == np.float32(sim.clock()[1])
+    assert sim.clock()[1] >= par.time_max * (1 - 1e-6)
