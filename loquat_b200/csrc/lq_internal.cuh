@@ -128,8 +128,6 @@ struct NeighborList {
 };
 
 /* ------------------------------------------------------------ operators */
-int launch_interaction(const Parameters* par_host, const Parameters* par_dev, const State& st, const Rates& r,
-                       const Cells& c, cudaStream_t s);
 int launch_neighbor_list(const Parameters* par_host, const Parameters* par_dev, const float4* pos, const Cells& c,
                          const NeighborList& nl, cudaStream_t s);
 /* With `rec` (np x 13 floats, 16-byte aligned) the neighbour data are first

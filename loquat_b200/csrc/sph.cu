@@ -14,6 +14,8 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <mutex>
+#include <vector>
 
 #include "lq_internal.cuh"
 #include "lq_device.cuh"
@@ -41,16 +43,15 @@ inline int blocks_for(long long n, int b) { return (int)((n + b - 1) / b); }
  * mu = h v_ij.x_ij / (r^2 + eta) for approaching pairs; R is the diagonal
  * artificial stress -eps sig_aa / rho^2 of tensile components, f = W/W(dr).
  *
- * Two ways to visit the neighbours share one pair body:
- *  - k_interaction_direct: one thread per particle walks its 27 cells
- *    (the reference operator, no scratch memory);
- *  - k_neighbor_list + k_interaction_list (native driver): a warp walks the
- *    union of its lanes' stencils in lockstep (one broadcast load per
- *    candidate, one distance test per lane) and writes each lane's hits to
- *    a global list in coalesced rows; a second kernel then evaluates each
- *    particle's pairs from its list with every lane busy.
- * Both visit a particle's neighbours in the same order, so their sums are
- * bit-identical. */
+ * Neighbours are visited through lists: k_neighbor_list walks the union
+ * of a warp's lanes' 27-cell stencils in lockstep (one broadcast load per
+ * candidate, one distance test per lane) and writes each lane's hits to a
+ * global list in coalesced rows; the pair kernels then evaluate each
+ * particle's pairs from its list with every lane busy.  The native driver
+ * keeps the lists across steps (Verlet lists with a skin); the drop-in
+ * ParticleInteraction builds them at each call in the caller's grid.  A
+ * particle whose list overflowed walks its stencil directly (walk_stencil),
+ * in the same order. */
 
 struct PairConst {
     float ih, h, eta, m, Cg, Cw, avc, eps, wdr, cut2;
@@ -305,18 +306,6 @@ __device__ __forceinline__ void walk_stencil(const Parameters* __restrict__ P, c
             }
         }
     }
-}
-
-__global__ void __launch_bounds__(kBlock) k_interaction_direct(const Parameters* __restrict__ P, int np, int npb,
-                                                               State st, Rates rt, Cells cells)
-{
-    const int i = npb + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= np) return;
-    const PairConst K = load_pair_const(P);
-    Target T;
-    load_target(K, st, i, true, T);
-    walk_stencil(P, K, st, cells, i, T.x, [&](int j) { pair_body(K, st, T, j); });
-    store_rates(P, K, rt, i, T);
 }
 
 #ifndef LQ_PAIR_MIN_BLOCKS
@@ -951,14 +940,6 @@ int bounds_count_sph(unsigned long long* v)
     return LQ_OK;
 }
 
-int launch_interaction(const Parameters* ph, const Parameters* pd, const State& st, const Rates& r, const Cells& c,
-                       cudaStream_t s)
-{
-    if (ph->npm <= 0) return LQ_OK;
-    k_interaction_direct<<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, r, c);
-    LQ_TRY_CUDA(cudaGetLastError(), "k_interaction_direct");
-    return LQ_OK;
-}
 
 int launch_neighbor_list(const Parameters* ph, const Parameters* pd, const float4* pos, const Cells& c,
                          const NeighborList& nl, cudaStream_t s)
@@ -1121,6 +1102,61 @@ lqb::State state_of(const float* pos, const float* vel, const float* idep, const
 
 }  // namespace
 
+namespace {
+
+/* Working arrays of the drop-in interaction: a neighbour list for the
+ * material targets and the packed neighbour data.  One set per device,
+ * allocated on the first call and grown when a call needs more (the device
+ * is synchronised before the old arrays are freed); calls that overlap on
+ * the GPU share it and must not. */
+struct DropInWorkspace {
+    int* list = nullptr;
+    int* count = nullptr;
+    float* rec = nullptr;
+    int stride = 0, np = 0;
+};
+std::mutex g_ws_mutex;
+std::vector<DropInWorkspace> g_ws;
+
+int dropin_workspace(int np, int npm, DropInWorkspace** out)
+{
+    int dev = 0;
+    LQ_TRY_CUDA(cudaGetDevice(&dev), "interaction workspace");
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    if ((int)g_ws.size() <= dev) g_ws.resize((size_t)dev + 1);
+    DropInWorkspace& w = g_ws[(size_t)dev];
+    const int stride = (npm + 31) / 32 * 32;
+    if (stride > w.stride || np > w.np) {
+        if (w.list || w.count || w.rec) LQ_TRY_CUDA(cudaDeviceSynchronize(), "interaction workspace");
+        cudaFree(w.list);
+        cudaFree(w.count);
+        cudaFree(w.rec);
+        w = DropInWorkspace{};
+        const int st = stride > 32 ? stride : 32;
+        cudaError_t e = cudaMalloc((void**)&w.list, sizeof(int) * (size_t)LQ_NBR_CAP * st);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&w.count, sizeof(int) * (size_t)st);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&w.rec, sizeof(float) * 13 * (size_t)(np > 1 ? np : 1));
+        if (e != cudaSuccess) {
+            cudaFree(w.list);
+            cudaFree(w.count);
+            cudaFree(w.rec);
+            w = DropInWorkspace{};
+            return lqb::set_error(LQ_ERR_ALLOC, "interaction workspace: %s", cudaGetErrorString(e));
+        }
+        w.stride = st;
+        w.np = np;
+    }
+    *out = &w;
+    return LQ_OK;
+}
+
+}  // namespace
+
+/* The reference's ParticleInteraction (src/particle_interaction.h:27-40):
+ * the pairs of each material target are found once per call in the
+ * caller's grid (cell_beg / cell_end, the 27-cell walk in the reference's
+ * visiting order) into a list, and summed by the list pair kernel over the
+ * packed neighbour data. */
 extern "C" int lq_particle_interaction(const void* par_host, const void* par_device, const float* pospres,
                                        const float* velrhop, const float* idep, const float* str, const float* stn,
                                        float* accad, float* spin, float* acestn, const int* cell_beg,
@@ -1130,11 +1166,21 @@ extern "C" int lq_particle_interaction(const void* par_host, const void* par_dev
     const Parameters* ph = static_cast<const Parameters*>(par_host);
     if (ph->npm > 0 && (!pospres || !velrhop || !str || !accad || !spin || !acestn || !cell_beg || !cell_end))
         return lqb::set_error(LQ_ERR_ARG, "lq_particle_interaction: null array");
+    if (ph->npm <= 0) return LQ_OK;
     lqb::Cells c{nullptr, cell_beg, cell_end};
     lqb::Rates r{(float4*)accad, (float4*)spin, (tensor2d*)acestn};
-    return lqb::launch_interaction(ph, static_cast<const Parameters*>(par_device),
-                                   state_of(pospres, velrhop, idep, str, stn), r, c,
-                                   static_cast<cudaStream_t>(stream));
+    const Parameters* pd = static_cast<const Parameters*>(par_device);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const lqb::State st = state_of(pospres, velrhop, idep, str, stn);
+    DropInWorkspace* w = nullptr;
+    LQ_TRY(dropin_workspace(ph->np, ph->npm, &w));
+    const lqb::NeighborList nl{w->list, w->count, w->stride};
+    /* the pair body's own cut-off test: q < 2 with the candidate slack of
+     * the cell walk */
+    const float cut = 2.0f * ph->h * sqrtf(1.0001f);
+    LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, ph->npb, ph->npm, 0, cut, st.pos, c, nl, nullptr, s, nullptr,
+                                           lqb::Frames()));
+    return lqb::launch_interaction_list(ph, pd, st, r, c, nl, s, lqb::Frames(), false, w->rec, 0, true);
 }
 
 extern "C" int lq_adami_boundary(const void* par_host, const void* par_device, const float* pospres,
