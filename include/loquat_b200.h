@@ -205,13 +205,20 @@ int lq_sim_set_frames(void* sim, int n, const int* rows);
  * with the Shepard pass; a rebuild adds lq_sim_rebuild_launches more. */
 int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard);
 int lq_sim_rebuild_launches(void* sim, int* launches);
-/* Launch shape of the pair kernel.  0-4: one thread per target, threads
- * per block x resident blocks per SM (which caps its registers): 0 = 128 x 6
- * (default), 1 = 64 x 12, 2 = 256 x 3, 3 = 128 x 5, 4 = 128 x 7; these give
- * bit-identical results.  5, 6: warp-cooperative, 8 or 32 lanes share a
- * target's list and combine their sums with shuffle reductions (for small
- * cases); the summation order differs, so results agree to rounding. */
+/* Launch shape of the pair kernel.  0-4: one thread per target in slot
+ * order, threads per block x resident blocks per SM (which caps its
+ * registers): 0 = 128 x 6, 1 = 64 x 12, 2 = 256 x 3, 3 = 128 x 5,
+ * 4 = 128 x 7.  7-10: one thread per target in tile order (the targets of a
+ * block form a compact box of cells, so its neighbours stay in L1; the
+ * order is rebuilt after every search): 7 = 768 x 1, 8 = 384 x 2,
+ * 9 = 640 x 1, 10 = 320 x 2.  All of these give bit-identical results.
+ * 5, 6: warp-cooperative, 8 or 32 lanes share a target's list and combine
+ * their sums with shuffle reductions (for small cases); the summation
+ * order differs, so results agree to rounding.  A new simulation starts
+ * with shape 9 when its material particles fill four waves of 640-thread
+ * blocks on every SM, else with shape 0.  No reference counterpart. */
 int lq_sim_set_pair_shape(void* sim, int shape);
+int lq_sim_pair_shape(void* sim, int* shape);
 /* Autotuner: times `steps` steps (after two untimed ones) for each pair
  * kernel shape at the current skin, then for skins of 0.02, 0.05, 0.1 and
  * 0.2 h with the fastest shape, and keeps the fastest pair.  Every trial

@@ -77,6 +77,7 @@ _SIGNATURES = {
     "lq_sim_rebuilds": (_I, [_VP, ctypes.POINTER(_LL)]),
     "lq_sim_rebuild_launches": (_I, [_VP, ctypes.POINTER(_I)]),
     "lq_sim_set_pair_shape": (_I, [_VP, _I]),
+    "lq_sim_pair_shape": (_I, [_VP, ctypes.POINTER(_I)]),
     "lq_sim_autotune": (_I, [_VP, _I, ctypes.POINTER(_I), ctypes.POINTER(_F)]),
     "lq_debug_bounds_violations": (_I, [ctypes.POINTER(_LL)]),
     "lq_sim_save_checkpoint": (_I, [_VP, ctypes.c_char_p]),
@@ -353,6 +354,11 @@ class Simulation:
 
     def set_pair_shape(self, shape: int):
         check(lib().lq_sim_set_pair_shape(self.handle, shape), "lq_sim_set_pair_shape")
+
+    def pair_shape(self) -> int:
+        v = ctypes.c_int()
+        check(lib().lq_sim_pair_shape(self.handle, ctypes.byref(v)), "lq_sim_pair_shape")
+        return v.value
 
     def autotune(self, steps: int = 20):
         """Chooses the pair kernel's launch shape and the list skin by timing

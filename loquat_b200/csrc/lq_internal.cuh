@@ -136,7 +136,8 @@ int launch_neighbor_list(const Parameters* par_host, const Parameters* par_dev, 
  * kernel reads the state arrays. */
 int launch_interaction_list(const Parameters* par_host, const Parameters* par_dev, const State& st, const Rates& r,
                             const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr = Frames(),
-                            bool compensated = false, float* rec = nullptr, int shape = 0, bool pack = true);
+                            bool compensated = false, float* rec = nullptr, int shape = 0, bool pack = true,
+                            const int* order = nullptr);
 /* The packed neighbour arrays of slots [first, np) from the state. */
 int launch_pack_neighbors(const Parameters* par_host, const State& st, float* rec, int first, cudaStream_t s);
 /* Adami over the boundary lists reading the packed arrays (material slots
@@ -145,10 +146,29 @@ int launch_pack_neighbors(const Parameters* par_host, const State& st, float* re
 int launch_adami_packed(const Parameters* par_host, const Parameters* par_dev, const State& st,
                         const NeighborList& nl, float* rec, cudaStream_t s);
 /* Launch shapes of the packed pair kernel: {threads per block, resident
- * blocks per SM}, or {128, -G} for the warp-cooperative form with G lanes
- * per target. */
-constexpr int kPairShapeCount = 7;
-extern const int kPairShapes[kPairShapeCount][2];
+ * blocks per SM, tile order}, or {128, -G, 0} for the warp-cooperative form
+ * with G lanes per target.  Shapes with the tile order take their targets
+ * from TileOrder::order (launch_tile_order, after each search). */
+constexpr int kPairShapeCount = 11;
+constexpr int kDefaultTiledShape = 9;   /* 640 x 1, tile order */
+extern const int kPairShapes[kPairShapeCount][3];
+/* Launch shape of a new simulation with npm material particles. */
+int default_pair_shape(int npm);
+/* Targets of the pair kernel in tile order, and the scratch that builds it:
+ * order holds npm target indices; seg holds 3 x nseg_cap ints (segment
+ * begin, length, offset). */
+struct TileOrder {
+    int* order = nullptr;
+    int* seg = nullptr;
+    int nseg_cap = 0;
+    void* scan_tmp = nullptr;
+    size_t scan_bytes = 0;
+};
+/* Segments (for the smallest tile height) and scan scratch bytes. */
+int tile_order_scratch(const Parameters* par_host, int* nseg, size_t* scan_bytes);
+/* The tile order for launch shape `shape` from the grid's cell starts
+ * (nothing for shapes without it). */
+int launch_tile_order(const Parameters* par_host, const int* start, int shape, const TileOrder& to, cudaStream_t s);
 int launch_adami(const Parameters* par_host, const Parameters* par_dev, const State& st, const Cells& c,
                  cudaStream_t s);
 /* Shepard filter of material stress into out_str[npb, np).  When `full` is

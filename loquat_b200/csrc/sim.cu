@@ -65,6 +65,7 @@ struct LqSim {
     float* rec = nullptr;              /* packed neighbour data, np x 13 floats */
     float* rho_f = nullptr;            /* density filter output (LQ_SIM_DENSITY_FILTER) */
     int pair_shape = 0;                /* launch shape of the pair kernel (lqb::kPairShapes) */
+    lqb::TileOrder tile;               /* targets in tile order (tiled shapes; allocated on first use) */
     unsigned* vmax2 = nullptr;         /* max |v|^2, |a|^2 bits (LQ_SIM_DYNAMIC_DT) */
     double* dtime = nullptr;           /* device-side time (LQ_SIM_DYNAMIC_DT) */
     lqb::Frames fr;                    /* per-object grid rows (optional) */
@@ -82,6 +83,26 @@ int dev_alloc(LqSim* S, void** p, size_t bytes)
     if (e != cudaSuccess)
         return lqb::set_error(LQ_ERR_ALLOC, "sim: cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
     S->allocs.push_back(*p);
+    return LQ_OK;
+}
+
+bool tiled(const LqSim* S) { return lqb::kPairShapes[S->pair_shape][2] != 0; }
+
+/* The pair kernel's target order for tiled launch shapes (null otherwise). */
+const int* tile_order(const LqSim* S) { return tiled(S) ? S->tile.order : nullptr; }
+
+/* Buffers of the tile order, on first use of a tiled shape. */
+int ensure_tile_order(LqSim* S)
+{
+    if (!tiled(S) || S->tile.order) return LQ_OK;
+    int nseg = 0;
+    size_t bytes = 0;
+    LQ_TRY(lqb::tile_order_scratch(&S->ph, &nseg, &bytes));
+    LQ_TRY(dev_alloc(S, (void**)&S->tile.seg, sizeof(int) * 3 * (size_t)nseg));
+    LQ_TRY(dev_alloc(S, &S->tile.scan_tmp, bytes));
+    LQ_TRY(dev_alloc(S, (void**)&S->tile.order, sizeof(int) * (size_t)(S->npm > 0 ? S->npm : 1)));
+    S->tile.nseg_cap = nseg;
+    S->tile.scan_bytes = bytes;
     return LQ_OK;
 }
 
@@ -245,7 +266,7 @@ int enqueue_rebuild(LqSim* S, cudaStream_t s)
     /* every slot's packed neighbour data (the boundary slots keep theirs
      * until the next build) */
     if (S->rec) LQ_TRY(lqb::launch_pack_neighbors(ph, S->S, S->rec, 0, s));
-    return LQ_OK;
+    return lqb::launch_tile_order(ph, S->g.start, S->pair_shape, S->tile, s);
 }
 
 /* Dynamic time step (LQ_SIM_DYNAMIC_DT): the next step's dt into the
@@ -293,12 +314,12 @@ int enqueue_stages(LqSim* S, cudaStream_t s)
     /* predictor stage (reference src/loquat.cu:343-368) */
     LQ_TRY(enqueue_adami_pack(S, S->S, s));
     LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S, S->R, cells, S->nlm, s, S->fr, S->flags & LQ_SIM_MIXED,
-                                        S->rec, S->pair_shape, false));
+                                        S->rec, S->pair_shape, false, tile_order(S)));
     LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt, S->vw));
     /* corrector stage (reference src/loquat.cu:371-396) */
     LQ_TRY(enqueue_adami_pack(S, S->S2, s));
     LQ_TRY(lqb::launch_interaction_list(ph, pd, S->S2, S->R, cells, S->nlm, s, S->fr, S->flags & LQ_SIM_MIXED,
-                                        S->rec, S->pair_shape, false));
+                                        S->rec, S->pair_shape, false, tile_order(S)));
     LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild, S->skin, s,
                                     S->mt, S->vw));
     return enqueue_dynamic_dt(S, s);
@@ -445,6 +466,7 @@ int build_graphs(LqSim* S)
     if (S->shep_exec) cudaGraphExecDestroy(S->shep_exec);
     S->step_exec = S->shep_exec = nullptr;
     S->conditional = false;
+    LQ_TRY(ensure_tile_order(S));
     if (!(S->flags & LQ_SIM_GRAPH)) return LQ_OK;
     /* model 3 steps need the von Wolffersdorff table; capture once it is set */
     if (S->ph.constitutive_model == 3 && S->vw.n == 0) return LQ_OK;
@@ -466,6 +488,7 @@ int create(LqSim* S, const Parameters* par, const float* pos, const float* vel, 
     S->npb = par->npb;
     S->npm = par->npm;
     S->flags = flags;
+    S->pair_shape = lqb::default_pair_shape(S->npm);
     if (S->np <= 0 || S->npb < 0 || S->npm < 0 || S->npb + S->npm != S->np)
         return lqb::set_error(LQ_ERR_ARG, "lq_sim_create: inconsistent counts np=%d npb=%d npm=%d", S->np, S->npb,
                               S->npm);
@@ -790,6 +813,13 @@ extern "C" int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard
 }
 
 /* ------------------------------------------------------------- autotuning */
+extern "C" int lq_sim_pair_shape(void* sim, int* shape)
+{
+    if (!sim || !shape) return lqb::set_error(LQ_ERR_ARG, "lq_sim_pair_shape: null argument");
+    *shape = static_cast<LqSim*>(sim)->pair_shape;
+    return LQ_OK;
+}
+
 extern "C" int lq_sim_set_pair_shape(void* sim, int shape)
 {
     if (!sim || shape < 0 || shape >= lqb::kPairShapeCount)
@@ -797,7 +827,15 @@ extern "C" int lq_sim_set_pair_shape(void* sim, int shape)
     LqSim* S = static_cast<LqSim*>(sim);
     LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "set pair shape");
     S->pair_shape = shape;
-    return build_graphs(S);
+    LQ_TRY(build_graphs(S));
+    if (!tiled(S)) return LQ_OK;
+    /* the lists are current unless a search is pending: order them now */
+    LQ_TRY_CUDA(cudaMemcpyAsync(S->host_flag, S->rebuild, sizeof(int), cudaMemcpyDeviceToHost, S->stream),
+                "flag read");
+    LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "flag read");
+    if (*S->host_flag == 0) LQ_TRY(lqb::launch_tile_order(&S->ph, S->g.start, S->pair_shape, S->tile, S->stream));
+    LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "tile order");
+    return LQ_OK;
 }
 
 namespace {
@@ -1167,8 +1205,9 @@ extern "C" int lq_sim_rebuild_launches(void* sim, int* launches)
     LqSim* S = static_cast<LqSim*>(sim);
     /* count reset, hash, scatter, cell order (the scan is a library
      * kernel), gather, copy, material list, boundary list (when npb > 0),
-     * full pack of the neighbour data */
-    *launches = 4 + 1 + 1 + 1 + (S->npb > 0 ? 1 : 0) + (S->rec ? 1 : 0);
+     * full pack of the neighbour data, tile segments and fill (tiled
+     * shapes; their scan is a library kernel) */
+    *launches = 4 + 1 + 1 + 1 + (S->npb > 0 ? 1 : 0) + (S->rec ? 1 : 0) + (tiled(S) && S->npm > 0 ? 2 : 0);
     return LQ_OK;
 }
 
@@ -1232,6 +1271,7 @@ int profiled_step(LqSim* S, PhaseTimer& T)
         LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, S->nlb, S->health, s,
                                                S->S.idep, S->fr));
         if (S->rec) LQ_TRY(lqb::launch_pack_neighbors(ph, S->S, S->rec, 0, s));
+        LQ_TRY(lqb::launch_tile_order(ph, S->g.start, S->pair_shape, S->tile, s));
         LQ_TRY(T.close(s));
     }
     State* cur[2] = {&S->S, &S->S2};
@@ -1241,7 +1281,7 @@ int profiled_step(LqSim* S, PhaseTimer& T)
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_INTERACTION));
         LQ_TRY(lqb::launch_interaction_list(ph, pd, *cur[stage], S->R, cells, S->nlm, s, S->fr,
-                                            S->flags & LQ_SIM_MIXED, S->rec, S->pair_shape, false));
+                                            S->flags & LQ_SIM_MIXED, S->rec, S->pair_shape, false, tile_order(S)));
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_INTEGRATE));
         if (stage == 0)

@@ -11,11 +11,14 @@
  * same runs and their loads hit L1.
  */
 #include <climits>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
 #include <vector>
+
+#include <cub/device/device_scan.cuh>
 
 #include "lq_internal.cuh"
 #include "lq_device.cuh"
@@ -68,7 +71,9 @@ __device__ __forceinline__ PairConst load_pair_const(const Parameters* __restric
     K.Cg = __ldg(&P->kernel_gradient_normalization_par);
     K.Cw = __ldg(&P->kernel_normalization_par);
     K.visc = __ldg(&P->viscosity_type) == 1;
-    K.avc = __ldg(&P->artificial_viscosity_alpha) * __ldg(&P->cs); /* alpha * cs */
+    /* alpha * cs; zero without viscosity, so the packed pair body can
+     * evaluate the term unconditionally (it then adds exact zeros) */
+    K.avc = K.visc ? __ldg(&P->artificial_viscosity_alpha) * __ldg(&P->cs) : 0.0f;
     K.artp = __ldg(&P->artificial_pressure) == 1;
     K.eps = __ldg(&P->artificial_pressure_coefficient);
     K.wdr = __ldg(&P->kernel_dr);
@@ -206,8 +211,15 @@ struct NbrArrays {
     float* s1;
 };
 
-template <bool kKahan = false>
-__device__ __forceinline__ void pair_body_rec(const PairConst& K, const NbrArrays& nb, Target& T, int j)
+/* One pair from the packed arrays, its density-rate and momentum terms
+ * added to (drho, ax, ay, az) and its velocity-gradient terms to T.  The
+ * viscosity term is always evaluated (K.avc is zero without viscosity), so
+ * a run of pairs has no branch between them; kArtp adds the artificial
+ * stress.  A pair of a particle with itself (the filler of a list's last
+ * group of four) adds exact zeros: r = 0 makes the kernel gradient zero. */
+template <bool kArtp>
+__device__ __forceinline__ void pair_terms(const PairConst& K, const NbrArrays& nb, Target& T, int j, float& drho,
+                                           float& ax, float& ay, float& az)
 {
     const float4 xr = __ldg(nb.xr + j);
     const float4 vs = __ldg(nb.vs + j);
@@ -222,23 +234,21 @@ __device__ __forceinline__ void pair_body_rec(const PairConst& K, const NbrArray
     const float fac = K.Cg * t * t * t;
     const float gx = fac * dx, gy = fac * dy, gz = fac * dz;
     const float vx = T.v.x - a[4], vy = T.v.y - a[5], vz = T.v.z - a[6];
-    if (kKahan)
-        kahan_add(T.drho, T.cdrho, vx * gx + vy * gy + vz * gz);
-    else
-        T.drho += vx * gx + vy * gy + vz * gz;
+    drho += vx * gx + vy * gy + vz * gz;
     const float Txx = T.Sxx + b[0], Tyy = T.Syy + b[1], Tzz = T.Szz + b[2];
     const float Txy = T.Sxy + b[3], Txz = T.Sxz + b[4], Tyz = T.Syz + b[5];
     float px = Txx * gx + Txy * gy + Txz * gz;
     float py = Txy * gx + Tyy * gy + Tyz * gz;
     float pz = Txz * gx + Tyz * gy + Tzz * gz;
-    if (K.visc) {
+    {
+        /* Pi = -alpha cs h vr / ((r^2 + eta) rhobar) for vr < 0 */
         const float vr = fminf(vx * dx + vy * dy + vz * dz, 0.0f);
         const float pi = __fdividef(-K.avc * K.h * vr, (r2 + K.eta) * (0.5f * (T.v.w + a[7])));
         px -= pi * gx;
         py -= pi * gy;
         pz -= pi * gz;
     }
-    if (K.artp) {
+    if (kArtp) {
         const float wk = K.Cw * t * t * t * t * (q + 0.5f);
         const float f = __fdividef(wk, K.wdr);
         const float f4 = (f * f) * (f * f);
@@ -249,20 +259,36 @@ __device__ __forceinline__ void pair_body_rec(const PairConst& K, const NbrArray
         py += (T.Ry + Rjy) * f4 * gy;
         pz += (T.Rz + Rjz) * f4 * gz;
     }
-    if (kKahan) {
-        kahan_add(T.ax, T.cax, px);
-        kahan_add(T.ay, T.cay, py);
-        kahan_add(T.az, T.caz, pz);
-    } else {
-        T.ax += px;
-        T.ay += py;
-        T.az += pz;
-    }
+    ax += px;
+    ay += py;
+    az += pz;
     const float Vj = K.m * __fdividef(1.0f, a[7]);
     const float wx = Vj * vx, wy = Vj * vy, wz = Vj * vz;
     T.l00 -= wx * gx; T.l01 -= wx * gy; T.l02 -= wx * gz;
     T.l10 -= wy * gx; T.l11 -= wy * gy; T.l12 -= wy * gz;
     T.l20 -= wz * gx; T.l21 -= wz * gy; T.l22 -= wz * gz;
+}
+
+/* One pair into T's sums; kKahan compensates the density and momentum
+ * sums pair by pair. */
+template <bool kKahan = false>
+__device__ __forceinline__ void pair_body_rec(const PairConst& K, const NbrArrays& nb, Target& T, int j)
+{
+    if (kKahan) {
+        float d = 0.f, x = 0.f, y = 0.f, z = 0.f;
+        if (K.artp)
+            pair_terms<true>(K, nb, T, j, d, x, y, z);
+        else
+            pair_terms<false>(K, nb, T, j, d, x, y, z);
+        kahan_add(T.drho, T.cdrho, d);
+        kahan_add(T.ax, T.cax, x);
+        kahan_add(T.ay, T.cay, y);
+        kahan_add(T.az, T.caz, z);
+    } else if (K.artp) {
+        pair_terms<true>(K, nb, T, j, T.drho, T.ax, T.ay, T.az);
+    } else {
+        pair_terms<false>(K, nb, T, j, T.drho, T.ax, T.ay, T.az);
+    }
 }
 
 __device__ __forceinline__ void store_rates(const Parameters* __restrict__ P, const PairConst& K, const Rates& rt,
@@ -309,7 +335,7 @@ __device__ __forceinline__ void walk_stencil(const Parameters* __restrict__ P, c
 }
 
 #ifndef LQ_PAIR_MIN_BLOCKS
-#define LQ_PAIR_MIN_BLOCKS 6   /* 128-thread blocks per SM: 75 registers, no spills (measured best of 1, 6, 8) */
+#define LQ_PAIR_MIN_BLOCKS 6   /* 128-thread blocks per SM: 80 registers */
 #endif
 
 constexpr int kListWarps = kBlock / 32;
@@ -481,6 +507,45 @@ __device__ __forceinline__ int ld_list(const int* p)
 #endif
 }
 
+/* The sums over one target's list (entry k at p[k * stride]), four
+ * entries per group, the next group's entries fetched ahead so the
+ * dependent neighbour loads do not wait on the list stream.  The last
+ * group is filled up with the target itself (exact zeros), so a group has
+ * no branch.  The compensated form adds each group's plain sum of four
+ * pairs to the compensated sums. */
+template <bool kKahan, bool kArtp>
+__device__ __forceinline__ void list_sums(const PairConst& K, const NbrArrays& nb, Target& T, const int* p, int n,
+                                          int stride, int i, int np)
+{
+    const size_t step4 = 4 * (size_t)stride;
+    int nxt[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) nxt[u] = u < n ? ld_list(p + u * stride) : i;
+    for (int k = 0; k < n; k += 4) {
+        p += step4;
+        int cur[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            cur[u] = nxt[u];
+            nxt[u] = k + 4 + u < n ? ld_list(p + u * stride) : i;
+        }
+        if (kKahan) {
+            float d = 0.f, x = 0.f, y = 0.f, z = 0.f;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (lq_in_range(cur[u], np)) pair_terms<kArtp>(K, nb, T, cur[u], d, x, y, z);
+            kahan_add(T.drho, T.cdrho, d);
+            kahan_add(T.ax, T.cax, x);
+            kahan_add(T.ay, T.cay, y);
+            kahan_add(T.az, T.caz, z);
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (lq_in_range(cur[u], np)) pair_terms<kArtp>(K, nb, T, cur[u], T.drho, T.ax, T.ay, T.az);
+        }
+    }
+}
+
 /* k_interaction_list over the packed neighbour arrays (same sums, same
  * order).  kThreads x kMinBlocks is the launch shape: the block size and
  * the resident blocks per SM the register allocation is capped for; the
@@ -489,37 +554,81 @@ __device__ __forceinline__ int ld_list(const int* p)
 template <bool kKahan, int kThreads, int kMinBlocks>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) k_interaction_rec(
     const Parameters* __restrict__ P, int np, int npb, State st, Rates rt, Cells cells, const int* __restrict__ list,
-    const int* __restrict__ count, int stride, Frames fr, NbrArrays nb)
+    const int* __restrict__ count, int stride, Frames fr, NbrArrays nb, const int* __restrict__ order)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= np - npb) return;
+    /* thread g takes target order[g] (tile order) or target g (slot order) */
+    const int t = order ? __ldg(order + g) : g;
+    if (!lq_in_range(t, np - npb)) return;
     const int i = npb + t;
-    if (i >= np) return;
     const PairConst K = load_pair_const(P);
     Target T;
     load_target(K, st, i, true, T);
     const int n = __ldg(count + t);
     if (n <= LQ_NBR_CAP) {
-        const int* p = list + t;
-        const size_t step4 = 4 * (size_t)stride;
-        int nxt[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) nxt[u] = u < n ? ld_list(p + u * stride) : i;
-        for (int k = 0; k < n; k += 4) {
-            p += step4;
-            int cur[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                cur[u] = nxt[u];
-                nxt[u] = k + 4 + u < n ? ld_list(p + u * stride) : i;
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (k + u < n && lq_in_range(cur[u], np)) pair_body_rec<kKahan>(K, nb, T, cur[u]);
-        }
+        if (K.artp)
+            list_sums<kKahan, true>(K, nb, T, list + t, n, stride, i, np);
+        else
+            list_sums<kKahan, false>(K, nb, T, list + t, n, stride, i, np);
     } else {
         walk_stencil(P, K, st, cells, i, T.x, [&](int j) { pair_body<kKahan>(K, st, T, j); }, fr);
     }
     store_rates(P, K, rt, i, T);
+}
+
+/* ------------------------------------------------- tile order of targets */
+/* The pair kernel's targets in tile order: the material layer's lattice is
+ * cut into tiles of 3 x 3 columns by tz cells, taken with tz fastest, and
+ * within a tile column by column, each column's tz cells being one run of
+ * consecutive slots (the grid's key is z fastest).  A block of the pair
+ * kernel then holds a compact box of targets whose neighbourhood fits in
+ * L1, instead of a thin z-run of one column whose neighbours the next
+ * block on the SM does not share.  Segment s < nseg - 2 is column s % 9 of
+ * tile s / 9; the last two hold the material slots below the material
+ * layer (none in a sound state) and the out-of-lattice cell.  Every
+ * segment is clamped to [npb, np), so the segments partition the
+ * material slots. */
+__global__ void __launch_bounds__(kBlock) k_tile_segments(const int* __restrict__ start, int nx, int ny, int nz,
+                                                          int L, int tz, int nty, int ntz, int npb, int np,
+                                                          int nseg, int* __restrict__ seg_beg,
+                                                          int* __restrict__ seg_len)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nseg) return;
+    int b = npb, e = npb;
+    if (s < nseg - 2) {
+        const int c = s % 9, tile = s / 9;
+        const int kz = tile % ntz, rest = tile / ntz;
+        const int X = 3 * (rest / nty) + c % 3, Y = 3 * (rest % nty) + c / 3, z0 = kz * tz;
+        if (X < nx && Y < ny && z0 < nz) {
+            const int key0 = L + (X * ny + Y) * nz + z0;
+            b = __ldg(start + key0);
+            e = __ldg(start + key0 + min(tz, nz - z0));
+        }
+    } else if (s == nseg - 2) {
+        e = __ldg(start + L);
+    } else {
+        b = __ldg(start + 2 * L);
+        e = np;
+    }
+    b = max(b, npb);
+    e = min(e, np);
+    seg_beg[s] = b;
+    seg_len[s] = max(e - b, 0);
+}
+
+/* One warp per segment writes its targets (slot - npb) at the segment's
+ * offset. */
+__global__ void __launch_bounds__(kBlock) k_tile_fill(int nseg, int npb, int npm, const int* __restrict__ seg_beg,
+                                                      const int* __restrict__ seg_len,
+                                                      const int* __restrict__ seg_off, int* __restrict__ order)
+{
+    const int w = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (w >= nseg) return;
+    const int b = __ldg(seg_beg + w), n = __ldg(seg_len + w), o = __ldg(seg_off + w);
+    for (int k = lane; k < n; k += 32)
+        if (o + k < npm) order[o + k] = b + k - npb;
 }
 
 /* Warp-cooperative form: a group of G lanes (G = 8 or 32) shares one
@@ -925,8 +1034,82 @@ int launch_density_filter_list(const Parameters* ph, const Parameters* pd, const
 /* Launch shapes of the pair kernel: threads per block x resident blocks
  * per SM (the register cap); a negative second entry -G marks the
  * warp-cooperative form with G lanes per target.  Shape 0 is the default. */
-const int kPairShapes[kPairShapeCount][2] = {{kBlock, LQ_PAIR_MIN_BLOCKS}, {64, 12}, {256, 3}, {128, 5},
-                                             {128, 7}, {128, -8}, {128, -32}};
+const int kPairShapes[kPairShapeCount][3] = {{kBlock, LQ_PAIR_MIN_BLOCKS, 0},
+                                             {64, 12, 0},
+                                             {256, 3, 0},
+                                             {128, 5, 0},
+                                             {128, 7, 0},
+                                             {128, -8, 0},
+                                             {128, -32, 0},
+                                             {768, 1, 1},
+                                             {384, 2, 1},
+                                             {640, 1, 1},
+                                             {320, 2, 1}};
+
+/* The native driver's launch shape before any tuning: the tiled 640 x 1
+ * shape once the targets fill at least four waves of 640-thread blocks on
+ * every SM, the 128-thread shape 0 below that (a small case would leave
+ * SMs idle with large blocks). */
+int default_pair_shape(int npm)
+{
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                  cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return (long long)npm >= 4LL * sms * kPairShapes[kDefaultTiledShape][0] ? kDefaultTiledShape : 0;
+}
+
+/* Tile height (cells) for a block of `threads` targets: a 3 x 3-column
+ * tile of that height holds about one block at (2 h / dr)^3 particles per
+ * cell. */
+static int tile_height(const Parameters* ph, int threads)
+{
+    const double ppc = std::pow(2.0 * (double)ph->hdr, 3.0);
+    const int tz = (int)std::lround((double)threads / (9.0 * (ppc > 1.0 ? ppc : 1.0)));
+    return tz < 1 ? 1 : tz;
+}
+
+static void tile_counts(const Parameters* ph, int tz, int* nty, int* ntz, int* nseg)
+{
+    const int nx = ph->cell_num_x, ny = ph->cell_num_y, nz = ph->cell_num_z;
+    *nty = (ny + 2) / 3;
+    *ntz = (nz + tz - 1) / tz;
+    *nseg = ((nx + 2) / 3) * *nty * *ntz * 9 + 2;
+}
+
+int tile_order_scratch(const Parameters* ph, int* nseg, size_t* scan_bytes)
+{
+    int nty, ntz;
+    tile_counts(ph, 1, &nty, &ntz, nseg);   /* the most segments any tile height needs */
+    *scan_bytes = 0;
+    LQ_TRY_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, *scan_bytes, (const int*)nullptr, (int*)nullptr, *nseg),
+                "tile scan scratch query");
+    return LQ_OK;
+}
+
+int launch_tile_order(const Parameters* ph, const int* start, int shape, const TileOrder& to, cudaStream_t s)
+{
+    if (shape < 0 || shape >= kPairShapeCount || !kPairShapes[shape][2] || ph->npm <= 0) return LQ_OK;
+    if (!to.order || !to.seg) return set_error(LQ_ERR_ARG, "tile order: buffers not allocated");
+    const int tz = tile_height(ph, kPairShapes[shape][0]);
+    int nty, ntz, nseg;
+    tile_counts(ph, tz, &nty, &ntz, &nseg);
+    if (nseg > to.nseg_cap) return set_error(LQ_ERR_ARG, "tile order: %d segments > capacity %d", nseg, to.nseg_cap);
+    int* beg = to.seg;
+    int* len = to.seg + to.nseg_cap;
+    int* off = to.seg + 2 * (size_t)to.nseg_cap;
+    k_tile_segments<<<blocks_for(nseg, kBlock), kBlock, 0, s>>>(start, ph->cell_num_x, ph->cell_num_y,
+                                                                ph->cell_num_z, ph->ncell_one_layer, tz, nty, ntz,
+                                                                ph->npb, ph->np, nseg, beg, len);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_tile_segments");
+    size_t bytes = to.scan_bytes;
+    LQ_TRY_CUDA(cub::DeviceScan::ExclusiveSum(to.scan_tmp, bytes, len, off, nseg, s), "tile scan");
+    k_tile_fill<<<blocks_for(nseg, kBlock / 32), kBlock, 0, s>>>(nseg, ph->npb, ph->npm, beg, len, off, to.order);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_tile_fill");
+    return LQ_OK;
+}
 
 /* This translation unit's count of bounds violations (always 0 without
  * LQ_CHECKED). */
@@ -1007,7 +1190,7 @@ int launch_shepard_list(const Parameters* ph, const Parameters* pd, const State&
 
 int launch_interaction_list(const Parameters* ph, const Parameters* pd, const State& st, const Rates& r,
                             const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr,
-                            bool compensated, float* rec, int shape, bool pack)
+                            bool compensated, float* rec, int shape, bool pack, const int* order)
 {
     if (ph->npm <= 0) return LQ_OK;
     if (rec) {
@@ -1020,12 +1203,19 @@ int launch_interaction_list(const Parameters* ph, const Parameters* pd, const St
             k_pack_neighbors<<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(0, ph->np, st, nb);
             LQ_TRY_CUDA(cudaGetLastError(), "k_pack_neighbors");
         }
+        if (shape >= 0 && shape < kPairShapeCount && kPairShapes[shape][2] && !order)
+            return set_error(LQ_ERR_ARG, "interaction: launch shape %d needs the tile order", shape);
+        if (shape < 0 || shape >= kPairShapeCount || !kPairShapes[shape][2]) order = nullptr;
 #define LQ_PAIR_LAUNCH(T, B)                                                                                \
     (compensated ? k_interaction_rec<true, T, B><<<blocks_for(ph->npm, T), T, 0, s>>>(                      \
-                       pd, ph->np, ph->npb, st, r, c, nl.list, nl.count, nl.stride, fr, nb)                   \
+                       pd, ph->np, ph->npb, st, r, c, nl.list, nl.count, nl.stride, fr, nb, order)            \
                  : k_interaction_rec<false, T, B><<<blocks_for(ph->npm, T), T, 0, s>>>(                     \
-                       pd, ph->np, ph->npb, st, r, c, nl.list, nl.count, nl.stride, fr, nb))
+                       pd, ph->np, ph->npb, st, r, c, nl.list, nl.count, nl.stride, fr, nb, order))
         switch (shape) {
+            case 7: LQ_PAIR_LAUNCH(768, 1); break;
+            case 8: LQ_PAIR_LAUNCH(384, 2); break;
+            case 9: LQ_PAIR_LAUNCH(640, 1); break;
+            case 10: LQ_PAIR_LAUNCH(320, 2); break;
             case 1: LQ_PAIR_LAUNCH(64, 12); break;
             case 2: LQ_PAIR_LAUNCH(256, 3); break;
             case 3: LQ_PAIR_LAUNCH(128, 5); break;

@@ -13,10 +13,13 @@ from loquat_b200 import cases
 pytestmark = pytest.mark.gpu
 
 
+THREAD_PER_TARGET = (0, 1, 2, 3, 4, 7, 8, 9, 10)   # 7-10 take their targets in tile order
+
+
 def test_all_pair_kernel_shapes_agree_bit_for_bit(lq, cuda):
     c = cases.small_column(velocity_noise=0.3, shepard=7, seed=81)
     out = []
-    for shape in range(5):
+    for shape in THREAD_PER_TARGET:
         s = lq.Simulation(c.par, *c.arrays(), mixed=True)
         s.set_pair_shape(shape)
         s.step(25)
@@ -25,7 +28,59 @@ def test_all_pair_kernel_shapes_agree_bit_for_bit(lq, cuda):
         for x, y in zip(out[0], other):
             assert np.array_equal(x, y)
     with pytest.raises(lq.LoquatError):
-        s.set_pair_shape(7)
+        s.set_pair_shape(11)
+
+
+@pytest.mark.parametrize("shape", [7, 8, 9, 10])
+def test_tile_order_switched_on_mid_run(lq, cuda, shape):
+    """A tiled shape chosen between steps orders the current lists at once
+    (no search is pending); the run goes on bit-identically, through later
+    searches, with any of them -- also with a particle outside the lattice,
+    whose slot sits in the out-of-lattice cell after every material cell."""
+    c = cases.small_column(velocity_noise=0.3, shepard=7, seed=84)
+    a = lq.Simulation(c.par, *c.arrays())
+    b = lq.Simulation(c.par, *c.arrays())
+    a.set_pair_shape(0)
+    a.step(9)
+    b.step(9)
+    pos, vel, idep, st, stn = a.download()
+    pos[c.par.npb + 5, 0] = -1.0
+    a.upload(pos, vel, idep, st, stn)
+    b.upload(pos, vel, idep, st, stn)
+    a.step(2)
+    b.step(2)
+    b.set_pair_shape(shape)
+    a.step(40)
+    b.step(40)
+    assert b.rebuilds() > 2
+    assert a.health()[1] >= 1
+    # the escaped particle is in no material cell, so the Shepard filter's
+    # sum over its cell neighbourhood is empty and gives 0/0, as the
+    # reference's filter does (no zero guard): compare NaN as equal
+    for x, y in zip(a.download(), b.download()):
+        assert np.array_equal(x, y, equal_nan=True)
+
+
+def test_default_shape_is_tiled_for_large_cases(lq, cuda):
+    """A new simulation starts with the tiled 640 x 1 shape when its targets
+    fill four waves of 640-thread blocks on every SM, with shape 0 below
+    that, and steps like one given that shape explicitly."""
+    import torch
+
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    small = cases.small_column(velocity_noise=0.3, seed=85)
+    assert lq.Simulation(small.par, *small.arrays()).pair_shape() == 0
+    n = int(np.ceil((4 * sms * 640 * 1.05) ** (1.0 / 3.0)))
+    c = cases.small_column(nsx=n, nsy=n, nsz=n, velocity_noise=0.3, seed=86)
+    assert c.par.npm >= 4 * sms * 640
+    a = lq.Simulation(c.par, *c.arrays())
+    assert a.pair_shape() == 9
+    b = lq.Simulation(c.par, *c.arrays())
+    b.set_pair_shape(0)
+    a.step(12)
+    b.step(12)
+    for x, y in zip(a.download(), b.download()):
+        assert np.array_equal(x, y)
 
 
 @pytest.mark.parametrize("mixed", [False, True])
@@ -59,7 +114,7 @@ def test_autotune_leaves_the_state_and_matches_a_fresh_run(lq, cuda):
     a.step(11)
     before, clock = a.download(), a.clock()
     shape, skin = a.autotune(steps=8)
-    assert 0 <= shape < 7
+    assert 0 <= shape < 11
     assert min(abs(skin - f) for f in (0.02, 0.05, 0.1, 0.2)) < 1e-6
     for x, y in zip(before, a.download()):
         assert np.array_equal(x, y)
