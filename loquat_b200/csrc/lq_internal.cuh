@@ -130,10 +130,10 @@ struct NeighborList {
 /* ------------------------------------------------------------ operators */
 int launch_neighbor_list(const Parameters* par_host, const Parameters* par_dev, const float4* pos, const Cells& c,
                          const NeighborList& nl, cudaStream_t s);
-/* With `rec` (np x 13 floats, 16-byte aligned) the neighbour data are first
- * packed into dense arrays (position and density, velocity and sigma/rho^2;
- * 52 bytes per particle) that the pair kernel gathers; without it the pair
- * kernel reads the state arrays. */
+/* `rec` (np x 13 floats, 16-byte aligned; required) holds the neighbour
+ * data packed into dense arrays (position and density, velocity and
+ * sigma/rho^2; 52 bytes per particle) that the pair kernel gathers; with
+ * `pack` they are packed from the state first. */
 int launch_interaction_list(const Parameters* par_host, const Parameters* par_dev, const State& st, const Rates& r,
                             const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr = Frames(),
                             bool compensated = false, float* rec = nullptr, int shape = 0, bool pack = true,
@@ -194,9 +194,7 @@ int launch_correct_into(const Parameters* par_host, const Parameters* par_dev, c
                         float skin, cudaStream_t s, const MaterialTable& mt = MaterialTable(),
                         const MaterialTable& vw = MaterialTable());
 
-/* List-driven Adami (boundary targets, material neighbours) and Shepard. */
-int launch_adami_list(const Parameters* par_host, const Parameters* par_dev, const State& st, const NeighborList& nl,
-                      cudaStream_t s);
+/* List-driven Shepard filter (material targets and neighbours). */
 int launch_shepard_list(const Parameters* par_host, const Parameters* par_dev, const State& st, tensor2d* out_str,
                         const NeighborList& nl, cudaStream_t s);
 /* Density Shepard filter of material slots into rho_out[npb, np) over the

@@ -265,7 +265,7 @@ int enqueue_rebuild(LqSim* S, cudaStream_t s)
                                            S->S.idep, S->fr));
     /* every slot's packed neighbour data (the boundary slots keep theirs
      * until the next build) */
-    if (S->rec) LQ_TRY(lqb::launch_pack_neighbors(ph, S->S, S->rec, 0, s));
+    LQ_TRY(lqb::launch_pack_neighbors(ph, S->S, S->rec, 0, s));
     return lqb::launch_tile_order(ph, S->g.start, S->pair_shape, S->tile, s);
 }
 
@@ -294,13 +294,11 @@ int enqueue_density_filter(LqSim* S, cudaStream_t s)
     return LQ_OK;
 }
 
-/* Adami for a stage.  With the packed neighbour arrays, the material slots
- * are packed first, Adami reads them and writes the boundary slots' packed
- * stress itself (boundary positions and velocities are packed at each list
+/* Adami for a stage.  The material slots are packed first, Adami reads
+ * them and writes the boundary slots' packed stress itself (boundary positions and velocities are packed at each list
  * build and do not change in between), so the pair kernel needs no pack. */
 int enqueue_adami_pack(LqSim* S, const State& st, cudaStream_t s)
 {
-    if (!S->rec) return lqb::launch_adami_list(&S->ph, S->pd, st, S->nlb, s);
     LQ_TRY(lqb::launch_pack_neighbors(&S->ph, st, S->rec, S->npb, s));
     return lqb::launch_adami_packed(&S->ph, S->pd, st, S->nlb, S->rec, s);
 }
@@ -801,10 +799,9 @@ extern "C" int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard
     if (!sim) return lqb::set_error(LQ_ERR_ARG, "lq_sim_launches_per_step: null sim");
     LqSim* S = static_cast<LqSim*>(sim);
     /* own kernels of a step without a rebuild: decide (graph only), Adami
-     * (when npb > 0), record packing (when used), interaction and
-     * integrator per stage; a Shepard pass
-     * adds the filter and its copy */
-    const int stage = (S->npb > 0 ? 1 : 0) + (S->rec ? 2 : 1) + 1;
+     * (when npb > 0), the material pack, interaction and integrator per
+     * stage; a Shepard pass adds the filter and its copy */
+    const int stage = (S->npb > 0 ? 1 : 0) + 2 + 1;
     const int decide = S->conditional ? 1 : 0;
     const int dyn = (S->flags & LQ_SIM_DYNAMIC_DT) ? (S->npm > 0 ? 2 : 1) : 0;
     if (plain) *plain = decide + 2 * stage + dyn;
@@ -1207,7 +1204,7 @@ extern "C" int lq_sim_rebuild_launches(void* sim, int* launches)
      * kernel), gather, copy, material list, boundary list (when npb > 0),
      * full pack of the neighbour data, tile segments and fill (tiled
      * shapes; their scan is a library kernel) */
-    *launches = 4 + 1 + 1 + 1 + (S->npb > 0 ? 1 : 0) + (S->rec ? 1 : 0) + (tiled(S) && S->npm > 0 ? 2 : 0);
+    *launches = 4 + 1 + 1 + 1 + (S->npb > 0 ? 1 : 0) + 1 + (tiled(S) && S->npm > 0 ? 2 : 0);
     return LQ_OK;
 }
 
@@ -1270,7 +1267,7 @@ int profiled_step(LqSim* S, PhaseTimer& T)
                                                s, S->S.idep, S->fr));
         LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, S->nlb, S->health, s,
                                                S->S.idep, S->fr));
-        if (S->rec) LQ_TRY(lqb::launch_pack_neighbors(ph, S->S, S->rec, 0, s));
+        LQ_TRY(lqb::launch_pack_neighbors(ph, S->S, S->rec, 0, s));
         LQ_TRY(lqb::launch_tile_order(ph, S->g.start, S->pair_shape, S->tile, s));
         LQ_TRY(T.close(s));
     }

@@ -435,47 +435,6 @@ __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __re
     }
 }
 
-/* Pair sums from the lists; a particle whose list overflowed walks its
- * stencil directly.  List entries are fetched four pairs ahead so the
- * dependent neighbour loads do not wait on the list stream. */
-template <bool kKahan>
-__global__ void __launch_bounds__(kBlock, LQ_PAIR_MIN_BLOCKS) k_interaction_list(
-    const Parameters* __restrict__ P, int np, int npb, State st, Rates rt, Cells cells, const int* __restrict__ list,
-    const int* __restrict__ count, int stride, Frames fr)
-{
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = npb + t;
-    if (i >= np) return;
-    const PairConst K = load_pair_const(P);
-    Target T;
-    load_target(K, st, i, true, T);
-    const int n = __ldg(count + t);
-    if (n <= LQ_NBR_CAP) {
-        /* entry k of this particle is at list[k * stride + t]; p walks
-         * four entries at a time, offsets within a group stay 32-bit */
-        const int* p = list + t;
-        const size_t step4 = 4 * (size_t)stride;
-        int nxt[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) nxt[u] = u < n ? __ldg(p + u * stride) : i;
-        for (int k = 0; k < n; k += 4) {
-            p += step4;
-            int cur[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                cur[u] = nxt[u];
-                nxt[u] = k + 4 + u < n ? __ldg(p + u * stride) : i;
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (k + u < n && lq_in_range(cur[u], np)) pair_body<kKahan>(K, st, T, cur[u]);
-        }
-    } else {
-        walk_stencil(P, K, st, cells, i, T.x, [&](int j) { pair_body<kKahan>(K, st, T, j); }, fr);
-    }
-    store_rates(P, K, rt, i, T);
-}
-
 __global__ void __launch_bounds__(kBlock) k_pack_neighbors(int first, int np, State st, NbrArrays nb)
 {
     const int i = first + blockIdx.x * blockDim.x + threadIdx.x;
@@ -546,8 +505,9 @@ __device__ __forceinline__ void list_sums(const PairConst& K, const NbrArrays& n
     }
 }
 
-/* k_interaction_list over the packed neighbour arrays (same sums, same
- * order).  kThreads x kMinBlocks is the launch shape: the block size and
+/* Pair sums over the lists from the packed neighbour arrays; a particle
+ * whose list overflowed walks its stencil over the state arrays instead.
+ * kThreads x kMinBlocks is the launch shape: the block size and
  * the resident blocks per SM the register allocation is capped for; the
  * shapes of kPairShapes are compiled and one is chosen per simulation
  * (lq_sim_autotune times them). */
@@ -824,57 +784,9 @@ __global__ void __launch_bounds__(kBlock) k_shepard(const Parameters* __restrict
 /* ------------------------------------------------- list-driven Adami */
 /* The Adami extrapolation of k_adami, summed over a boundary particle's
  * list of material neighbours (built with a skin; pairs at q >= 2 are
- * skipped exactly as the cell walk skips them). */
-__global__ void __launch_bounds__(kBlock) k_adami_list(const Parameters* __restrict__ P, int npb, State st,
-                                                       const int* __restrict__ list, const int* __restrict__ count,
-                                                       int stride)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= npb) return;
-    const int n = min(__ldg(count + i), LQ_NBR_CAP);
-    if (n == 0) return;
-    const float ih = __ldg(&P->i_h), m = __ldg(&P->m), Cw = __ldg(&P->kernel_normalization_par);
-    const float4 xi = __ldg(st.pos + i);
-    tensor2d S = make_tensor2d(0.0f);
-    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int np_all = __ldg(&P->np);
-    for (int k = 0; k < n; ++k) {
-        const int j = __ldg(list + (size_t)k * stride + i);
-        if (!lq_in_range(j, np_all)) continue;
-        const float4 xj = __ldg(st.pos + j);
-        const float3 d = make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
-        const float q = norm3df(d.x, d.y, d.z) * ih;
-        if (q < 2.0f) {
-            const float ker = Cw * (2.0f - q) * (2.0f - q) * (2.0f - q) * (2.0f - q) * (q + 0.5f);
-            const float vol = m / __ldg(&st.vel[j].w);
-            const tensor2d sj = load_t2(st.str, j);
-            S.xx += sj.xx * ker * vol;
-            S.yy += sj.yy * ker * vol;
-            S.zz += sj.zz * ker * vol;
-            S.xy += sj.xy * ker * vol;
-            S.xz += sj.xz * ker * vol;
-            S.yz += sj.yz * ker * vol;
-            acc.x += d.x * ker * vol;
-            acc.y += d.y * ker * vol;
-            acc.z += d.z * ker * vol;
-            acc.w += ker * vol;
-        }
-    }
-    if (acc.w > 0.0f) {
-        const float rho0 = __ldg(&P->rho0);
-        tensor2d out;
-        out.xx = (S.xx - rho0 * __ldg(&P->acc_x) * acc.x) / acc.w;
-        out.yy = (S.yy - rho0 * __ldg(&P->acc_y) * acc.y) / acc.w;
-        out.zz = (S.zz - rho0 * __ldg(&P->acc_z) * acc.z) / acc.w;
-        out.xy = S.xy / acc.w;
-        out.xz = S.xz / acc.w;
-        out.yz = S.yz / acc.w;
-        store_t2(st.str, i, out);
-    }
-}
-
-/* k_adami_list reading the material neighbours from the packed arrays
- * (sigma_j V_j W = s_j rho_j m W with s = sigma / rho^2), and writing the
+ * skipped exactly as the cell walk skips them), reading the neighbours from
+ * the packed arrays (sigma_j V_j W = s_j rho_j m W with s = sigma / rho^2),
+ * and writing the
  * boundary particle's new stress both into the state and, scaled, into the
  * packed arrays, which then need no pack of the boundary slots before the
  * pair kernel.  Targets without neighbours keep both as they were. */
@@ -1169,15 +1081,6 @@ int launch_adami_packed(const Parameters* ph, const Parameters* pd, const State&
     return LQ_OK;
 }
 
-int launch_adami_list(const Parameters* ph, const Parameters* pd, const State& st, const NeighborList& nl,
-                      cudaStream_t s)
-{
-    if (ph->npb <= 0) return LQ_OK;
-    k_adami_list<<<blocks_for(ph->npb, kBlock), kBlock, 0, s>>>(pd, ph->npb, st, nl.list, nl.count, nl.stride);
-    LQ_TRY_CUDA(cudaGetLastError(), "k_adami_list");
-    return LQ_OK;
-}
-
 int launch_shepard_list(const Parameters* ph, const Parameters* pd, const State& st, tensor2d* out_str,
                         const NeighborList& nl, cudaStream_t s)
 {
@@ -1248,14 +1151,7 @@ int launch_interaction_list(const Parameters* ph, const Parameters* pd, const St
         LQ_TRY_CUDA(cudaGetLastError(), "k_interaction_rec");
         return LQ_OK;
     }
-    if (compensated)
-        k_interaction_list<true><<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, r, c,
-                                                                               nl.list, nl.count, nl.stride, fr);
-    else
-        k_interaction_list<false><<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, r, c,
-                                                                                nl.list, nl.count, nl.stride, fr);
-    LQ_TRY_CUDA(cudaGetLastError(), "k_interaction_list");
-    return LQ_OK;
+    return set_error(LQ_ERR_ARG, "interaction: the packed neighbour arrays are required");
 }
 
 int launch_adami(const Parameters* ph, const Parameters* pd, const State& st, const Cells& c, cudaStream_t s)

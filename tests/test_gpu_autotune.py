@@ -128,3 +128,32 @@ def test_autotune_leaves_the_state_and_matches_a_fresh_run(lq, cuda):
     b.step(20)
     for x, y in zip(a.download(), b.download()):
         assert np.array_equal(x, y)
+
+
+def test_tile_order_with_frames_materials_and_model_3(lq, cuda):
+    """Tile order on a batched ensemble (per-object grid rows and materials)
+    and on the von Wolffersdorff model in the mixed form: bit-identical to
+    slot order."""
+    comb, _ = cases.ensemble(n=5, count_range=(2.0e3, 4.0e3), seed=14, shepard=7)
+    out = []
+    for shape in (0, 8, 9):
+        s = lq.Simulation(comb.par, *comb.arrays())
+        s.set_materials(comb.meta["materials"])
+        s.set_frames(comb.meta["frames"])
+        s.set_pair_shape(shape)
+        s.step(35)
+        assert not s.health().any()
+        out.append(s.download())
+    for other in out[1:]:
+        for x, y in zip(out[0], other):
+            assert np.array_equal(x, y)
+    v = cases.small_column(model=3, velocity_noise=0.05, shepard=7, seed=63)
+    out = []
+    for shape in (0, 10):
+        s = lq.Simulation(v.par, *v.arrays(), mixed=True)
+        s.set_hypoplastic(v.meta["hypoplastic"])
+        s.set_pair_shape(shape)
+        s.step(25)
+        out.append(s.download())
+    for x, y in zip(*out):
+        assert np.array_equal(x, y)

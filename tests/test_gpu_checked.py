@@ -23,19 +23,23 @@ import numpy as np
 import loquat_b200 as lq
 from loquat_b200 import cases
 c = cases.small_column(velocity_noise=0.3, shepard=7, seed=61)
-for mixed in (False, True):
+for mixed, shape in ((False, 0), (True, 0), (True, 9), (False, 10)):
     s = lq.Simulation(c.par, *c.arrays(), mixed=mixed)
+    s.set_pair_shape(shape)          # 9, 10: targets in tile order
     s.step(60)
     assert s.rebuilds() >= 2
     assert not s.health().any()
 comb, _ = cases.ensemble(n=4, count_range=(1.5e3, 4.0e3), seed=13, shepard=7)
-s = lq.Simulation(comb.par, *comb.arrays())
-s.set_materials(comb.meta["materials"])
-s.set_frames(comb.meta["frames"])
-s.step(30)
+for shape in (0, 8):
+    s = lq.Simulation(comb.par, *comb.arrays())
+    s.set_materials(comb.meta["materials"])
+    s.set_frames(comb.meta["frames"])
+    s.set_pair_shape(shape)
+    s.step(30)
 v = cases.small_column(model=3, velocity_noise=0.05, shepard=7, seed=62)
 s = lq.Simulation(v.par, *v.arrays(), mixed=True)
 s.set_hypoplastic(v.meta["hypoplastic"])
+s.set_pair_shape(7)
 s.step(20)
 print("VIOLATIONS", lq.bounds_violations())
 """
