@@ -475,10 +475,16 @@ def bench_ensemble(args):
         sim.set_materials(comb.meta["materials"])
         sim.set_frames(comb.meta["frames"])
         sim.step(args.warmup)
-        return sim
+        tuned = None
+        if not args.no_autotune:
+            # the batched form's launch shape and list skin by the project's
+            # autotuner (state, step and time put back)
+            shape, skin = sim.autotune(args.tune_steps)
+            tuned = {"pair_shape": shape, "skin_over_h": skin, "steps_per_trial": args.tune_steps}
+        return sim, tuned
 
     # the batched ensemble in the chosen form (the line's value), then in the other
-    sim = batched(args.form == "mixed")
+    sim, tuned = batched(args.form == "mixed")
     rb0 = sim.rebuilds()
     sim.synchronize()
     if dist:
@@ -491,7 +497,7 @@ def bench_ensemble(args):
     plain_launches, _ = sim.launches_per_step()
     sim.close()
     other = "plain" if args.form == "mixed" else "mixed"
-    sim = batched(other == "mixed")
+    sim, tuned_other = batched(other == "mixed")
     if dist:
         dist.barrier()
     ms_other = replicas.max_over_ranks(timed(sim, args.steps), device="cuda")
@@ -518,7 +524,8 @@ def bench_ensemble(args):
                        "npm": npm, "rank0_np": par.np, "rank0_ncell": par.ncell,
                        "parallelism": "scenarios split over %d ranks by particle count" % world,
                        "form": "batched (%s): one simulation, per-scenario frames and materials, CUDA-graph step"
-                               % ("mixed precision" if args.form == "mixed" else "plain FP32")},
+                               % ("mixed precision" if args.form == "mixed" else "plain FP32"),
+                       "autotuned": {args.form: tuned, other: tuned_other}},
             "forms": {args.form: {"value": v_batch, "ms_per_step": ms_batch / args.steps},
                       other: {"value": v_other, "ms_per_step": ms_other / args.steps}},
             "sequential": {"value": v_seq, "ms_per_step": ms_seq / args.steps,
