@@ -513,9 +513,7 @@ int create(LqSim* S, const Parameters* par, const float* pos, const float* vel, 
         LQ_TRY(dev_alloc(S, (void**)&S->vmax2, 2 * sizeof(unsigned)));
         LQ_TRY(dev_alloc(S, (void**)&S->dtime, sizeof(double)));
     }
-#ifndef LQ_NO_NBR_RECORD
     LQ_TRY(dev_alloc(S, (void**)&S->rec, n * 13 * sizeof(float)));   /* cudaMalloc: 256-byte aligned */
-#endif
     LQ_TRY(dev_alloc(S, (void**)&S->R.accad, n * sizeof(float4)));
     LQ_TRY(dev_alloc(S, (void**)&S->R.spin, n * sizeof(float4)));
     LQ_TRY(dev_alloc(S, (void**)&S->R.acestn, n * sizeof(tensor2d)));

@@ -455,15 +455,9 @@ __global__ void __launch_bounds__(kBlock) k_pack_neighbors(int first, int np, St
  * targets of a block share. */
 __device__ __forceinline__ int ld_list(const int* p)
 {
-#if defined(LQ_LIST_LDG)
-    return __ldg(p);
-#elif defined(LQ_LIST_CS)
-    return __ldcs(p);
-#else
     int v;
     asm("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
     return v;
-#endif
 }
 
 /* The sums over one target's list (entry k at p[k * stride]), four
