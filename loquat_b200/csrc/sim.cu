@@ -295,8 +295,9 @@ int enqueue_density_filter(LqSim* S, cudaStream_t s)
 }
 
 /* Adami for a stage.  The material slots are packed first, Adami reads
- * them and writes the boundary slots' packed stress itself (boundary positions and velocities are packed at each list
- * build and do not change in between), so the pair kernel needs no pack. */
+ * them and writes the boundary slots' packed stress itself (boundary
+ * positions and velocities are packed at each list build and do not change
+ * in between), so the pair kernel needs no pack. */
 int enqueue_adami_pack(LqSim* S, const State& st, cudaStream_t s)
 {
     LQ_TRY(lqb::launch_pack_neighbors(&S->ph, st, S->rec, S->npb, s));
