@@ -1,0 +1,43 @@
+"""The reference arm of bench.py on the CPU: `--impl reference` times the
+FP64 oracle on a bounded sample of the workload and prints one JSON line
+with the keys the bench contract asks for; under torchrun only rank 0 runs
+and prints it, the other ranks exit 0 without work."""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def run_bench(args, **env):
+    e = dict(os.environ, PYTHONPATH=str(ROOT), **env)
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), *args], capture_output=True, text=True, env=e,
+                       cwd=ROOT, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    return [l for l in r.stdout.splitlines() if l.startswith("{")]
+
+
+def test_reference_arm_prints_one_contract_line():
+    lines = run_bench(["--impl", "reference", "--config", "column", "--steps", "1", "--warmup", "0"])
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    assert d["metric"] == "particle-steps/s" and d["unit"] == "particle-steps/s"
+    assert d["higher_is_better"] is True
+    assert d["steps"] == 1 and d["warmup"] == 0 and d["n_gpus"] == 1
+    assert d["value"] > 0 and d["ms_per_step"] > 0
+    assert d["config"]["workload"].startswith("column collapse")
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_other_ranks_exit_quietly():
+    lines = run_bench(["--impl", "reference", "--config", "column", "--steps", "1", "--warmup", "0"],
+                      RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    assert lines == []
