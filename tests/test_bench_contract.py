@@ -41,3 +41,28 @@ def test_reference_arm_other_ranks_exit_quietly():
     lines = run_bench(["--impl", "reference", "--config", "column", "--steps", "1", "--warmup", "0"],
                       RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
     assert lines == []
+
+
+def test_clock_sampler_reads_clocks_and_throttle_reasons(tmp_path, monkeypatch):
+    """The clock record beside each bench line: median SM clock under load,
+    the maximum, and every throttle reason seen active (a fake nvidia-smi
+    prints the sampled rows)."""
+    fake = tmp_path / "nvidia-smi"
+    fake.write_text("#!/bin/sh\n"
+                    "echo '0, 1965, 1965, 700.1, 0x0, Not Active, Not Active, Not Active, Not Active'\n"
+                    "echo '0, 1800, 1965, 990.5, 0x4, Not Active, Not Active, Not Active, Active'\n"
+                    "echo '0, 1950, 1965, 950.0, 0x0, Not Active, Not Active, Not Active, Not Active'\n"
+                    "exec sleep 30\n")
+    fake.chmod(0o755)
+    monkeypatch.setenv("PATH", f"{tmp_path}{os.pathsep}{os.environ['PATH']}")
+    sys.path.insert(0, str(ROOT))
+    try:
+        import bench
+    finally:
+        sys.path.pop(0)
+    import time
+
+    s = bench.ClockSampler(None)
+    time.sleep(0.5)
+    c = s.stop()
+    assert c == {"sm_mhz": 1950.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3}
