@@ -21,6 +21,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include "lq_internal.cuh"
+#include "lq_tile.h"
 #include "lq_device.cuh"
 #include <adami_boundary.h>
 #include <field_smoothing.h>
@@ -532,44 +533,21 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_interaction_rec(
 }
 
 /* ------------------------------------------------- tile order of targets */
-/* The pair kernel's targets in tile order: the material layer's lattice is
- * cut into tiles of 3 x 3 columns by tz cells, taken with tz fastest, and
- * within a tile column by column, each column's tz cells being one run of
- * consecutive slots (the grid's key is z fastest).  A block of the pair
- * kernel then holds a compact box of targets whose neighbourhood fits in
- * L1, instead of a thin z-run of one column whose neighbours the next
- * block on the SM does not share.  Segment s < nseg - 2 is column s % 9 of
- * tile s / 9; the last two hold the material slots below the material
- * layer (none in a sound state) and the out-of-lattice cell.  Every
- * segment is clamped to [npb, np), so the segments partition the
- * material slots. */
-__global__ void __launch_bounds__(kBlock) k_tile_segments(const int* __restrict__ start, int nx, int ny, int nz,
-                                                          int L, int tz, int nty, int ntz, int npb, int np,
-                                                          int nseg, int* __restrict__ seg_beg,
+/* The pair kernel's targets in tile order (lq_tile.h has the index
+ * arithmetic): tiles of 3 x 3 columns by tz cells, each tile column one run
+ * of consecutive slots.  A block of the pair kernel then holds a compact
+ * box of targets whose neighbourhood fits in L1, instead of a thin z-run of
+ * one column whose neighbours the next block on the SM does not share. */
+__global__ void __launch_bounds__(kBlock) k_tile_segments(const int* __restrict__ start, TileGrid tg, int npb,
+                                                          int np, int* __restrict__ seg_beg,
                                                           int* __restrict__ seg_len)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nseg) return;
-    int b = npb, e = npb;
-    if (s < nseg - 2) {
-        const int c = s % 9, tile = s / 9;
-        const int kz = tile % ntz, rest = tile / ntz;
-        const int X = 3 * (rest / nty) + c % 3, Y = 3 * (rest % nty) + c / 3, z0 = kz * tz;
-        if (X < nx && Y < ny && z0 < nz) {
-            const int key0 = L + (X * ny + Y) * nz + z0;
-            b = __ldg(start + key0);
-            e = __ldg(start + key0 + min(tz, nz - z0));
-        }
-    } else if (s == nseg - 2) {
-        e = __ldg(start + L);
-    } else {
-        b = __ldg(start + 2 * L);
-        e = np;
-    }
-    b = max(b, npb);
-    e = min(e, np);
+    if (s >= tg.nseg) return;
+    int b, len;
+    tile_segment(tg, start, npb, np, s, &b, &len);
     seg_beg[s] = b;
-    seg_len[s] = max(e - b, 0);
+    seg_len[s] = len;
 }
 
 /* One warp per segment writes its targets (slot - npb) at the segment's
@@ -977,18 +955,14 @@ static int tile_height(const Parameters* ph, int threads)
     return tz < 1 ? 1 : tz;
 }
 
-static void tile_counts(const Parameters* ph, int tz, int* nty, int* ntz, int* nseg)
+static TileGrid tile_grid_of(const Parameters* ph, int tz)
 {
-    const int nx = ph->cell_num_x, ny = ph->cell_num_y, nz = ph->cell_num_z;
-    *nty = (ny + 2) / 3;
-    *ntz = (nz + tz - 1) / tz;
-    *nseg = ((nx + 2) / 3) * *nty * *ntz * 9 + 2;
+    return tile_grid(ph->cell_num_x, ph->cell_num_y, ph->cell_num_z, ph->ncell_one_layer, tz);
 }
 
 int tile_order_scratch(const Parameters* ph, int* nseg, size_t* scan_bytes)
 {
-    int nty, ntz;
-    tile_counts(ph, 1, &nty, &ntz, nseg);   /* the most segments any tile height needs */
+    *nseg = tile_grid_of(ph, 1).nseg;   /* the most segments any tile height needs */
     *scan_bytes = 0;
     LQ_TRY_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, *scan_bytes, (const int*)nullptr, (int*)nullptr, *nseg),
                 "tile scan scratch query");
@@ -999,16 +973,13 @@ int launch_tile_order(const Parameters* ph, const int* start, int shape, const T
 {
     if (shape < 0 || shape >= kPairShapeCount || !kPairShapes[shape][2] || ph->npm <= 0) return LQ_OK;
     if (!to.order || !to.seg) return set_error(LQ_ERR_ARG, "tile order: buffers not allocated");
-    const int tz = tile_height(ph, kPairShapes[shape][0]);
-    int nty, ntz, nseg;
-    tile_counts(ph, tz, &nty, &ntz, &nseg);
+    const TileGrid tg = tile_grid_of(ph, tile_height(ph, kPairShapes[shape][0]));
+    const int nseg = tg.nseg;
     if (nseg > to.nseg_cap) return set_error(LQ_ERR_ARG, "tile order: %d segments > capacity %d", nseg, to.nseg_cap);
     int* beg = to.seg;
     int* len = to.seg + to.nseg_cap;
     int* off = to.seg + 2 * (size_t)to.nseg_cap;
-    k_tile_segments<<<blocks_for(nseg, kBlock), kBlock, 0, s>>>(start, ph->cell_num_x, ph->cell_num_y,
-                                                                ph->cell_num_z, ph->ncell_one_layer, tz, nty, ntz,
-                                                                ph->npb, ph->np, nseg, beg, len);
+    k_tile_segments<<<blocks_for(nseg, kBlock), kBlock, 0, s>>>(start, tg, ph->npb, ph->np, beg, len);
     LQ_TRY_CUDA(cudaGetLastError(), "k_tile_segments");
     size_t bytes = to.scan_bytes;
     LQ_TRY_CUDA(cub::DeviceScan::ExclusiveSum(to.scan_tmp, bytes, len, off, nseg, s), "tile scan");
