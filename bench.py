@@ -79,6 +79,13 @@ def parse_args(argv=None):
     ap.add_argument("--tune-steps", type=int, default=40, help="timed steps per autotuner trial")
     ap.add_argument("--pair-shape", type=int, default=None,
                     help="fix the pair kernel's launch shape (lq_sim_set_pair_shape, 0-10) instead of autotuning")
+    ap.add_argument("--no-dropin", action="store_true",
+                    help="skip timing the reference's step sequence through the drop-in entry points")
+    ap.add_argument("--no-ensemble", action="store_true",
+                    help="skip the config-4 ensemble leg of the default run")
+    ap.add_argument("--amortized-steps", type=int, default=250,
+                    help="length of the second, longer timed window that carries the neighbour-list rebuilds at "
+                         "their natural rate (0 to skip)")
     ap.add_argument("--eager", action="store_true",
                     help="launch kernels one by one instead of replaying the step graph (for ncu, which cannot "
                          "profile kernels inside graphs with conditional nodes)")
@@ -115,6 +122,11 @@ def cpu_sample_case(args):
         s = (1.0e5 / 2.856e6) ** (1.0 / 3.0)
         return cases.slope_failure(dr=0.005 / s, seed=1), "slope failure at dr=%.2f mm (~100 k soil)" % (5.0 / s)
     return cases.column_collapse(seed=1), "column collapse 50k"
+
+
+def workload_config(args, par):
+    """The line's `config`: the workload and its sizes, the same in both arms."""
+    return {"workload": workload_name(args), "np": par.np, "npm": par.npm, "npb": par.npb, "ncell": par.ncell}
 
 
 def measured_peaks():
@@ -218,32 +230,60 @@ def run_cpu_baseline(args, steps=5, warmup=1):
                       f"particles), {warmup} warm-up + {steps} timed steps, FP64"}, dt
 
 
+# the CPU arm times at most this many particle-steps per leg (about a minute
+# of FP64 work on 16 host threads); larger workloads run fewer timed steps
+REFERENCE_BUDGET_PARTICLE_STEPS = 1.2e8
+
+
 def bench_reference(args):
+    """The reference's algorithm on the host: the FP64 OpenMP restatement
+    (oracle/) of reference src/loquat.cu:322-409 on the same workload as
+    the GPU arm, with every host thread, then the same state stepped on one
+    thread.  The case's Parameters are derived by the oracle, so this arm
+    loads no library of the product."""
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
+    if args.config == "ensemble":
+        print(json.dumps({"impl": "reference", "unavailable": "the CPU arm times the single-domain workloads; the "
+                                                              "ensemble's 30 M particles exceed its budget"}))
+        return 0
     import oracle
+    from loquat_b200 import cases
 
-    case, desc = cpu_sample_case(args)
+    cases.use_parameter_initializer(oracle.initialize_parameters)
+    case = make_case(args)
+    par = case.par
     threads = os.cpu_count() or 1
+    steps = max(1, min(args.steps, int(REFERENCE_BUDGET_PARTICLE_STEPS // max(par.np, 1))))
     oracle.set_threads(threads)
-    sim = oracle.OracleSim(case.par, *case.arrays())
+    sim = oracle.OracleSim(par, *case.arrays())
     if "hypoplastic" in case.meta:
         sim.set_vw(case.meta["hypoplastic"])
-    sim.step(args.warmup)
+    sim.step(min(args.warmup, 2))
     t0 = time.perf_counter()
-    sim.step(args.steps)
+    sim.step(steps)
     dt = time.perf_counter() - t0
-    value = case.par.npm * args.steps / dt
+    value = par.npm * steps / dt
+    # the same state, one host thread, one step (reference-free single-core figure)
+    oracle.set_threads(1)
+    t1 = time.perf_counter()
+    sim.step(1)
+    dt1 = time.perf_counter() - t1
+    sim.close()
+    single = par.npm / dt1
+    sample = (f"the full workload ({par.npm} soil + {par.npb} boundary particles), {steps} timed steps after "
+              f"{min(args.warmup, 2)} warm-up steps")
     out = {
         "impl": "reference",
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / max(args.steps, 1),
+        "steps": steps, "warmup": min(args.warmup, 2), "ms_per_step": 1e3 * dt / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(args), "sample": desc, "np": case.par.np, "npm": case.par.npm},
+        "config": workload_config(args, par),
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
-                         "sample": f"{desc} ({case.par.npm} soil particles), FP64 OpenMP restatement of the "
-                                   "reference algorithm"},
+                         "sample": sample + ", FP64 OpenMP restatement of the reference algorithm"},
+        "single_thread": {"value": single, "unit": "particle-steps/s", "cores": 1,
+                          "sample": "one further step of the same state on one host thread"},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
@@ -260,6 +300,34 @@ def workload_name(args):
         return ("von Wolffersdorff 1.0x1.0x0.25 m block on a 30 deg plane dr=%.1f mm h=1.2dr e0=0.65 "
                 "(FP64 sub-stepping, tol 1e-4)" % (1e3 * (args.dr or 0.0025)))
     return "column collapse 0.2x0.1x0.02 m dr=2 mm h=1.2dr DP phi=19.8"
+
+
+def dropin_measurement(args, case, torch, dist):
+    """The reference's step sequence (src/loquat.cu:322-409: a search and
+    re-sort before each stage, Adami, ParticleInteraction, Predictor /
+    Corrector, Shepard every N steps) through the drop-in entry points on
+    the same workload, as a caller of the reference's headers runs it;
+    CUDA events on its stream, max over ranks."""
+    from loquat_b200 import dropin, replicas
+
+    stream = torch.cuda.Stream()
+    seq = dropin.ReferenceStep(case.par, *case.arrays(), stream=stream)
+    seq.step(args.warmup)
+    stream.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    seq.step(args.steps)
+    e1.record(stream)
+    stream.synchronize()
+    ms = replicas.max_over_ranks(e0.elapsed_time(e1), device="cuda")
+    seq.close()
+    world = dist.get_world_size() if dist else 1
+    return {"value": case.par.npm * args.steps * world / (ms / 1e3), "unit": "particle-steps/s",
+            "ms_per_step": ms / args.steps, "steps": args.steps,
+            "form": "plain FP32, the reference's call sequence through lq_grid_*, lq_adami_boundary, "
+                    "lq_particle_interaction, lq_predictor / lq_corrector, lq_stress_regularization"}
 
 
 def bench_ours(args):
@@ -323,6 +391,25 @@ def bench_ours(args):
     launches = (s1 - s0) * plain + shep_steps * (with_shep - plain) + rebuilds * sim.rebuild_launches()
     value = npm * args.steps * world / (ms / 1e3)
     health = sim.health()
+
+    # a longer window of the same run: its rebuilds come at their natural
+    # rate, so its time per step carries their amortised cost
+    amortized = None
+    if args.amortized_steps > 0:
+        rb_a = sim.rebuilds()
+        sim.synchronize()
+        if dist:
+            dist.barrier()
+        aext = torch.cuda.ExternalStream(sim.stream())
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(aext)
+        sim.step(args.amortized_steps)
+        a1.record(aext)
+        sim.synchronize()
+        ams = replicas.max_over_ranks(a0.elapsed_time(a1), device="cuda")
+        amortized = {"form": args.form, "value": npm * args.amortized_steps * world / (ams / 1e3),
+                     "ms_per_step": ams / args.amortized_steps, "steps": args.amortized_steps,
+                     "neighbour_list_rebuilds": sim.rebuilds() - rb_a}
 
     # live per-phase device times (eager launches, CUDA events on the same stream)
     prof = sim.profile(args.profile_steps) if args.profile_steps > 0 else {}
@@ -388,6 +475,17 @@ def bench_ours(args):
         forms[other] = {"value": npm * args.steps * world / (oms / 1e3), "ms_per_step": oms / args.steps}
         sim = osim
 
+    sim.close()
+    sim = None
+
+    dropin = None
+    if not args.no_dropin and args.config in ("cylinder", "column"):
+        dropin = dropin_measurement(args, case, torch, dist)
+
+    ensemble = None
+    if not args.no_ensemble and args.config == "cylinder":
+        ensemble = ensemble_measurement(args, torch, world, rank, local, dist)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu, _ = run_cpu_baseline(args)
@@ -397,14 +495,14 @@ def bench_ours(args):
             "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.form == "plain" else "f32+f64", "data": "synthetic",
-            "config": {"workload": workload, "np": np_, "npm": npm, "npb": par.npb, "ncell": par.ncell,
-                       "autotuned": tuned,
-                       "form": "%s, %s, Verlet lists" % (
-                           "plain FP32" if args.form == "plain" else "mixed precision (FP64 integrator)",
-                           "eager launches" if args.eager else "CUDA-graph step"),
-                       "timed_window": "steps %d..%d of the run" % (s0, s1),
-                       "l2": "state larger than L2 (3 x %.0f MB state buffers)" % (np_ * 96 / 1e6),
-                       "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
+            "config": workload_config(args, par),
+            "run": {"autotuned": tuned,
+                    "form": "%s, %s, Verlet lists" % (
+                        "plain FP32" if args.form == "plain" else "mixed precision (FP64 integrator)",
+                        "eager launches" if args.eager else "CUDA-graph step"),
+                    "timed_window": "steps %d..%d of the run" % (s0, s1),
+                    "l2": "state larger than L2 (3 x %.0f MB state buffers)" % (np_ * 96 / 1e6),
+                    "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                          "frac": (achieved_gbs / peak) if achieved_gbs else None, "traffic": traffic,
                          "kernel": "k_interaction_rec", "peak_kind": peak_kind,
@@ -423,36 +521,39 @@ def bench_ours(args):
             "health": [int(x) for x in health],
             "clocks": clk,
             "e2e": e2e,
+            "amortized": amortized,
+            "dropin": dropin,
+            "ensemble": ensemble,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))
-    sim.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return 0
 
 
-def bench_ensemble(args):
-    """Batched ensemble (one simulation holding every scenario, one graph
-    launch per step) against the same scenarios run one after another, each
-    as its own plain simulation.  Both timed with CUDA events on the
-    simulations' streams, after the same warm-up."""
-    import torch
+def size_classes(counts, nclass=4):
+    """Scenario indices grouped by particle count into nclass log-spaced
+    classes (empty classes dropped)."""
+    c = np.log(np.asarray(counts, np.float64))
+    lo, hi = c.min(), c.max() + 1e-9
+    cls = np.minimum(((c - lo) / max(hi - lo, 1e-9) * nclass).astype(int), nclass - 1)
+    return [list(np.nonzero(cls == k)[0]) for k in range(nclass) if np.any(cls == k)]
 
+
+def ensemble_measurement(args, torch, world, rank, local, dist, sample_clocks=False):
+    """Batched ensemble of config 4 (one simulation holding every scenario,
+    one graph launch per step) in both precision forms, against the same
+    scenarios run one after another, each as its own plain simulation.  The
+    batched forms are autotuned as a whole; the sequential runs are tuned by
+    size class (one autotuner run on the median scenario of each of four
+    log-spaced particle-count classes, its shape and skin applied to the
+    class).  All timed with CUDA events on the simulations' streams after
+    the same warm-up; max over ranks."""
     import loquat_b200 as lq
-    from loquat_b200 import cases
+    from loquat_b200 import cases, replicas
 
-    from loquat_b200 import replicas
-
-    world, rank, local = dist_setup()
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
     _, all_parts = cases.ensemble(n=args.scenarios, seed=4)
     shares = replicas.partition([p.par.npm for p in all_parts], world)
     parts = [all_parts[k] for k in shares[rank]]
@@ -477,63 +578,97 @@ def bench_ensemble(args):
         sim.step(args.warmup)
         tuned = None
         if not args.no_autotune:
-            # the batched form's launch shape and list skin by the project's
-            # autotuner (state, step and time put back)
             shape, skin = sim.autotune(args.tune_steps)
             tuned = {"pair_shape": shape, "skin_over_h": skin, "steps_per_trial": args.tune_steps}
         return sim, tuned
 
-    # the batched ensemble in the chosen form (the line's value), then in the other
-    sim, tuned = batched(args.form == "mixed")
-    rb0 = sim.rebuilds()
-    sim.synchronize()
-    if dist:
-        dist.barrier()
-    clocks = ClockSampler(gpu_uuid(torch, local)) if rank == 0 else None
-    ms_batch = replicas.max_over_ranks(timed(sim, args.steps), device="cuda")
-    clk = clocks.stop() if clocks else None
-    rebuilds = sim.rebuilds() - rb0
-    health = sim.health()
-    plain_launches, _ = sim.launches_per_step()
-    sim.close()
-    other = "plain" if args.form == "mixed" else "mixed"
-    sim, tuned_other = batched(other == "mixed")
-    if dist:
-        dist.barrier()
-    ms_other = replicas.max_over_ranks(timed(sim, args.steps), device="cuda")
-    sim.close()
+    forms, tuned_by_form, extra = {}, {}, {}
+    for form in (args.form, "plain" if args.form == "mixed" else "mixed"):
+        sim, tuned = batched(form == "mixed")
+        rb0 = sim.rebuilds()
+        sim.synchronize()
+        if dist:
+            dist.barrier()
+        clocks = ClockSampler(gpu_uuid(torch, local)) if (sample_clocks and rank == 0 and not forms) else None
+        ms = replicas.max_over_ranks(timed(sim, args.steps), device="cuda")
+        if not forms:
+            extra = {"clocks": clocks.stop() if clocks else None, "neighbour_list_rebuilds": sim.rebuilds() - rb0,
+                     "health": [int(x) for x in sim.health()], "gpu_launches_per_step": sim.launches_per_step()[0]}
+        sim.close()
+        forms[form] = {"value": total_npm * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps}
+        tuned_by_form[form] = tuned
+
+    # sequential plain runs, tuned by size class
+    class_tuning = []
+    seq_shape = {}
+    if not args.no_autotune:
+        counts = [p.par.npm for p in parts]
+        for members in size_classes(counts):
+            rep = members[int(np.argsort([counts[k] for k in members])[len(members) // 2])]
+            p = parts[rep]
+            s = lq.Simulation(p.par, *p.arrays())
+            s.step(args.warmup)
+            shape, skin = s.autotune(args.tune_steps)
+            s.close()
+            for k in members:
+                seq_shape[k] = (shape, skin)
+            class_tuning.append({"scenarios": len(members), "representative_npm": counts[rep],
+                                 "pair_shape": shape, "skin_over_h": skin})
     ms_seq = 0.0
-    for p in parts:
+    for k, p in enumerate(parts):
         s = lq.Simulation(p.par, *p.arrays())
+        if k in seq_shape:
+            s.set_pair_shape(seq_shape[k][0])
+            s.set_skin(seq_shape[k][1])
         s.step(args.warmup)
         ms_seq += timed(s, args.steps)
         s.close()
     ms_seq = replicas.max_over_ranks(ms_seq, device="cuda")
-    npm = total_npm
-    v_batch = npm * args.steps / (ms_batch / 1e3)
-    v_other = npm * args.steps / (ms_other / 1e3)
-    v_seq = npm * args.steps / (ms_seq / 1e3)
+    v_seq = total_npm * args.steps / (ms_seq / 1e3)
+    out = {
+        "workload": "ensemble of %d Drucker-Prager column collapses (counts log-uniform 5e3-2e5, H/L 0.5-4, "
+                    "phi 20-40 deg, c 0-5 kPa, dr=2 mm, h=1.2dr)" % args.scenarios,
+        "npm": total_npm, "rank0_np": par.np, "rank0_ncell": par.ncell, "steps": args.steps,
+        "forms": forms,
+        "sequential": {"value": v_seq, "ms_per_step": ms_seq / args.steps,
+                       "form": "the same scenarios one after another, one plain FP32 simulation each, tuned by "
+                               "size class", "tuning": class_tuning},
+        "batched_over_sequential": {f: forms[f]["value"] / v_seq for f in forms},
+        "autotuned": tuned_by_form,
+        "partition": {"ranks": world, "imbalance": replicas.imbalance([p.par.npm for p in all_parts], shares)},
+    }
+    out.update(extra)
+    return out
+
+
+def bench_ensemble(args):
+    """--config ensemble: the batched ensemble as the line's value."""
+    import torch
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    m = ensemble_measurement(args, torch, world, rank, local, dist, sample_clocks=True)
     if rank == 0:
+        v = m["forms"][args.form]
         print(json.dumps({
-            "metric": "particle-steps/s", "value": v_batch, "unit": "particle-steps/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batch / args.steps,
+            "metric": "particle-steps/s", "value": v["value"], "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v["ms_per_step"],
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "f32" if args.form == "plain" else "f32+f64", "data": "synthetic",
-            "config": {"workload": "ensemble of %d Drucker-Prager column collapses (counts log-uniform 5e3-2e5, "
-                                   "H/L 0.5-4, phi 20-40 deg, c 0-5 kPa, dr=2 mm, h=1.2dr)" % args.scenarios,
-                       "npm": npm, "rank0_np": par.np, "rank0_ncell": par.ncell,
-                       "parallelism": "scenarios split over %d ranks by particle count" % world,
-                       "form": "batched (%s): one simulation, per-scenario frames and materials, CUDA-graph step"
-                               % ("mixed precision" if args.form == "mixed" else "plain FP32"),
-                       "autotuned": {args.form: tuned, other: tuned_other}},
-            "forms": {args.form: {"value": v_batch, "ms_per_step": ms_batch / args.steps},
-                      other: {"value": v_other, "ms_per_step": ms_other / args.steps}},
-            "sequential": {"value": v_seq, "ms_per_step": ms_seq / args.steps,
-                           "form": "the same scenarios one after another, one plain FP32 simulation each"},
-            "batched_over_sequential": v_batch / v_seq,
-            "gpu_launches_per_step": plain_launches,
-            "neighbour_list_rebuilds": rebuilds, "health": [int(x) for x in health], "clocks": clk,
-            "partition": {"ranks": world, "imbalance": replicas.imbalance([p.par.npm for p in all_parts], shares)},
+            "config": {"workload": m["workload"], "npm": m["npm"]},
+            "form": "batched (%s): one simulation, per-scenario frames and materials, CUDA-graph step"
+                    % ("mixed precision" if args.form == "mixed" else "plain FP32"),
+            "forms": m["forms"], "sequential": m["sequential"],
+            "batched_over_sequential": m["batched_over_sequential"][args.form],
+            "autotuned": m["autotuned"], "gpu_launches_per_step": m["gpu_launches_per_step"],
+            "neighbour_list_rebuilds": m["neighbour_list_rebuilds"], "health": m["health"],
+            "clocks": m["clocks"], "partition": m["partition"],
         }))
     if dist:
         dist.barrier()

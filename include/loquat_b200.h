@@ -80,9 +80,13 @@ int lq_grid_sort_tensor2d(void* grid, int np, float* data, float* cache, void* s
  * device array inside the library, held on every device that loads it
  * until exit.  Limits: np <= LQ_NOALLOC_MAX_PARTICLES, ncell <=
  * LQ_NOALLOC_MAX_CELLS, else LQ_ERR_ARG.  All calls on a device share that
- * array: calls that overlap on the GPU race.  The first call on a device
- * looks up the array's device address (with that device current); make
- * it before any stream capture begins. */
+ * array: calls that overlap on the GPU race.  Each call made outside
+ * stream capture looks up the array's device address (with that device
+ * current, so a module reloaded after cudaDeviceReset is found again);
+ * calls during a capture reuse the last address, so make one call on the
+ * device before any capture begins (a first call inside a capture returns
+ * LQ_ERR_ARG).  Particles outside the lattice share one cell, ordered by
+ * a single thread: keep their number small. */
 #define LQ_NOALLOC_MAX_PARTICLES 1048576
 #define LQ_NOALLOC_MAX_CELLS     1048575
 int lq_grid_neighbor_search_noalloc(const void* par_host, const void* par_device, const float* pospres,

@@ -84,6 +84,29 @@ def _base_parameters(dr, hdr, rho0, domain, E, nu, cfl, model, model_pars, shepa
     return p
 
 
+_initializer = None
+
+
+def use_parameter_initializer(fn):
+    """Derive the constants of every generated case's Parameters with `fn`
+    in place of the library's lq_initialize_parameters; both restate
+    reference src/loquat.cu:111-139 in the same float arithmetic, so the
+    records are bit-identical.  A caller that must not load the CUDA
+    library (a CPU-only timing of the same workload) passes its own; None
+    restores the library's.  Returns the previous setting."""
+    global _initializer
+    prev, _initializer = _initializer, fn
+    return prev
+
+
+def _parameter_initializer():
+    if _initializer is not None:
+        return _initializer
+    from . import initialize_parameters
+
+    return initialize_parameters
+
+
 def assemble(name, par, boundary_xyz, soil_xyz, rng, jitter, rho0, gravity_z, top_z, floor_z, K0,
              object_ids=(0, 1), meta=None) -> Case:
     """Stacks boundary then soil particles, jitters them, sets geostatic stress.
@@ -91,7 +114,7 @@ def assemble(name, par, boundary_xyz, soil_xyz, rng, jitter, rho0, gravity_z, to
     Soil stress: sigma_zz = rho0 g (top - z) (negative: compression), sigma_xx =
     sigma_yy = K0 sigma_zz, pressure = -tr(sigma)/3.  Boundary stress starts at
     0 (the Adami pass overwrites it)."""
-    from . import initialize_parameters
+    initialize_parameters = _parameter_initializer()
 
     nb, ns = boundary_xyz.shape[0], soil_xyz.shape[0]
     xyz = np.concatenate([boundary_xyz, soil_xyz], axis=0)
@@ -483,7 +506,7 @@ def combine(parts):
         slices.append(((ob, ob + pb), (om, om + pm)))
         ob += pb
         om += pm
-    from . import initialize_parameters
+    initialize_parameters = _parameter_initializer()
 
     par.np, par.npb, par.npm = nb + ns, nb, ns
     initialize_parameters(par)

@@ -20,9 +20,16 @@
  * the array and produce wrong results: serialise them.
  *
  * Host code sees only a host-side stand-in for the array; its device
- * address is looked up with cudaGetSymbolAddress the first time the entry
- * point runs on a device (with that device current) and cached.  That first
- * call per device should be made before any stream capture begins.
+ * address is looked up with cudaGetSymbolAddress (with the device current)
+ * on every call made outside stream capture, so a module reloaded after
+ * cudaDeviceReset is found again, and cached per device for calls made
+ * while the stream is being captured.  A call inside a capture before any
+ * call outside one on that device is rejected with LQ_ERR_ARG: make one
+ * call before capture begins.
+ *
+ * Particles outside the lattice all land in the last cell, whose in-cell
+ * ordering is one thread's insertion sort: keep their number small (the
+ * health word of the native driver counts them).
  */
 #include <mutex>
 
@@ -42,19 +49,29 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 void* g_addr[kMaxDevices] = {};
 
-/* Device address of the scratch array on the current device (looked up
- * once per device). */
-int scratch_address(void** out)
+/* Device address of the scratch array on the current device: asked of
+ * the runtime outside stream capture, the cached answer inside one. */
+int scratch_address(cudaStream_t stream, void** out)
 {
     int dev = 0;
     LQ_TRY_CUDA(cudaGetDevice(&dev), "noalloc search: cudaGetDevice");
     if (dev < 0 || dev >= kMaxDevices) return lqb::set_error(LQ_ERR_ARG, "noalloc search: device %d out of range", dev);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess) {
+        cudaGetLastError();
+        cs = cudaStreamCaptureStatusActive;   /* cannot tell: treat as capturing, ask nothing */
+    }
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_addr[dev]) {
+    if (cs == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_search_scratch);
         if (e != cudaSuccess) return lqb::cuda_status(e, "noalloc search: cudaGetSymbolAddress");
         g_addr[dev] = p;
+    } else if (!g_addr[dev]) {
+        return lqb::set_error(LQ_ERR_ARG,
+                              "lq_grid_neighbor_search_noalloc: first call on device %d made during stream capture; "
+                              "make one call before capture begins",
+                              dev);
     }
     *out = g_addr[dev];
     return LQ_OK;
@@ -84,7 +101,7 @@ extern "C" int lq_grid_neighbor_search_noalloc(const void* par_host, const void*
         return lqb::set_error(LQ_ERR_ARG, "lq_grid_neighbor_search_noalloc: scan needs %zu bytes of scratch, %zu fixed",
                               scan, kScanBytes);
     void* base = nullptr;
-    LQ_TRY(scratch_address(&base));
+    LQ_TRY(scratch_address(static_cast<cudaStream_t>(stream), &base));
     char* b = static_cast<char*>(base);
     lqb::GridBuffers g;
     g.np_cap = np;

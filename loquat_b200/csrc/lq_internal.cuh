@@ -194,13 +194,15 @@ int launch_correct_into(const Parameters* par_host, const Parameters* par_dev, c
                         float skin, cudaStream_t s, const MaterialTable& mt = MaterialTable(),
                         const MaterialTable& vw = MaterialTable());
 
-/* List-driven Shepard filter (material targets and neighbours). */
+/* List-driven Shepard filter (material targets and neighbours); a target
+ * whose list overflowed walks its 27 cells in `c` instead. */
 int launch_shepard_list(const Parameters* par_host, const Parameters* par_dev, const State& st, tensor2d* out_str,
-                        const NeighborList& nl, cudaStream_t s);
+                        const NeighborList& nl, const Cells& c, cudaStream_t s, const Frames& fr = Frames());
 /* Density Shepard filter of material slots into rho_out[npb, np) over the
- * material lists. */
+ * material lists (overflowed lists walk their 27 cells in `c`). */
 int launch_density_filter_list(const Parameters* par_host, const Parameters* par_dev, const State& st,
-                               float* rho_out, const NeighborList& nl, cudaStream_t s);
+                               float* rho_out, const NeighborList& nl, const Cells& c, cudaStream_t s,
+                               const Frames& fr = Frames());
 /* Neighbour lists of targets [first, first + n) from grid layers
  * layer_lo..1 with cut-off radius `cut` (2h plus skin); list overflows are
  * counted in health[HEALTH_NBR_OVERFLOW]. */

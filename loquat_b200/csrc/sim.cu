@@ -286,7 +286,8 @@ int enqueue_dynamic_dt(LqSim* S, cudaStream_t s)
 /* Density Shepard filter (LQ_SIM_DENSITY_FILTER) on the lists. */
 int enqueue_density_filter(LqSim* S, cudaStream_t s)
 {
-    LQ_TRY(lqb::launch_density_filter_list(&S->ph, S->pd, S->S, S->rho_f, S->nlm, s));
+    const lqb::Cells cells{S->g.start, nullptr, nullptr};
+    LQ_TRY(lqb::launch_density_filter_list(&S->ph, S->pd, S->S, S->rho_f, S->nlm, cells, s, S->fr));
     if (S->npm > 0) {
         k_set_density<<<blocks(S->npm), 256, 0, s>>>(S->npb, S->npm, S->rho_f, S->S.vel, S->S.vd);
         LQ_TRY_CUDA(cudaGetLastError(), "k_set_density");
@@ -327,7 +328,8 @@ int enqueue_stages(LqSim* S, cudaStream_t s)
 /* Shepard stress filter (reference src/loquat.cu:400-409) on the lists. */
 int enqueue_shepard(LqSim* S, cudaStream_t s)
 {
-    LQ_TRY(lqb::launch_shepard_list(&S->ph, S->pd, S->S, S->T.str, S->nlm, s));
+    const lqb::Cells cells{S->g.start, nullptr, nullptr};
+    LQ_TRY(lqb::launch_shepard_list(&S->ph, S->pd, S->S, S->T.str, S->nlm, cells, s, S->fr));
     if (S->npm > 0) {
         k_copy_t2<<<blocks(S->npm), 256, 0, s>>>(S->npb, S->npm, S->T.str, S->S.str);
         LQ_TRY_CUDA(cudaGetLastError(), "k_copy_t2");

@@ -827,7 +827,8 @@ __global__ void __launch_bounds__(kBlock) k_adami_packed(const Parameters* __res
 __global__ void __launch_bounds__(kBlock) k_shepard_list(const Parameters* __restrict__ P, int np, int npb, State st,
                                                          tensor2d* __restrict__ out_str,
                                                          const int* __restrict__ list,
-                                                         const int* __restrict__ count, int stride)
+                                                         const int* __restrict__ count, int stride, Cells cells,
+                                                         Frames fr)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = npb + t;
@@ -858,11 +859,11 @@ __global__ void __launch_bounds__(kBlock) k_shepard_list(const Parameters* __res
     if (n <= LQ_NBR_CAP) {
         for (int k = 0; k < n; ++k) add(__ldg(list + (size_t)k * stride + t));
     } else {
-        /* overflowed list: the 27 cells of the material layer (no grid here:
-         * a full scan of material slots in its place is too slow, so the
-         * caller guarantees lists were built without overflow or accepts
-         * the counted overflow in the health word) */
-        for (int k = 0; k < LQ_NBR_CAP; ++k) add(__ldg(list + (size_t)k * stride + t));
+        /* overflowed list (counted in the health word): the particle itself
+         * and its 27-cell walk in the grid the lists were built from, as
+         * the pair kernel does */
+        add(i);
+        walk_stencil(P, load_pair_const(P), st, cells, i, xi, add, fr);
     }
     S.xx /= w;
     S.yy /= w;
@@ -879,18 +880,18 @@ __global__ void __launch_bounds__(kBlock) k_shepard_list(const Parameters* __res
 __global__ void __launch_bounds__(kBlock) k_density_filter_list(const Parameters* __restrict__ P, int np, int npb,
                                                                 State st, float* __restrict__ rho_out,
                                                                 const int* __restrict__ list,
-                                                                const int* __restrict__ count, int stride)
+                                                                const int* __restrict__ count, int stride,
+                                                                Cells cells, Frames fr)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = npb + t;
     if (i >= np) return;
-    const int n = min(__ldg(count + t), LQ_NBR_CAP);
+    const int n = __ldg(count + t);
     const float ih = __ldg(&P->i_h), m = __ldg(&P->m), Cw = __ldg(&P->kernel_normalization_par);
     const float4 xi = __ldg(st.pos + i);
     float num = 0.0f, den = 0.0f;
-    for (int k = 0; k < n; ++k) {
-        const int j = __ldg(list + (size_t)k * stride + t);
-        if (j < npb || !lq_in_range(j, np)) continue;
+    auto add = [&](int j) {
+        if (j < npb || !lq_in_range(j, np)) return;
         const float4 xj = __ldg(st.pos + j);
         const float3 d = make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
         const float q = norm3df(d.x, d.y, d.z) * ih;
@@ -899,6 +900,13 @@ __global__ void __launch_bounds__(kBlock) k_density_filter_list(const Parameters
             num += m * ker;
             den += ker * (m / __ldg(&st.vel[j].w));
         }
+    };
+    if (n <= LQ_NBR_CAP) {
+        for (int k = 0; k < n; ++k) add(__ldg(list + (size_t)k * stride + t));
+    } else {
+        /* overflowed list: the particle itself and its 27-cell walk */
+        add(i);
+        walk_stencil(P, load_pair_const(P), st, cells, i, xi, add, fr);
     }
     rho_out[i] = num / den;
 }
@@ -906,11 +914,11 @@ __global__ void __launch_bounds__(kBlock) k_density_filter_list(const Parameters
 }  // namespace
 
 int launch_density_filter_list(const Parameters* ph, const Parameters* pd, const State& st, float* rho_out,
-                               const NeighborList& nl, cudaStream_t s)
+                               const NeighborList& nl, const Cells& c, cudaStream_t s, const Frames& fr)
 {
     if (ph->npm <= 0) return LQ_OK;
     k_density_filter_list<<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, rho_out, nl.list,
-                                                                        nl.count, nl.stride);
+                                                                        nl.count, nl.stride, c, fr);
     LQ_TRY_CUDA(cudaGetLastError(), "k_density_filter_list");
     return LQ_OK;
 }
@@ -1047,11 +1055,11 @@ int launch_adami_packed(const Parameters* ph, const Parameters* pd, const State&
 }
 
 int launch_shepard_list(const Parameters* ph, const Parameters* pd, const State& st, tensor2d* out_str,
-                        const NeighborList& nl, cudaStream_t s)
+                        const NeighborList& nl, const Cells& c, cudaStream_t s, const Frames& fr)
 {
     if (ph->npm <= 0) return LQ_OK;
     k_shepard_list<<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, out_str, nl.list,
-                                                                 nl.count, nl.stride);
+                                                                 nl.count, nl.stride, c, fr);
     LQ_TRY_CUDA(cudaGetLastError(), "k_shepard_list");
     return LQ_OK;
 }

@@ -6,6 +6,7 @@ checker) and bench.py's CPU-baseline leg; never by the product package.
 from __future__ import annotations
 
 import ctypes
+import os
 import subprocess
 from pathlib import Path
 
@@ -14,7 +15,10 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liblq_oracle.so"
 REF_LIB = HERE / "_ref" / "libref_kernels.so"
-REFERENCE_TREE = Path("/root/reference")
+# Where the reference's sources are read from when its open kernels are
+# compiled into _ref/ (LOQUAT_REFERENCE overrides the default location of
+# the read-only checkout).
+REFERENCE_TREE = Path(os.environ.get("LOQUAT_REFERENCE") or "/root/reference")
 
 _lib = None
 _ref = None
@@ -26,7 +30,7 @@ def build(ref: bool = True) -> None:
     reference-kernel harness)."""
     subprocess.run(["make", "-C", str(HERE), "liblq_oracle.so"], check=True, capture_output=True)
     if ref and (REFERENCE_TREE / "src" / "predictor_corrector.cu").exists():
-        subprocess.run(["make", "-C", str(HERE), "ref"], check=True, capture_output=True)
+        subprocess.run(["make", "-C", str(HERE), "ref", f"REF={REFERENCE_TREE}"], check=True, capture_output=True)
 
 
 def lib():

@@ -1,7 +1,9 @@
 """The reference arm of bench.py on the CPU: `--impl reference` times the
-FP64 oracle on a bounded sample of the workload and prints one JSON line
-with the keys the bench contract asks for; under torchrun only rank 0 runs
-and prints it, the other ranks exit 0 without work."""
+FP64 oracle on the workload itself (all host threads, then one thread) and
+prints one JSON line with the keys the bench contract asks for, with the
+same `config` as the GPU arm; it loads no library of the product.  Under
+torchrun only rank 0 runs and prints it, the other ranks exit 0 without
+work."""
 from __future__ import annotations
 
 import json
@@ -35,6 +37,21 @@ def test_reference_arm_prints_one_contract_line():
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
+    assert d["single_thread"]["cores"] == 1 and d["single_thread"]["value"] > 0
+    # the workload itself, not a sample: the column's 50,000 soil particles
+    assert d["config"]["npm"] == 50000 and set(d["config"]) == {"workload", "np", "npm", "npb", "ncell"}
+
+
+def test_reference_arm_loads_no_product_library():
+    """The CPU arm derives the case's Parameters with the oracle, so the
+    CUDA library of the product is never mapped into its process."""
+    code = ("import sys, bench; rc = bench.main(['--impl', 'reference', '--config', 'column', '--steps', '1', "
+            "'--warmup', '0']); maps = open('/proc/self/maps').read(); "
+            "assert 'liblqb200' not in maps, 'product library loaded'; "
+            "assert 'liblq_oracle' in maps; sys.exit(rc)")
+    e = dict(os.environ, PYTHONPATH=str(ROOT))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=e, cwd=ROOT, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
 
 
 def test_reference_arm_other_ranks_exit_quietly():

@@ -61,6 +61,28 @@ def test_noalloc_search_matches_allocating_search_two_calls_in_a_row(lq, cuda):
             assert np.array_equal(a, b), name
 
 
+def test_noalloc_search_allocates_no_device_memory(lq, cuda):
+    """The entry point's promise: after a first call of each problem (which
+    loads its kernels), further calls of different sizes leave the device's
+    free memory exactly where it was."""
+    probs = []
+    for case, seed in ((cases.column_collapse(), 3), (cases.small_column(seed=5), 4)):
+        par = case.par
+        pos_d, pd = dev(scrambled(case, seed)), par_dev(par)
+        outs = [cuda.empty((n,), dtype=cuda.int32, device="cuda") for n in (par.np, par.np, par.ncell, par.ncell)]
+        probs.append((par, pos_d, pd, outs))
+    for par, pos_d, pd, outs in probs:
+        lq.grid_neighbor_search_noalloc(par, pd, pos_d, *outs)
+    sync()
+    free0, _ = cuda.cuda.mem_get_info()
+    for _ in range(3):
+        for par, pos_d, pd, outs in probs:
+            lq.grid_neighbor_search_noalloc(par, pd, pos_d, *outs)
+    sync()
+    free1, _ = cuda.cuda.mem_get_info()
+    assert free1 == free0, f"free device memory changed by {free0 - free1} bytes"
+
+
 def test_noalloc_search_rejects_sizes_beyond_its_limits(lq, cuda):
     c = cases.small_column()
     par = c.par.copy()
