@@ -93,6 +93,17 @@ int lq_grid_neighbor_search_noalloc(const void* par_host, const void* par_device
                                     int* part_cel, int* part_idx, int* cell_beg, int* cell_end, void* stream);
 
 /* ---- per-stage operators ------------------------------------------------ */
+/* Sizes the working arrays of lq_particle_interaction on the current device
+ * (cell starts, target order, neighbour lists, packed neighbour data) for
+ * the particle and cell counts of par_host.  No counterpart in the
+ * reference, whose ParticleInteraction is closed; it plays the part of the
+ * reference's set-up allocation (src/loquat.cu:142-165) for this
+ * operator: the drop-in LoquatGrid::GridConfig calls it, and a C caller
+ * makes it once before its step loop, after which a call with the same or
+ * smaller counts allocates nothing (a larger one grows the arrays,
+ * synchronising the device first). */
+int lq_interaction_reserve(const void* par_host);
+
 /* reference src/particle_interaction.h:27-40 */
 int lq_particle_interaction(const void* par_host, const void* par_device,
                             const float* pospres, const float* velrhop, const float* idep,

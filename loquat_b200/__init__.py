@@ -53,6 +53,7 @@ _SIGNATURES = {
     "lq_grid_sort_float4": (_I, [_VP, _I, _VP, _VP, _VP]),
     "lq_grid_sort_tensor2d": (_I, [_VP, _I, _VP, _VP, _VP]),
     "lq_grid_neighbor_search_noalloc": (_I, [_VP] * 8),
+    "lq_interaction_reserve": (_I, [_VP]),
     "lq_particle_interaction": (_I, [_VP] * 13),
     "lq_adami_boundary": (_I, [_VP] * 8),
     "lq_stress_regularization": (_I, [_VP] * 9),
@@ -164,6 +165,12 @@ def grid_neighbor_search_noalloc(par_host, par_dev, pospres, part_cel, part_idx,
 
 
 # ------------------------------------------------------------------ operators
+def interaction_reserve(par_host) -> None:
+    """lq_interaction_reserve: sizes particle_interaction's working arrays
+    for par_host's particle and cell counts, once, before a step loop."""
+    check(lib().lq_interaction_reserve(ptr(par_host)), "lq_interaction_reserve")
+
+
 def particle_interaction(par_host, par_dev, pospres, velrhop, idep, str_, stn, accad, spin, acestn,
                          cell_beg, cell_end, stream=None):
     """lq_particle_interaction (reference src/particle_interaction.h:27-40)."""

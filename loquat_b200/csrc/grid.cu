@@ -423,6 +423,9 @@ LoquatGrid::~LoquatGrid()
 void LoquatGrid::GridConfig(Parameters* par_host)
 {
     ResizeArrayLength(par_host->np, par_host->ncell);
+    /* ParticleInteraction's working arrays too, at set-up as the reference
+     * allocates its own, so the step loop allocates nothing */
+    if (lq_interaction_reserve(par_host) != LQ_OK) die("GridConfig");
 }
 
 void LoquatGrid::ResizeArrayLength(int np_new, int ncell_new)

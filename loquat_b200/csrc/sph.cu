@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include <cub/device/device_scan.cuh>
@@ -1660,59 +1661,147 @@ lqb::State state_of(const float* pos, const float* vel, const float* idep, const
 
 namespace {
 
-/* Working arrays of the drop-in interaction: a neighbour list for the
- * material targets and the packed neighbour data.  One set per device,
- * allocated on the first call and grown when a call needs more (the device
- * is synchronised before the old arrays are freed); calls that overlap on
- * the GPU share it and must not. */
+/* Launch shape of the drop-in interaction's pair kernel (lqb::kPairShapes). */
+constexpr int kDropInShape = 11;
+
+/* Working arrays of the drop-in interaction, one set per device: the cell
+ * starts derived from the caller's cell_beg / cell_end, the pair kernel's
+ * target order (tile or twin order) with its scratch, the neighbour lists
+ * and the packed neighbour data.  lq_interaction_reserve sizes them from a
+ * Parameters record (the drop-in LoquatGrid's GridConfig calls it, where
+ * the reference allocates its arrays); a call that needs more than was
+ * reserved grows them itself, synchronising the device before the old
+ * arrays are freed.  Calls that overlap on the GPU share the arrays and
+ * must not. */
 struct DropInWorkspace {
-    int* list = nullptr;
-    int* count = nullptr;
-    float* rec = nullptr;
-    int stride = 0, np = 0;
+    int np = 0, ncell = 0, nseg = 0, npm = 0, twin_cap = 0;
+    int* start = nullptr;           /* ncell + 1 cell starts */
+    int* counts = nullptr;          /* ncell + 1 particles per cell */
+    void* scan_tmp = nullptr;       /* cell-start scan */
+    size_t scan_bytes = 0;
+    lqb::TileOrder to;              /* tile order (tiled shape) or segment scratch (twin shape) */
+    lqb::NeighborList nl;           /* thread-per-target lists (tiled shape) */
+    lqb::TwinLists tw;              /* union lists (twin shape) */
+    float* rec = nullptr;           /* packed neighbour data, 13 floats per particle */
+    std::vector<void*> allocs;
 };
 std::mutex g_ws_mutex;
 std::vector<DropInWorkspace> g_ws;
 
-int dropin_workspace(int np, int npm, DropInWorkspace** out)
+void free_workspace(DropInWorkspace& w)
+{
+    for (void* p : w.allocs) cudaFree(p);
+    w = DropInWorkspace{};
+}
+
+int ws_alloc(DropInWorkspace& w, void** p, size_t bytes)
+{
+    cudaError_t e = cudaMalloc(p, bytes > 0 ? bytes : 16);
+    if (e != cudaSuccess)
+        return lqb::set_error(LQ_ERR_ALLOC, "interaction workspace: cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    w.allocs.push_back(*p);
+    return LQ_OK;
+}
+
+/* Sizes every array for the Parameters' particle and cell counts. */
+int size_workspace(DropInWorkspace& w, const Parameters* ph)
+{
+    const int np = ph->np > 1 ? ph->np : 1, ncell = ph->ncell, npm = ph->npm > 1 ? ph->npm : 1;
+    int nseg = 0;
+    size_t seg_scan = 0, cell_scan = 0;
+    LQ_TRY(lqb::tile_order_scratch(ph, &nseg, &seg_scan));
+    LQ_TRY(lqb::scan_scratch_bytes(ncell, &cell_scan));
+    const int cap = lqb::twin_shape(kDropInShape) ? lqb::twin_capacity(ph, kDropInShape) : 0;
+    if (np <= w.np && ncell <= w.ncell && nseg <= w.nseg && npm <= w.npm && cap <= w.twin_cap && w.rec) return LQ_OK;
+    if (!w.allocs.empty()) LQ_TRY_CUDA(cudaDeviceSynchronize(), "interaction workspace");
+    free_workspace(w);
+    DropInWorkspace n;
+    int st = LQ_OK;
+    auto A = [&](void** p, size_t bytes) {
+        if (st == LQ_OK) st = ws_alloc(n, p, bytes);
+    };
+    A((void**)&n.start, sizeof(int) * ((size_t)ncell + 1));
+    A((void**)&n.counts, sizeof(int) * ((size_t)ncell + 1));
+    A(&n.scan_tmp, cell_scan);
+    n.scan_bytes = cell_scan;
+    A((void**)&n.to.seg, sizeof(int) * 4 * (size_t)nseg);
+    A(&n.to.scan_tmp, seg_scan);
+    n.to.nseg_cap = nseg;
+    n.to.scan_bytes = seg_scan;
+    A((void**)&n.rec, sizeof(float) * 13 * (size_t)np);
+    if (lqb::twin_shape(kDropInShape)) {
+        n.tw.cap = cap;
+        n.tw.stride = (cap + 31) / 32 * 32;
+        A((void**)&n.tw.twin, sizeof(int) * (size_t)(cap > 0 ? cap : 1));
+        A((void**)&n.tw.list, sizeof(int) * (size_t)LQ_TWIN_CAP * n.tw.stride);
+        A((void**)&n.tw.count, sizeof(int) * (size_t)n.tw.stride);
+        A((void**)&n.tw.hits, sizeof(int) * (size_t)n.tw.stride);
+    } else {
+        n.nl.stride = (npm + 31) / 32 * 32;
+        A((void**)&n.nl.list, sizeof(int) * (size_t)LQ_NBR_CAP * n.nl.stride);
+        A((void**)&n.nl.count, sizeof(int) * (size_t)n.nl.stride);
+        A((void**)&n.to.order, sizeof(int) * (size_t)npm);
+    }
+    if (st != LQ_OK) {
+        free_workspace(n);
+        return st;
+    }
+    n.np = np;
+    n.ncell = ncell;
+    n.nseg = nseg;
+    n.npm = npm;
+    n.twin_cap = cap;
+    w = std::move(n);
+    return LQ_OK;
+}
+
+int dropin_workspace(const Parameters* ph, DropInWorkspace** out)
 {
     int dev = 0;
     LQ_TRY_CUDA(cudaGetDevice(&dev), "interaction workspace");
     std::lock_guard<std::mutex> lock(g_ws_mutex);
     if ((int)g_ws.size() <= dev) g_ws.resize((size_t)dev + 1);
     DropInWorkspace& w = g_ws[(size_t)dev];
-    const int stride = (npm + 31) / 32 * 32;
-    if (stride > w.stride || np > w.np) {
-        if (w.list || w.count || w.rec) LQ_TRY_CUDA(cudaDeviceSynchronize(), "interaction workspace");
-        cudaFree(w.list);
-        cudaFree(w.count);
-        cudaFree(w.rec);
-        w = DropInWorkspace{};
-        const int st = stride > 32 ? stride : 32;
-        cudaError_t e = cudaMalloc((void**)&w.list, sizeof(int) * (size_t)LQ_NBR_CAP * st);
-        if (e == cudaSuccess) e = cudaMalloc((void**)&w.count, sizeof(int) * (size_t)st);
-        if (e == cudaSuccess) e = cudaMalloc((void**)&w.rec, sizeof(float) * 13 * (size_t)(np > 1 ? np : 1));
-        if (e != cudaSuccess) {
-            cudaFree(w.list);
-            cudaFree(w.count);
-            cudaFree(w.rec);
-            w = DropInWorkspace{};
-            return lqb::set_error(LQ_ERR_ALLOC, "interaction workspace: %s", cudaGetErrorString(e));
-        }
-        w.stride = st;
-        w.np = np;
-    }
+    LQ_TRY(size_workspace(w, ph));
     *out = &w;
     return LQ_OK;
 }
 
+/* Particles per cell from the reference's per-cell bounds (-1: empty). */
+__global__ void __launch_bounds__(256) k_cell_counts(int ncell, const int* __restrict__ beg,
+                                                     const int* __restrict__ end, int* __restrict__ counts)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c > ncell) return;
+    int n = 0;
+    if (c < ncell) {
+        const int b = __ldg(beg + c);
+        n = b == -1 ? 0 : __ldg(end + c) - b;
+    }
+    counts[c] = n;
+}
+
 }  // namespace
 
-/* The reference's ParticleInteraction (src/particle_interaction.h:27-40):
- * the pairs of each material target are found once per call in the
- * caller's grid (cell_beg / cell_end, the 27-cell walk in the reference's
- * visiting order) into a list, and summed by the list pair kernel over the
- * packed neighbour data. */
+extern "C" int lq_interaction_reserve(const void* par_host)
+{
+    if (!par_host) return lqb::set_error(LQ_ERR_ARG, "lq_interaction_reserve: null Parameters");
+    const Parameters* ph = static_cast<const Parameters*>(par_host);
+    if (ph->np < 0 || ph->npm < 0 || ph->ncell < 1)
+        return lqb::set_error(LQ_ERR_ARG, "lq_interaction_reserve: bad sizes np=%d npm=%d ncell=%d", ph->np, ph->npm,
+                              ph->ncell);
+    DropInWorkspace* w = nullptr;
+    return dropin_workspace(ph, &w);
+}
+
+/* The reference's ParticleInteraction (src/particle_interaction.h:27-40).
+ * The caller's grid (cell_beg / cell_end: every particle sorted into its
+ * cell, cells in key order) gives the cell starts; the material targets
+ * are ordered into compact tiles (twins of two consecutive targets for a
+ * twin shape), their neighbours within 2h are found by the 27-cell walk in
+ * the reference's visiting order into lists, and the pair kernel sums over
+ * the lists from the packed neighbour data, in plain FP32 as the
+ * reference computes. */
 extern "C" int lq_particle_interaction(const void* par_host, const void* par_device, const float* pospres,
                                        const float* velrhop, const float* idep, const float* str, const float* stn,
                                        float* accad, float* spin, float* acestn, const int* cell_beg,
@@ -1723,20 +1812,32 @@ extern "C" int lq_particle_interaction(const void* par_host, const void* par_dev
     if (ph->npm > 0 && (!pospres || !velrhop || !str || !accad || !spin || !acestn || !cell_beg || !cell_end))
         return lqb::set_error(LQ_ERR_ARG, "lq_particle_interaction: null array");
     if (ph->npm <= 0) return LQ_OK;
-    lqb::Cells c{nullptr, cell_beg, cell_end};
     lqb::Rates r{(float4*)accad, (float4*)spin, (tensor2d*)acestn};
     const Parameters* pd = static_cast<const Parameters*>(par_device);
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
     const lqb::State st = state_of(pospres, velrhop, idep, str, stn);
     DropInWorkspace* w = nullptr;
-    LQ_TRY(dropin_workspace(ph->np, ph->npm, &w));
-    const lqb::NeighborList nl{w->list, w->count, w->stride};
+    LQ_TRY(dropin_workspace(ph, &w));
+    const int ncell = ph->ncell;
+    k_cell_counts<<<(ncell + 256) / 256, 256, 0, s>>>(ncell, cell_beg, cell_end, w->counts);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_cell_counts");
+    size_t bytes = w->scan_bytes;
+    LQ_TRY_CUDA(cub::DeviceScan::ExclusiveSum(w->scan_tmp, bytes, w->counts, w->start, ncell + 1, s),
+                "cell start scan");
+    const lqb::Cells c{w->start, nullptr, nullptr};
     /* the pair body's own cut-off test: q < 2 with the candidate slack of
      * the cell walk */
     const float cut = 2.0f * ph->h * sqrtf(1.0001f);
-    LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, ph->npb, ph->npm, 0, cut, st.pos, c, nl, nullptr, s, nullptr,
-                                           lqb::Frames()));
-    return lqb::launch_interaction_list(ph, pd, st, r, c, nl, s, lqb::Frames(), false, w->rec, 0, true);
+    if (lqb::twin_shape(kDropInShape)) {
+        LQ_TRY(lqb::launch_twin_order(ph, w->start, kDropInShape, w->to, w->tw, s));
+        LQ_TRY(lqb::launch_neighbor_list_twin(ph, pd, cut, st.pos, c, w->tw, nullptr, s));
+        LQ_TRY(lqb::launch_pack_neighbors(ph, st, w->rec, 0, s));
+        return lqb::launch_interaction_twin(ph, pd, st, r, c, w->tw, s, lqb::Frames(), false, w->rec, kDropInShape);
+    }
+    LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, ph->npb, ph->npm, 0, cut, st.pos, c, w->nl, nullptr, s));
+    LQ_TRY(lqb::launch_tile_order(ph, w->start, kDropInShape, w->to, s));
+    return lqb::launch_interaction_list(ph, pd, st, r, c, w->nl, s, lqb::Frames(), false, w->rec, kDropInShape, true,
+                                        w->to.order);
 }
 
 extern "C" int lq_adami_boundary(const void* par_host, const void* par_device, const float* pospres,

@@ -19,7 +19,7 @@ import ctypes
 
 import numpy as np
 
-from . import (Grid, Parameters, adami_boundary, corrector, particle_interaction, predictor,
+from . import (Grid, Parameters, adami_boundary, corrector, interaction_reserve, particle_interaction, predictor,
                stress_regularization)
 
 
@@ -48,6 +48,7 @@ class ReferenceStep:
         self.f4_cache, self.t2_cache = f4(), t2()
         self.par_dev = torch.empty(ctypes.sizeof(Parameters), dtype=torch.uint8, device=dev)
         self.grid = Grid(n, par.ncell)
+        interaction_reserve(self.par)    # set-up allocation, as LoquatGrid::GridConfig makes it
         self.step_count = 0
         self.time = 0.0
 
