@@ -47,6 +47,7 @@ def lib():
         L.or_sim_steps_done.restype = _LL
         L.or_sim_steps_done.argtypes = [_VP]
         L.or_set_threads.argtypes = [_I]
+        L.or_set_gather_rounding.argtypes = [_I]
         L.or_initialize_parameters.argtypes = [_VP]
         L.or_grid_float.argtypes = [_VP, _I, _I] + [_VP] * 6
         L.or_interaction.argtypes = [_VP, _I, _I] + [_VP] * 8
@@ -93,6 +94,17 @@ def _p(a):
 
 def set_threads(n: int = 0) -> int:
     return lib().or_set_threads(n)
+
+
+GATHER_F16_VELOCITY, GATHER_F16_STRESS, GATHER_BF16_VELOCITY, GATHER_BF16_STRESS = 1, 2, 4, 8
+
+
+def set_gather_rounding(mode: int = 0) -> None:
+    """Precision experiment: the interaction rounds a neighbour's gathered
+    velocity and/or sigma/rho^2 to FP16 or BF16 (bit mask of the GATHER_*
+    constants), as a GPU form with 16-bit packed gathers would; 0 restores
+    exact gathers.  Applies to every later interaction of this process."""
+    lib().or_set_gather_rounding(int(mode))
 
 
 def initialize_parameters(par) -> None:

@@ -231,6 +231,21 @@ void adami(const OrParams& P, int np, int npb, const double* pos, const double* 
  * accad = (a + gravity, drho); acestn = sym L; spin = (W_yx, W_zx, W_zy, 0),
  * W = (L - L^T)/2, the convention the Jaumann code needs
  * (reference src/predictor_corrector.cu:40-45). */
+/* Precision experiment (test infrastructure): rounding applied to a
+ * neighbour's velocity and sigma/rho^2 as the interaction gathers them,
+ * as a GPU form that packed those gathers into 16-bit floats would see
+ * them; the target's own values stay exact.  Bit 0: velocity to FP16,
+ * bit 1: sigma/rho^2 to FP16, bit 2: velocity to BF16, bit 3: sigma/rho^2
+ * to BF16 (round to nearest even).  0 (the default) rounds nothing. */
+int g_gather_rounding = 0;
+
+inline double gather_round(double x, int f16_bit, int bf16_bit)
+{
+    if (g_gather_rounding & f16_bit) return (double)(_Float16)x;
+    if (g_gather_rounding & bf16_bit) return (double)(float)(__bf16)(float)x;
+    return x;
+}
+
 void interaction(const OrParams& P, int np, int npb, const double* pos, const double* vel, const double* str,
                  double* accad, double* spin, double* acestn, const int* beg, const int* end, bool float_cells)
 {
@@ -266,13 +281,14 @@ void interaction(const OrParams& P, int np, int npb, const double* pos, const do
             double t = 2.0 - q;
             double fac = Cg * t * t * t;
             double g[3] = {fac * d[0], fac * d[1], fac * d[2]};
-            double vij[3] = {vi[0] - vj[0], vi[1] - vj[1], vi[2] - vj[2]};
+            double vij[3] = {vi[0] - gather_round(vj[0], 1, 4), vi[1] - gather_round(vj[1], 1, 4),
+                             vi[2] - gather_round(vj[2], 1, 4)};
             drho += vij[0] * g[0] + vij[1] * g[1] + vij[2] * g[2];
             double rhoj = vj[3];
             double rj2 = 1.0 / (rhoj * rhoj);
             /* symmetric stress term; full 3x3 from the 6 components */
             double T[6];
-            for (int k = 0; k < 6; ++k) T[k] = si[k] * ri2 + sj[k] * rj2;
+            for (int k = 0; k < 6; ++k) T[k] = si[k] * ri2 + gather_round(sj[k] * rj2, 2, 8);
             a[0] += m * (T[0] * g[0] + T[3] * g[1] + T[4] * g[2]);
             a[1] += m * (T[3] * g[0] + T[1] * g[1] + T[5] * g[2]);
             a[2] += m * (T[4] * g[0] + T[5] * g[1] + T[2] * g[2]);
@@ -813,6 +829,8 @@ struct OrSim {
 extern "C" {
 
 int or_parameters_size(void) { return (int)sizeof(OrParams); }
+
+void or_set_gather_rounding(int mode) { g_gather_rounding = mode; }
 
 int or_set_threads(int n)
 {

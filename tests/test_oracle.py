@@ -281,3 +281,26 @@ def test_oracle_extensions_density_filter_and_dynamic_step(orc):
     p.step(2)
     after = p.get()[1][nb:, 3]
     assert np.std(after) < 0.6 * np.std(noisy[nb:, 3])
+
+
+def test_gather_rounding_experiment_switch(orc):
+    """The oracle's precision experiment rounds only the neighbours'
+    gathered velocity / sigma over rho^2: the rates move by about the
+    16-bit rounding, and switching it off restores the exact rates."""
+    p, pos, vel, interior = lattice_block()
+    rng = np.random.default_rng(7)
+    vel[:, :3] = rng.normal(0.0, 0.3, size=(pos.shape[0], 3))
+    s = np.tile(np.array([-3.0e4, -2.0e4, -5.0e4, 1.0e3, -2.0e3, 4.0e3]), (pos.shape[0], 1))
+    s *= 1.0 + 0.1 * rng.random((pos.shape[0], 1))
+    exact = run_interaction(orc, p, pos, vel, s)
+    try:
+        for mode, field in ((orc.GATHER_F16_VELOCITY, 2), (orc.GATHER_BF16_STRESS, 0)):
+            orc.set_gather_rounding(mode)
+            got = run_interaction(orc, p, pos, vel, s)
+            d = np.linalg.norm(got[field][interior] - exact[field][interior]) / np.linalg.norm(exact[field][interior])
+            assert 1e-6 < d < 5e-2, (mode, d)
+    finally:
+        orc.set_gather_rounding(0)
+    again = run_interaction(orc, p, pos, vel, s)
+    for a, b in zip(again, exact):
+        assert np.array_equal(a, b)
