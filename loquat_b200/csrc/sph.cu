@@ -376,9 +376,16 @@ constexpr int kUnroll = 8;
  * skin.  Lanes are grouped by grid column; each group
  * walks the union of its lanes' stencils, so the loop and every candidate
  * load are warp-uniform and each lane only runs its distance test.  A lane's
- * own slot passes the test too: its pair adds exactly zero.  Candidates
- * outside a lane's own three z-cells are farther than 2h from it.  Hits are
- * staged per lane in shared memory and flushed as coalesced rows. */
+ * own slot passes the test too: its pair adds exactly zero.  Along z the
+ * walk covers every cell the lane's cut-off sphere reaches (two cells down
+ * or up when the particle lies within the skin of a cell face), so a list
+ * holds all its particle's pairs within the cut-off in those columns,
+ * whatever the group; across columns it covers the 3 x 3 around the
+ * particle's own, which holds every pair within 2h (a pair reaching 2h + skin
+ * only across two columns is left out: it is beyond 2h when the list is
+ * built and can come within 2h - skin only by q > 2 - skin/h, where the
+ * kernel factor (2 - q)^3 is below (skin/h)^3).  Hits are staged per lane in
+ * shared memory and flushed as coalesced rows. */
 __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __restrict__ P, int first, int ntarget,
                                                           int layer_lo, float cut2, const float4* __restrict__ pos,
                                                           Cells cells, int* __restrict__ list,
@@ -416,11 +423,16 @@ __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __re
         }
     };
 
-    int cx = 0, cy = 0, cz = 0;
+    /* the z cells the particle's cut-off sphere reaches (a run walks the
+     * group's union of them), so a lane's list never depends on which
+     * other lanes share its group */
+    const float cut = sqrtf(cut2);
+    int cx = 0, cy = 0, czl = 0, czh = 0;
     if (active) {
         cx = stencil_axis(xi.x, K.ih);
         cy = stencil_axis(xi.y, K.ih);
-        cz = stencil_axis(xi.z, K.ih);
+        czl = stencil_axis(xi.z - cut, K.ih);
+        czh = stencil_axis(xi.z + cut, K.ih);
         if (fr.rows) cy = frame_stencil_row(fr, __ldg(&idep[i].x), cy);
     }
     unsigned todo = __ballot_sync(FULL, active);
@@ -429,9 +441,9 @@ __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __re
         const int gx = __shfl_sync(FULL, cx, leader), gy = __shfl_sync(FULL, cy, leader);
         const bool mine = active && cx == gx && cy == gy;
         todo &= ~__ballot_sync(FULL, mine);
-        const int zmin = __reduce_min_sync(FULL, mine ? cz : INT_MAX);
-        const int zmax = __reduce_max_sync(FULL, mine ? cz : INT_MIN);
-        const int zlo = max(zmin - 1, 0), zhi = min(zmax + 1, nz - 1);
+        const int zmin = __reduce_min_sync(FULL, mine ? czl : INT_MAX);
+        const int zmax = __reduce_max_sync(FULL, mine ? czh : INT_MIN);
+        const int zlo = max(zmin, 0), zhi = min(zmax, nz - 1);
         if (zlo > zhi) continue;
         for (int layer = layer_lo; layer < 2; ++layer) {
             const int off = layer ? L : 0;
@@ -761,13 +773,15 @@ __global__ void __launch_bounds__(kBlock) k_neighbor_list_twin(const Parameters*
         hB += hb;
     };
 
-    int cx = 0, cy = 0, czA = 0, czB = 0;
+    /* the z cells both cut-off spheres reach, as in k_neighbor_list */
+    const float cut = sqrtf(cut2);
+    int cx = 0, cy = 0, czl = 0, czh = 0;
     bool split = false;
     if (active) {
         cx = stencil_axis(xA.x, K.ih);
         cy = stencil_axis(xA.y, K.ih);
-        czA = stencil_axis(xA.z, K.ih);
-        czB = stencil_axis(xB.z, K.ih);
+        czl = min(stencil_axis(xA.z - cut, K.ih), stencil_axis(xB.z - cut, K.ih));
+        czh = max(stencil_axis(xA.z + cut, K.ih), stencil_axis(xB.z + cut, K.ih));
         int cyB = stencil_axis(xB.y, K.ih);
         if (fr.rows) {
             cy = frame_stencil_row(fr, __ldg(&idep[iA].x), cy);
@@ -782,9 +796,9 @@ __global__ void __launch_bounds__(kBlock) k_neighbor_list_twin(const Parameters*
         const int gx = __shfl_sync(FULL, cx, leader), gy = __shfl_sync(FULL, cy, leader);
         const bool mine = active && cx == gx && cy == gy;
         todo &= ~__ballot_sync(FULL, mine);
-        const int zmin = __reduce_min_sync(FULL, mine ? min(czA, czB) : INT_MAX);
-        const int zmax = __reduce_max_sync(FULL, mine ? max(czA, czB) : INT_MIN);
-        const int zlo = max(zmin - 1, 0), zhi = min(zmax + 1, nz - 1);
+        const int zmin = __reduce_min_sync(FULL, mine ? czl : INT_MAX);
+        const int zmax = __reduce_max_sync(FULL, mine ? czh : INT_MIN);
+        const int zlo = max(zmin, 0), zhi = min(zmax, nz - 1);
         if (zlo > zhi) continue;
         for (int layer = 0; layer < 2; ++layer) {
             const int off = layer ? L : 0;
@@ -1662,7 +1676,7 @@ lqb::State state_of(const float* pos, const float* vel, const float* idep, const
 namespace {
 
 /* Launch shape of the drop-in interaction's pair kernel (lqb::kPairShapes). */
-constexpr int kDropInShape = 11;
+constexpr int kDropInShape = 9;
 
 /* Working arrays of the drop-in interaction, one set per device: the cell
  * starts derived from the caller's cell_beg / cell_end, the pair kernel's
