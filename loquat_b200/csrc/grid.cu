@@ -155,9 +155,9 @@ __global__ void __launch_bounds__(kBlock) k_gather_state(int n, const int* __res
     out.idep[i] = __ldg(in.idep + j);
     store_t2(out.str, i, load_t2(in.str, j));
     store_t2(out.stn, i, load_t2(in.stn, j));
-    if (in.xd) {
-        out.xd[i] = in.xd[j];
-        out.vd[i] = in.vd[j];
+    if (in.xlo) {
+        out.xlo[i] = in.xlo[j];
+        out.vlo[i] = in.vlo[j];
     }
 }
 

@@ -31,6 +31,28 @@ constexpr int kBlock = 128;
 
 inline int blocks_for(long long n, int b) { return (int)((n + b - 1) / b); }
 
+/* FP64 position (pressure p in the float word's w) and velocity into the
+ * float high words x, v and the low words of `out` at slot i. */
+__device__ __forceinline__ void split_words(const State& out, int i, const double4& xd, const double4& vd, float p,
+                                            float4& x, float4& v)
+{
+    float4 xl, vl;
+    split4(make_double4(xd.x, xd.y, xd.z, 0.0), x, xl);
+    split4(vd, v, vl);
+    x.w = p;
+    out.xlo[i] = xl;
+    out.vlo[i] = vl;
+}
+
+/* The same, storing the high words too. */
+__device__ __forceinline__ void store_split(const State& out, int i, const double4& xd, const double4& vd, float p)
+{
+    float4 x, v;
+    split_words(out, i, xd, vd, p, x, v);
+    out.pos[i] = x;
+    out.vel[i] = v;
+}
+
 /* Half step of the material slots (reference src/predictor_corrector.cu:169-218):
  * v += dt/2 a; rho += dt/2 drho; x += dt/2 v_new; eps += dt/2 deps;
  * stress and plastic strain from the model at dt/2. */
@@ -61,8 +83,8 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_predict(
             store_t2(out.str, i, s0);
             store_t2(out.stn, i, e0);
             if (kMixed) {
-                out.xd[i] = in.xd[i];
-                out.vd[i] = in.vd[i];
+                out.xlo[i] = in.xlo[i];
+                out.vlo[i] = in.vlo[i];
             }
         }
         return;
@@ -76,7 +98,7 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_predict(
     if (kMixed) {
         /* FP64 accumulation of velocity, density and position; FP64 stress update */
         const double hdt = 0.5 * (double)dt;
-        double4 vd = in.vd[i], xd = in.xd[i];
+        double4 vd = join4(v0, in.vlo[i]), xd = join4(x0, in.xlo[i]);
         vd.x += hdt * a.x; vd.y += hdt * a.y; vd.z += hdt * a.z; vd.w += hdt * a.w;
         xd.x += hdt * vd.x; xd.y += hdt * vd.y; xd.z += hdt * vd.z;
         T6d e = widen6(e0), dd = widen6(de);
@@ -87,10 +109,7 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_predict(
         if (kVW) {
             /* the kinematics are stored before the sub-stepping, whose FP64
              * registers then need not share the SM with them */
-            out.xd[i] = xd;
-            out.vd[i] = vd;
-            out.pos[i] = make_float4((float)xd.x, (float)xd.y, (float)xd.z, x0.w);
-            out.vel[i] = make_float4((float)vd.x, (float)vd.y, (float)vd.z, (float)vd.w);
+            store_split(out, i, xd, vd, x0.w);
             store_t2(out.stn, i, narrow6(e));
             const float epf = (float)sqrt(2.0 / 3.0 * contract6(e, e));
             vw_update_d(vw_const(vw, id.x), hdt, de, w, sd, ev);
@@ -104,10 +123,7 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_predict(
             hypo_update_d(M, hdt, dd, w, sd);
             ep = sqrt(2.0 / 3.0 * contract6(e, e));
         }
-        out.xd[i] = xd;
-        out.vd[i] = vd;
-        out.pos[i] = make_float4((float)xd.x, (float)xd.y, (float)xd.z, (float)p);
-        out.vel[i] = make_float4((float)vd.x, (float)vd.y, (float)vd.z, (float)vd.w);
+        store_split(out, i, xd, vd, (float)p);
         out.idep[i] = make_float4(id.x, (float)ep, (float)ev, id.w);
         store_t2(out.str, i, narrow6(sd));
         store_t2(out.stn, i, narrow6(e));
@@ -187,8 +203,8 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(
         store_t2(out.str, i, load_t2_rw(cur.str, i));
         store_t2(out.stn, i, load_t2_rw(cur.stn, i));
         if (kMixed) {
-            out.xd[i] = cur.xd[i];
-            out.vd[i] = cur.vd[i];
+            out.xlo[i] = cur.xlo[i];
+            out.vlo[i] = cur.vlo[i];
         }
         return;
     }
@@ -216,7 +232,7 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(
         float ep;
         if (kMixed) {
             const double ddt = dt;
-            const double4 v0d = ini.vd[k], x0d = ini.xd[k];
+            const double4 v0d = join4(v0, ini.vlo[k]), x0d = join4(x0, ini.xlo[k]);
             double4 vd, xd;
             vd.x = v0d.x + ddt * a.x; vd.y = v0d.y + ddt * a.y; vd.z = v0d.z + ddt * a.z; vd.w = v0d.w + ddt * a.w;
             xd.x = 0.5 * (vd.x + v0d.x) * ddt + x0d.x;
@@ -227,10 +243,7 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(
             const T6d dd = widen6(de);
             ed.xx += dd.xx * ddt; ed.yy += dd.yy * ddt; ed.zz += dd.zz * ddt;
             ed.xy += dd.xy * ddt; ed.xz += dd.xz * ddt; ed.yz += dd.yz * ddt;
-            out.xd[i] = xd;
-            out.vd[i] = vd;
-            v = make_float4((float)vd.x, (float)vd.y, (float)vd.z, (float)vd.w);
-            x = make_float4((float)xd.x, (float)xd.y, (float)xd.z, xc.w);
+            split_words(out, i, xd, vd, xc.w, x, v);
             e = narrow6(ed);
             ep = (float)sqrt(2.0 / 3.0 * contract6(ed, ed));
         } else {
@@ -276,7 +289,7 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(
     float ep, ev = id.z;
     if (kMixed) {
         const double ddt = dt;
-        const double4 v0d = ini.vd[k], x0d = ini.xd[k];
+        const double4 v0d = join4(v0, ini.vlo[k]), x0d = join4(x0, ini.xlo[k]);
         double4 vd, xd;
         vd.x = v0d.x + ddt * a.x; vd.y = v0d.y + ddt * a.y; vd.z = v0d.z + ddt * a.z; vd.w = v0d.w + ddt * a.w;
         xd.x = 0.5 * (vd.x + v0d.x) * ddt + x0d.x;
@@ -294,10 +307,7 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(
             hypo_update_d(M, ddt, dd, w, sd);
             epd = sqrt(2.0 / 3.0 * contract6(ed, ed));
         }
-        out.xd[i] = xd;
-        out.vd[i] = vd;
-        v = make_float4((float)vd.x, (float)vd.y, (float)vd.z, (float)vd.w);
-        x = make_float4((float)xd.x, (float)xd.y, (float)xd.z, (float)pd);
+        split_words(out, i, xd, vd, (float)pd, x, v);
         s = narrow6(sd);
         e = narrow6(ed);
         ep = (float)epd;
@@ -360,7 +370,7 @@ int launch_predict(const Parameters* ph, const Parameters* pd, const State& in, 
      * more registers than the other models' kernels */
     const bool vwm = ph->constitutive_model == 3;
     const int nb = blocks_for(ph->np, kBlock);
-    if (in.xd && out.xd) {
+    if (in.xlo && out.xlo) {
         if (vwm) k_predict<true, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw);
         else k_predict<true, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw);
     } else {
@@ -395,7 +405,7 @@ int launch_correct_into(const Parameters* ph, const Parameters* pd, const State&
     const VerletCheck vc{xbuild, rebuild, 0.5f * skin, ph->dt};
     const bool vwm = ph->constitutive_model == 3;
     const int nb = blocks_for(ph->np, kBlock);
-    if (cur.xd && ini.xd && out.xd) {
+    if (cur.xlo && ini.xlo && out.xlo) {
         if (vwm) k_correct<true, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw);
         else k_correct<true, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw);
     } else {

@@ -258,6 +258,21 @@ struct T6d {
     double xx, yy, zz, xy, xz, yz;
 };
 
+/* A double from float high and low words, and back: hi is the value
+ * rounded to float, lo the float rounding of what hi leaves out. */
+__device__ __forceinline__ double4 join4(const float4& hi, const float4& lo)
+{
+    return make_double4((double)hi.x + (double)lo.x, (double)hi.y + (double)lo.y, (double)hi.z + (double)lo.z,
+                        (double)hi.w + (double)lo.w);
+}
+
+__device__ __forceinline__ void split4(const double4& d, float4& hi, float4& lo)
+{
+    hi = make_float4((float)d.x, (float)d.y, (float)d.z, (float)d.w);
+    lo = make_float4((float)(d.x - (double)hi.x), (float)(d.y - (double)hi.y), (float)(d.z - (double)hi.z),
+                     (float)(d.w - (double)hi.w));
+}
+
 __device__ __forceinline__ T6d widen6(const tensor2d& t) { return T6d{t.xx, t.yy, t.zz, t.xy, t.xz, t.yz}; }
 
 __device__ __forceinline__ tensor2d narrow6(const T6d& t)

@@ -37,11 +37,14 @@ struct State {
     float4* idep;    /* object id, plastic strain, -, -   */
     tensor2d* str;   /* Cauchy stress, tension positive   */
     tensor2d* stn;   /* total strain                      */
-    /* mixed-precision form only: FP64 copies that the integrator
-     * accumulates in (x, y, z, -) and (vx, vy, vz, density); the float
-     * fields above are their rounded copies read by the neighbour kernels */
-    double4* xd = nullptr;
-    double4* vd = nullptr;
+    /* mixed-precision form only: the low words of the position (x, y, z, 0)
+     * and of the velocity and density (vx, vy, vz, density).  With the
+     * float high words above (the reference's pospres / velrhop, which the
+     * neighbour kernels read) they carry the FP64 values the integrator
+     * accumulates in, hi + lo to about 48 bits, in half the bytes of FP64
+     * copies. */
+    float4* xlo = nullptr;
+    float4* vlo = nullptr;
 };
 
 /* Per-stage rates written by the interaction pass (reference src/loquat.h:74-77). */

@@ -138,8 +138,8 @@ int alloc_state(LqSim* S, State& st)
     LQ_TRY(dev_alloc(S, (void**)&st.str, n * sizeof(tensor2d)));
     LQ_TRY(dev_alloc(S, (void**)&st.stn, n * sizeof(tensor2d)));
     if (S->flags & LQ_SIM_MIXED) {
-        LQ_TRY(dev_alloc(S, (void**)&st.xd, n * sizeof(double4)));
-        LQ_TRY(dev_alloc(S, (void**)&st.vd, n * sizeof(double4)));
+        LQ_TRY(dev_alloc(S, (void**)&st.xlo, n * sizeof(float4)));
+        LQ_TRY(dev_alloc(S, (void**)&st.vlo, n * sizeof(float4)));
     }
     return LQ_OK;
 }
@@ -180,20 +180,19 @@ __global__ void k_copy_state(int n, State in, State out, float4* __restrict__ xb
     b[0] = a[0];
     b[1] = a[1];
     b[2] = a[2];
-    if (in.xd) {
-        out.xd[i] = in.xd[i];
-        out.vd[i] = in.vd[i];
+    if (in.xlo) {
+        out.xlo[i] = in.xlo[i];
+        out.vlo[i] = in.vlo[i];
     }
 }
 
-/* Widens the float state into the FP64 copies (mixed form, after upload). */
+/* Low words of an uploaded float state: zero (mixed form). */
 __global__ void k_widen(int n, State st)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float4 x = st.pos[i], v = st.vel[i];
-    st.xd[i] = make_double4(x.x, x.y, x.z, 0.0);
-    st.vd[i] = make_double4(v.x, v.y, v.z, v.w);
+    st.xlo[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    st.vlo[i] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
 __global__ void k_copy_t2(int first, int n, const tensor2d* __restrict__ in, tensor2d* __restrict__ out)
@@ -220,16 +219,16 @@ __global__ void k_decide(cudaGraphConditionalHandle h, int* flag, int* count)
 
 inline int blocks(int n) { return (n + 255) / 256; }
 
-/* Density filter result into the state (and the FP64 copy of the mixed form). */
+/* Density filter result into the state (its low word zero in the mixed form). */
 __global__ void k_set_density(int npb, int npm, const float* __restrict__ rho, float4* __restrict__ vel,
-                              double4* __restrict__ vd)
+                              float4* __restrict__ vlo)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= npm) return;
     const int i = npb + t;
     const float r = rho[i];
     vel[i].w = r;
-    if (vd) vd[i].w = (double)r;
+    if (vlo) vlo[i].w = 0.0f;
 }
 
 /* Largest |v|^2 and |a|^2 over the material particles: non-negative floats
@@ -340,7 +339,7 @@ int enqueue_density_filter(LqSim* S, cudaStream_t s)
     else
         LQ_TRY(lqb::launch_density_filter_list(&S->ph, S->pd, S->S, S->rho_f, S->nlm, cells, s, S->fr));
     if (S->npm > 0) {
-        k_set_density<<<blocks(S->npm), 256, 0, s>>>(S->npb, S->npm, S->rho_f, S->S.vel, S->S.vd);
+        k_set_density<<<blocks(S->npm), 256, 0, s>>>(S->npb, S->npm, S->rho_f, S->S.vel, S->S.vlo);
         LQ_TRY_CUDA(cudaGetLastError(), "k_set_density");
     }
     return LQ_OK;
@@ -506,7 +505,7 @@ int set_flag(LqSim* S, int v) { return lqb::fill_int(S->rebuild, 1, v, S->stream
 
 int widen(LqSim* S)
 {
-    if (!S->S.xd) return LQ_OK;
+    if (!S->S.xlo) return LQ_OK;
     k_widen<<<blocks(S->np), 256, 0, S->stream>>>(S->np, S->S);
     LQ_TRY_CUDA(cudaGetLastError(), "k_widen");
     return LQ_OK;
@@ -912,9 +911,9 @@ struct Snapshot {
                  {S->S.idep, n * sizeof(float4)}, {S->S.str, n * sizeof(tensor2d)},
                  {S->S.stn, n * sizeof(tensor2d)}, {S->health, sizeof(int) * lqb::HEALTH_WORDS},
                  {S->rebuilds, sizeof(int)},      {S->pd, sizeof(Parameters)}};
-        if (S->S.xd) {
-            items.push_back({S->S.xd, n * sizeof(double4)});
-            items.push_back({S->S.vd, n * sizeof(double4)});
+        if (S->S.xlo) {
+            items.push_back({S->S.xlo, n * sizeof(float4)});
+            items.push_back({S->S.vlo, n * sizeof(float4)});
         }
         if (S->dtime) items.push_back({S->dtime, sizeof(double)});
         for (auto& it : items) {
@@ -1070,14 +1069,20 @@ extern "C" int lq_sim_save_checkpoint(void* sim, const char* path)
     std::vector<float> pos(4 * n), vel(4 * n), idep(4 * n), str(6 * n), stn(6 * n);
     std::vector<double> xd, vd;
     LQ_TRY(lq_sim_download(sim, pos.data(), vel.data(), idep.data(), str.data(), stn.data()));
-    if (S->S.xd) {
-        xd.resize(4 * n);
-        vd.resize(4 * n);
-        LQ_TRY_CUDA(cudaMemcpyAsync(xd.data(), S->S.xd, n * sizeof(double4), cudaMemcpyDeviceToHost, S->stream),
+    if (S->S.xlo) {
+        /* the file keeps the mixed form's values in FP64: high + low words */
+        std::vector<float> xl(4 * n), vl(4 * n);
+        LQ_TRY_CUDA(cudaMemcpyAsync(xl.data(), S->S.xlo, n * sizeof(float4), cudaMemcpyDeviceToHost, S->stream),
                     "checkpoint x");
-        LQ_TRY_CUDA(cudaMemcpyAsync(vd.data(), S->S.vd, n * sizeof(double4), cudaMemcpyDeviceToHost, S->stream),
+        LQ_TRY_CUDA(cudaMemcpyAsync(vl.data(), S->S.vlo, n * sizeof(float4), cudaMemcpyDeviceToHost, S->stream),
                     "checkpoint v");
         LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "checkpoint read");
+        xd.resize(4 * n);
+        vd.resize(4 * n);
+        for (size_t k = 0; k < 4 * n; ++k) {
+            xd[k] = (k % 4 == 3) ? 0.0 : (double)pos[k] + (double)xl[k];
+            vd[k] = (double)vel[k] + (double)vl[k];
+        }
     }
     Parameters par = S->ph;
     double time = S->time;
@@ -1198,12 +1203,18 @@ extern "C" int lq_sim_load_checkpoint(const char* path, int flags, void** sim)
         return st;
     };
     if (xd) {
+        /* low words: what the FP64 values leave beyond the float state */
         std::vector<double> hx(4 * n), hv(4 * n);
         memcpy(hx.data(), xd, n * sizeof(double4));
         memcpy(hv.data(), vd, n * sizeof(double4));
-        cudaError_t e = cudaMemcpyAsync(S->S.xd, hx.data(), n * sizeof(double4), cudaMemcpyHostToDevice, S->stream);
+        std::vector<float> xl(4 * n), vl(4 * n);
+        for (size_t k = 0; k < 4 * n; ++k) {
+            xl[k] = (k % 4 == 3) ? 0.0f : (float)(hx[k] - (double)a[0][k]);
+            vl[k] = (float)(hv[k] - (double)a[1][k]);
+        }
+        cudaError_t e = cudaMemcpyAsync(S->S.xlo, xl.data(), n * sizeof(float4), cudaMemcpyHostToDevice, S->stream);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(S->S.vd, hv.data(), n * sizeof(double4), cudaMemcpyHostToDevice, S->stream);
+            e = cudaMemcpyAsync(S->S.vlo, vl.data(), n * sizeof(float4), cudaMemcpyHostToDevice, S->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
         if (e != cudaSuccess)
             return fail(lqb::set_error(LQ_ERR_CUDA, "checkpoint FP64 state: %s", cudaGetErrorString(e)));
