@@ -381,11 +381,12 @@ constexpr int kUnroll = 8;
  * or up when the particle lies within the skin of a cell face), so a list
  * holds all its particle's pairs within the cut-off in those columns,
  * whatever the group; across columns it covers the 3 x 3 around the
- * particle's own, which holds every pair within 2h (a pair reaching 2h + skin
- * only across two columns is left out: it is beyond 2h when the list is
- * built and can come within 2h - skin only by q > 2 - skin/h, where the
- * kernel factor (2 - q)^3 is below (skin/h)^3).  Hits are staged per lane in
- * shared memory and flushed as coalesced rows. */
+ * particle's own, which holds every pair within 2h.  A pair within
+ * 2h + skin that lies two columns apart is left out: it is more than 2h
+ * apart when the list is built, so until the next build its distance stays
+ * above 2h - skin (q > 2 - skin/h), where the kernel factor (2 - q)^3 stays
+ * below (skin/h)^3.  Hits are staged per lane in shared memory and flushed
+ * as coalesced rows. */
 __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __restrict__ P, int first, int ntarget,
                                                           int layer_lo, float cut2, const float4* __restrict__ pos,
                                                           Cells cells, int* __restrict__ list,
