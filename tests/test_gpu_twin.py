@@ -2,11 +2,11 @@
 consecutive targets of one tile column and walks the union of their
 neighbour lists, gathering each neighbour once for both.
 
-* Plain FP32: a target's sums run over its own pairs in the order of its
-  thread-per-target list (entries out of its reach add exact zeros), so a
-  twin shape steps bit-identically to the thread-per-target shapes.
-* Mixed form: the compensated sums group the union's entries, not the
-  target's own, so it agrees to rounding.
+* A target's sums run over its own pairs in the order of its
+  thread-per-target list (entries out of its reach add exact zeros), but
+  the twin kernel's instruction schedule rounds differently (and the
+  compensated sums of the mixed form group the union's entries), so a twin
+  shape agrees with the thread-per-target shapes to float rounding.
 * The union lists also drive the Shepard and density filters, the batched
   ensemble (frames, per-object materials), model 3, a particle outside the
   lattice (its twin walks its stencil), and switching shapes mid-run.
@@ -24,18 +24,26 @@ pytestmark = pytest.mark.gpu
 TWINS = (11, 12, 13, 14)
 
 
+def assert_close(a_arrays, b_arrays, tol):
+    """Same NaN pattern, and each state array within tol relative L2."""
+    for k, (x, y) in enumerate(zip(a_arrays, b_arrays)):
+        x, y = np.asarray(x, np.float64), np.asarray(y, np.float64)
+        assert np.array_equal(np.isnan(x), np.isnan(y)), k
+        ok = ~np.isnan(x)
+        assert rel_l2(x[ok], y[ok]) <= tol, (k, rel_l2(x[ok], y[ok]))
+
+
 @pytest.mark.parametrize("shape", TWINS)
 def test_twin_shapes_step_like_thread_per_target_plain(lq, cuda, shape):
-    c = cases.small_column(velocity_noise=0.3, shepard=7, seed=91)
+    c = cases.small_column(velocity_noise=0.3, shepard=7, seed=91).with_ids()
     runs = []
     for sh in (0, shape):
         s = lq.Simulation(c.par, *c.arrays())
         s.set_pair_shape(sh)
         s.step(30)
         assert not s.health().any()
-        runs.append(s.download())
-    for x, y in zip(*runs):
-        assert np.array_equal(x, y)
+        runs.append(by_id(s.download()))
+    assert_close(runs[1], runs[0], 1e-5)
 
 
 @pytest.mark.parametrize("shape", (11, 12))
@@ -60,6 +68,7 @@ def test_twin_shapes_mixed_form_agree_to_rounding(lq, orc, cuda, shape):
 
 def test_twin_lists_with_frames_materials_filters_and_model_3(lq, cuda):
     comb, _ = cases.ensemble(n=5, count_range=(2.0e3, 4.0e3), seed=14, shepard=7)
+    comb.idep[:, 3] = np.arange(comb.par.np, dtype=np.float32)
     comb.par.density_shepard_filter = 5
     out = []
     for shape in (0, 11):
@@ -69,19 +78,17 @@ def test_twin_lists_with_frames_materials_filters_and_model_3(lq, cuda):
         s.set_pair_shape(shape)
         s.step(35)
         assert not s.health().any()
-        out.append(s.download())
-    for x, y in zip(*out):
-        assert np.array_equal(x, y)
-    v = cases.small_column(model=3, velocity_noise=0.05, shepard=7, seed=63)
+        out.append(by_id(s.download()))
+    assert_close(out[1], out[0], 1e-5)
+    v = cases.small_column(model=3, velocity_noise=0.05, shepard=7, seed=63).with_ids()
     out = []
     for shape in (0, 12):
         s = lq.Simulation(v.par, *v.arrays())
         s.set_hypoplastic(v.meta["hypoplastic"])
         s.set_pair_shape(shape)
         s.step(25)
-        out.append(s.download())
-    for x, y in zip(*out):
-        assert np.array_equal(x, y)
+        out.append(by_id(s.download()))
+    assert_close(out[1], out[0], 1e-5)
 
 
 @pytest.mark.parametrize("shape", (11, 13))
@@ -90,7 +97,7 @@ def test_twin_shape_switched_on_and_off_mid_run_with_escaped_particles(lq, cuda,
     the lists in the new kind), with particles outside the lattice: their
     slots sit in the out-of-lattice cell, whose twins are split and walk
     their stencils."""
-    c = cases.small_column(velocity_noise=0.3, shepard=7, seed=84)
+    c = cases.small_column(velocity_noise=0.3, shepard=7, seed=84).with_ids()
     a = lq.Simulation(c.par, *c.arrays())
     b = lq.Simulation(c.par, *c.arrays())
     a.set_pair_shape(0)
@@ -111,8 +118,7 @@ def test_twin_shape_switched_on_and_off_mid_run_with_escaped_particles(lq, cuda,
     a.step(20)
     b.step(20)
     assert a.health()[1] >= 2
-    for x, y in zip(a.download(), b.download()):
-        assert np.array_equal(x, y, equal_nan=True)
+    assert_close(by_id(b.download()), by_id(a.download()), 1e-5)
 
 
 def test_twin_neighbour_entries_count_each_targets_own_pairs(lq, cuda):
