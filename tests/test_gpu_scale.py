@@ -10,6 +10,10 @@
   Plain FP32 is held to 3e-3: at 0.5 m from the origin a float position
   cannot take a step's displacement of ~1e-7 m whole, and a float density
   of ~2000 kg/m^3 resolves its change only to ~1e-4 kg/m^3.
+* The same material and spacing on a cylinder scaled by 1/4 for the
+  workload's 5000 steps and on to 20000: the runout radius and the
+  free-surface profile against the oracle's within 1 %
+  (tests/golden/cylinder_runout.npz).
 * A batched ensemble of Drucker-Prager columns with their own friction
   angle and cohesion (per-object material rows and frames): each scenario
   of the batch against the oracle run on that scenario alone with its own
@@ -114,3 +118,41 @@ def test_batched_scenarios_with_own_materials_vs_oracle(lq, orc, cuda, mixed):
         o.close()
     for key, v in worst.items():
         assert v <= TOL, (key, v)
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_scaled_cylinder_runout_and_surface_vs_oracle(lq, cuda, mixed):
+    """The cylinder's material and spacing on a cylinder scaled by 1/4
+    (R = 0.05 m, H = 0.1 m) for the workload's 5000 steps and on to 20000,
+    against the oracle's run (tests/golden/cylinder_runout.npz): the runout
+    radius (advance of the largest radial distance of a soil particle from
+    the axis) and the free-surface profile (highest soil particle per
+    radial bin) within 1 %."""
+    from make_cylinder import radius_and_profile, runout_case
+
+    z = np.load(GOLDEN / "cylinder_runout.npz")
+    c = runout_case()
+    assert c.par.np == int(z["np"])
+    dr, axis, nbins = float(z["dr"]), tuple(z["axis"]), z["profiles"].shape[1]
+    sim = lq.Simulation(c.par, *c.arrays(), mixed=mixed)
+    done = 0
+    report = []
+    for k, n in enumerate(z["steps"]):
+        sim.step(int(n) - done)
+        done = int(n)
+        pos, vel, idep, s, e = sim.download()
+        r, prof = radius_and_profile(pos, idep, dr, axis, nbins)
+        run_gpu = r - float(z["radius0"])
+        run_ref = float(z["radii"][k]) - float(z["radius0"])
+        occ = z["profiles"][k] > 0
+        surf = np.linalg.norm(prof[occ] - z["profiles"][k][occ]) / np.linalg.norm(z["profiles"][k][occ])
+        report.append((int(n), run_gpu, run_ref, surf))
+    print("mixed" if mixed else "plain", [(n, f"{a * 1e3:.3f} mm", f"{b * 1e3:.3f} mm", f"{s_:.2e}")
+                                          for n, a, b, s_ in report])
+    assert not sim.health().any()
+    sim.close()
+    for n, run_gpu, run_ref, surf in report:
+        if n in (5000, int(z["steps"][-1])):
+            assert run_ref > dr, (n, run_ref)           # the front has moved
+            assert abs(run_gpu - run_ref) <= 0.01 * run_ref, (n, run_gpu, run_ref)
+            assert surf < 0.01, (n, surf)
