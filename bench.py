@@ -19,10 +19,18 @@ buffers: state upload, every step followed by a device->host read of the
 region.  Under torchrun every rank runs an independent replica (weak
 scaling, no collective in the data path).
 
+The default run adds three legs to the line: `amortized` (a 250-step
+window of the same run, carrying the neighbour-list rebuilds at their
+natural rate), `dropin` (the reference's step sequence through the drop-in
+entry points on the same workload) and `ensemble` (config 4: 256 batched
+scenarios in both precision forms against the same scenarios run one
+after another, each side autotuned).
+
 `--impl reference` times the CPU FP64 OpenMP restatement of the reference's
 algorithm (the reference has no CPU implementation of its own and its GPU
-build cannot be assembled: two of its libraries are not distributed) on a
-bounded sample of the workload.
+build cannot be assembled: two of its libraries are not distributed) on the
+same workload, with every host thread and then on one thread; it derives
+the case's Parameters with the oracle and loads no library of the product.
 """
 from __future__ import annotations
 
