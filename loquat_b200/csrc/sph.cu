@@ -289,11 +289,59 @@ __device__ __forceinline__ void pair_terms_rec(const PairConst& K, const NbrRec&
     T.l20 -= wz * gx; T.l21 -= wz * gy; T.l22 -= wz * gz;
 }
 
+/* The same pair gathering its record itself: the thread-per-target kernels
+ * issue the four loads where the arithmetic needs them, which schedules
+ * better there than a record gathered ahead. */
 template <bool kArtp>
 __device__ __forceinline__ void pair_terms(const PairConst& K, const NbrArrays& nb, Target& T, int j, float& drho,
                                            float& ax, float& ay, float& az)
 {
-    pair_terms_rec<kArtp>(K, fetch_rec(nb, j), T, drho, ax, ay, az);
+    const float4 xr = __ldg(nb.xr + j);
+    const float4 vs = __ldg(nb.vs + j);
+    const float4 s3 = __ldg(nb.s3 + j);
+    const float s1 = __ldg(nb.s1 + j);
+    const float a[8] = {xr.x, xr.y, xr.z, 0.0f, vs.x, vs.y, vs.z, xr.w};
+    const float b[6] = {vs.w, s3.x, s3.y, s3.z, s3.w, s1};
+    const float dx = T.x.x - a[0], dy = T.x.y - a[1], dz = T.x.z - a[2];
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    const float q = sqrt_approx(r2) * K.ih;
+    const float t = fmaxf(2.0f - q, 0.0f);
+    const float fac = K.Cg * t * t * t;
+    const float gx = fac * dx, gy = fac * dy, gz = fac * dz;
+    const float vx = T.v.x - a[4], vy = T.v.y - a[5], vz = T.v.z - a[6];
+    drho += vx * gx + vy * gy + vz * gz;
+    const float Txx = T.Sxx + b[0], Tyy = T.Syy + b[1], Tzz = T.Szz + b[2];
+    const float Txy = T.Sxy + b[3], Txz = T.Sxz + b[4], Tyz = T.Syz + b[5];
+    float px = Txx * gx + Txy * gy + Txz * gz;
+    float py = Txy * gx + Tyy * gy + Tyz * gz;
+    float pz = Txz * gx + Tyz * gy + Tzz * gz;
+    {
+        /* Pi = -alpha cs h vr / ((r^2 + eta) rhobar) for vr < 0 */
+        const float vr = fminf(vx * dx + vy * dy + vz * dz, 0.0f);
+        const float pi = __fdividef(-K.avc * K.h * vr, (r2 + K.eta) * (0.5f * (T.v.w + a[7])));
+        px -= pi * gx;
+        py -= pi * gy;
+        pz -= pi * gz;
+    }
+    if (kArtp) {
+        const float wk = K.Cw * t * t * t * t * (q + 0.5f);
+        const float f = __fdividef(wk, K.wdr);
+        const float f4 = (f * f) * (f * f);
+        const float Rjx = b[0] > 0.f ? -K.eps * b[0] : 0.f;
+        const float Rjy = b[1] > 0.f ? -K.eps * b[1] : 0.f;
+        const float Rjz = b[2] > 0.f ? -K.eps * b[2] : 0.f;
+        px += (T.Rx + Rjx) * f4 * gx;
+        py += (T.Ry + Rjy) * f4 * gy;
+        pz += (T.Rz + Rjz) * f4 * gz;
+    }
+    ax += px;
+    ay += py;
+    az += pz;
+    const float Vj = K.m * __fdividef(1.0f, a[7]);
+    const float wx = Vj * vx, wy = Vj * vy, wz = Vj * vz;
+    T.l00 -= wx * gx; T.l01 -= wx * gy; T.l02 -= wx * gz;
+    T.l10 -= wy * gx; T.l11 -= wy * gy; T.l12 -= wy * gz;
+    T.l20 -= wz * gx; T.l21 -= wz * gy; T.l22 -= wz * gz;
 }
 
 /* One pair into T's sums; kKahan compensates the density and momentum
