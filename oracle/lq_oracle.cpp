@@ -239,10 +239,25 @@ void adami(const OrParams& P, int np, int npb, const double* pos, const double* 
  * to BF16 (round to nearest even).  0 (the default) rounds nothing. */
 int g_gather_rounding = 0;
 
+/* x rounded to nearest even with `bits` significant bits, numbers below
+ * 2^emin keeping the quantum of 2^emin (the subnormals of a format whose
+ * least normal exponent is emin).  On a float input it equals the FP16
+ * (bits 11, emin -14) and BF16 (bits 8, emin -126) conversions for every
+ * value below the FP16 maximum, without their software calls on the host. */
+inline double round_significand(double x, int bits, int emin)
+{
+    if (x == 0.0 || !std::isfinite(x)) return x;
+    int e;
+    std::frexp(x, &e);
+    if (e - 1 < emin) e = emin + 1;
+    const double q = std::ldexp(1.0, e - bits);
+    return std::nearbyint(x / q) * q;
+}
+
 inline double gather_round(double x, int f16_bit, int bf16_bit)
 {
-    if (g_gather_rounding & f16_bit) return (double)(_Float16)x;
-    if (g_gather_rounding & bf16_bit) return (double)(float)(__bf16)(float)x;
+    if (g_gather_rounding & f16_bit) return round_significand((double)(float)x, 11, -14);
+    if (g_gather_rounding & bf16_bit) return round_significand((double)(float)x, 8, -126);
     return x;
 }
 
