@@ -76,17 +76,11 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_predict(
         store_t2(snap.stn, i, e0);
     }
     if (i < npb) {
-        if (out.pos != in.pos) {
-            out.pos[i] = x0;
-            out.vel[i] = v0;
-            out.idep[i] = id;
-            store_t2(out.str, i, s0);
-            store_t2(out.stn, i, e0);
-            if (kMixed) {
-                out.xlo[i] = in.xlo[i];
-                out.vlo[i] = in.vlo[i];
-            }
-        }
+        /* a boundary slot of another output buffer takes only the stress
+         * (the Adami extrapolation): its position, velocity, idep and
+         * strain never change, and the native driver copies them whole at
+         * each list rebuild */
+        if (out.pos != in.pos) store_t2(out.str, i, s0);
         return;
     }
     const float dt = __ldg(&P->dt);
@@ -197,15 +191,9 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(
     const int i = first + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
     if (i < npb) {
-        out.pos[i] = cur.pos[i];
-        out.vel[i] = cur.vel[i];
-        out.idep[i] = cur.idep[i];
+        /* boundary slots: the latest Adami stress; the rest of a boundary
+         * slot is the same in both buffers (see k_predict) */
         store_t2(out.str, i, load_t2_rw(cur.str, i));
-        store_t2(out.stn, i, load_t2_rw(cur.stn, i));
-        if (kMixed) {
-            out.xlo[i] = cur.xlo[i];
-            out.vlo[i] = cur.vlo[i];
-        }
         return;
     }
     const int k = ini_idx ? __ldg(ini_idx + i) : i;

@@ -215,8 +215,10 @@ int launch_adami(const Parameters* par_host, const Parameters* par_dev, const St
  * from `st` to `out`, producing a complete new state. */
 int launch_shepard(const Parameters* par_host, const Parameters* par_dev, const State& st, tensor2d* out_str,
                    const State* full, const Cells& c, cudaStream_t s);
-/* Predictor: out <- in advanced by dt/2 on material slots, boundary slots
- * copied when out != in; `snap` (may be all-null) receives a copy of `in`. */
+/* Predictor: out <- in advanced by dt/2 on material slots; when out != in
+ * only the boundary slots' stress is copied (the rest of a boundary slot
+ * never changes and must already be in `out`); `snap` (may be all-null)
+ * receives a copy of `in`. */
 int launch_predict(const Parameters* par_host, const Parameters* par_dev, const State& in, const State& out,
                    const State* snap, const Rates& r, cudaStream_t s, const MaterialTable& mt = MaterialTable(),
                    const MaterialTable& vw = MaterialTable());
@@ -225,8 +227,9 @@ int launch_predict(const Parameters* par_host, const Parameters* par_dev, const 
 int launch_correct(const Parameters* par_host, const Parameters* par_dev, const State& cur, const State& ini,
                    const int* ini_idx, const Rates& r, int* health, cudaStream_t s);
 
-/* Corrector from snapshot `ini` and current `cur` into `out` (boundary slots
- * copied from cur); material particles raise *rebuild when neighbour lists
+/* Corrector from snapshot `ini` and current `cur` into `out` (boundary
+ * slots take cur's stress; the rest of a boundary slot must already be the
+ * same in both); material particles raise *rebuild when neighbour lists
  * built at xbuild with this skin may not hold through the next step. */
 int launch_correct_into(const Parameters* par_host, const Parameters* par_dev, const State& cur, const State& ini,
                         const State& out, const Rates& r, int* health, const float4* xbuild, int* rebuild,

@@ -161,10 +161,32 @@ void release(LqSim* S)
 
 /* ------------------------------------------------------------- kernels */
 
-__global__ void k_copy_state(int n, State in, State out, float4* __restrict__ xbuild)
+/* The gathered state back into S and the build positions; boundary slots
+ * also into S2 (they never change between rebuilds, so the integrators
+ * pass only their stress between the two buffers). */
+__global__ void k_copy_state(int n, int npb, State in, State out, State out2, float4* __restrict__ xbuild)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (i < npb) {
+        out2.pos[i] = in.pos[i];
+        out2.vel[i] = in.vel[i];
+        out2.idep[i] = in.idep[i];
+        const float2* a = reinterpret_cast<const float2*>(in.str) + 3 * (size_t)i;
+        float2* b = reinterpret_cast<float2*>(out2.str) + 3 * (size_t)i;
+        b[0] = a[0];
+        b[1] = a[1];
+        b[2] = a[2];
+        a = reinterpret_cast<const float2*>(in.stn) + 3 * (size_t)i;
+        b = reinterpret_cast<float2*>(out2.stn) + 3 * (size_t)i;
+        b[0] = a[0];
+        b[1] = a[1];
+        b[2] = a[2];
+        if (in.xlo) {
+            out2.xlo[i] = in.xlo[i];
+            out2.vlo[i] = in.vlo[i];
+        }
+    }
     const float4 x = in.pos[i];
     out.pos[i] = x;
     xbuild[i] = x;
@@ -307,7 +329,7 @@ int enqueue_rebuild(LqSim* S, cudaStream_t s)
     const Parameters* pd = S->pd;
     LQ_TRY(lqb::grid_search(ph, pd, S->S.pos, S->g, false, S->health, s, S->S.idep, S->fr));
     LQ_TRY(lqb::gather_state(S->np, S->g.part_idx, S->S, S->T, s));
-    k_copy_state<<<blocks(S->np), 256, 0, s>>>(S->np, S->T, S->S, S->xbuild);
+    k_copy_state<<<blocks(S->np), 256, 0, s>>>(S->np, S->npb, S->T, S->S, S->S2, S->xbuild);
     LQ_TRY_CUDA(cudaGetLastError(), "k_copy_state");
     LQ_TRY(build_lists(S, s));
     /* every slot's packed neighbour data (the boundary slots keep theirs
@@ -1335,7 +1357,7 @@ int profiled_step(LqSim* S, PhaseTimer& T)
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_GATHER));
         LQ_TRY(lqb::gather_state(S->np, S->g.part_idx, S->S, S->T, s));
-        k_copy_state<<<blocks(S->np), 256, 0, s>>>(S->np, S->T, S->S, S->xbuild);
+        k_copy_state<<<blocks(S->np), 256, 0, s>>>(S->np, S->npb, S->T, S->S, S->S2, S->xbuild);
         LQ_TRY_CUDA(cudaGetLastError(), "k_copy_state");
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_LIST));
