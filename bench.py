@@ -330,10 +330,23 @@ def dropin_measurement(args, case, torch, dist):
     e1.record(stream)
     stream.synchronize()
     ms = replicas.max_over_ranks(e0.elapsed_time(e1), device="cuda")
+    # one ParticleInteraction call on its own (cell starts, tile order,
+    # list build in the caller's grid, pack, pair kernel)
+    from loquat_b200 import particle_interaction
+
+    beg, end = seq._cells()
+    calls = 5
+    i0, i1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    i0.record(stream)
+    for _ in range(calls):
+        particle_interaction(seq.par, seq.par_dev, *seq.state, *seq.rates, beg, end, stream=seq._s)
+    i1.record(stream)
+    stream.synchronize()
+    call_ms = replicas.max_over_ranks(i0.elapsed_time(i1) / calls, device="cuda")
     seq.close()
     world = dist.get_world_size() if dist else 1
     return {"value": case.par.npm * args.steps * world / (ms / 1e3), "unit": "particle-steps/s",
-            "ms_per_step": ms / args.steps, "steps": args.steps,
+            "ms_per_step": ms / args.steps, "steps": args.steps, "interaction_ms_per_call": call_ms,
             "form": "plain FP32, the reference's call sequence through lq_grid_*, lq_adami_boundary, "
                     "lq_particle_interaction, lq_predictor / lq_corrector, lq_stress_regularization"}
 
