@@ -86,7 +86,7 @@ def parse_args(argv=None):
                     help="keep the default pair-kernel shape and list skin instead of lq_sim_autotune's choice")
     ap.add_argument("--tune-steps", type=int, default=40, help="timed steps per autotuner trial")
     ap.add_argument("--pair-shape", type=int, default=None,
-                    help="fix the pair kernel's launch shape (lq_sim_set_pair_shape, 0-14) instead of autotuning")
+                    help="fix the pair kernel's launch shape (lq_sim_set_pair_shape, 0-10) instead of autotuning")
     ap.add_argument("--no-dropin", action="store_true",
                     help="skip timing the reference's step sequence through the drop-in entry points")
     ap.add_argument("--no-ensemble", action="store_true",

@@ -149,28 +149,12 @@ int launch_pack_neighbors(const Parameters* par_host, const State& st, float* re
 int launch_adami_packed(const Parameters* par_host, const Parameters* par_dev, const State& st,
                         const NeighborList& nl, float* rec, cudaStream_t s);
 /* Launch shapes of the packed pair kernel: {threads per block, resident
- * blocks per SM, order}, or {128, -G, 0} for the warp-cooperative form
- * with G lanes per target.  Order 0 takes targets in slot order, 1 in tile
- * order (TileOrder::order, launch_tile_order after each search), 2 in
- * twins of two targets per thread over union lists (TwinLists, built by
- * launch_twin_order and launch_neighbor_list_twin after each search). */
-constexpr int kPairShapeCount = 15;
+ * blocks per SM, tile order}, or {128, -G, 0} for the warp-cooperative form
+ * with G lanes per target.  Shapes with the tile order take their targets
+ * from TileOrder::order (launch_tile_order, after each search). */
+constexpr int kPairShapeCount = 11;
 constexpr int kDefaultTiledShape = 9;   /* 640 x 1, tile order */
 extern const int kPairShapes[kPairShapeCount][3];
-inline bool twin_shape(int shape) { return shape >= 0 && shape < kPairShapeCount && kPairShapes[shape][2] == 2; }
-/* Twins of consecutive material targets, in tile order, with the union
- * lists of their neighbours (the twin launch shapes' material lists). */
-#define LQ_TWIN_CAP 256
-struct TwinLists {
-    int* twin = nullptr;    /* twin codes (2 t + single) in tile order, -1 past the last: int[cap] */
-    int cap = 0;            /* twin slots */
-    int* list = nullptr;    /* int[LQ_TWIN_CAP * stride], entry k of twin g at k * stride + g */
-    int* count = nullptr;   /* int[stride]; LQ_TWIN_CAP + 1: the twin walks its stencils */
-    int* hits = nullptr;    /* int[stride]: the two targets' own neighbour counts (16 bits each) */
-    int stride = 0;         /* >= cap, multiple of 32 */
-};
-/* Twin slots launch shape `shape` needs (0 for other shapes). */
-int twin_capacity(const Parameters* par_host, int shape);
 /* Launch shape of a new simulation with npm material particles. */
 int default_pair_shape(int npm);
 /* Targets of the pair kernel in tile order, and the scratch that builds it:
@@ -184,30 +168,11 @@ struct TileOrder {
     size_t scan_bytes = 0;
 };
 /* Segments (for the smallest tile height) and scan scratch bytes; the
- * segment scratch is 4 x nseg ints. */
+ * segment scratch is 3 x nseg ints. */
 int tile_order_scratch(const Parameters* par_host, int* nseg, size_t* scan_bytes);
 /* The tile order for launch shape `shape` from the grid's cell starts
  * (nothing for shapes without it). */
 int launch_tile_order(const Parameters* par_host, const int* start, int shape, const TileOrder& to, cudaStream_t s);
-/* The twin order of a twin launch shape from the grid's cell starts, into
- * tw.twin (with the segment scratch of `to`). */
-int launch_twin_order(const Parameters* par_host, const int* start, int shape, const TileOrder& to,
-                      const TwinLists& tw, cudaStream_t s);
-/* Union lists of the twins in tw.twin with cut-off radius `cut`; overflows
- * are counted in health[HEALTH_NBR_OVERFLOW]. */
-int launch_neighbor_list_twin(const Parameters* par_host, const Parameters* par_dev, float cut, const float4* pos,
-                              const Cells& c, const TwinLists& tw, int* health, cudaStream_t s,
-                              const float4* idep = nullptr, const Frames& fr = Frames());
-/* Pair sums of a twin launch shape over the union lists. */
-int launch_interaction_twin(const Parameters* par_host, const Parameters* par_dev, const State& st, const Rates& r,
-                            const Cells& c, const TwinLists& tw, cudaStream_t s, const Frames& fr, bool compensated,
-                            float* rec, int shape);
-/* Shepard and density filters over the union lists. */
-int launch_shepard_twin(const Parameters* par_host, const Parameters* par_dev, const State& st, tensor2d* out_str,
-                        const TwinLists& tw, const Cells& c, cudaStream_t s, const Frames& fr = Frames());
-int launch_density_filter_twin(const Parameters* par_host, const Parameters* par_dev, const State& st,
-                               float* rho_out, const TwinLists& tw, const Cells& c, cudaStream_t s,
-                               const Frames& fr = Frames());
 int launch_adami(const Parameters* par_host, const Parameters* par_dev, const State& st, const Cells& c,
                  cudaStream_t s);
 /* Shepard filter of material stress into out_str[npb, np).  When `full` is

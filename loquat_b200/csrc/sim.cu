@@ -66,7 +66,6 @@ struct LqSim {
     float* rho_f = nullptr;            /* density filter output (LQ_SIM_DENSITY_FILTER) */
     int pair_shape = 0;                /* launch shape of the pair kernel (lqb::kPairShapes) */
     lqb::TileOrder tile;               /* targets in tile order (tiled shapes; allocated on first use) */
-    lqb::TwinLists tw;                 /* twins and their union lists (twin shapes; allocated on first use) */
     unsigned* vmax2 = nullptr;         /* max |v|^2, |a|^2 bits (LQ_SIM_DYNAMIC_DT) */
     double* dtime = nullptr;           /* device-side time (LQ_SIM_DYNAMIC_DT) */
     lqb::Frames fr;                    /* per-object grid rows (optional) */
@@ -87,45 +86,23 @@ int dev_alloc(LqSim* S, void** p, size_t bytes)
     return LQ_OK;
 }
 
-bool tiled(const LqSim* S) { return lqb::kPairShapes[S->pair_shape][2] == 1; }
-bool twin(const LqSim* S) { return lqb::twin_shape(S->pair_shape); }
+bool tiled(const LqSim* S) { return lqb::kPairShapes[S->pair_shape][2] != 0; }
 
 /* The pair kernel's target order for tiled launch shapes (null otherwise). */
 const int* tile_order(const LqSim* S) { return tiled(S) ? S->tile.order : nullptr; }
 
-/* Buffers of the tile or twin order, on first use of such a shape; the
- * twins' union lists use the thread-per-target material lists' storage
- * when it is large enough (a simulation builds one kind at a time). */
+/* Buffers of the tile order, on first use of a tiled shape. */
 int ensure_tile_order(LqSim* S)
 {
-    if (!tiled(S) && !twin(S)) return LQ_OK;
-    if (!S->tile.seg) {
-        int nseg = 0;
-        size_t bytes = 0;
-        LQ_TRY(lqb::tile_order_scratch(&S->ph, &nseg, &bytes));
-        LQ_TRY(dev_alloc(S, (void**)&S->tile.seg, sizeof(int) * 4 * (size_t)nseg));
-        LQ_TRY(dev_alloc(S, &S->tile.scan_tmp, bytes));
-        S->tile.nseg_cap = nseg;
-        S->tile.scan_bytes = bytes;
-    }
-    if (tiled(S) && !S->tile.order)
-        LQ_TRY(dev_alloc(S, (void**)&S->tile.order, sizeof(int) * (size_t)(S->npm > 0 ? S->npm : 1)));
-    if (twin(S)) {
-        const int cap = lqb::twin_capacity(&S->ph, S->pair_shape);
-        if (cap > S->tw.cap) {
-            lqb::TwinLists t;
-            t.cap = cap;
-            t.stride = (cap + 31) / 32 * 32;
-            LQ_TRY(dev_alloc(S, (void**)&t.twin, sizeof(int) * (size_t)cap));
-            LQ_TRY(dev_alloc(S, (void**)&t.count, sizeof(int) * (size_t)t.stride));
-            LQ_TRY(dev_alloc(S, (void**)&t.hits, sizeof(int) * (size_t)t.stride));
-            if ((size_t)LQ_TWIN_CAP * t.stride <= (size_t)LQ_NBR_CAP * S->nlm.stride)
-                t.list = S->nlm.list;
-            else
-                LQ_TRY(dev_alloc(S, (void**)&t.list, sizeof(int) * (size_t)LQ_TWIN_CAP * t.stride));
-            S->tw = t;
-        }
-    }
+    if (!tiled(S) || S->tile.order) return LQ_OK;
+    int nseg = 0;
+    size_t bytes = 0;
+    LQ_TRY(lqb::tile_order_scratch(&S->ph, &nseg, &bytes));
+    LQ_TRY(dev_alloc(S, (void**)&S->tile.seg, sizeof(int) * 3 * (size_t)nseg));
+    LQ_TRY(dev_alloc(S, &S->tile.scan_tmp, bytes));
+    LQ_TRY(dev_alloc(S, (void**)&S->tile.order, sizeof(int) * (size_t)(S->npm > 0 ? S->npm : 1)));
+    S->tile.nseg_cap = nseg;
+    S->tile.scan_bytes = bytes;
     return LQ_OK;
 }
 
@@ -292,21 +269,15 @@ __global__ void k_dt_update(Parameters* P, unsigned* m2, double* time)
 
 /* ------------------------------------------------------------ sequences */
 
-/* Material lists (thread-per-target, or the twins' union lists) and
- * boundary lists from the sorted state in S. */
+/* Material and boundary lists from the sorted state in S. */
 int build_lists(LqSim* S, cudaStream_t s)
 {
     const Parameters* ph = &S->ph;
     const Parameters* pd = S->pd;
     const lqb::Cells cells{S->g.start, nullptr, nullptr};
     const float cut = 2.0f * ph->h + S->skin;
-    if (twin(S)) {
-        LQ_TRY(lqb::launch_twin_order(ph, S->g.start, S->pair_shape, S->tile, S->tw, s));
-        LQ_TRY(lqb::launch_neighbor_list_twin(ph, pd, cut, S->S.pos, cells, S->tw, S->health, s, S->S.idep, S->fr));
-    } else {
-        LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, S->npb, S->npm, 0, cut, S->S.pos, cells, S->nlm, S->health,
-                                               s, S->S.idep, S->fr));
-    }
+    LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, S->npb, S->npm, 0, cut, S->S.pos, cells, S->nlm, S->health, s,
+                                           S->S.idep, S->fr));
     return lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, S->nlb, S->health, s,
                                            S->S.idep, S->fr);
 }
@@ -315,9 +286,6 @@ int build_lists(LqSim* S, cudaStream_t s)
 int enqueue_interaction(LqSim* S, const State& st, cudaStream_t s)
 {
     const lqb::Cells cells{S->g.start, nullptr, nullptr};
-    if (twin(S))
-        return lqb::launch_interaction_twin(&S->ph, S->pd, st, S->R, cells, S->tw, s, S->fr,
-                                            S->flags & LQ_SIM_MIXED, S->rec, S->pair_shape);
     return lqb::launch_interaction_list(&S->ph, S->pd, st, S->R, cells, S->nlm, s, S->fr, S->flags & LQ_SIM_MIXED,
                                         S->rec, S->pair_shape, false, tile_order(S));
 }
@@ -356,10 +324,7 @@ int enqueue_dynamic_dt(LqSim* S, cudaStream_t s)
 int enqueue_density_filter(LqSim* S, cudaStream_t s)
 {
     const lqb::Cells cells{S->g.start, nullptr, nullptr};
-    if (twin(S))
-        LQ_TRY(lqb::launch_density_filter_twin(&S->ph, S->pd, S->S, S->rho_f, S->tw, cells, s, S->fr));
-    else
-        LQ_TRY(lqb::launch_density_filter_list(&S->ph, S->pd, S->S, S->rho_f, S->nlm, cells, s, S->fr));
+    LQ_TRY(lqb::launch_density_filter_list(&S->ph, S->pd, S->S, S->rho_f, S->nlm, cells, s, S->fr));
     if (S->npm > 0) {
         k_set_density<<<blocks(S->npm), 256, 0, s>>>(S->npb, S->npm, S->rho_f, S->S.vel, S->S.vlo);
         LQ_TRY_CUDA(cudaGetLastError(), "k_set_density");
@@ -398,10 +363,7 @@ int enqueue_stages(LqSim* S, cudaStream_t s)
 int enqueue_shepard(LqSim* S, cudaStream_t s)
 {
     const lqb::Cells cells{S->g.start, nullptr, nullptr};
-    if (twin(S))
-        LQ_TRY(lqb::launch_shepard_twin(&S->ph, S->pd, S->S, S->T.str, S->tw, cells, s, S->fr));
-    else
-        LQ_TRY(lqb::launch_shepard_list(&S->ph, S->pd, S->S, S->T.str, S->nlm, cells, s, S->fr));
+    LQ_TRY(lqb::launch_shepard_list(&S->ph, S->pd, S->S, S->T.str, S->nlm, cells, s, S->fr));
     if (S->npm > 0) {
         k_copy_t2<<<blocks(S->npm), 256, 0, s>>>(S->npb, S->npm, S->T.str, S->S.str);
         LQ_TRY_CUDA(cudaGetLastError(), "k_copy_t2");
@@ -896,10 +858,7 @@ extern "C" int lq_sim_set_pair_shape(void* sim, int shape)
         return lqb::set_error(LQ_ERR_ARG, "lq_sim_set_pair_shape: shape must be in [0, %d)", lqb::kPairShapeCount);
     LqSim* S = static_cast<LqSim*>(sim);
     LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "set pair shape");
-    const bool was_twin = twin(S);
     S->pair_shape = shape;
-    /* into or out of a twin shape the material lists change kind: rebuild */
-    if (was_twin || twin(S)) LQ_TRY(set_flag(S, 1));
     LQ_TRY(build_graphs(S));
     if (!tiled(S)) return LQ_OK;
     /* the lists are current unless a search is pending: order them now */
@@ -1279,18 +1238,7 @@ extern "C" int lq_sim_neighbor_entries(void* sim, long long* material, long long
         *out = t;
         return LQ_OK;
     };
-    if (twin(S)) {
-        /* each target's own neighbours among its twin's union list */
-        std::vector<int> h((size_t)(S->tw.cap > 0 ? S->tw.cap : 0));
-        if (S->tw.cap > 0)
-            LQ_TRY_CUDA(cudaMemcpy(h.data(), S->tw.hits, sizeof(int) * (size_t)S->tw.cap, cudaMemcpyDeviceToHost),
-                        "twin hits");
-        long long t = 0;
-        for (int c : h) t += (c & 0xffff) + ((unsigned)c >> 16);
-        *material = t;
-    } else {
-        LQ_TRY(total(S->nlm.count, S->npm, material));
-    }
+    LQ_TRY(total(S->nlm.count, S->npm, material));
     LQ_TRY(total(S->nlb.count, S->npb, boundary));
     return LQ_OK;
 }
@@ -1303,8 +1251,7 @@ extern "C" int lq_sim_rebuild_launches(void* sim, int* launches)
      * kernel), gather, copy, material list, boundary list (when npb > 0),
      * full pack of the neighbour data, tile segments and fill (tiled
      * shapes; their scan is a library kernel) */
-    *launches = 4 + 1 + 1 + 1 + (S->npb > 0 ? 1 : 0) + 1 + (tiled(S) && S->npm > 0 ? 2 : 0) +
-                (twin(S) && S->npm > 0 ? 3 : 0);
+    *launches = 4 + 1 + 1 + 1 + (S->npb > 0 ? 1 : 0) + 1 + (tiled(S) && S->npm > 0 ? 2 : 0);
     return LQ_OK;
 }
 

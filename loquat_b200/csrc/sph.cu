@@ -213,85 +213,12 @@ struct NbrArrays {
     float* s1;
 };
 
-/* One neighbour's packed record, gathered once and used for every target
- * that shares it. */
-struct NbrRec {
-    float4 xr, vs, s3;
-    float s1;
-};
-
-__device__ __forceinline__ NbrRec fetch_rec(const NbrArrays& nb, int j)
-{
-    NbrRec r;
-    r.xr = __ldg(nb.xr + j);
-    r.vs = __ldg(nb.vs + j);
-    r.s3 = __ldg(nb.s3 + j);
-    r.s1 = __ldg(nb.s1 + j);
-    return r;
-}
-
-/* One pair from a neighbour's packed record, its density-rate and momentum
- * terms added to (drho, ax, ay, az) and its velocity-gradient terms to T.
- * The viscosity term is always evaluated (K.avc is zero without
- * viscosity), so a run of pairs has no branch between them; kArtp adds the
- * artificial stress.  A pair of a particle with itself (the filler of a
- * list's last group of four) adds exact zeros: r = 0 makes the kernel
- * gradient zero. */
-template <bool kArtp>
-__device__ __forceinline__ void pair_terms_rec(const PairConst& K, const NbrRec& rec, Target& T, float& drho,
-                                               float& ax, float& ay, float& az)
-{
-    const float4 xr = rec.xr;
-    const float4 vs = rec.vs;
-    const float4 s3 = rec.s3;
-    const float s1 = rec.s1;
-    const float a[8] = {xr.x, xr.y, xr.z, 0.0f, vs.x, vs.y, vs.z, xr.w};
-    const float b[6] = {vs.w, s3.x, s3.y, s3.z, s3.w, s1};
-    const float dx = T.x.x - a[0], dy = T.x.y - a[1], dz = T.x.z - a[2];
-    const float r2 = dx * dx + dy * dy + dz * dz;
-    const float q = sqrt_approx(r2) * K.ih;
-    const float t = fmaxf(2.0f - q, 0.0f);
-    const float fac = K.Cg * t * t * t;
-    const float gx = fac * dx, gy = fac * dy, gz = fac * dz;
-    const float vx = T.v.x - a[4], vy = T.v.y - a[5], vz = T.v.z - a[6];
-    drho += vx * gx + vy * gy + vz * gz;
-    const float Txx = T.Sxx + b[0], Tyy = T.Syy + b[1], Tzz = T.Szz + b[2];
-    const float Txy = T.Sxy + b[3], Txz = T.Sxz + b[4], Tyz = T.Syz + b[5];
-    float px = Txx * gx + Txy * gy + Txz * gz;
-    float py = Txy * gx + Tyy * gy + Tyz * gz;
-    float pz = Txz * gx + Tyz * gy + Tzz * gz;
-    {
-        /* Pi = -alpha cs h vr / ((r^2 + eta) rhobar) for vr < 0 */
-        const float vr = fminf(vx * dx + vy * dy + vz * dz, 0.0f);
-        const float pi = __fdividef(-K.avc * K.h * vr, (r2 + K.eta) * (0.5f * (T.v.w + a[7])));
-        px -= pi * gx;
-        py -= pi * gy;
-        pz -= pi * gz;
-    }
-    if (kArtp) {
-        const float wk = K.Cw * t * t * t * t * (q + 0.5f);
-        const float f = __fdividef(wk, K.wdr);
-        const float f4 = (f * f) * (f * f);
-        const float Rjx = b[0] > 0.f ? -K.eps * b[0] : 0.f;
-        const float Rjy = b[1] > 0.f ? -K.eps * b[1] : 0.f;
-        const float Rjz = b[2] > 0.f ? -K.eps * b[2] : 0.f;
-        px += (T.Rx + Rjx) * f4 * gx;
-        py += (T.Ry + Rjy) * f4 * gy;
-        pz += (T.Rz + Rjz) * f4 * gz;
-    }
-    ax += px;
-    ay += py;
-    az += pz;
-    const float Vj = K.m * __fdividef(1.0f, a[7]);
-    const float wx = Vj * vx, wy = Vj * vy, wz = Vj * vz;
-    T.l00 -= wx * gx; T.l01 -= wx * gy; T.l02 -= wx * gz;
-    T.l10 -= wy * gx; T.l11 -= wy * gy; T.l12 -= wy * gz;
-    T.l20 -= wz * gx; T.l21 -= wz * gy; T.l22 -= wz * gz;
-}
-
-/* The same pair gathering its record itself: the thread-per-target kernels
- * issue the four loads where the arithmetic needs them, which schedules
- * better there than a record gathered ahead. */
+/* One pair from the packed arrays, its density-rate and momentum terms
+ * added to (drho, ax, ay, az) and its velocity-gradient terms to T.  The
+ * viscosity term is always evaluated (K.avc is zero without viscosity), so
+ * a run of pairs has no branch between them; kArtp adds the artificial
+ * stress.  A pair of a particle with itself (the filler of a list's last
+ * group of four) adds exact zeros: r = 0 makes the kernel gradient zero. */
 template <bool kArtp>
 __device__ __forceinline__ void pair_terms(const PairConst& K, const NbrArrays& nb, Target& T, int j, float& drho,
                                            float& ax, float& ay, float& az)
@@ -648,378 +575,6 @@ __global__ void __launch_bounds__(kBlock) k_tile_fill(int nseg, int npb, int npm
     const int b = __ldg(seg_beg + w), n = __ldg(seg_len + w), o = __ldg(seg_off + w);
     for (int k = lane; k < n; k += 32)
         if (o + k < npm) order[o + k] = b + k - npb;
-}
-
-/* ------------------------------------------------------- twin targets */
-/* Twin form of the pair sums.  A thread owns two targets, consecutive
- * slots of one tile column (a twin), and walks one list that holds the
- * union of their neighbours: each neighbour's 52-byte record is gathered
- * once and serves both.  The thread-per-target kernel is bound by the L1
- * data pipe, whose work follows the bytes gathered (a warp's gathers are
- * already near-coalesced), and two neighbour spheres about one particle
- * spacing apart have a union of ~1.3 spheres, so a target costs ~0.65 of
- * the gathers for ~1.3 times the pair bodies.  An entry out of one target's
- * reach adds exact zeros to that target's sums (its kernel gradient is
- * zero), so each target's plain sums are the thread-per-target sums over
- * the same pairs in the same order.  A twin is coded 2 t + single: targets
- * npb + t and npb + t + 1, or the first alone (the last of a tile column of
- * odd length).  A twin whose two particles are not in one grid column
- * (only outside the lattice) walks both stencils instead of a list. */
-
-/* A position far from every particle: a list's filler entries get it, so
- * their pairs have a zero kernel gradient and add exact zeros to both
- * targets (r^2 stays finite). */
-constexpr float kFarAway = 1.0e18f;
-
-__device__ __forceinline__ void twin_targets(int code, int npb, int np, int& iA, int& iB, bool& single)
-{
-    iA = npb + (code >> 1);
-    single = (code & 1) != 0;
-    iB = single ? iA : iA + 1;
-    if (iB >= np) {
-        iB = iA;
-        single = true;
-    }
-}
-
-/* The sums of both targets over the union list (entry k at p[k * stride]),
- * in groups of four entries with the next group's entries fetched ahead;
- * the last group is filled up with entries placed far away. */
-template <bool kKahan, bool kArtp>
-__device__ __forceinline__ void twin_sums(const PairConst& K, const NbrArrays& nb, Target& A, Target& B, const int* p,
-                                          int n, int stride, int iA, int np)
-{
-    const size_t step4 = 4 * (size_t)stride;
-    int nxt[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) nxt[u] = u < n ? ld_list(p + u * stride) : iA;
-    for (int k = 0; k < n; k += 4) {
-        p += step4;
-        int cur[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            cur[u] = nxt[u];
-            nxt[u] = k + 4 + u < n ? ld_list(p + u * stride) : iA;
-        }
-        if (kKahan) {
-            float da = 0.f, xa = 0.f, ya = 0.f, za = 0.f, db = 0.f, xb = 0.f, yb = 0.f, zb = 0.f;
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                if (!lq_in_range(cur[u], np)) continue;
-                NbrRec r = fetch_rec(nb, cur[u]);
-                if (k + u >= n) r.xr.x = kFarAway;
-                pair_terms_rec<kArtp>(K, r, A, da, xa, ya, za);
-                pair_terms_rec<kArtp>(K, r, B, db, xb, yb, zb);
-            }
-            kahan_add(A.drho, A.cdrho, da);
-            kahan_add(A.ax, A.cax, xa);
-            kahan_add(A.ay, A.cay, ya);
-            kahan_add(A.az, A.caz, za);
-            kahan_add(B.drho, B.cdrho, db);
-            kahan_add(B.ax, B.cax, xb);
-            kahan_add(B.ay, B.cay, yb);
-            kahan_add(B.az, B.caz, zb);
-        } else {
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                if (!lq_in_range(cur[u], np)) continue;
-                NbrRec r = fetch_rec(nb, cur[u]);
-                if (k + u >= n) r.xr.x = kFarAway;
-                pair_terms_rec<kArtp>(K, r, A, A.drho, A.ax, A.ay, A.az);
-                pair_terms_rec<kArtp>(K, r, B, B.drho, B.ax, B.ay, B.az);
-            }
-        }
-    }
-}
-
-/* Pair sums of twins over their union lists from the packed neighbour
- * arrays; thread g takes twin twin[g] (tile order: a block is a compact box
- * of targets), and a twin whose list overflowed walks both targets'
- * stencils over the state arrays. */
-template <bool kKahan, int kThreads, int kMinBlocks>
-__global__ void __launch_bounds__(kThreads, kMinBlocks) k_interaction_twin(
-    const Parameters* __restrict__ P, int np, int npb, State st, Rates rt, Cells cells, const int* __restrict__ list,
-    const int* __restrict__ count, int stride, Frames fr, NbrArrays nb, const int* __restrict__ twin, int ncap)
-{
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= ncap) return;
-    const int code = __ldg(twin + g);
-    if (code < 0) return;
-    int iA, iB;
-    bool single;
-    twin_targets(code, npb, np, iA, iB, single);
-    if (!lq_in_range(iA, np)) return;
-    const PairConst K = load_pair_const(P);
-    Target A, B;
-    load_target(K, st, iA, true, A);
-    load_target(K, st, iB, true, B);
-    const int n = __ldg(count + g);
-    if (n <= LQ_TWIN_CAP) {
-        if (K.artp)
-            twin_sums<kKahan, true>(K, nb, A, B, list + g, n, stride, iA, np);
-        else
-            twin_sums<kKahan, false>(K, nb, A, B, list + g, n, stride, iA, np);
-    } else {
-        walk_stencil(P, K, st, cells, iA, A.x, [&](int j) { pair_body<kKahan>(K, st, A, j); }, fr);
-        if (!single) walk_stencil(P, K, st, cells, iB, B.x, [&](int j) { pair_body<kKahan>(K, st, B, j); }, fr);
-    }
-    store_rates(P, K, rt, iA, A);
-    if (!single) store_rates(P, K, rt, iB, B);
-}
-
-/* Union lists of twins: list[k * stride + g] is the k-th entry of twin g,
- * count[g] their number (LQ_TWIN_CAP + 1 marks a twin that walks its
- * stencils instead: an overflowed union, or two particles that are not in
- * one grid column), hits[g] the two targets' own neighbour counts (low and
- * high 16 bits).  The walk is k_neighbor_list's: lanes grouped by grid
- * column walk the union of their stencils in lockstep; a candidate is kept
- * when it lies within the cut-off of either target, so both targets'
- * neighbours appear in the order of their own lists. */
-__global__ void __launch_bounds__(kBlock) k_neighbor_list_twin(const Parameters* __restrict__ P, int npb, int np,
-                                                               int ncap, const int* __restrict__ twin, float cut2,
-                                                               const float4* __restrict__ pos, Cells cells,
-                                                               int* __restrict__ list, int* __restrict__ count_out,
-                                                               int* __restrict__ hits_out, int stride,
-                                                               int* __restrict__ health,
-                                                               const float4* __restrict__ idep, Frames fr)
-{
-    __shared__ int stage[kListWarps][kStage][32];
-    const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    const int code = g < ncap ? __ldg(twin + g) : -1;
-    int iA = 0, iB = 0;
-    bool single = true;
-    if (code >= 0) twin_targets(code, npb, np, iA, iB, single);
-    bool active = code >= 0 && lq_in_range(iA, np);
-    const PairConst K = load_pair_const(P);
-    const int nx = __ldg(&P->cell_num_x), ny = __ldg(&P->cell_num_y), nz = __ldg(&P->cell_num_z);
-    const int L = __ldg(&P->ncell_one_layer);
-    const int np_all = __ldg(&P->np);
-    const float4 xA = active ? __ldg(pos + iA) : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 xB = active ? __ldg(pos + iB) : xA;
-    int* my_stage = &stage[w][0][lane];
-
-    int staged = 0, total = 0, hA = 0, hB = 0;
-    auto flush = [&]() {
-        const int maxc = (int)__reduce_max_sync(FULL, (unsigned)staged);
-        for (int k = 0; k < maxc; ++k)
-            if (k < staged && total + k < LQ_TWIN_CAP) list[(size_t)(total + k) * stride + g] = my_stage[32 * k];
-        total += staged;
-        staged = 0;
-        __syncwarp();
-    };
-    auto test = [&](bool mine, const float4& xj, int j) {
-        const float ax = xA.x - xj.x, ay = xA.y - xj.y, az = xA.z - xj.z;
-        const float bx = xB.x - xj.x, by = xB.y - xj.y, bz = xB.z - xj.z;
-        const bool ha = mine && ax * ax + ay * ay + az * az < cut2;
-        const bool hb = mine && !single && bx * bx + by * by + bz * bz < cut2;
-        if (ha || hb) {
-            my_stage[32 * staged] = j;
-            ++staged;
-        }
-        hA += ha;
-        hB += hb;
-    };
-
-    /* the z cells both cut-off spheres reach, as in k_neighbor_list */
-    const float cut = sqrtf(cut2);
-    int cx = 0, cy = 0, czl = 0, czh = 0;
-    bool split = false;
-    if (active) {
-        cx = stencil_axis(xA.x, K.ih);
-        cy = stencil_axis(xA.y, K.ih);
-        czl = min(stencil_axis(xA.z - cut, K.ih), stencil_axis(xB.z - cut, K.ih));
-        czh = max(stencil_axis(xA.z + cut, K.ih), stencil_axis(xB.z + cut, K.ih));
-        int cyB = stencil_axis(xB.y, K.ih);
-        if (fr.rows) {
-            cy = frame_stencil_row(fr, __ldg(&idep[iA].x), cy);
-            cyB = frame_stencil_row(fr, __ldg(&idep[iB].x), cyB);
-        }
-        split = !single && (stencil_axis(xB.x, K.ih) != cx || cyB != cy);
-        if (split) active = false;
-    }
-    unsigned todo = __ballot_sync(FULL, active);
-    while (todo) {
-        const int leader = __ffs(todo) - 1;
-        const int gx = __shfl_sync(FULL, cx, leader), gy = __shfl_sync(FULL, cy, leader);
-        const bool mine = active && cx == gx && cy == gy;
-        todo &= ~__ballot_sync(FULL, mine);
-        const int zmin = __reduce_min_sync(FULL, mine ? czl : INT_MAX);
-        const int zmax = __reduce_max_sync(FULL, mine ? czh : INT_MIN);
-        const int zlo = max(zmin, 0), zhi = min(zmax, nz - 1);
-        if (zlo > zhi) continue;
-        for (int layer = 0; layer < 2; ++layer) {
-            const int off = layer ? L : 0;
-            for (int col = 0; col < 9; ++col) {
-                const int X = gx + (col % 3) - 1, Y = gy + (col / 3) - 1;
-                if (X < 0 || X >= nx || Y < 0 || Y >= ny) continue;
-                int s, e;
-                if (!zrun_range(cells, off + (X * ny + Y) * nz, zlo, zhi, s, e)) continue;
-                if (!lq_in_range(s, np_all) || !lq_in_range(e - 1, np_all)) continue;
-                int j = s;
-                for (; j + kUnroll <= e; j += kUnroll) {
-                    if (__any_sync(FULL, staged > kStage - kUnroll)) flush();
-                    float4 xj[kUnroll];
-#pragma unroll
-                    for (int u = 0; u < kUnroll; ++u) xj[u] = __ldg(pos + j + u);
-#pragma unroll
-                    for (int u = 0; u < kUnroll; ++u) test(mine, xj[u], j + u);
-                }
-                if (__any_sync(FULL, staged > kStage - kUnroll)) flush();
-                for (; j < e; ++j) test(mine, __ldg(pos + j), j);
-            }
-        }
-    }
-    flush();
-    if (g < ncap) {
-        count_out[g] = split ? LQ_TWIN_CAP + 1 : total;
-        hits_out[g] = (min(hB, 0xffff) << 16) | min(hA, 0xffff);
-        if (total > LQ_TWIN_CAP && health) atomicAdd(health + HEALTH_NBR_OVERFLOW, 1);
-    }
-}
-
-/* The twin order: the tile order's segments (tile columns) cut into twins
- * of consecutive slots, the last one alone when a segment's length is odd. */
-__global__ void __launch_bounds__(kBlock) k_twin_segments(const int* __restrict__ start, TileGrid tg, int npb, int np,
-                                                          int* __restrict__ seg_beg, int* __restrict__ seg_len,
-                                                          int* __restrict__ seg_cnt)
-{
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= tg.nseg) return;
-    int b, len;
-    tile_segment(tg, start, npb, np, s, &b, &len);
-    seg_beg[s] = b;
-    seg_len[s] = len;
-    seg_cnt[s] = (len + 1) >> 1;
-}
-
-/* One warp per segment writes its twins at the segment's offset. */
-__global__ void __launch_bounds__(kBlock) k_twin_fill(int nseg, int npb, int ncap, const int* __restrict__ seg_beg,
-                                                      const int* __restrict__ seg_len,
-                                                      const int* __restrict__ seg_off, int* __restrict__ twin)
-{
-    const int w = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-    if (w >= nseg) return;
-    const int b = __ldg(seg_beg + w), len = __ldg(seg_len + w), o = __ldg(seg_off + w);
-    const int nt = (len + 1) >> 1;
-    for (int k = lane; k < nt; k += 32)
-        if (o + k < ncap) twin[o + k] = 2 * (b - npb + 2 * k) + (2 * k + 1 == len ? 1 : 0);
-}
-
-/* Shepard stress filter and density filter over the twins' union lists
- * (each target's own neighbours, boundary ones skipped, self included; an
- * entry beyond 2h of a target is skipped for it by the exact q < 2 test). */
-__global__ void __launch_bounds__(kBlock) k_shepard_twin(const Parameters* __restrict__ P, int np, int npb, State st,
-                                                         tensor2d* __restrict__ out_str, const int* __restrict__ twin,
-                                                         int ncap, const int* __restrict__ list,
-                                                         const int* __restrict__ count, int stride, Cells cells,
-                                                         Frames fr)
-{
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= ncap) return;
-    const int code = __ldg(twin + g);
-    if (code < 0) return;
-    int iA, iB;
-    bool single;
-    twin_targets(code, npb, np, iA, iB, single);
-    const float ih = __ldg(&P->i_h), m = __ldg(&P->m), Cw = __ldg(&P->kernel_normalization_par);
-    const float4 xA = __ldg(st.pos + iA), xB = __ldg(st.pos + iB);
-    tensor2d SA = make_tensor2d(0.0f), SB = make_tensor2d(0.0f);
-    float wA = 0.0f, wB = 0.0f;
-    auto add = [&](int j, const float4& xi, tensor2d& S, float& w) {
-        if (j < npb || !lq_in_range(j, np)) return;
-        const float4 xj = __ldg(st.pos + j);
-        const float3 d = make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
-        const float q = norm3df(d.x, d.y, d.z) * ih;
-        if (q < 2.0f) {
-            const float ker = Cw * (2.0f - q) * (2.0f - q) * (2.0f - q) * (2.0f - q) * (q + 0.5f);
-            const float vol = m / __ldg(&st.vel[j].w);
-            const tensor2d sj = load_t2(st.str, j);
-            S.xx += sj.xx * ker * vol;
-            S.yy += sj.yy * ker * vol;
-            S.zz += sj.zz * ker * vol;
-            S.xy += sj.xy * ker * vol;
-            S.xz += sj.xz * ker * vol;
-            S.yz += sj.yz * ker * vol;
-            w += ker * vol;
-        }
-    };
-    const int n = __ldg(count + g);
-    if (n <= LQ_TWIN_CAP) {
-        for (int k = 0; k < n; ++k) {
-            const int j = __ldg(list + (size_t)k * stride + g);
-            add(j, xA, SA, wA);
-            if (!single) add(j, xB, SB, wB);
-        }
-    } else {
-        const PairConst K = load_pair_const(P);
-        add(iA, xA, SA, wA);
-        walk_stencil(P, K, st, cells, iA, xA, [&](int j) { add(j, xA, SA, wA); }, fr);
-        if (!single) {
-            add(iB, xB, SB, wB);
-            walk_stencil(P, K, st, cells, iB, xB, [&](int j) { add(j, xB, SB, wB); }, fr);
-        }
-    }
-    for (int q = 0; q < (single ? 1 : 2); ++q) {
-        tensor2d S = q ? SB : SA;
-        const float w = q ? wB : wA;
-        S.xx /= w;
-        S.yy /= w;
-        S.zz /= w;
-        S.xy /= w;
-        S.xz /= w;
-        S.yz /= w;
-        store_t2(out_str, q ? iB : iA, S);
-    }
-}
-
-__global__ void __launch_bounds__(kBlock) k_density_filter_twin(const Parameters* __restrict__ P, int np, int npb,
-                                                                State st, float* __restrict__ rho_out,
-                                                                const int* __restrict__ twin, int ncap,
-                                                                const int* __restrict__ list,
-                                                                const int* __restrict__ count, int stride,
-                                                                Cells cells, Frames fr)
-{
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= ncap) return;
-    const int code = __ldg(twin + g);
-    if (code < 0) return;
-    int iA, iB;
-    bool single;
-    twin_targets(code, npb, np, iA, iB, single);
-    const float ih = __ldg(&P->i_h), m = __ldg(&P->m), Cw = __ldg(&P->kernel_normalization_par);
-    const float4 xA = __ldg(st.pos + iA), xB = __ldg(st.pos + iB);
-    float numA = 0.0f, denA = 0.0f, numB = 0.0f, denB = 0.0f;
-    auto add = [&](int j, const float4& xi, float& num, float& den) {
-        if (j < npb || !lq_in_range(j, np)) return;
-        const float4 xj = __ldg(st.pos + j);
-        const float3 d = make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
-        const float q = norm3df(d.x, d.y, d.z) * ih;
-        if (q < 2.0f) {
-            const float ker = Cw * (2.0f - q) * (2.0f - q) * (2.0f - q) * (2.0f - q) * (q + 0.5f);
-            num += m * ker;
-            den += ker * (m / __ldg(&st.vel[j].w));
-        }
-    };
-    const int n = __ldg(count + g);
-    if (n <= LQ_TWIN_CAP) {
-        for (int k = 0; k < n; ++k) {
-            const int j = __ldg(list + (size_t)k * stride + g);
-            add(j, xA, numA, denA);
-            if (!single) add(j, xB, numB, denB);
-        }
-    } else {
-        const PairConst K = load_pair_const(P);
-        add(iA, xA, numA, denA);
-        walk_stencil(P, K, st, cells, iA, xA, [&](int j) { add(j, xA, numA, denA); }, fr);
-        if (!single) {
-            add(iB, xB, numB, denB);
-            walk_stencil(P, K, st, cells, iB, xB, [&](int j) { add(j, xB, numB, denB); }, fr);
-        }
-    }
-    rho_out[iA] = numA / denA;
-    if (!single) rho_out[iB] = numB / denB;
 }
 
 /* Warp-cooperative form: a group of G lanes (G = 8 or 32) shares one
@@ -1395,11 +950,7 @@ const int kPairShapes[kPairShapeCount][3] = {{kBlock, LQ_PAIR_MIN_BLOCKS, 0},
                                              {768, 1, 1},
                                              {384, 2, 1},
                                              {640, 1, 1},
-                                             {320, 2, 1},
-                                             {256, 2, 2},
-                                             {512, 1, 2},
-                                             {384, 1, 2},
-                                             {128, 4, 2}};
+                                             {320, 2, 1}};
 
 /* The native driver's launch shape before any tuning: the tiled 640 x 1
  * shape once the targets fill at least four waves of 640-thread blocks on
@@ -1445,103 +996,6 @@ static NbrArrays nbr_arrays(float* rec, int np)
     const size_t n = (size_t)np;
     return NbrArrays{reinterpret_cast<float4*>(rec), reinterpret_cast<float4*>(rec) + n,
                      reinterpret_cast<float4*>(rec) + 2 * n, rec + 12 * n};
-}
-
-/* Tile height of a twin shape: its blocks hold two targets per thread. */
-static int twin_tile_height(const Parameters* ph, int shape)
-{
-    return tile_height(ph, 2 * kPairShapes[shape][0]);
-}
-
-int twin_capacity(const Parameters* ph, int shape)
-{
-    if (!twin_shape(shape) || ph->npm <= 0) return 0;
-    /* at most one odd twin per non-empty segment, and no more twins than targets */
-    const long long nseg = tile_grid_of(ph, twin_tile_height(ph, shape)).nseg;
-    const long long c = ((long long)ph->npm + nseg + 1) / 2;
-    return (int)(c < ph->npm ? c : ph->npm);
-}
-
-int launch_twin_order(const Parameters* ph, const int* start, int shape, const TileOrder& to, const TwinLists& tw,
-                      cudaStream_t s)
-{
-    if (!twin_shape(shape) || ph->npm <= 0) return LQ_OK;
-    if (!to.seg || !tw.twin) return set_error(LQ_ERR_ARG, "twin order: buffers not allocated");
-    const TileGrid tg = tile_grid_of(ph, twin_tile_height(ph, shape));
-    const int nseg = tg.nseg;
-    if (nseg > to.nseg_cap) return set_error(LQ_ERR_ARG, "twin order: %d segments > capacity %d", nseg, to.nseg_cap);
-    const int cap = twin_capacity(ph, shape);
-    if (cap > tw.cap) return set_error(LQ_ERR_ARG, "twin order: %d twins > capacity %d", cap, tw.cap);
-    int* beg = to.seg;
-    int* len = to.seg + to.nseg_cap;
-    int* off = to.seg + 2 * (size_t)to.nseg_cap;
-    int* cnt = to.seg + 3 * (size_t)to.nseg_cap;
-    k_twin_segments<<<blocks_for(nseg, kBlock), kBlock, 0, s>>>(start, tg, ph->npb, ph->np, beg, len, cnt);
-    LQ_TRY_CUDA(cudaGetLastError(), "k_twin_segments");
-    size_t bytes = to.scan_bytes;
-    LQ_TRY_CUDA(cub::DeviceScan::ExclusiveSum(to.scan_tmp, bytes, cnt, off, nseg, s), "twin scan");
-    LQ_TRY(fill_int(tw.twin, tw.cap, -1, s));
-    k_twin_fill<<<blocks_for(nseg, kBlock / 32), kBlock, 0, s>>>(nseg, ph->npb, tw.cap, beg, len, off, tw.twin);
-    LQ_TRY_CUDA(cudaGetLastError(), "k_twin_fill");
-    return LQ_OK;
-}
-
-int launch_neighbor_list_twin(const Parameters* ph, const Parameters* pd, float cut, const float4* pos, const Cells& c,
-                              const TwinLists& tw, int* health, cudaStream_t s, const float4* idep, const Frames& fr)
-{
-    if (fr.rows && !idep) return set_error(LQ_ERR_ARG, "twin lists: frames need the idep array");
-    if (ph->npm <= 0 || tw.cap <= 0) return LQ_OK;
-    if (tw.stride < tw.cap) return set_error(LQ_ERR_ARG, "twin lists: stride %d < capacity %d", tw.stride, tw.cap);
-    k_neighbor_list_twin<<<blocks_for(tw.cap, kBlock), kBlock, 0, s>>>(pd, ph->npb, ph->np, tw.cap, tw.twin,
-                                                                      cut * cut, pos, c, tw.list, tw.count, tw.hits,
-                                                                      tw.stride, health, idep, fr);
-    LQ_TRY_CUDA(cudaGetLastError(), "k_neighbor_list_twin");
-    return LQ_OK;
-}
-
-int launch_interaction_twin(const Parameters* ph, const Parameters* pd, const State& st, const Rates& r,
-                            const Cells& c, const TwinLists& tw, cudaStream_t s, const Frames& fr, bool compensated,
-                            float* rec, int shape)
-{
-    if (ph->npm <= 0) return LQ_OK;
-    if (!twin_shape(shape)) return set_error(LQ_ERR_ARG, "interaction: shape %d is not a twin shape", shape);
-    if (!rec || reinterpret_cast<uintptr_t>(rec) % 16 != 0)
-        return set_error(LQ_ERR_ARG, "interaction: packed neighbour arrays missing or not 16-byte aligned");
-    const NbrArrays nb = nbr_arrays(rec, ph->np);
-#define LQ_TWIN_LAUNCH(T, B)                                                                                      \
-    (compensated ? k_interaction_twin<true, T, B><<<blocks_for(tw.cap, T), T, 0, s>>>(                              \
-                       pd, ph->np, ph->npb, st, r, c, tw.list, tw.count, tw.stride, fr, nb, tw.twin, tw.cap)        \
-                 : k_interaction_twin<false, T, B><<<blocks_for(tw.cap, T), T, 0, s>>>(                             \
-                       pd, ph->np, ph->npb, st, r, c, tw.list, tw.count, tw.stride, fr, nb, tw.twin, tw.cap))
-    switch (shape) {
-        case 11: LQ_TWIN_LAUNCH(256, 2); break;
-        case 12: LQ_TWIN_LAUNCH(512, 1); break;
-        case 13: LQ_TWIN_LAUNCH(384, 1); break;
-        default: LQ_TWIN_LAUNCH(128, 4); break;
-    }
-#undef LQ_TWIN_LAUNCH
-    LQ_TRY_CUDA(cudaGetLastError(), "k_interaction_twin");
-    return LQ_OK;
-}
-
-int launch_shepard_twin(const Parameters* ph, const Parameters* pd, const State& st, tensor2d* out_str,
-                        const TwinLists& tw, const Cells& c, cudaStream_t s, const Frames& fr)
-{
-    if (ph->npm <= 0 || tw.cap <= 0) return LQ_OK;
-    k_shepard_twin<<<blocks_for(tw.cap, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, out_str, tw.twin, tw.cap,
-                                                                tw.list, tw.count, tw.stride, c, fr);
-    LQ_TRY_CUDA(cudaGetLastError(), "k_shepard_twin");
-    return LQ_OK;
-}
-
-int launch_density_filter_twin(const Parameters* ph, const Parameters* pd, const State& st, float* rho_out,
-                               const TwinLists& tw, const Cells& c, cudaStream_t s, const Frames& fr)
-{
-    if (ph->npm <= 0 || tw.cap <= 0) return LQ_OK;
-    k_density_filter_twin<<<blocks_for(tw.cap, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, rho_out, tw.twin,
-                                                                       tw.cap, tw.list, tw.count, tw.stride, c, fr);
-    LQ_TRY_CUDA(cudaGetLastError(), "k_density_filter_twin");
-    return LQ_OK;
 }
 
 int launch_tile_order(const Parameters* ph, const int* start, int shape, const TileOrder& to, cudaStream_t s)
@@ -1639,7 +1093,6 @@ int launch_interaction_list(const Parameters* ph, const Parameters* pd, const St
             k_pack_neighbors<<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(0, ph->np, st, nb);
             LQ_TRY_CUDA(cudaGetLastError(), "k_pack_neighbors");
         }
-        if (twin_shape(shape)) return set_error(LQ_ERR_ARG, "interaction: twin shape %d needs the twin lists", shape);
         if (shape >= 0 && shape < kPairShapeCount && kPairShapes[shape][2] == 1 && !order)
             return set_error(LQ_ERR_ARG, "interaction: launch shape %d needs the tile order", shape);
         if (shape < 0 || shape >= kPairShapeCount || kPairShapes[shape][2] != 1) order = nullptr;
@@ -1729,7 +1182,7 @@ constexpr int kDropInShape = 9;
 
 /* Working arrays of the drop-in interaction, one set per device: the cell
  * starts derived from the caller's cell_beg / cell_end, the pair kernel's
- * target order (tile or twin order) with its scratch, the neighbour lists
+ * tile order with its scratch, the neighbour lists
  * and the packed neighbour data.  lq_interaction_reserve sizes them from a
  * Parameters record (the drop-in LoquatGrid's GridConfig calls it, where
  * the reference allocates its arrays); a call that needs more than was
@@ -1737,14 +1190,13 @@ constexpr int kDropInShape = 9;
  * arrays are freed.  Calls that overlap on the GPU share the arrays and
  * must not. */
 struct DropInWorkspace {
-    int np = 0, ncell = 0, nseg = 0, npm = 0, twin_cap = 0;
+    int np = 0, ncell = 0, nseg = 0, npm = 0;
     int* start = nullptr;           /* ncell + 1 cell starts */
     int* counts = nullptr;          /* ncell + 1 particles per cell */
     void* scan_tmp = nullptr;       /* cell-start scan */
     size_t scan_bytes = 0;
-    lqb::TileOrder to;              /* tile order (tiled shape) or segment scratch (twin shape) */
-    lqb::NeighborList nl;           /* thread-per-target lists (tiled shape) */
-    lqb::TwinLists tw;              /* union lists (twin shape) */
+    lqb::TileOrder to;              /* tile order and its segment scratch */
+    lqb::NeighborList nl;           /* material targets' lists */
     float* rec = nullptr;           /* packed neighbour data, 13 floats per particle */
     std::vector<void*> allocs;
 };
@@ -1774,8 +1226,7 @@ int size_workspace(DropInWorkspace& w, const Parameters* ph)
     size_t seg_scan = 0, cell_scan = 0;
     LQ_TRY(lqb::tile_order_scratch(ph, &nseg, &seg_scan));
     LQ_TRY(lqb::scan_scratch_bytes(ncell, &cell_scan));
-    const int cap = lqb::twin_shape(kDropInShape) ? lqb::twin_capacity(ph, kDropInShape) : 0;
-    if (np <= w.np && ncell <= w.ncell && nseg <= w.nseg && npm <= w.npm && cap <= w.twin_cap && w.rec) return LQ_OK;
+    if (np <= w.np && ncell <= w.ncell && nseg <= w.nseg && npm <= w.npm && w.rec) return LQ_OK;
     if (!w.allocs.empty()) LQ_TRY_CUDA(cudaDeviceSynchronize(), "interaction workspace");
     free_workspace(w);
     DropInWorkspace n;
@@ -1787,24 +1238,15 @@ int size_workspace(DropInWorkspace& w, const Parameters* ph)
     A((void**)&n.counts, sizeof(int) * ((size_t)ncell + 1));
     A(&n.scan_tmp, cell_scan);
     n.scan_bytes = cell_scan;
-    A((void**)&n.to.seg, sizeof(int) * 4 * (size_t)nseg);
+    A((void**)&n.to.seg, sizeof(int) * 3 * (size_t)nseg);
     A(&n.to.scan_tmp, seg_scan);
     n.to.nseg_cap = nseg;
     n.to.scan_bytes = seg_scan;
     A((void**)&n.rec, sizeof(float) * 13 * (size_t)np);
-    if (lqb::twin_shape(kDropInShape)) {
-        n.tw.cap = cap;
-        n.tw.stride = (cap + 31) / 32 * 32;
-        A((void**)&n.tw.twin, sizeof(int) * (size_t)(cap > 0 ? cap : 1));
-        A((void**)&n.tw.list, sizeof(int) * (size_t)LQ_TWIN_CAP * n.tw.stride);
-        A((void**)&n.tw.count, sizeof(int) * (size_t)n.tw.stride);
-        A((void**)&n.tw.hits, sizeof(int) * (size_t)n.tw.stride);
-    } else {
-        n.nl.stride = (npm + 31) / 32 * 32;
-        A((void**)&n.nl.list, sizeof(int) * (size_t)LQ_NBR_CAP * n.nl.stride);
-        A((void**)&n.nl.count, sizeof(int) * (size_t)n.nl.stride);
-        A((void**)&n.to.order, sizeof(int) * (size_t)npm);
-    }
+    n.nl.stride = (npm + 31) / 32 * 32;
+    A((void**)&n.nl.list, sizeof(int) * (size_t)LQ_NBR_CAP * n.nl.stride);
+    A((void**)&n.nl.count, sizeof(int) * (size_t)n.nl.stride);
+    A((void**)&n.to.order, sizeof(int) * (size_t)npm);
     if (st != LQ_OK) {
         free_workspace(n);
         return st;
@@ -1813,7 +1255,6 @@ int size_workspace(DropInWorkspace& w, const Parameters* ph)
     n.ncell = ncell;
     n.nseg = nseg;
     n.npm = npm;
-    n.twin_cap = cap;
     w = std::move(n);
     return LQ_OK;
 }
@@ -1860,11 +1301,10 @@ extern "C" int lq_interaction_reserve(const void* par_host)
 /* The reference's ParticleInteraction (src/particle_interaction.h:27-40).
  * The caller's grid (cell_beg / cell_end: every particle sorted into its
  * cell, cells in key order) gives the cell starts; the material targets
- * are ordered into compact tiles (twins of two consecutive targets for a
- * twin shape), their neighbours within 2h are found by the 27-cell walk in
- * the reference's visiting order into lists, and the pair kernel sums over
- * the lists from the packed neighbour data, in plain FP32 as the
- * reference computes. */
+ * are ordered into compact tiles, their neighbours within 2h are found by
+ * the 27-cell walk in the reference's visiting order into lists, and the
+ * pair kernel sums over the lists from the packed neighbour data, in plain
+ * FP32 as the reference computes. */
 extern "C" int lq_particle_interaction(const void* par_host, const void* par_device, const float* pospres,
                                        const float* velrhop, const float* idep, const float* str, const float* stn,
                                        float* accad, float* spin, float* acestn, const int* cell_beg,
@@ -1891,12 +1331,6 @@ extern "C" int lq_particle_interaction(const void* par_host, const void* par_dev
     /* the pair body's own cut-off test: q < 2 with the candidate slack of
      * the cell walk */
     const float cut = 2.0f * ph->h * sqrtf(1.0001f);
-    if (lqb::twin_shape(kDropInShape)) {
-        LQ_TRY(lqb::launch_twin_order(ph, w->start, kDropInShape, w->to, w->tw, s));
-        LQ_TRY(lqb::launch_neighbor_list_twin(ph, pd, cut, st.pos, c, w->tw, nullptr, s));
-        LQ_TRY(lqb::launch_pack_neighbors(ph, st, w->rec, 0, s));
-        return lqb::launch_interaction_twin(ph, pd, st, r, c, w->tw, s, lqb::Frames(), false, w->rec, kDropInShape);
-    }
     LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, ph->npb, ph->npm, 0, cut, st.pos, c, w->nl, nullptr, s));
     LQ_TRY(lqb::launch_tile_order(ph, w->start, kDropInShape, w->to, s));
     return lqb::launch_interaction_list(ph, pd, st, r, c, w->nl, s, lqb::Frames(), false, w->rec, kDropInShape, true,

@@ -28,7 +28,7 @@ def test_all_pair_kernel_shapes_agree_bit_for_bit(lq, cuda):
         for x, y in zip(out[0], other):
             assert np.array_equal(x, y)
     with pytest.raises(lq.LoquatError):
-        s.set_pair_shape(15)
+        s.set_pair_shape(11)
 
 
 @pytest.mark.parametrize("shape", [7, 8, 9, 10])
@@ -114,7 +114,7 @@ def test_autotune_leaves_the_state_and_matches_a_fresh_run(lq, cuda):
     a.step(11)
     before, clock = a.download(), a.clock()
     shape, skin = a.autotune(steps=8)
-    assert 0 <= shape < 15
+    assert 0 <= shape < 11
     assert min(abs(skin - f) for f in (0.02, 0.05, 0.1, 0.2)) < 1e-6
     for x, y in zip(before, a.download()):
         assert np.array_equal(x, y)
