@@ -104,6 +104,16 @@ int lq_grid_neighbor_search_noalloc(const void* par_host, const void* par_device
  * synchronising the device first). */
 int lq_interaction_reserve(const void* par_host);
 
+/* How often lq_particle_interaction on the current device built its
+ * neighbour lists afresh and how often it carried them over from an
+ * earlier call.  No counterpart in the reference.  Lists are carried when
+ * the cell_beg passed belongs to a grid of this library (lq_grid_* or the
+ * drop-in LoquatGrid), whose searches track each particle's identity,
+ * the caller has re-sorted its arrays after each search (as the reference
+ * does), and no particle has moved half a skin of 0.05 h since the build;
+ * the grid's searches and the interaction must run on one stream. */
+int lq_interaction_stats(long long* rebuilds, long long* reuses);
+
 /* reference src/particle_interaction.h:27-40 */
 int lq_particle_interaction(const void* par_host, const void* par_device,
                             const float* pospres, const float* velrhop, const float* idep,

@@ -54,6 +54,7 @@ _SIGNATURES = {
     "lq_grid_sort_tensor2d": (_I, [_VP, _I, _VP, _VP, _VP]),
     "lq_grid_neighbor_search_noalloc": (_I, [_VP] * 8),
     "lq_interaction_reserve": (_I, [_VP]),
+    "lq_interaction_stats": (_I, [ctypes.POINTER(_LL), ctypes.POINTER(_LL)]),
     "lq_particle_interaction": (_I, [_VP] * 13),
     "lq_adami_boundary": (_I, [_VP] * 8),
     "lq_stress_regularization": (_I, [_VP] * 9),
@@ -169,6 +170,14 @@ def interaction_reserve(par_host) -> None:
     """lq_interaction_reserve: sizes particle_interaction's working arrays
     for par_host's particle and cell counts, once, before a step loop."""
     check(lib().lq_interaction_reserve(ptr(par_host)), "lq_interaction_reserve")
+
+
+def interaction_stats():
+    """lq_interaction_stats: (fresh list builds, calls that carried the
+    lists over) of particle_interaction on the current device."""
+    a, b = _LL(), _LL()
+    check(lib().lq_interaction_stats(ctypes.byref(a), ctypes.byref(b)), "lq_interaction_stats")
+    return a.value, b.value
 
 
 def particle_interaction(par_host, par_dev, pospres, velrhop, idep, str_, stn, accad, spin, acestn,

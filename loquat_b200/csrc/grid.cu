@@ -21,6 +21,10 @@
  */
 #include <cstdio>
 #include <cstdlib>
+#include <mutex>
+#include <unordered_map>
+#include <utility>
+
 #include <cub/device/device_scan.cuh>
 
 #include "lq_internal.cuh"
@@ -247,6 +251,102 @@ int bounds_count_grid(unsigned long long* v)
     return LQ_OK;
 }
 
+/* --------------------------------------------- identities of the grids */
+namespace {
+
+struct IdentityRecord {
+    int* ident = nullptr;
+    int* tmp = nullptr;
+    int np = 0;
+    long long gen = 0;
+};
+std::mutex g_id_mu;
+std::unordered_map<const int*, IdentityRecord> g_ids;
+long long g_id_gen = 0;
+
+__global__ void __launch_bounds__(kBlock) k_iota(int n, int* __restrict__ p)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = i;
+}
+
+__global__ void __launch_bounds__(kBlock) k_follow(int n, const int* __restrict__ part_idx,
+                                                   const int* __restrict__ in, int* __restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int j = __ldg(part_idx + i);
+    out[i] = lq_in_range(j, n) ? __ldg(in + j) : -1;
+}
+
+}  // namespace
+
+int identity_reset(const int* key, int np)
+{
+    std::lock_guard<std::mutex> lock(g_id_mu);
+    IdentityRecord& r = g_ids[key];
+    if (r.np != np || !r.ident) {
+        cudaFree(r.ident);
+        cudaFree(r.tmp);
+        r = IdentityRecord{};
+        const size_t b = sizeof(int) * (size_t)(np > 0 ? np : 1);
+        cudaError_t e = cudaMalloc((void**)&r.ident, b);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&r.tmp, b);
+        if (e != cudaSuccess) {
+            cudaFree(r.ident);
+            cudaFree(r.tmp);
+            g_ids.erase(key);
+            return set_error(LQ_ERR_ALLOC, "grid identities: %s", cudaGetErrorString(e));
+        }
+        r.np = np;
+    }
+    r.gen = ++g_id_gen;
+    if (np > 0) {
+        k_iota<<<blocks_for(np), kBlock>>>(np, r.ident);
+        LQ_TRY_CUDA(cudaGetLastError(), "k_iota");
+    }
+    return LQ_OK;
+}
+
+int identity_after_search(const int* key, const int* part_idx, int np, cudaStream_t s)
+{
+    std::lock_guard<std::mutex> lock(g_id_mu);
+    auto it = g_ids.find(key);
+    if (it == g_ids.end()) return LQ_OK;
+    IdentityRecord& r = it->second;
+    if (np != r.np) {
+        /* a search over another particle count: identities restart */
+        r.gen = ++g_id_gen;
+        if (np > r.np || np <= 0) return LQ_OK;
+    }
+    if (np <= 0) return LQ_OK;
+    k_follow<<<blocks_for(np), kBlock, 0, s>>>(np, part_idx, r.ident, r.tmp);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_follow");
+    std::swap(r.ident, r.tmp);
+    return LQ_OK;
+}
+
+void identity_release(const int* key)
+{
+    std::lock_guard<std::mutex> lock(g_id_mu);
+    auto it = g_ids.find(key);
+    if (it == g_ids.end()) return;
+    cudaFree(it->second.ident);
+    cudaFree(it->second.tmp);
+    g_ids.erase(it);
+}
+
+bool identity_find(const int* key, GridIdentity* out)
+{
+    std::lock_guard<std::mutex> lock(g_id_mu);
+    auto it = g_ids.find(key);
+    if (it == g_ids.end() || !it->second.ident) return false;
+    out->ident = it->second.ident;
+    out->np = it->second.np;
+    out->gen = it->second.gen;
+    return true;
+}
+
 int gather_state(int n, const int* idx, const State& in, const State& out, cudaStream_t s)
 {
     if (n <= 0) return LQ_OK;
@@ -267,6 +367,7 @@ struct LqGrid {
 
 void free_grid_buffers(lqb::GridBuffers& g)
 {
+    if (g.beg) lqb::identity_release(g.beg);
     cudaFree(g.key);
     cudaFree(g.rank);
     cudaFree(g.count);
@@ -302,7 +403,7 @@ int alloc_grid_buffers(lqb::GridBuffers& g, int np, int ncell)
     }
     g.np_cap = np;
     g.ncell_cap = ncell;
-    return LQ_OK;
+    return lqb::identity_reset(g.beg, np);
 }
 
 }  // namespace
@@ -343,9 +444,10 @@ extern "C" int lq_grid_neighbor_search(void* grid, const void* par_host, const v
     if (!grid || !par_host || !par_device || (!pospres && static_cast<const Parameters*>(par_host)->np > 0))
         return lqb::set_error(LQ_ERR_ARG, "lq_grid_neighbor_search: null argument");
     LqGrid* G = static_cast<LqGrid*>(grid);
-    return lqb::grid_search(static_cast<const Parameters*>(par_host), static_cast<const Parameters*>(par_device),
-                            reinterpret_cast<const float4*>(pospres), G->g, true, nullptr,
-                            static_cast<cudaStream_t>(stream));
+    const Parameters* ph = static_cast<const Parameters*>(par_host);
+    LQ_TRY(lqb::grid_search(ph, static_cast<const Parameters*>(par_device), reinterpret_cast<const float4*>(pospres),
+                            G->g, true, nullptr, static_cast<cudaStream_t>(stream)));
+    return lqb::identity_after_search(G->g.beg, G->g.part_idx, ph->np, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int lq_grid_arrays(void* grid, const int** part_cel, const int** part_idx, const int** cell_beg,
@@ -411,6 +513,7 @@ LoquatGrid::LoquatGrid()
 
 LoquatGrid::~LoquatGrid()
 {
+    if (cell_beg) lqb::identity_release(cell_beg);
     cudaFree(part_cel);
     cudaFree(part_idx);
     cudaFree(cell_beg);
@@ -434,6 +537,7 @@ void LoquatGrid::ResizeArrayLength(int np_new, int ncell_new)
         lqb::set_error(LQ_ERR_ARG, "bad sizes np=%d ncell=%d", np_new, ncell_new);
         die("ResizeArrayLength");
     }
+    if (cell_beg) lqb::identity_release(cell_beg);
     cudaFree(part_cel);
     cudaFree(part_idx);
     cudaFree(cell_beg);
@@ -459,6 +563,9 @@ void LoquatGrid::ResizeArrayLength(int np_new, int ncell_new)
         lqb::set_error(LQ_ERR_ALLOC, "%s", cudaGetErrorString(e));
         die("ResizeArrayLength");
     }
+    /* particle identities through the searches (ParticleInteraction keeps
+     * its neighbour lists across searches with them) */
+    if (lqb::identity_reset(cell_beg, np_new) != LQ_OK) die("ResizeArrayLength");
 }
 
 void LoquatGrid::SortParticleByCellIndex(Parameters* par_host)
@@ -485,6 +592,7 @@ void LoquatGrid::NeighborSearch(Parameters* par_host, Parameters* par_device, fl
     g.beg = cell_beg;
     g.end = cell_end;
     if (lqb::grid_search(par_host, par_device, pospres, g, true, nullptr, 0) != LQ_OK) die("NeighborSearch");
+    if (lqb::identity_after_search(cell_beg, part_idx, par_host->np, 0) != LQ_OK) die("NeighborSearch");
 }
 
 void LoquatGrid::SortArrayFloat4(int np, float4* data, float4* data_cache)

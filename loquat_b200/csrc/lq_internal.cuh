@@ -114,6 +114,24 @@ int grid_search(const Parameters* par_host, const Parameters* par_dev, const flo
                 bool bounds, int* health, cudaStream_t s, const float4* idep = nullptr,
                 const Frames& fr = Frames());
 
+/* Particle identities of the drop-in grids (lq_grid_* and LoquatGrid),
+ * keyed by the grid's cell_beg array: ident[slot] is the slot the particle
+ * now there had when the grid was sized (its order before the first
+ * search), updated by every search through the grid's part_idx.  A caller
+ * that re-sorts its arrays after each search, as the reference does,
+ * keeps its particles and these identities in step, which lets the
+ * drop-in interaction carry neighbour lists across searches.  `gen`
+ * changes when the grid is resized. */
+struct GridIdentity {
+    const int* ident = nullptr;
+    int np = 0;
+    long long gen = 0;
+};
+int identity_reset(const int* key, int np);
+int identity_after_search(const int* key, const int* part_idx, int np, cudaStream_t s);
+void identity_release(const int* key);
+bool identity_find(const int* key, GridIdentity* out);
+
 int gather_float4(int n, const int* idx, const float4* in, float4* out, cudaStream_t s);
 int gather_tensor2d(int n, const int* idx, const tensor2d* in, tensor2d* out, cudaStream_t s);
 /* Gathers all five state arrays in one pass: out[i] = in[idx[i]]. */

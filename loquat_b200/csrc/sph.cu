@@ -1179,6 +1179,11 @@ namespace {
 
 /* Launch shape of the drop-in interaction's pair kernel (lqb::kPairShapes). */
 constexpr int kDropInShape = 9;
+/* Skin of the drop-in interaction's lists (of h) when the caller's grid
+ * tracks particle identities: the lists then hold every pair within
+ * 2h + skin and are carried across calls until some particle has moved
+ * half the skin. */
+constexpr float kDropInSkinOverH = 0.05f;
 
 /* Working arrays of the drop-in interaction, one set per device: the cell
  * starts derived from the caller's cell_beg / cell_end, the pair kernel's
@@ -1198,6 +1203,19 @@ struct DropInWorkspace {
     lqb::TileOrder to;              /* tile order and its segment scratch */
     lqb::NeighborList nl;           /* material targets' lists */
     float* rec = nullptr;           /* packed neighbour data, 13 floats per particle */
+    /* lists carried across calls (caller grids that track identities) */
+    int* list_id = nullptr;         /* LQ_NBR_CAP x stride: the lists at their build, as particle identities */
+    int* count_b = nullptr;         /* stride: their counts, by target slot at the build */
+    float4* xbuild = nullptr;       /* np: positions at the build, by identity */
+    int* build_of = nullptr;        /* np: identity -> slot at the build */
+    int* cur_of = nullptr;          /* np: identity -> current slot */
+    int* moved = nullptr;           /* device flag: a particle moved half the skin since the build */
+    int* moved_host = nullptr;      /* pinned copy of the flag */
+    const int* key = nullptr;       /* the grid (its cell_beg) the carried lists belong to */
+    long long gen = -1;
+    int np_built = 0, npb_built = 0;
+    bool built = false;
+    long long rebuilds = 0, reuses = 0;
     std::vector<void*> allocs;
 };
 std::mutex g_ws_mutex;
@@ -1206,6 +1224,7 @@ std::vector<DropInWorkspace> g_ws;
 void free_workspace(DropInWorkspace& w)
 {
     for (void* p : w.allocs) cudaFree(p);
+    if (w.moved_host) cudaFreeHost(w.moved_host);
     w = DropInWorkspace{};
 }
 
@@ -1247,6 +1266,16 @@ int size_workspace(DropInWorkspace& w, const Parameters* ph)
     A((void**)&n.nl.list, sizeof(int) * (size_t)LQ_NBR_CAP * n.nl.stride);
     A((void**)&n.nl.count, sizeof(int) * (size_t)n.nl.stride);
     A((void**)&n.to.order, sizeof(int) * (size_t)npm);
+    A((void**)&n.list_id, sizeof(int) * (size_t)LQ_NBR_CAP * n.nl.stride);
+    A((void**)&n.count_b, sizeof(int) * (size_t)n.nl.stride);
+    A((void**)&n.xbuild, sizeof(float4) * (size_t)np);
+    A((void**)&n.build_of, sizeof(int) * (size_t)np);
+    A((void**)&n.cur_of, sizeof(int) * (size_t)np);
+    A((void**)&n.moved, sizeof(int));
+    if (st == LQ_OK) {
+        const cudaError_t e = cudaMallocHost((void**)&n.moved_host, sizeof(int));
+        if (e != cudaSuccess) st = lqb::set_error(LQ_ERR_ALLOC, "interaction workspace: %s", cudaGetErrorString(e));
+    }
     if (st != LQ_OK) {
         free_workspace(n);
         return st;
@@ -1271,6 +1300,87 @@ int dropin_workspace(const Parameters* ph, DropInWorkspace** out)
     return LQ_OK;
 }
 
+/* Carrying lists across calls.  The caller's grid gives each slot's
+ * particle identity (lqb::identity_*); at a build the lists are stored as
+ * identities with the build positions, and a later call whose particles
+ * have all moved less than half the skin maps them to the current slots. */
+__global__ void __launch_bounds__(256) k_moved_half_skin(int np, const float4* __restrict__ pos,
+                                                         const int* __restrict__ ident,
+                                                         const float4* __restrict__ xbuild, float half_skin2,
+                                                         int* __restrict__ moved)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= np) return;
+    const int id = __ldg(ident + c);
+    bool far = true;
+    if ((unsigned)id < (unsigned)np) {
+        const float4 x = __ldg(pos + c), b = __ldg(xbuild + id);
+        const float dx = x.x - b.x, dy = x.y - b.y, dz = x.z - b.z;
+        far = !(dx * dx + dy * dy + dz * dz < half_skin2);
+    }
+    if (far) *moved = 1;
+}
+
+__global__ void __launch_bounds__(256) k_identity_slots(int np, const int* __restrict__ ident, int* __restrict__ slot)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= np) return;
+    const int id = __ldg(ident + c);
+    if ((unsigned)id < (unsigned)np) slot[id] = c;
+}
+
+/* The carried lists in the current slots: target t takes the list its
+ * particle had at the build, each entry mapped from identity to slot. */
+__global__ void __launch_bounds__(256) k_remap_lists(int np, int npb, int npm, const int* __restrict__ ident,
+                                                     const int* __restrict__ build_of,
+                                                     const int* __restrict__ list_id,
+                                                     const int* __restrict__ count_b,
+                                                     const int* __restrict__ cur_of, int* __restrict__ list,
+                                                     int* __restrict__ count, int stride)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= npm) return;
+    const int id = __ldg(ident + npb + t);
+    const int b = (unsigned)id < (unsigned)np ? __ldg(build_of + id) - npb : -1;
+    if (b < 0 || b >= npm) {
+        count[t] = LQ_NBR_CAP + 1;    /* no carried list: the pair kernel walks the stencil */
+        return;
+    }
+    const int n = __ldg(count_b + b);
+    count[t] = n;
+    const int m = n < LQ_NBR_CAP ? n : LQ_NBR_CAP;
+    for (int k = 0; k < m; ++k) {
+        const int jid = __ldg(list_id + (size_t)k * stride + b);
+        list[(size_t)k * stride + t] = (unsigned)jid < (unsigned)np ? __ldg(cur_of + jid) : npb + t;
+    }
+}
+
+/* A fresh build stored for carrying: lists as identities, build positions
+ * and slots by identity. */
+__global__ void __launch_bounds__(256) k_store_build(int np, int npb, int npm, const int* __restrict__ ident,
+                                                     const float4* __restrict__ pos, const int* __restrict__ list,
+                                                     const int* __restrict__ count, int stride,
+                                                     int* __restrict__ list_id, int* __restrict__ count_b,
+                                                     float4* __restrict__ xbuild, int* __restrict__ build_of)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= np) return;
+    const int id = __ldg(ident + c);
+    if ((unsigned)id < (unsigned)np) {
+        xbuild[id] = __ldg(pos + c);
+        build_of[id] = c;
+    }
+    const int t = c - npb;
+    if (t < 0 || t >= npm) return;
+    const int n = __ldg(count + t);
+    count_b[t] = n;
+    const int m = n < LQ_NBR_CAP ? n : LQ_NBR_CAP;
+    for (int k = 0; k < m; ++k) {
+        const int j = __ldg(list + (size_t)k * stride + t);
+        list_id[(size_t)k * stride + t] = (unsigned)j < (unsigned)np ? __ldg(ident + j) : -1;
+    }
+}
+
 /* Particles per cell from the reference's per-cell bounds (-1: empty). */
 __global__ void __launch_bounds__(256) k_cell_counts(int ncell, const int* __restrict__ beg,
                                                      const int* __restrict__ end, int* __restrict__ counts)
@@ -1286,6 +1396,21 @@ __global__ void __launch_bounds__(256) k_cell_counts(int ncell, const int* __res
 }
 
 }  // namespace
+
+extern "C" int lq_interaction_stats(long long* rebuilds, long long* reuses)
+{
+    if (!rebuilds || !reuses) return lqb::set_error(LQ_ERR_ARG, "lq_interaction_stats: null argument");
+    int dev = 0;
+    LQ_TRY_CUDA(cudaGetDevice(&dev), "interaction stats");
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    *rebuilds = 0;
+    *reuses = 0;
+    if (dev < (int)g_ws.size()) {
+        *rebuilds = g_ws[(size_t)dev].rebuilds;
+        *reuses = g_ws[(size_t)dev].reuses;
+    }
+    return LQ_OK;
+}
 
 extern "C" int lq_interaction_reserve(const void* par_host)
 {
@@ -1328,10 +1453,51 @@ extern "C" int lq_particle_interaction(const void* par_host, const void* par_dev
     LQ_TRY_CUDA(cub::DeviceScan::ExclusiveSum(w->scan_tmp, bytes, w->counts, w->start, ncell + 1, s),
                 "cell start scan");
     const lqb::Cells c{w->start, nullptr, nullptr};
-    /* the pair body's own cut-off test: q < 2 with the candidate slack of
-     * the cell walk */
-    const float cut = 2.0f * ph->h * sqrtf(1.0001f);
-    LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, ph->npb, ph->npm, 0, cut, st.pos, c, w->nl, nullptr, s));
+    const int np = ph->np, npb = ph->npb, npm = ph->npm;
+    const int nb256 = (np + 255) / 256;
+    lqb::GridIdentity gi;
+    if (lqb::identity_find(cell_beg, &gi) && gi.np == np) {
+        /* the caller's grid tracks its particles: carry the lists while
+         * every particle stays within half the skin of its build position */
+        const float skin = kDropInSkinOverH * ph->h;
+        bool reuse = false;
+        if (w->built && w->key == cell_beg && w->gen == gi.gen && w->np_built == np && w->npb_built == npb) {
+            LQ_TRY_CUDA(cudaMemsetAsync(w->moved, 0, sizeof(int), s), "moved flag");
+            k_moved_half_skin<<<nb256, 256, 0, s>>>(np, st.pos, gi.ident, w->xbuild, 0.25f * skin * skin, w->moved);
+            LQ_TRY_CUDA(cudaGetLastError(), "k_moved_half_skin");
+            LQ_TRY_CUDA(cudaMemcpyAsync(w->moved_host, w->moved, sizeof(int), cudaMemcpyDeviceToHost, s),
+                        "moved flag");
+            LQ_TRY_CUDA(cudaStreamSynchronize(s), "moved flag");
+            reuse = *w->moved_host == 0;
+        }
+        if (reuse) {
+            k_identity_slots<<<nb256, 256, 0, s>>>(np, gi.ident, w->cur_of);
+            LQ_TRY_CUDA(cudaGetLastError(), "k_identity_slots");
+            k_remap_lists<<<(npm + 255) / 256, 256, 0, s>>>(np, npb, npm, gi.ident, w->build_of, w->list_id,
+                                                            w->count_b, w->cur_of, w->nl.list, w->nl.count,
+                                                            w->nl.stride);
+            LQ_TRY_CUDA(cudaGetLastError(), "k_remap_lists");
+            ++w->reuses;
+        } else {
+            LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, npb, npm, 0, 2.0f * ph->h + skin, st.pos, c, w->nl,
+                                                   nullptr, s));
+            k_store_build<<<nb256, 256, 0, s>>>(np, npb, npm, gi.ident, st.pos, w->nl.list, w->nl.count,
+                                                w->nl.stride, w->list_id, w->count_b, w->xbuild, w->build_of);
+            LQ_TRY_CUDA(cudaGetLastError(), "k_store_build");
+            w->built = true;
+            w->key = cell_beg;
+            w->gen = gi.gen;
+            w->np_built = np;
+            w->npb_built = npb;
+            ++w->rebuilds;
+        }
+    } else {
+        /* the pair body's own cut-off test: q < 2 with the candidate slack
+         * of the cell walk */
+        const float cut = 2.0f * ph->h * sqrtf(1.0001f);
+        LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, npb, npm, 0, cut, st.pos, c, w->nl, nullptr, s));
+        w->built = false;
+    }
     LQ_TRY(lqb::launch_tile_order(ph, w->start, kDropInShape, w->to, s));
     return lqb::launch_interaction_list(ph, pd, st, r, c, w->nl, s, lqb::Frames(), false, w->rec, kDropInShape, true,
                                         w->to.order);

@@ -12,6 +12,14 @@ Each call goes through the C ABI (``lq_grid_*``, ``lq_adami_boundary``,
 ``lq_stress_regularization``) on one CUDA stream; device memory comes from
 torch.  It measures what a reference caller gets, and lets tests check that
 sequence against the oracle.
+
+The grid is this library's (``lq_grid_*``), whose searches track each
+particle's identity, so ``lq_particle_interaction`` carries its neighbour
+lists from call to call while the particles stay within half a skin of
+their positions at the lists' build.  ``carry=False`` hands the
+interaction copies of the grid's cell bounds instead, which it cannot
+match to a grid: it then builds its lists afresh at every call, as it does
+for a caller's own grid.
 """
 from __future__ import annotations
 
@@ -24,7 +32,8 @@ from . import (Grid, Parameters, adami_boundary, corrector, interaction_reserve,
 
 
 class ReferenceStep:
-    def __init__(self, par: Parameters, pospres, velrhop, idep, str_, stn, device="cuda", stream=None):
+    def __init__(self, par: Parameters, pospres, velrhop, idep, str_, stn, device="cuda", stream=None,
+                 carry: bool = True):
         import torch
 
         self.torch = torch
@@ -49,6 +58,10 @@ class ReferenceStep:
         self.par_dev = torch.empty(ctypes.sizeof(Parameters), dtype=torch.uint8, device=dev)
         self.grid = Grid(n, par.ncell)
         interaction_reserve(self.par)    # set-up allocation, as LoquatGrid::GridConfig makes it
+        self.carry = carry
+        if not carry:
+            self._beg = torch.empty(par.ncell, dtype=torch.int32, device=dev)
+            self._end = torch.empty(par.ncell, dtype=torch.int32, device=dev)
         self.step_count = 0
         self.time = 0.0
 
@@ -77,7 +90,18 @@ class ReferenceStep:
 
     def _cells(self):
         a = self.grid.arrays()
-        return a["cell_beg"], a["cell_end"]
+        if self.carry:
+            return a["cell_beg"], a["cell_end"]
+        # copies of the grid's bounds, at addresses the library does not know
+        from cuda.bindings import runtime as rt
+
+        nbytes = 4 * self.par.ncell
+        kind = rt.cudaMemcpyKind.cudaMemcpyDeviceToDevice
+        for dst, src in ((self._beg, a["cell_beg"]), (self._end, a["cell_end"])):
+            err, = rt.cudaMemcpyAsync(dst.data_ptr(), src, nbytes, kind, self._s)
+            if int(err) != 0:
+                raise RuntimeError(f"cell bounds copy failed: {err}")
+        return self._beg, self._end
 
     def step(self, nsteps: int = 1):
         s = self._s
@@ -94,6 +118,7 @@ class ReferenceStep:
             predictor(ph, pd, st, ini, rt, stream=s)
             # corrector stage (src/loquat.cu:371-396)
             self._search_sort(st + ini)
+            beg, end = self._cells()
             adami_boundary(ph, pd, st[0], st[1], st[3], beg, end, stream=s)
             particle_interaction(ph, pd, *st, *rt, beg, end, stream=s)
             corrector(ph, pd, st, ini, rt, stream=s)
@@ -101,6 +126,7 @@ class ReferenceStep:
             N = ph.stress_shepard_filter
             if N != 0 and self.step_count % N == 0 and self.step_count != 0:
                 self._search_sort(st)
+                beg, end = self._cells()
                 stress_regularization(ph, pd, st[0], st[1], st[3], self.t2_cache, beg, end, stream=s)
             self.time += float(ph.dt)
             self.step_count += 1

@@ -1,9 +1,10 @@
 """The reference's time step through the drop-in entry points
 (loquat_b200.dropin.ReferenceStep: src/loquat.cu:322-409 with a search and
-re-sort before each stage) against the FP64 oracle, and the drop-in
-interaction's working arrays: once reserved at set-up
-(lq_interaction_reserve, as LoquatGrid::GridConfig does), its calls
-allocate no device memory."""
+re-sort before each stage) against the FP64 oracle; the neighbour lists the
+drop-in interaction carries across calls (its grid tracks particle
+identities) against lists built afresh at every call; and the interaction's
+working arrays: once reserved at set-up (lq_interaction_reserve, as
+LoquatGrid::GridConfig does), its calls allocate no device memory."""
 from __future__ import annotations
 
 import numpy as np
@@ -19,10 +20,13 @@ def test_reference_step_sequence_through_drop_in_entry_points_vs_oracle(lq, orc,
     from loquat_b200 import dropin
 
     c = cases.small_column(velocity_noise=0.05, shepard=4, seed=15).with_ids()
+    r0, u0 = lq.interaction_stats()
     seq = dropin.ReferenceStep(c.par, *c.arrays())
     seq.step(10)
     got = by_id(seq.download())
     seq.close()
+    r1, u1 = lq.interaction_stats()
+    assert u1 - u0 > 0 and r1 - r0 >= 1       # the lists were carried over
     o = orc.OracleSim(c.par, *c.arrays())
     o.step(10)
     want = by_id(o.get())
@@ -32,6 +36,31 @@ def test_reference_step_sequence_through_drop_in_entry_points_vs_oracle(lq, orc,
     assert rel_l2(got[1][nb:, 3], want[1][nb:, 3]) < 1e-6
     assert rel_l2(got[3][nb:], want[3][nb:]) < 1e-4
     assert rel_l2(got[0][nb:, :3], want[0][nb:, :3]) < 1e-6
+
+
+def test_carried_lists_match_fresh_lists(lq, cuda):
+    """Fast particles (0.3 m/s noise) force several rebuilds in 30 steps;
+    between them the carried lists (mapped to the re-sorted slots) give the
+    fresh lists' results to float rounding: the same pairs, summed in the
+    build's order."""
+    from loquat_b200 import dropin
+
+    c = cases.small_column(velocity_noise=0.3, shepard=7, seed=16).with_ids()
+    runs = []
+    for carry in (True, False):
+        r0, u0 = lq.interaction_stats()
+        seq = dropin.ReferenceStep(c.par, *c.arrays(), carry=carry)
+        seq.step(30)
+        runs.append(by_id(seq.download()))
+        seq.close()
+        r1, u1 = lq.interaction_stats()
+        if carry:
+            assert r1 - r0 >= 2 and u1 - u0 >= 10, (r1 - r0, u1 - u0)
+        else:
+            assert (r1, u1) == (r0, u0)
+    nb = c.par.npb
+    for k, tol in ((0, 1e-7), (1, 1e-5), (3, 1e-5)):
+        assert rel_l2(runs[0][k][nb:], runs[1][k][nb:]) < tol, k
 
 
 def test_reserved_interaction_allocates_nothing_per_call(lq, cuda):
