@@ -479,7 +479,12 @@ def bench_ours(args):
             osim.set_hypoplastic(case.meta["hypoplastic"])
         if args.start_step > 0:
             osim.step(args.start_step)
-        if tuned:
+        other_tuned = tuned
+        if args.pair_shape is None and not args.no_autotune:
+            # each form tuned on its own: its best launch shape and skin
+            shape, skin = osim.autotune(args.tune_steps)
+            other_tuned = {"pair_shape": shape, "skin_over_h": skin, "steps_per_trial": args.tune_steps}
+        elif tuned:
             osim.set_pair_shape(tuned["pair_shape"])
             osim.set_skin(tuned["skin_over_h"])
         osim.step(args.warmup)
@@ -493,7 +498,8 @@ def bench_ours(args):
         o1.record(oext)
         osim.synchronize()
         oms = replicas.max_over_ranks(o0.elapsed_time(o1), device="cuda")
-        forms[other] = {"value": npm * args.steps * world / (oms / 1e3), "ms_per_step": oms / args.steps}
+        forms[other] = {"value": npm * args.steps * world / (oms / 1e3), "ms_per_step": oms / args.steps,
+                        "autotuned": other_tuned}
         sim = osim
 
     sim.close()

@@ -153,19 +153,23 @@ int launch_neighbor_list(const Parameters* par_host, const Parameters* par_dev, 
                          const NeighborList& nl, cudaStream_t s);
 /* `rec` (np x 13 floats, 16-byte aligned; required) holds the neighbour
  * data packed into dense arrays (position and density, velocity and
- * sigma/rho^2; 52 bytes per particle) that the pair kernel gathers; with
- * `pack` they are packed from the state first. */
+ * sigma/rho^2: 52 bytes per particle, 48 in the compensated form, whose
+ * velocity is packed into two words) that the pair kernel gathers; with
+ * `pack` they are packed from the state first, in the form of
+ * `compensated`. */
 int launch_interaction_list(const Parameters* par_host, const Parameters* par_dev, const State& st, const Rates& r,
                             const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr = Frames(),
                             bool compensated = false, float* rec = nullptr, int shape = 0, bool pack = true,
                             const int* order = nullptr);
-/* The packed neighbour arrays of slots [first, np) from the state. */
-int launch_pack_neighbors(const Parameters* par_host, const State& st, float* rec, int first, cudaStream_t s);
+/* The packed neighbour arrays of slots [first, np) from the state;
+ * packed_velocity selects the compensated pair kernel's record. */
+int launch_pack_neighbors(const Parameters* par_host, const State& st, float* rec, int first, cudaStream_t s,
+                          bool packed_velocity);
 /* Adami over the boundary lists reading the packed arrays (material slots
  * packed), writing the boundary stress into the state and the packed
  * arrays. */
 int launch_adami_packed(const Parameters* par_host, const Parameters* par_dev, const State& st,
-                        const NeighborList& nl, float* rec, cudaStream_t s);
+                        const NeighborList& nl, float* rec, cudaStream_t s, bool packed_velocity);
 /* Launch shapes of the packed pair kernel: {threads per block, resident
  * blocks per SM, tile order}, or {128, -G, 0} for the warp-cooperative form
  * with G lanes per target.  Shapes with the tile order take their targets

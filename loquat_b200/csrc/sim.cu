@@ -302,7 +302,7 @@ int enqueue_rebuild(LqSim* S, cudaStream_t s)
     LQ_TRY(build_lists(S, s));
     /* every slot's packed neighbour data (the boundary slots keep theirs
      * until the next build) */
-    LQ_TRY(lqb::launch_pack_neighbors(ph, S->S, S->rec, 0, s));
+    LQ_TRY(lqb::launch_pack_neighbors(ph, S->S, S->rec, 0, s, S->flags & LQ_SIM_MIXED));
     return lqb::launch_tile_order(ph, S->g.start, S->pair_shape, S->tile, s);
 }
 
@@ -338,8 +338,8 @@ int enqueue_density_filter(LqSim* S, cudaStream_t s)
  * in between), so the pair kernel needs no pack. */
 int enqueue_adami_pack(LqSim* S, const State& st, cudaStream_t s)
 {
-    LQ_TRY(lqb::launch_pack_neighbors(&S->ph, st, S->rec, S->npb, s));
-    return lqb::launch_adami_packed(&S->ph, S->pd, st, S->nlb, S->rec, s);
+    LQ_TRY(lqb::launch_pack_neighbors(&S->ph, st, S->rec, S->npb, s, S->flags & LQ_SIM_MIXED));
+    return lqb::launch_adami_packed(&S->ph, S->pd, st, S->nlb, S->rec, s, S->flags & LQ_SIM_MIXED);
 }
 
 /* The two stages of a step on the current lists. */
@@ -1309,7 +1309,7 @@ int profiled_step(LqSim* S, PhaseTimer& T)
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_LIST));
         LQ_TRY(build_lists(S, s));
-        LQ_TRY(lqb::launch_pack_neighbors(ph, S->S, S->rec, 0, s));
+        LQ_TRY(lqb::launch_pack_neighbors(ph, S->S, S->rec, 0, s, S->flags & LQ_SIM_MIXED));
         LQ_TRY(lqb::launch_tile_order(ph, S->g.start, S->pair_shape, S->tile, s));
         LQ_TRY(T.close(s));
     }

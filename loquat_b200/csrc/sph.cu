@@ -22,6 +22,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include "lq_internal.cuh"
+#include "lq_pack.h"
 #include "lq_tile.h"
 #include "lq_device.cuh"
 #include <adami_boundary.h>
@@ -196,22 +197,58 @@ __device__ __forceinline__ void pair_body(const PairConst& K, const State& st, T
     T.l20 -= wz * gx; T.l21 -= wz * gy; T.l22 -= wz * gz;
 }
 
-/* Packed neighbour data for the list pair kernel: four dense arrays over
- * all slots, 52 bytes per particle,
- *   nb.xr[j] = (x, y, z, rho), nb.vs[j] = (vx, vy, vz, sxx),
- *   nb.s3[j] = (syy, szz, sxy, sxz), nb.s1[j] = syz,
- * with s = sigma / rho^2.  The pair kernel is bound by the L1 data pipe: a
+/* Packed neighbour data for the list pair kernel: dense arrays over all
+ * slots, with s = sigma / rho^2,
+ *   nb.xr[j] = (x, y, z, rho), nb.sa[j] = (sxx, syy, szz, sxy),
+ *   nb.sb[j] = (sxz, syz, v0, v1),
+ * where the plain form keeps (v0, v1) = (vx, vy) and vz in nb.vz[j]
+ * (52 bytes per particle, four gathers per pair) and the mixed form packs
+ * the whole velocity into v0, v1 (pack_velocity: 48 bytes, three 16-byte
+ * gathers per pair).  The pair kernel is bound by the L1 data pipe: a
  * warp's gathered neighbours sit close together in memory and the pipe's
- * work follows the bytes each load instruction gathers, so the 13 floats a
- * pair needs are gathered without the pressure word of pospres and without
- * the 24-byte stress records (read as three 8-byte loads).  1 / rho is
- * formed as the state-array pair body forms it. */
+ * work follows the load instructions and the sectors each gathers, so the
+ * record holds only the 13 values a pair needs (no pressure word of
+ * pospres, no 24-byte stress records read as three 8-byte loads).
+ * 1 / rho is formed as the state-array pair body forms it. */
 struct NbrArrays {
     float4* xr;
-    float4* vs;
-    float4* s3;
-    float* s1;
+    float4* sa;
+    float4* sb;
+    float* vz;
 };
+
+/* The mixed form's gathered velocity in two words (lq_pack.h: a shared
+ * exponent and three 18-bit mantissas). */
+__device__ __forceinline__ float2 pack_velocity(float vx, float vy, float vz)
+{
+    unsigned w0, w1;
+    pack_velocity_words(vx, vy, vz, w0, w1);
+    return make_float2(__uint_as_float(w0), __uint_as_float(w1));
+}
+
+__device__ __forceinline__ float3 unpack_velocity(float v0, float v1)
+{
+    float3 v;
+    unpack_velocity_words(__float_as_uint(v0), __float_as_uint(v1), v.x, v.y, v.z);
+    return v;
+}
+
+/* One slot's entry of the packed arrays from its velocity, density and
+ * stress (the pack kernel and the list-driven Adami write it alike). */
+template <bool kPk>
+__device__ __forceinline__ void store_packed(const NbrArrays& nb, int i, const float4& v, const tensor2d& str)
+{
+    const float rinv = __fdividef(1.0f, v.w);
+    const float r2 = rinv * rinv;
+    nb.sa[i] = make_float4(str.xx * r2, str.yy * r2, str.zz * r2, str.xy * r2);
+    if (kPk) {
+        const float2 w = pack_velocity(v.x, v.y, v.z);
+        nb.sb[i] = make_float4(str.xz * r2, str.yz * r2, w.x, w.y);
+    } else {
+        nb.sb[i] = make_float4(str.xz * r2, str.yz * r2, v.x, v.y);
+        nb.vz[i] = v.z;
+    }
+}
 
 /* One pair from the packed arrays, its density-rate and momentum terms
  * added to (drho, ax, ay, az) and its velocity-gradient terms to T.  The
@@ -219,16 +256,16 @@ struct NbrArrays {
  * a run of pairs has no branch between them; kArtp adds the artificial
  * stress.  A pair of a particle with itself (the filler of a list's last
  * group of four) adds exact zeros: r = 0 makes the kernel gradient zero. */
-template <bool kArtp>
+template <bool kArtp, bool kPk>
 __device__ __forceinline__ void pair_terms(const PairConst& K, const NbrArrays& nb, Target& T, int j, float& drho,
                                            float& ax, float& ay, float& az)
 {
     const float4 xr = __ldg(nb.xr + j);
-    const float4 vs = __ldg(nb.vs + j);
-    const float4 s3 = __ldg(nb.s3 + j);
-    const float s1 = __ldg(nb.s1 + j);
-    const float a[8] = {xr.x, xr.y, xr.z, 0.0f, vs.x, vs.y, vs.z, xr.w};
-    const float b[6] = {vs.w, s3.x, s3.y, s3.z, s3.w, s1};
+    const float4 sa = __ldg(nb.sa + j);
+    const float4 sb = __ldg(nb.sb + j);
+    const float3 vj = kPk ? unpack_velocity(sb.z, sb.w) : make_float3(sb.z, sb.w, __ldg(nb.vz + j));
+    const float a[8] = {xr.x, xr.y, xr.z, 0.0f, vj.x, vj.y, vj.z, xr.w};
+    const float b[6] = {sa.x, sa.y, sa.z, sa.w, sb.x, sb.y};
     const float dx = T.x.x - a[0], dy = T.x.y - a[1], dz = T.x.z - a[2];
     const float r2 = dx * dx + dy * dy + dz * dz;
     const float q = sqrt_approx(r2) * K.ih;
@@ -271,25 +308,26 @@ __device__ __forceinline__ void pair_terms(const PairConst& K, const NbrArrays& 
     T.l20 -= wz * gx; T.l21 -= wz * gy; T.l22 -= wz * gz;
 }
 
-/* One pair into T's sums; kKahan compensates the density and momentum
- * sums pair by pair. */
+/* One pair into T's sums.  kKahan selects the mixed form: the density
+ * and momentum sums compensated pair by pair, and the neighbour's velocity
+ * gathered in the packed record. */
 template <bool kKahan = false>
 __device__ __forceinline__ void pair_body_rec(const PairConst& K, const NbrArrays& nb, Target& T, int j)
 {
     if (kKahan) {
         float d = 0.f, x = 0.f, y = 0.f, z = 0.f;
         if (K.artp)
-            pair_terms<true>(K, nb, T, j, d, x, y, z);
+            pair_terms<true, true>(K, nb, T, j, d, x, y, z);
         else
-            pair_terms<false>(K, nb, T, j, d, x, y, z);
+            pair_terms<false, true>(K, nb, T, j, d, x, y, z);
         kahan_add(T.drho, T.cdrho, d);
         kahan_add(T.ax, T.cax, x);
         kahan_add(T.ay, T.cay, y);
         kahan_add(T.az, T.caz, z);
     } else if (K.artp) {
-        pair_terms<true>(K, nb, T, j, T.drho, T.ax, T.ay, T.az);
+        pair_terms<true, false>(K, nb, T, j, T.drho, T.ax, T.ay, T.az);
     } else {
-        pair_terms<false>(K, nb, T, j, T.drho, T.ax, T.ay, T.az);
+        pair_terms<false, false>(K, nb, T, j, T.drho, T.ax, T.ay, T.az);
     }
 }
 
@@ -450,19 +488,15 @@ __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __re
     }
 }
 
+template <bool kPk>
 __global__ void __launch_bounds__(kBlock) k_pack_neighbors(int first, int np, State st, NbrArrays nb)
 {
     const int i = first + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
     const float4 x = __ldg(st.pos + i);
     const float4 v = __ldg(st.vel + i);
-    const tensor2d s = load_t2(st.str, i);
-    const float rinv = __fdividef(1.0f, v.w);
-    const float rj2 = rinv * rinv;
     nb.xr[i] = make_float4(x.x, x.y, x.z, v.w);
-    nb.vs[i] = make_float4(v.x, v.y, v.z, s.xx * rj2);
-    nb.s3[i] = make_float4(s.yy * rj2, s.zz * rj2, s.xy * rj2, s.xz * rj2);
-    nb.s1[i] = s.yz * rj2;
+    store_packed<kPk>(nb, i, v, load_t2(st.str, i));
 }
 
 /* A list entry: each 128-byte row of a list is read once per launch, so it
@@ -479,8 +513,8 @@ __device__ __forceinline__ int ld_list(const int* p)
  * entries per group, the next group's entries fetched ahead so the
  * dependent neighbour loads do not wait on the list stream.  The last
  * group is filled up with the target itself (exact zeros), so a group has
- * no branch.  The compensated form adds each group's plain sum of four
- * pairs to the compensated sums. */
+ * no branch.  The compensated (mixed) form adds each group's plain sum of
+ * four pairs to the compensated sums and reads the packed velocity. */
 template <bool kKahan, bool kArtp>
 __device__ __forceinline__ void list_sums(const PairConst& K, const NbrArrays& nb, Target& T, const int* p, int n,
                                           int stride, int i, int np)
@@ -501,7 +535,7 @@ __device__ __forceinline__ void list_sums(const PairConst& K, const NbrArrays& n
             float d = 0.f, x = 0.f, y = 0.f, z = 0.f;
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                if (lq_in_range(cur[u], np)) pair_terms<kArtp>(K, nb, T, cur[u], d, x, y, z);
+                if (lq_in_range(cur[u], np)) pair_terms<kArtp, true>(K, nb, T, cur[u], d, x, y, z);
             kahan_add(T.drho, T.cdrho, d);
             kahan_add(T.ax, T.cax, x);
             kahan_add(T.ay, T.cay, y);
@@ -509,7 +543,8 @@ __device__ __forceinline__ void list_sums(const PairConst& K, const NbrArrays& n
         } else {
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                if (lq_in_range(cur[u], np)) pair_terms<kArtp>(K, nb, T, cur[u], T.drho, T.ax, T.ay, T.az);
+                if (lq_in_range(cur[u], np))
+                    pair_terms<kArtp, false>(K, nb, T, cur[u], T.drho, T.ax, T.ay, T.az);
         }
     }
 }
@@ -776,6 +811,7 @@ __global__ void __launch_bounds__(kBlock) k_shepard(const Parameters* __restrict
  * boundary particle's new stress both into the state and, scaled, into the
  * packed arrays, which then need no pack of the boundary slots before the
  * pair kernel.  Targets without neighbours keep both as they were. */
+template <bool kPk>
 __global__ void __launch_bounds__(kBlock) k_adami_packed(const Parameters* __restrict__ P, int npb, State st,
                                                          const int* __restrict__ list,
                                                          const int* __restrict__ count, int stride, NbrArrays nb)
@@ -799,15 +835,14 @@ __global__ void __launch_bounds__(kBlock) k_adami_packed(const Parameters* __res
             const float ker = Cw * (2.0f - q) * (2.0f - q) * (2.0f - q) * (2.0f - q) * (q + 0.5f);
             const float vol = m / xr.w;
             const float cs = m * xr.w * ker;
-            const float4 vs = __ldg(nb.vs + j);
-            const float4 s3 = __ldg(nb.s3 + j);
-            const float s1 = __ldg(nb.s1 + j);
-            S.xx += vs.w * cs;
-            S.yy += s3.x * cs;
-            S.zz += s3.y * cs;
-            S.xy += s3.z * cs;
-            S.xz += s3.w * cs;
-            S.yz += s1 * cs;
+            const float4 sa = __ldg(nb.sa + j);
+            const float2 sb = __ldg(reinterpret_cast<const float2*>(nb.sb + j));
+            S.xx += sa.x * cs;
+            S.yy += sa.y * cs;
+            S.zz += sa.z * cs;
+            S.xy += sa.w * cs;
+            S.xz += sb.x * cs;
+            S.yz += sb.y * cs;
             acc.x += d.x * ker * vol;
             acc.y += d.y * ker * vol;
             acc.z += d.z * ker * vol;
@@ -824,13 +859,7 @@ __global__ void __launch_bounds__(kBlock) k_adami_packed(const Parameters* __res
         out.xz = S.xz / acc.w;
         out.yz = S.yz / acc.w;
         store_t2(st.str, i, out);
-        /* as k_pack_neighbors scales it */
-        const float rinv = __fdividef(1.0f, __ldg(&st.vel[i].w));
-        const float ri2 = rinv * rinv;
-        const float4 v = __ldg(st.vel + i);
-        nb.vs[i] = make_float4(v.x, v.y, v.z, out.xx * ri2);
-        nb.s3[i] = make_float4(out.yy * ri2, out.zz * ri2, out.xy * ri2, out.xz * ri2);
-        nb.s1[i] = out.yz * ri2;
+        store_packed<kPk>(nb, i, __ldg(st.vel + i), out);
     }
 }
 
@@ -1049,21 +1078,31 @@ int launch_neighbor_list_range(const Parameters* ph, const Parameters* pd, int f
     return LQ_OK;
 }
 
-int launch_pack_neighbors(const Parameters* ph, const State& st, float* rec, int first, cudaStream_t s)
+int launch_pack_neighbors(const Parameters* ph, const State& st, float* rec, int first, cudaStream_t s,
+                          bool packed_velocity)
 {
     const int n = ph->np - first;
     if (n <= 0) return LQ_OK;
-    k_pack_neighbors<<<blocks_for(n, kBlock), kBlock, 0, s>>>(first, ph->np, st, nbr_arrays(rec, ph->np));
+    const NbrArrays nb = nbr_arrays(rec, ph->np);
+    if (packed_velocity)
+        k_pack_neighbors<true><<<blocks_for(n, kBlock), kBlock, 0, s>>>(first, ph->np, st, nb);
+    else
+        k_pack_neighbors<false><<<blocks_for(n, kBlock), kBlock, 0, s>>>(first, ph->np, st, nb);
     LQ_TRY_CUDA(cudaGetLastError(), "k_pack_neighbors");
     return LQ_OK;
 }
 
 int launch_adami_packed(const Parameters* ph, const Parameters* pd, const State& st, const NeighborList& nl,
-                        float* rec, cudaStream_t s)
+                        float* rec, cudaStream_t s, bool packed_velocity)
 {
     if (ph->npb <= 0) return LQ_OK;
-    k_adami_packed<<<blocks_for(ph->npb, kBlock), kBlock, 0, s>>>(pd, ph->npb, st, nl.list, nl.count, nl.stride,
-                                                                 nbr_arrays(rec, ph->np));
+    const NbrArrays nb = nbr_arrays(rec, ph->np);
+    if (packed_velocity)
+        k_adami_packed<true><<<blocks_for(ph->npb, kBlock), kBlock, 0, s>>>(pd, ph->npb, st, nl.list, nl.count,
+                                                                           nl.stride, nb);
+    else
+        k_adami_packed<false><<<blocks_for(ph->npb, kBlock), kBlock, 0, s>>>(pd, ph->npb, st, nl.list, nl.count,
+                                                                            nl.stride, nb);
     LQ_TRY_CUDA(cudaGetLastError(), "k_adami_packed");
     return LQ_OK;
 }
@@ -1086,13 +1125,8 @@ int launch_interaction_list(const Parameters* ph, const Parameters* pd, const St
     if (rec) {
         if (reinterpret_cast<uintptr_t>(rec) % 16 != 0)
             return set_error(LQ_ERR_ARG, "interaction: packed neighbour arrays must be 16-byte aligned");
-        const size_t n = (size_t)ph->np;
-        NbrArrays nb{reinterpret_cast<float4*>(rec), reinterpret_cast<float4*>(rec) + n,
-                     reinterpret_cast<float4*>(rec) + 2 * n, rec + 12 * n};
-        if (pack) {
-            k_pack_neighbors<<<blocks_for(ph->np, kBlock), kBlock, 0, s>>>(0, ph->np, st, nb);
-            LQ_TRY_CUDA(cudaGetLastError(), "k_pack_neighbors");
-        }
+        const NbrArrays nb = nbr_arrays(rec, ph->np);
+        if (pack) LQ_TRY(launch_pack_neighbors(ph, st, rec, 0, s, compensated));
         if (shape >= 0 && shape < kPairShapeCount && kPairShapes[shape][2] == 1 && !order)
             return set_error(LQ_ERR_ARG, "interaction: launch shape %d needs the tile order", shape);
         if (shape < 0 || shape >= kPairShapeCount || kPairShapes[shape][2] != 1) order = nullptr;

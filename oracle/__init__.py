@@ -97,13 +97,17 @@ def set_threads(n: int = 0) -> int:
 
 
 GATHER_F16_VELOCITY, GATHER_F16_STRESS, GATHER_BF16_VELOCITY, GATHER_BF16_STRESS = 1, 2, 4, 8
+GATHER_FP21_VELOCITY, GATHER_SHARED_EXP18_VELOCITY = 16, 32
 
 
 def set_gather_rounding(mode: int = 0) -> None:
     """Precision experiment: the interaction rounds a neighbour's gathered
-    velocity and/or sigma/rho^2 to FP16 or BF16 (bit mask of the GATHER_*
-    constants), as a GPU form with 16-bit packed gathers would; 0 restores
-    exact gathers.  Applies to every later interaction of this process."""
+    velocity and/or sigma/rho^2 to FP16 or BF16, or the velocity to three
+    21-bit floats (GATHER_FP21_VELOCITY) or to one shared exponent with
+    three 18-bit mantissas (GATHER_SHARED_EXP18_VELOCITY) (bit mask of the
+    GATHER_* constants), as a GPU form with packed gathers would; 0
+    restores exact gathers.  Applies to every later interaction of this
+    process."""
     lib().or_set_gather_rounding(int(mode))
 
 

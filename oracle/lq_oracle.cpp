@@ -236,7 +236,8 @@ void adami(const OrParams& P, int np, int npb, const double* pos, const double* 
  * as a GPU form that packed those gathers into 16-bit floats would see
  * them; the target's own values stay exact.  Bit 0: velocity to FP16,
  * bit 1: sigma/rho^2 to FP16, bit 2: velocity to BF16, bit 3: sigma/rho^2
- * to BF16 (round to nearest even).  0 (the default) rounds nothing. */
+ * to BF16 (round to nearest even); bits 4 and 5: the packed velocity forms
+ * of gather_velocity.  0 (the default) rounds nothing. */
 int g_gather_rounding = 0;
 
 /* x rounded to nearest even with `bits` significant bits, numbers below
@@ -259,6 +260,43 @@ inline double gather_round(double x, int f16_bit, int bf16_bit)
     if (g_gather_rounding & f16_bit) return round_significand((double)(float)x, 11, -14);
     if (g_gather_rounding & bf16_bit) return round_significand((double)(float)x, 8, -126);
     return x;
+}
+
+/* A neighbour's gathered velocity under the rounding experiment: bits 0
+ * and 2 as above; bit 4, each component as a 21-bit float (FP32's sign and
+ * exponent, 13 significant bits); bit 5, one shared exponent and three
+ * signed 18-bit mantissas: the quantum is 2^(E - 17) for the least E with
+ * max |v_k| < 2^E, doubled once if a rounded mantissa leaves
+ * [-2^17, 2^17 - 1]. */
+inline void gather_velocity(const double* vj, double out[3])
+{
+    for (int k = 0; k < 3; ++k) out[k] = gather_round(vj[k], 1, 4);
+    if (g_gather_rounding & 16)
+        for (int k = 0; k < 3; ++k) out[k] = round_significand((double)(float)out[k], 13, -126);
+    if (g_gather_rounding & 32) {
+        double f[3], m = 0.0;
+        for (int k = 0; k < 3; ++k) {
+            f[k] = (double)(float)out[k];
+            m = std::max(m, std::fabs(f[k]));
+        }
+        if (m == 0.0 || !std::isfinite(m)) return;
+        int e;
+        std::frexp(m, &e);          /* m < 2^e */
+        for (int pass = 0; pass < 2; ++pass) {
+            const double q = std::ldexp(1.0, e - 17);
+            bool fits = true;
+            double r[3];
+            for (int k = 0; k < 3; ++k) {
+                r[k] = std::nearbyint(f[k] / q);
+                fits = fits && r[k] >= -131072.0 && r[k] <= 131071.0;
+            }
+            if (fits || pass == 1) {
+                for (int k = 0; k < 3; ++k) out[k] = r[k] * q;
+                return;
+            }
+            ++e;
+        }
+    }
 }
 
 void interaction(const OrParams& P, int np, int npb, const double* pos, const double* vel, const double* str,
@@ -296,8 +334,9 @@ void interaction(const OrParams& P, int np, int npb, const double* pos, const do
             double t = 2.0 - q;
             double fac = Cg * t * t * t;
             double g[3] = {fac * d[0], fac * d[1], fac * d[2]};
-            double vij[3] = {vi[0] - gather_round(vj[0], 1, 4), vi[1] - gather_round(vj[1], 1, 4),
-                             vi[2] - gather_round(vj[2], 1, 4)};
+            double vg[3];
+            gather_velocity(vj, vg);
+            double vij[3] = {vi[0] - vg[0], vi[1] - vg[1], vi[2] - vg[2]};
             drho += vij[0] * g[0] + vij[1] * g[1] + vij[2] * g[2];
             double rhoj = vj[3];
             double rj2 = 1.0 / (rhoj * rhoj);

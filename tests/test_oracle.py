@@ -293,14 +293,20 @@ def test_gather_rounding_experiment_switch(orc):
     s = np.tile(np.array([-3.0e4, -2.0e4, -5.0e4, 1.0e3, -2.0e3, 4.0e3]), (pos.shape[0], 1))
     s *= 1.0 + 0.1 * rng.random((pos.shape[0], 1))
     exact = run_interaction(orc, p, pos, vel, s)
+    err = {}
     try:
-        for mode, field in ((orc.GATHER_F16_VELOCITY, 2), (orc.GATHER_BF16_STRESS, 0)):
+        for mode, field in ((orc.GATHER_F16_VELOCITY, 2), (orc.GATHER_BF16_STRESS, 0),
+                            (orc.GATHER_FP21_VELOCITY, 2), (orc.GATHER_SHARED_EXP18_VELOCITY, 2)):
             orc.set_gather_rounding(mode)
             got = run_interaction(orc, p, pos, vel, s)
             d = np.linalg.norm(got[field][interior] - exact[field][interior]) / np.linalg.norm(exact[field][interior])
-            assert 1e-6 < d < 5e-2, (mode, d)
+            err[mode] = d
+            assert 1e-9 < d < 5e-2, (mode, d)
     finally:
         orc.set_gather_rounding(0)
+    # finer packing, smaller error: FP16 (11 bits) > 21-bit floats (13) >
+    # a shared exponent with 18-bit mantissas
+    assert err[orc.GATHER_F16_VELOCITY] > err[orc.GATHER_FP21_VELOCITY] > err[orc.GATHER_SHARED_EXP18_VELOCITY]
     again = run_interaction(orc, p, pos, vel, s)
     for a, b in zip(again, exact):
         assert np.array_equal(a, b)
