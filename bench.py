@@ -87,6 +87,10 @@ def parse_args(argv=None):
     ap.add_argument("--tune-steps", type=int, default=40, help="timed steps per autotuner trial")
     ap.add_argument("--pair-shape", type=int, default=None,
                     help="fix the pair kernel's launch shape (lq_sim_set_pair_shape, 0-10) instead of autotuning")
+    ap.add_argument("--skin", type=float, default=None,
+                    help="with --pair-shape: the list skin / h (lq_sim_set_skin; default 0.05)")
+    ap.add_argument("--wide", type=float, default=None,
+                    help="with --pair-shape: two-level lists' wide cut-off beyond 2h, / h (lq_sim_set_wide_skin)")
     ap.add_argument("--no-dropin", action="store_true",
                     help="skip timing the reference's step sequence through the drop-in entry points")
     ap.add_argument("--no-ensemble", action="store_true",
@@ -378,19 +382,25 @@ def bench_ours(args):
 
     tuned = None
     if args.pair_shape is not None:
-        # a fixed shape applies to the whole run (profiling runs)
+        # a fixed shape and lists apply to the whole run (profiling runs)
         sim.set_pair_shape(args.pair_shape)
-        tuned = {"pair_shape": args.pair_shape, "skin_over_h": 0.05, "steps_per_trial": 0}
+        skin = 0.05 if args.skin is None else args.skin
+        sim.set_skin(skin)
+        if args.wide is not None:
+            sim.set_wide_skin(args.wide)
+        tuned = {"pair_shape": args.pair_shape, "skin_over_h": skin, "wide_over_h": sim.wide_skin(),
+                 "steps_per_trial": 0}
     if args.start_step > 0:
         sim.step(args.start_step)
     if args.pair_shape is None and not args.no_autotune:
         # the project's autotuner: pair-kernel launch shape and list skin by
         # timing, the state left as it was (outside the timed region)
         shape, skin = sim.autotune(args.tune_steps)
-        tuned = {"pair_shape": shape, "skin_over_h": skin, "steps_per_trial": args.tune_steps}
+        tuned = {"pair_shape": shape, "skin_over_h": skin, "wide_over_h": sim.wide_skin(),
+                 "steps_per_trial": args.tune_steps}
     sim.step(args.warmup)
     sim.synchronize()
-    rb0 = sim.rebuilds()
+    rb0, rn0 = sim.rebuilds(), sim.renewals()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -408,8 +418,9 @@ def bench_ours(args):
     ms = replicas.max_over_ranks(start.elapsed_time(end), device="cuda")
     shep_steps = sum(1 for s in range(s0, s1) if par.stress_shepard_filter and s % par.stress_shepard_filter == 0
                      and s != 0)
-    rebuilds = sim.rebuilds() - rb0
-    launches = (s1 - s0) * plain + shep_steps * (with_shep - plain) + rebuilds * sim.rebuild_launches()
+    rebuilds, renewals = sim.rebuilds() - rb0, sim.renewals() - rn0
+    launches = ((s1 - s0) * plain + shep_steps * (with_shep - plain) + rebuilds * sim.rebuild_launches()
+                + renewals * sim.renewal_launches())
     value = npm * args.steps * world / (ms / 1e3)
     health = sim.health()
 
@@ -417,7 +428,7 @@ def bench_ours(args):
     # rate, so its time per step carries their amortised cost
     amortized = None
     if args.amortized_steps > 0:
-        rb_a = sim.rebuilds()
+        rb_a, rn_a = sim.rebuilds(), sim.renewals()
         sim.synchronize()
         if dist:
             dist.barrier()
@@ -430,7 +441,8 @@ def bench_ours(args):
         ams = replicas.max_over_ranks(a0.elapsed_time(a1), device="cuda")
         amortized = {"form": args.form, "value": npm * args.amortized_steps * world / (ams / 1e3),
                      "ms_per_step": ams / args.amortized_steps, "steps": args.amortized_steps,
-                     "neighbour_list_rebuilds": sim.rebuilds() - rb_a}
+                     "neighbour_list_rebuilds": sim.rebuilds() - rb_a,
+                     "neighbour_list_renewals": sim.renewals() - rn_a}
 
     # live per-phase device times (eager launches, CUDA events on the same stream)
     prof = sim.profile(args.profile_steps) if args.profile_steps > 0 else {}
@@ -483,10 +495,12 @@ def bench_ours(args):
         if args.pair_shape is None and not args.no_autotune:
             # each form tuned on its own: its best launch shape and skin
             shape, skin = osim.autotune(args.tune_steps)
-            other_tuned = {"pair_shape": shape, "skin_over_h": skin, "steps_per_trial": args.tune_steps}
+            other_tuned = {"pair_shape": shape, "skin_over_h": skin, "wide_over_h": osim.wide_skin(),
+                           "steps_per_trial": args.tune_steps}
         elif tuned:
             osim.set_pair_shape(tuned["pair_shape"])
             osim.set_skin(tuned["skin_over_h"])
+            osim.set_wide_skin(tuned.get("wide_over_h", 0.0))
         osim.step(args.warmup)
         osim.synchronize()
         if dist:
@@ -511,7 +525,10 @@ def bench_ours(args):
 
     ensemble = None
     if not args.no_ensemble and args.config == "cylinder":
-        ensemble = ensemble_measurement(args, torch, world, rank, local, dist)
+        # a window long enough that list sorts and renewals come at their
+        # natural rate (the line's own value keeps exactly --steps steps)
+        ensemble = ensemble_measurement(args, torch, world, rank, local, dist,
+                                        steps=max(args.steps, ENSEMBLE_KEY_STEPS))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -545,6 +562,7 @@ def bench_ours(args):
             "forms": forms,
             "gpu_launches": launches,
             "neighbour_list_rebuilds": rebuilds,
+            "neighbour_list_renewals": renewals,
             "health": [int(x) for x in health],
             "clocks": clk,
             "e2e": e2e,
@@ -569,7 +587,11 @@ def size_classes(counts, nclass=4):
     return [list(np.nonzero(cls == k)[0]) for k in range(nclass) if np.any(cls == k)]
 
 
-def ensemble_measurement(args, torch, world, rank, local, dist, sample_clocks=False):
+# timed steps of the ensemble measurement carried by the default line
+ENSEMBLE_KEY_STEPS = 100
+
+
+def ensemble_measurement(args, torch, world, rank, local, dist, sample_clocks=False, steps=None):
     """Batched ensemble of config 4 (one simulation holding every scenario,
     one graph launch per step) in both precision forms, against the same
     scenarios run one after another, each as its own plain simulation.  The
@@ -577,7 +599,8 @@ def ensemble_measurement(args, torch, world, rank, local, dist, sample_clocks=Fa
     size class (one autotuner run on the median scenario of each of four
     log-spaced particle-count classes, its shape and skin applied to the
     class).  All timed with CUDA events on the simulations' streams after
-    the same warm-up; max over ranks."""
+    the same warm-up; max over ranks.  `steps` (default --steps) is the
+    timed window of every run."""
     import loquat_b200 as lq
     from loquat_b200 import cases, replicas
 
@@ -586,6 +609,7 @@ def ensemble_measurement(args, torch, world, rank, local, dist, sample_clocks=Fa
     parts = [all_parts[k] for k in shares[rank]]
     comb = cases.combine(parts)
     par = comb.par
+    nsteps = steps or args.steps
     total_npm = sum(p.par.npm for p in all_parts)
 
     def timed(sim, steps):
@@ -606,23 +630,25 @@ def ensemble_measurement(args, torch, world, rank, local, dist, sample_clocks=Fa
         tuned = None
         if not args.no_autotune:
             shape, skin = sim.autotune(args.tune_steps)
-            tuned = {"pair_shape": shape, "skin_over_h": skin, "steps_per_trial": args.tune_steps}
+            tuned = {"pair_shape": shape, "skin_over_h": skin, "wide_over_h": sim.wide_skin(),
+                     "steps_per_trial": args.tune_steps}
         return sim, tuned
 
     forms, tuned_by_form, extra = {}, {}, {}
     for form in (args.form, "plain" if args.form == "mixed" else "mixed"):
         sim, tuned = batched(form == "mixed")
-        rb0 = sim.rebuilds()
+        rb0, rn0 = sim.rebuilds(), sim.renewals()
         sim.synchronize()
         if dist:
             dist.barrier()
         clocks = ClockSampler(gpu_uuid(torch, local)) if (sample_clocks and rank == 0 and not forms) else None
-        ms = replicas.max_over_ranks(timed(sim, args.steps), device="cuda")
+        ms = replicas.max_over_ranks(timed(sim, nsteps), device="cuda")
         if not forms:
             extra = {"clocks": clocks.stop() if clocks else None, "neighbour_list_rebuilds": sim.rebuilds() - rb0,
+                     "neighbour_list_renewals": sim.renewals() - rn0,
                      "health": [int(x) for x in sim.health()], "gpu_launches_per_step": sim.launches_per_step()[0]}
         sim.close()
-        forms[form] = {"value": total_npm * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps}
+        forms[form] = {"value": total_npm * nsteps / (ms / 1e3), "ms_per_step": ms / nsteps}
         tuned_by_form[form] = tuned
 
     # sequential plain runs, tuned by size class
@@ -636,28 +662,30 @@ def ensemble_measurement(args, torch, world, rank, local, dist, sample_clocks=Fa
             s = lq.Simulation(p.par, *p.arrays())
             s.step(args.warmup)
             shape, skin = s.autotune(args.tune_steps)
+            wide = s.wide_skin()
             s.close()
             for k in members:
-                seq_shape[k] = (shape, skin)
+                seq_shape[k] = (shape, skin, wide)
             class_tuning.append({"scenarios": len(members), "representative_npm": counts[rep],
-                                 "pair_shape": shape, "skin_over_h": skin})
+                                 "pair_shape": shape, "skin_over_h": skin, "wide_over_h": wide})
     ms_seq = 0.0
     for k, p in enumerate(parts):
         s = lq.Simulation(p.par, *p.arrays())
         if k in seq_shape:
             s.set_pair_shape(seq_shape[k][0])
             s.set_skin(seq_shape[k][1])
+            s.set_wide_skin(seq_shape[k][2])
         s.step(args.warmup)
-        ms_seq += timed(s, args.steps)
+        ms_seq += timed(s, nsteps)
         s.close()
     ms_seq = replicas.max_over_ranks(ms_seq, device="cuda")
-    v_seq = total_npm * args.steps / (ms_seq / 1e3)
+    v_seq = total_npm * nsteps / (ms_seq / 1e3)
     out = {
         "workload": "ensemble of %d Drucker-Prager column collapses (counts log-uniform 5e3-2e5, H/L 0.5-4, "
                     "phi 20-40 deg, c 0-5 kPa, dr=2 mm, h=1.2dr)" % args.scenarios,
-        "npm": total_npm, "rank0_np": par.np, "rank0_ncell": par.ncell, "steps": args.steps,
+        "npm": total_npm, "rank0_np": par.np, "rank0_ncell": par.ncell, "steps": nsteps,
         "forms": forms,
-        "sequential": {"value": v_seq, "ms_per_step": ms_seq / args.steps,
+        "sequential": {"value": v_seq, "ms_per_step": ms_seq / nsteps,
                        "form": "the same scenarios one after another, one plain FP32 simulation each, tuned by "
                                "size class", "tuning": class_tuning},
         "batched_over_sequential": {f: forms[f]["value"] / v_seq for f in forms},
@@ -694,7 +722,8 @@ def bench_ensemble(args):
             "forms": m["forms"], "sequential": m["sequential"],
             "batched_over_sequential": m["batched_over_sequential"][args.form],
             "autotuned": m["autotuned"], "gpu_launches_per_step": m["gpu_launches_per_step"],
-            "neighbour_list_rebuilds": m["neighbour_list_rebuilds"], "health": m["health"],
+            "neighbour_list_rebuilds": m["neighbour_list_rebuilds"],
+            "neighbour_list_renewals": m["neighbour_list_renewals"], "health": m["health"],
             "clocks": m["clocks"], "partition": m["partition"],
         }))
     if dist:

@@ -201,6 +201,19 @@ int lq_sim_health(void* sim, int* health4);
  * rebuild before the next step.  lq_sim_rebuilds counts rebuilds so far. */
 int lq_sim_set_skin(void* sim, float skin_over_h);
 int lq_sim_rebuilds(void* sim, long long* count);
+/* Two-level lists: with wide_over_h above the skin, a rebuild builds wider
+ * lists (every pair within 2h + wide) and the lists the stages read are
+ * renewed from them at the current positions, without a search, whenever
+ * the skin runs out; the search and sort wait until a particle has moved
+ * (wide - skin) / 2 from its position at the wide build.  0 (the default)
+ * or a value not above the skin gives one-level lists.  Forces a rebuild
+ * before the next step; the first call allocates the wide lists.
+ * lq_sim_wide_skin reads the setting in effect (0 for one level),
+ * lq_sim_renewals counts renewals without a search so far.  No reference
+ * counterpart. */
+int lq_sim_set_wide_skin(void* sim, float wide_over_h);
+int lq_sim_wide_skin(void* sim, float* wide_over_h);
+int lq_sim_renewals(void* sim, long long* count);
 /* Per-object materials, for many independent scenarios in one simulation
  * (each scenario's particles placed farther than 2h from the others):
  * a material particle uses row (int)idep.x of the n x 5 host table (the
@@ -227,9 +240,12 @@ int lq_sim_set_hypoplastic(void* sim, int n, const float* table);
  * No reference counterpart. */
 int lq_sim_set_frames(void* sim, int n, const int* rows);
 /* Own kernel launches of a step without a rebuild (plain) and of a step
- * with the Shepard pass; a rebuild adds lq_sim_rebuild_launches more. */
+ * with the Shepard pass; a rebuild adds lq_sim_rebuild_launches more (the
+ * renewal that follows it with two-level lists included) and a renewal
+ * without a search lq_sim_renewal_launches. */
 int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard);
 int lq_sim_rebuild_launches(void* sim, int* launches);
+int lq_sim_renewal_launches(void* sim, int* launches);
 /* Launch shape of the pair kernel.  0-4: one thread per target in slot
  * order, threads per block x resident blocks per SM (which caps its
  * registers): 0 = 128 x 6, 1 = 64 x 12, 2 = 256 x 3, 3 = 128 x 5,
@@ -244,13 +260,17 @@ int lq_sim_rebuild_launches(void* sim, int* launches);
  * blocks on every SM, else with shape 0.  No reference counterpart. */
 int lq_sim_set_pair_shape(void* sim, int shape);
 int lq_sim_pair_shape(void* sim, int* shape);
-/* Autotuner: times `steps` steps (after two untimed ones) for each pair
- * kernel shape at the current skin, then for skins of 0.02, 0.05, 0.1 and
- * 0.2 h with the fastest shape, and keeps the fastest pair.  Every trial
- * starts from a device copy of the state taken at the call, and the state,
- * step, time and health word are put back afterwards, so tuning does not
- * advance the simulation (it rebuilds its lists before the next step).
- * Allocates the state copy for the duration of the call. */
+/* Autotuner: times `steps` steps for each pair kernel shape at the current
+ * lists, then for one-level skins of 0.02, 0.05, 0.1 and 0.2 h with the
+ * fastest shape, then two-level lists over the fastest skin with wide
+ * margins of 0.1 and 0.2 h, and keeps the fastest setting (the wide one is
+ * read with lq_sim_wide_skin).  Every trial starts from a device copy of
+ * the state taken at the call and its window opens with the search and
+ * list build that start every run, so settings whose lists last long pay
+ * for one build per window.  The state, step, time and health word are put
+ * back afterwards, so tuning does not advance the simulation (it rebuilds
+ * its lists before the next step).  Allocates the state copy for the
+ * duration of the call. */
 int lq_sim_autotune(void* sim, int steps, int* shape, float* skin_over_h);
 /* Bounds violations counted so far in this process by a library built with
  * -D LQ_CHECKED (loquat_b200/liblqb200_checked.so): its list and grid
@@ -275,11 +295,12 @@ int lq_sim_load_checkpoint(const char* path, int flags, void** sim);
 int lq_sim_neighbor_entries(void* sim, long long* material, long long* boundary);
 /* Advances nsteps steps launching kernels one by one with CUDA events
  * around each phase, then synchronises and returns the summed device time
- * per phase in phase_ms[7]: search, gather, Adami, interaction pairs,
- * integrate, Shepard, neighbour-list build (the phases of the reference's
- * Timer, include/types.h:158-173, timed on the device instead of with
- * std::clock, with the search and the list build split out).
- * phase_launches[7] (may be NULL) receives how many times each phase ran. */
+ * per phase in phase_ms[8]: search, gather, Adami, interaction pairs,
+ * integrate, Shepard, neighbour-list build, renewal of two-level lists
+ * (the phases of the reference's Timer, include/types.h:158-173, timed on
+ * the device instead of with std::clock, with the search and the list
+ * build and renewal split out).  phase_launches[8] (may be NULL) receives
+ * how many times each phase ran. */
 int lq_sim_profile(void* sim, int nsteps, double* phase_ms, int* phase_launches);
 
 /* ---- XML / .dat formats (reference src/loquat_io.cu:69-370) ------------ */

@@ -78,6 +78,10 @@ _SIGNATURES = {
     "lq_sim_set_frames": (_I, [_VP, _I, _VP]),
     "lq_sim_rebuilds": (_I, [_VP, ctypes.POINTER(_LL)]),
     "lq_sim_rebuild_launches": (_I, [_VP, ctypes.POINTER(_I)]),
+    "lq_sim_set_wide_skin": (_I, [_VP, _F]),
+    "lq_sim_wide_skin": (_I, [_VP, ctypes.POINTER(_F)]),
+    "lq_sim_renewals": (_I, [_VP, ctypes.POINTER(_LL)]),
+    "lq_sim_renewal_launches": (_I, [_VP, ctypes.POINTER(_I)]),
     "lq_sim_set_pair_shape": (_I, [_VP, _I]),
     "lq_sim_pair_shape": (_I, [_VP, ctypes.POINTER(_I)]),
     "lq_sim_autotune": (_I, [_VP, _I, ctypes.POINTER(_I), ctypes.POINTER(_F)]),
@@ -327,7 +331,7 @@ class Simulation:
         check(lib().lq_sim_health(self.handle, h.ctypes.data), "lq_sim_health")
         return h
 
-    PHASES = ("search", "gather", "adami", "interaction", "integrate", "shepard", "list")
+    PHASES = ("search", "gather", "adami", "interaction", "integrate", "shepard", "list", "renew")
 
     def profile(self, n: int) -> dict:
         """Runs n steps eagerly with CUDA events around each phase; returns
@@ -366,6 +370,28 @@ class Simulation:
     def rebuild_launches(self) -> int:
         c = _I()
         check(lib().lq_sim_rebuild_launches(self.handle, ctypes.byref(c)), "lq_sim_rebuild_launches")
+        return c.value
+
+    def set_wide_skin(self, wide_over_h: float):
+        """Two-level lists: wide lists with cut-off 2h + wide_over_h h from
+        each sort, the stages' lists renewed from them without a search; 0
+        (or a value not above the skin) gives one-level lists."""
+        check(lib().lq_sim_set_wide_skin(self.handle, wide_over_h), "lq_sim_set_wide_skin")
+
+    def wide_skin(self) -> float:
+        c = _F()
+        check(lib().lq_sim_wide_skin(self.handle, ctypes.byref(c)), "lq_sim_wide_skin")
+        return c.value
+
+    def renewals(self) -> int:
+        """Lists renewed from the wide lists without a search so far."""
+        c = _LL()
+        check(lib().lq_sim_renewals(self.handle, ctypes.byref(c)), "lq_sim_renewals")
+        return c.value
+
+    def renewal_launches(self) -> int:
+        c = _I()
+        check(lib().lq_sim_renewal_launches(self.handle, ctypes.byref(c)), "lq_sim_renewal_launches")
         return c.value
 
     def set_pair_shape(self, shape: int):

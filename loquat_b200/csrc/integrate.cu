@@ -180,7 +180,32 @@ struct VerletCheck {
     int* rebuild;
     float half_skin;
     float dt_bound;   /* the largest step the next one can take */
+    const float4* xwide;   /* two-level lists: positions at the wide build */
+    float half_margin;     /* (wide - skin) / 2 */
 };
+
+/* The list checks of one material particle at its new position x. */
+__device__ __forceinline__ void verlet_check(const VerletCheck& vc, int i, const float4& x, const float4& v,
+                                             const float4& a)
+{
+    const float4 xb = __ldg(vc.xbuild + i);
+    const float dx = x.x - xb.x, dy = x.y - xb.y, dz = x.z - xb.z;
+    const float moved = sqrtf(dx * dx + dy * dy + dz * dz);
+    const float speed = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
+    const float accel = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
+    /* next step: the predictor half step and the corrector full step
+     * move a particle by at most dt |v| + dt^2 |a| each; 2x covers both */
+    const float dtb = vc.dt_bound;
+    const float ahead = 2.0f * dtb * (speed + dtb * accel);
+    if (!(moved + ahead < vc.half_skin)) atomicOr(vc.rebuild, 1);
+    if (vc.xwide) {
+        /* lists renewed at x from the wide ones hold every pair within
+         * 2h + skin while no particle is (wide - skin) / 2 from xwide */
+        const float4 xw = __ldg(vc.xwide + i);
+        const float ex = x.x - xw.x, ey = x.y - xw.y, ez = x.z - xw.z;
+        if (!(sqrtf(ex * ex + ey * ey + ez * ez) < vc.half_margin)) atomicOr(vc.rebuild, 2);
+    }
+}
 
 template <bool kMixed, bool kVW>
 __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(const Parameters* __restrict__ P, int np, int npb, State cur,
@@ -251,16 +276,7 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(
         store_t2(out.stn, i, e);
         const bool bad = !(isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(v.x) && isfinite(v.y) &&
                            isfinite(v.z) && isfinite(v.w));
-        if (verlet.xbuild) {
-            const float4 xb = __ldg(verlet.xbuild + i);
-            const float dx = x.x - xb.x, dy = x.y - xb.y, dz = x.z - xb.z;
-            const float moved = sqrtf(dx * dx + dy * dy + dz * dz);
-            const float speed = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
-            const float accel = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
-            const float dtb = verlet.dt_bound;
-            const float ahead = 2.0f * dtb * (speed + dtb * accel);
-            if (!(moved + ahead < verlet.half_skin)) atomicOr(verlet.rebuild, 1);
-        }
+        if (verlet.xbuild) verlet_check(verlet, i, x, v, a);
         T6d sd = widen6(s0);
         double evd = id0.z;
         vw_update_d(vw_const(vw, id.x), (double)dt, de, w, sd, evd);
@@ -330,18 +346,7 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(
                         isfinite(s.xy) && isfinite(s.xz) && isfinite(s.yz);
         if (!ok) atomicAdd(health + HEALTH_NONFINITE, 1);
     }
-    if (verlet.xbuild) {
-        const float4 xb = __ldg(verlet.xbuild + i);
-        const float dx = x.x - xb.x, dy = x.y - xb.y, dz = x.z - xb.z;
-        const float moved = sqrtf(dx * dx + dy * dy + dz * dz);
-        const float speed = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
-        const float accel = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
-        /* next step: the predictor half step and the corrector full step
-         * move a particle by at most dt |v| + dt^2 |a| each; 2x covers both */
-        const float dtb = verlet.dt_bound;
-        const float ahead = 2.0f * dtb * (speed + dtb * accel);
-        if (!(moved + ahead < verlet.half_skin)) atomicOr(verlet.rebuild, 1);
-    }
+    if (verlet.xbuild) verlet_check(verlet, i, x, v, a);
 }
 
 }  // namespace
@@ -376,7 +381,7 @@ int launch_correct(const Parameters* ph, const Parameters* pd, const State& cur,
     if (ph->constitutive_model == 3)
         return set_error(LQ_ERR_ARG, "corrector: constitutive model 3 needs a von Wolffersdorff table");
     k_correct<false, false><<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, ini_idx, cur, r, health,
-                                                             VerletCheck{nullptr, nullptr, 0.0f, 0.0f}, ph->npb,
+                                                             VerletCheck{nullptr, nullptr, 0.0f, 0.0f, nullptr, 0.0f}, ph->npb,
                                                              MaterialTable(), MaterialTable());
     LQ_TRY_CUDA(cudaGetLastError(), "k_correct");
     return LQ_OK;
@@ -384,13 +389,15 @@ int launch_correct(const Parameters* ph, const Parameters* pd, const State& cur,
 
 int launch_correct_into(const Parameters* ph, const Parameters* pd, const State& cur, const State& ini,
                         const State& out, const Rates& r, int* health, const float4* xbuild, int* rebuild,
-                        float skin, cudaStream_t s, const MaterialTable& mt, const MaterialTable& vw)
+                        float skin, cudaStream_t s, const MaterialTable& mt, const MaterialTable& vw,
+                        const float4* xwide, float wide)
 {
     if (ph->np <= 0) return LQ_OK;
     if (ph->constitutive_model == 3 && (!vw.p || vw.n <= 0))
         return set_error(LQ_ERR_ARG, "corrector: constitutive model 3 needs a von Wolffersdorff table");
     /* a dynamic step never exceeds the fixed one, cfl h / cs (ph->dt) */
-    const VerletCheck vc{xbuild, rebuild, 0.5f * skin, ph->dt};
+    if (xwide && !(wide > skin)) return set_error(LQ_ERR_ARG, "corrector: the wide cut-off must exceed the skin");
+    const VerletCheck vc{xbuild, rebuild, 0.5f * skin, ph->dt, xwide, 0.5f * (wide - skin)};
     const bool vwm = ph->constitutive_model == 3;
     const int nb = blocks_for(ph->np, kBlock);
     if (cur.xlo && ini.xlo && out.xlo) {

@@ -216,12 +216,16 @@ int launch_correct(const Parameters* par_host, const Parameters* par_dev, const 
 
 /* Corrector from snapshot `ini` and current `cur` into `out` (boundary
  * slots take cur's stress; the rest of a boundary slot must already be the
- * same in both); material particles raise *rebuild when neighbour lists
- * built at xbuild with this skin may not hold through the next step. */
+ * same in both); material particles raise bit 1 of *rebuild when neighbour
+ * lists built at xbuild with this skin may not hold through the next step,
+ * and (with xwide) bit 2 when a particle has moved (wide - skin) / 2 or
+ * more from xwide, where lists with cut-off 2h + wide were built: lists
+ * renewed from those now could miss a pair. */
 int launch_correct_into(const Parameters* par_host, const Parameters* par_dev, const State& cur, const State& ini,
                         const State& out, const Rates& r, int* health, const float4* xbuild, int* rebuild,
                         float skin, cudaStream_t s, const MaterialTable& mt = MaterialTable(),
-                        const MaterialTable& vw = MaterialTable());
+                        const MaterialTable& vw = MaterialTable(), const float4* xwide = nullptr,
+                        float wide = 0.0f);
 
 /* List-driven Shepard filter (material targets and neighbours); a target
  * whose list overflowed walks its 27 cells in `c` instead. */
@@ -238,6 +242,10 @@ int launch_density_filter_list(const Parameters* par_host, const Parameters* par
 int launch_neighbor_list_range(const Parameters* par_host, const Parameters* par_dev, int first, int n, int layer_lo,
                                float cut, const float4* pos, const Cells& c, const NeighborList& nl, int* health,
                                cudaStream_t s, const float4* idep = nullptr, const Frames& fr = Frames());
+/* Lists of targets [first, first + n) with cut-off `cut` renewed from
+ * their wide lists at the positions pos (two-level lists). */
+int launch_list_refresh(const Parameters* par_host, int first, int n, float cut, const float4* pos,
+                        const NeighborList& wide, const NeighborList& nl, cudaStream_t s);
 /* Fills n ints with v; adds v to one int. */
 int fill_int(int* p, int n, int v, cudaStream_t s);
 int add_int(int* p, int v, cudaStream_t s);

@@ -24,6 +24,13 @@
  * graphs (or if the driver cannot build the conditional node) the host
  * reads the flag before each step, which gives the same sequence of
  * rebuilds.  dt = cfl h / cs is constant, as in the reference.
+ *
+ * Two-level lists (a wide cut-off 2h + wide above 2h + skin): the rebuild
+ * after a sort builds wide lists, and the lists the stages read are renewed
+ * from them (filtered at the current positions, no search) whenever the
+ * skin runs out; a sort happens only once a particle has moved
+ * (wide - skin) / 2 from its position at the wide build.  A second IF node
+ * holds the renewal.
  */
 #include <cstdint>
 #include <cstdio>
@@ -53,6 +60,10 @@ struct LqSim {
     cudaStream_t side = nullptr;       /* captures the rebuild body */
     State S{}, S2{}, T{};
     float4* xbuild = nullptr;          /* positions when the lists were built */
+    float wide = 0.0f;                 /* two-level lists: wide cut-off 2h + wide (0: one level) */
+    float4* xwide = nullptr;           /* positions when the wide lists were built */
+    lqb::NeighborList wlm, wlb;        /* wide lists of material and boundary targets */
+    int* renewals = nullptr;           /* device counter of lists renewed from the wide ones */
     lqb::Rates R{};
     lqb::GridBuffers g;
     lqb::NeighborList nlm, nlb;        /* material targets, boundary targets */
@@ -87,6 +98,26 @@ int dev_alloc(LqSim* S, void** p, size_t bytes)
 }
 
 bool tiled(const LqSim* S) { return lqb::kPairShapes[S->pair_shape][2] != 0; }
+
+/* Bits of the device flag: the lists must be renewed before the next step;
+ * the wide lists no longer cover a renewal (a sort is due). */
+constexpr int kFlagLists = 1, kFlagSort = 2, kFlagAll = 3;
+
+bool two_level(const LqSim* S) { return S->wide > S->skin && S->wlm.list != nullptr; }
+
+/* Wide lists and their build positions, on first use of two-level lists. */
+int ensure_wide_lists(LqSim* S)
+{
+    if (S->wlm.list) return LQ_OK;
+    LQ_TRY(dev_alloc(S, (void**)&S->xwide, (size_t)S->np * sizeof(float4)));
+    S->wlm.stride = S->nlm.stride;
+    LQ_TRY(dev_alloc(S, (void**)&S->wlm.list, sizeof(int) * (size_t)LQ_NBR_CAP * S->wlm.stride));
+    LQ_TRY(dev_alloc(S, (void**)&S->wlm.count, sizeof(int) * (size_t)S->wlm.stride));
+    S->wlb.stride = S->nlb.stride;
+    LQ_TRY(dev_alloc(S, (void**)&S->wlb.list, sizeof(int) * (size_t)LQ_NBR_CAP * S->wlb.stride));
+    LQ_TRY(dev_alloc(S, (void**)&S->wlb.count, sizeof(int) * (size_t)S->wlb.stride));
+    return LQ_OK;
+}
 
 /* The pair kernel's target order for tiled launch shapes (null otherwise). */
 const int* tile_order(const LqSim* S) { return tiled(S) ? S->tile.order : nullptr; }
@@ -209,11 +240,32 @@ __global__ void k_copy_t2(int first, int n, const tensor2d* __restrict__ in, ten
 __global__ void k_decide(cudaGraphConditionalHandle h, int* flag, int* count)
 {
     const int f = *flag;
-    cudaGraphSetConditional(h, f ? 1u : 0u);
-    if (f) {
-        *flag = 0;
-        *count += 1;
-    }
+    cudaGraphSetConditional(h, (f & kFlagLists) ? 1u : 0u);
+    if (f & kFlagLists) *count += 1;
+    *flag = 0;
+}
+
+/* Two-level lists: a sort and wide build when the lists are due and the
+ * wide ones no longer cover a renewal; a renewal whenever the lists are
+ * due (after a sort too, which leaves only wide lists). */
+__global__ void k_decide2(cudaGraphConditionalHandle h_sort, cudaGraphConditionalHandle h_renew, int* flag,
+                          int* sorts, int* renewals)
+{
+    const int f = *flag;
+    const bool due = (f & kFlagLists) != 0;
+    const bool sort = due && (f & kFlagSort) != 0;
+    cudaGraphSetConditional(h_sort, sort ? 1u : 0u);
+    cudaGraphSetConditional(h_renew, due ? 1u : 0u);
+    if (sort) *sorts += 1;
+    else if (due) *renewals += 1;
+    *flag = 0;
+}
+
+/* The positions the current lists were renewed at. */
+__global__ void k_record_positions(int n, const float4* __restrict__ pos, float4* __restrict__ xbuild)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) xbuild[i] = pos[i];
 }
 
 inline int blocks(int n) { return (n + 255) / 256; }
@@ -269,17 +321,32 @@ __global__ void k_dt_update(Parameters* P, unsigned* m2, double* time)
 
 /* ------------------------------------------------------------ sequences */
 
-/* Material and boundary lists from the sorted state in S. */
+/* Material and boundary lists from the sorted state in S: the lists the
+ * stages read, or with two-level lists the wide ones. */
 int build_lists(LqSim* S, cudaStream_t s)
 {
     const Parameters* ph = &S->ph;
     const Parameters* pd = S->pd;
     const lqb::Cells cells{S->g.start, nullptr, nullptr};
+    const bool two = two_level(S);
+    const float cut = 2.0f * ph->h + (two ? S->wide : S->skin);
+    LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, S->npb, S->npm, 0, cut, S->S.pos, cells, two ? S->wlm : S->nlm,
+                                           S->health, s, S->S.idep, S->fr));
+    return lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, two ? S->wlb : S->nlb,
+                                           S->health, s, S->S.idep, S->fr);
+}
+
+/* Two-level lists: the lists the stages read renewed from the wide ones at
+ * the current positions, and those positions recorded. */
+int enqueue_renewal(LqSim* S, cudaStream_t s)
+{
+    const Parameters* ph = &S->ph;
     const float cut = 2.0f * ph->h + S->skin;
-    LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, S->npb, S->npm, 0, cut, S->S.pos, cells, S->nlm, S->health, s,
-                                           S->S.idep, S->fr));
-    return lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, S->nlb, S->health, s,
-                                           S->S.idep, S->fr);
+    LQ_TRY(lqb::launch_list_refresh(ph, S->npb, S->npm, cut, S->S.pos, S->wlm, S->nlm, s));
+    LQ_TRY(lqb::launch_list_refresh(ph, 0, S->npb, cut, S->S.pos, S->wlb, S->nlb, s));
+    k_record_positions<<<blocks(S->np), 256, 0, s>>>(S->np, S->S.pos, S->xbuild);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_record_positions");
+    return LQ_OK;
 }
 
 /* The pair sums of a stage in the current launch shape. */
@@ -297,7 +364,8 @@ int enqueue_rebuild(LqSim* S, cudaStream_t s)
     const Parameters* pd = S->pd;
     LQ_TRY(lqb::grid_search(ph, pd, S->S.pos, S->g, false, S->health, s, S->S.idep, S->fr));
     LQ_TRY(lqb::gather_state(S->np, S->g.part_idx, S->S, S->T, s));
-    k_copy_state<<<blocks(S->np), 256, 0, s>>>(S->np, S->npb, S->T, S->S, S->S2, S->xbuild);
+    k_copy_state<<<blocks(S->np), 256, 0, s>>>(S->np, S->npb, S->T, S->S, S->S2,
+                                               two_level(S) ? S->xwide : S->xbuild);
     LQ_TRY_CUDA(cudaGetLastError(), "k_copy_state");
     LQ_TRY(build_lists(S, s));
     /* every slot's packed neighbour data (the boundary slots keep theirs
@@ -355,7 +423,7 @@ int enqueue_stages(LqSim* S, cudaStream_t s)
     LQ_TRY(enqueue_adami_pack(S, S->S2, s));
     LQ_TRY(enqueue_interaction(S, S->S2, s));
     LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild, S->skin, s,
-                                    S->mt, S->vw));
+                                    S->mt, S->vw, two_level(S) ? S->xwide : nullptr, S->wide));
     return enqueue_dynamic_dt(S, s);
 }
 
@@ -371,7 +439,42 @@ int enqueue_shepard(LqSim* S, cudaStream_t s)
     return LQ_OK;
 }
 
-/* Step graph: decide -> IF(rebuild) -> stages. */
+/* An IF node on handle h after the capture's current dependencies, its body
+ * captured from `body` on the side stream; the capture continues after it. */
+int capture_if(LqSim* S, cudaGraphConditionalHandle h, int (*body)(LqSim*, cudaStream_t))
+{
+    cudaStream_t s = S->stream;
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    LQ_TRY_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &ndeps), "capture info");
+    /* the parameter record's C union has no usable C++ default
+     * constructor: zero raw storage and view it as the record */
+    alignas(cudaGraphNodeParams) unsigned char cp_raw[sizeof(cudaGraphNodeParams)];
+    memset(cp_raw, 0, sizeof(cp_raw));
+    cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_raw);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    LQ_TRY_CUDA(cudaGraphAddNode(&cnode, cg, deps, ndeps, &cp), "conditional node");
+    cudaGraph_t graph_body = cp.conditional.phGraph_out[0];
+    LQ_TRY_CUDA(cudaStreamBeginCaptureToGraph(S->side, graph_body, nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal),
+                "body capture");
+    const int st = body(S, S->side);
+    cudaGraph_t body_out = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(S->side, &body_out);
+    LQ_TRY(st);
+    LQ_TRY_CUDA(e, "body end capture");
+    LQ_TRY_CUDA(cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies),
+                "capture dependencies");
+    return LQ_OK;
+}
+
+/* Step graph: decide -> IF(rebuild) [-> IF(renewal)] -> stages. */
 int capture_step(LqSim* S)
 {
     cudaStream_t s = S->stream;
@@ -381,40 +484,21 @@ int capture_step(LqSim* S)
     do {
         cudaStreamCaptureStatus cs;
         cudaGraph_t cg = nullptr;
-        const cudaGraphNode_t* deps = nullptr;
-        size_t ndeps = 0;
-        cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &ndeps);
+        cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, nullptr, nullptr);
         if (e != cudaSuccess) { st = lqb::cuda_status(e, "capture info"); break; }
-        cudaGraphConditionalHandle h;
-        e = cudaGraphConditionalHandleCreate(&h, cg, 0, 0);
+        cudaGraphConditionalHandle h_sort, h_renew;
+        e = cudaGraphConditionalHandleCreate(&h_sort, cg, 0, 0);
+        if (e == cudaSuccess && two_level(S)) e = cudaGraphConditionalHandleCreate(&h_renew, cg, 0, 0);
         if (e != cudaSuccess) { st = lqb::cuda_status(e, "conditional handle"); break; }
-        k_decide<<<1, 1, 0, s>>>(h, S->rebuild, S->rebuilds);
+        if (two_level(S))
+            k_decide2<<<1, 1, 0, s>>>(h_sort, h_renew, S->rebuild, S->rebuilds, S->renewals);
+        else
+            k_decide<<<1, 1, 0, s>>>(h_sort, S->rebuild, S->rebuilds);
         e = cudaGetLastError();
         if (e != cudaSuccess) { st = lqb::cuda_status(e, "k_decide"); break; }
-        e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &ndeps);
-        if (e != cudaSuccess) { st = lqb::cuda_status(e, "capture info"); break; }
-        /* the parameter record's C union has no usable C++ default
-         * constructor: zero raw storage and view it as the record */
-        alignas(cudaGraphNodeParams) unsigned char cp_raw[sizeof(cudaGraphNodeParams)];
-        memset(cp_raw, 0, sizeof(cp_raw));
-        cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_raw);
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = h;
-        cp.conditional.type = cudaGraphCondTypeIf;
-        cp.conditional.size = 1;
-        cudaGraphNode_t cnode;
-        e = cudaGraphAddNode(&cnode, cg, deps, ndeps, &cp);
-        if (e != cudaSuccess) { st = lqb::cuda_status(e, "conditional node"); break; }
-        cudaGraph_t body = cp.conditional.phGraph_out[0];
-        e = cudaStreamBeginCaptureToGraph(S->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) { st = lqb::cuda_status(e, "body capture"); break; }
-        st = enqueue_rebuild(S, S->side);
-        cudaGraph_t body_out = nullptr;
-        e = cudaStreamEndCapture(S->side, &body_out);
+        st = capture_if(S, h_sort, enqueue_rebuild);
+        if (st == LQ_OK && two_level(S)) st = capture_if(S, h_renew, enqueue_renewal);
         if (st != LQ_OK) break;
-        if (e != cudaSuccess) { st = lqb::cuda_status(e, "body end capture"); break; }
-        e = cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies);
-        if (e != cudaSuccess) { st = lqb::cuda_status(e, "capture dependencies"); break; }
         st = enqueue_stages(S, s);
     } while (0);
     cudaError_t e = cudaStreamEndCapture(s, &graph);
@@ -449,26 +533,31 @@ int capture_plain(LqSim* S, int (*fn)(LqSim*, cudaStream_t), cudaGraphExec_t* ex
     return LQ_OK;
 }
 
-/* Reads the rebuild flag on the host; clears it and counts the rebuild when set. */
-int host_take_flag(LqSim* S, bool* set)
+/* Reads the rebuild flag on the host and decides as k_decide / k_decide2
+ * do: clears it and counts the sort or the renewal. */
+int host_take_flag(LqSim* S, bool* sort, bool* renew)
 {
     cudaStream_t s = S->stream;
     LQ_TRY_CUDA(cudaMemcpyAsync(S->host_flag, S->rebuild, sizeof(int), cudaMemcpyDeviceToHost, s), "flag read");
     LQ_TRY_CUDA(cudaStreamSynchronize(s), "flag read");
-    *set = *S->host_flag != 0;
-    if (*set) {
-        LQ_TRY(lqb::fill_int(S->rebuild, 1, 0, s));
-        LQ_TRY(lqb::add_int(S->rebuilds, 1, s));
-    }
+    const int f = *S->host_flag;
+    const bool due = (f & kFlagLists) != 0;
+    const bool two = two_level(S);
+    *sort = due && (!two || (f & kFlagSort) != 0);
+    *renew = two && due;
+    if (f) LQ_TRY(lqb::fill_int(S->rebuild, 1, 0, s));
+    if (*sort) LQ_TRY(lqb::add_int(S->rebuilds, 1, s));
+    else if (*renew) LQ_TRY(lqb::add_int(S->renewals, 1, s));
     return LQ_OK;
 }
 
 /* One step without the step graph: the host reads the flag. */
 int eager_step(LqSim* S)
 {
-    bool rebuild = false;
-    LQ_TRY(host_take_flag(S, &rebuild));
-    if (rebuild) LQ_TRY(enqueue_rebuild(S, S->stream));
+    bool sort = false, renew = false;
+    LQ_TRY(host_take_flag(S, &sort, &renew));
+    if (sort) LQ_TRY(enqueue_rebuild(S, S->stream));
+    if (renew) LQ_TRY(enqueue_renewal(S, S->stream));
     return enqueue_stages(S, S->stream);
 }
 
@@ -486,6 +575,9 @@ int upload(LqSim* S, const float* pos, const float* vel, const float* idep, cons
 }
 
 int set_flag(LqSim* S, int v) { return lqb::fill_int(S->rebuild, 1, v, S->stream); }
+
+/* New positions, order or list settings: sort and build all lists first. */
+int flag_full_rebuild(LqSim* S) { return set_flag(S, kFlagAll); }
 
 int widen(LqSim* S)
 {
@@ -557,6 +649,7 @@ int create(LqSim* S, const Parameters* par, const float* pos, const float* vel, 
     LQ_TRY(dev_alloc(S, (void**)&S->health, sizeof(int) * lqb::HEALTH_WORDS));
     LQ_TRY(dev_alloc(S, (void**)&S->rebuild, sizeof(int)));
     LQ_TRY(dev_alloc(S, (void**)&S->rebuilds, sizeof(int)));
+    LQ_TRY(dev_alloc(S, (void**)&S->renewals, sizeof(int)));
     S->nlm.stride = ((S->npm > 0 ? S->npm : 1) + 31) / 32 * 32;
     LQ_TRY(dev_alloc(S, (void**)&S->nlm.list, sizeof(int) * (size_t)LQ_NBR_CAP * S->nlm.stride));
     LQ_TRY(dev_alloc(S, (void**)&S->nlm.count, sizeof(int) * (size_t)S->nlm.stride));
@@ -581,6 +674,7 @@ int create(LqSim* S, const Parameters* par, const float* pos, const float* vel, 
     LQ_TRY_CUDA(cudaMemsetAsync(S->R.acestn, 0, n * sizeof(tensor2d), S->stream), "zero rates");
     LQ_TRY_CUDA(cudaMemsetAsync(S->health, 0, sizeof(int) * lqb::HEALTH_WORDS, S->stream), "zero health");
     LQ_TRY_CUDA(cudaMemsetAsync(S->rebuilds, 0, sizeof(int), S->stream), "zero counter");
+    LQ_TRY_CUDA(cudaMemsetAsync(S->renewals, 0, sizeof(int), S->stream), "zero counter");
     LQ_TRY_CUDA(cudaMemcpyAsync(S->pd, &S->ph, sizeof(Parameters), cudaMemcpyHostToDevice, S->stream),
                 "upload Parameters");
     LQ_TRY(upload(S, pos, vel, idep, str, stn, S->S));
@@ -591,7 +685,7 @@ int create(LqSim* S, const Parameters* par, const float* pos, const float* vel, 
                     "device time");
     }
     /* the first step searches and sorts (reference src/loquat.cu:297-298) */
-    LQ_TRY(set_flag(S, 1));
+    LQ_TRY(flag_full_rebuild(S));
     LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "sim create");
     LQ_TRY(build_graphs(S));
     return LQ_OK;
@@ -682,7 +776,7 @@ extern "C" int lq_sim_upload(void* sim, const float* pospres, const float* velrh
     LqSim* S = static_cast<LqSim*>(sim);
     LQ_TRY(upload(S, pospres, velrhop, idep, str, stn, S->S));
     LQ_TRY(widen(S));
-    return set_flag(S, 1); /* new positions: search and rebuild the lists first */
+    return flag_full_rebuild(S); /* new positions: search and rebuild the lists first */
 }
 
 extern "C" int lq_sim_download(void* sim, float* pospres, float* velrhop, float* idep, float* str, float* stn)
@@ -758,8 +852,32 @@ extern "C" int lq_sim_set_skin(void* sim, float skin_over_h)
     LqSim* S = static_cast<LqSim*>(sim);
     LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "set skin");
     S->skin = skin_over_h * S->ph.h;
-    LQ_TRY(set_flag(S, 1));
+    LQ_TRY(flag_full_rebuild(S));
     LQ_TRY(build_graphs(S));
+    return LQ_OK;
+}
+
+extern "C" int lq_sim_set_wide_skin(void* sim, float wide_over_h)
+{
+    if (!sim || !(wide_over_h >= 0.0f) || wide_over_h > 2.0f)
+        return lqb::set_error(LQ_ERR_ARG, "lq_sim_set_wide_skin: wide/h must be in [0, 2]");
+    LqSim* S = static_cast<LqSim*>(sim);
+    LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "set wide skin");
+    if (wide_over_h > 0.0f) LQ_TRY(ensure_wide_lists(S));
+    S->wide = wide_over_h * S->ph.h;
+    LQ_TRY(flag_full_rebuild(S));
+    LQ_TRY(build_graphs(S));
+    return LQ_OK;
+}
+
+extern "C" int lq_sim_renewals(void* sim, long long* count)
+{
+    if (!sim || !count) return lqb::set_error(LQ_ERR_ARG, "lq_sim_renewals: null argument");
+    LqSim* S = static_cast<LqSim*>(sim);
+    int c = 0;
+    LQ_TRY_CUDA(cudaMemcpyAsync(&c, S->renewals, sizeof(int), cudaMemcpyDeviceToHost, S->stream), "renewal count");
+    LQ_TRY_CUDA(cudaStreamSynchronize(S->stream), "renewal count");
+    *count = c;
     return LQ_OK;
 }
 
@@ -824,7 +942,7 @@ extern "C" int lq_sim_set_frames(void* sim, int n, const int* rows)
     S->fr.rows = d;
     S->fr.n = n;
     S->fr_host.assign(rows, rows + 2 * (size_t)n);
-    LQ_TRY(set_flag(S, 1));
+    LQ_TRY(flag_full_rebuild(S));
     LQ_TRY(build_graphs(S));
     return LQ_OK;
 }
@@ -879,7 +997,7 @@ struct Snapshot {
     std::vector<void*> copies;
     long long step = 0;
     double time = 0.0;
-    float skin = 0.0f;
+    float skin = 0.0f, wide = 0.0f;
     int shape = 0;
     ~Snapshot()
     {
@@ -891,7 +1009,8 @@ struct Snapshot {
         items = {{S->S.pos, n * sizeof(float4)},  {S->S.vel, n * sizeof(float4)},
                  {S->S.idep, n * sizeof(float4)}, {S->S.str, n * sizeof(tensor2d)},
                  {S->S.stn, n * sizeof(tensor2d)}, {S->health, sizeof(int) * lqb::HEALTH_WORDS},
-                 {S->rebuilds, sizeof(int)},      {S->pd, sizeof(Parameters)}};
+                 {S->rebuilds, sizeof(int)},      {S->pd, sizeof(Parameters)},
+                 {S->renewals, sizeof(int)}};
         if (S->S.xlo) {
             items.push_back({S->S.xlo, n * sizeof(float4)});
             items.push_back({S->S.vlo, n * sizeof(float4)});
@@ -909,6 +1028,7 @@ struct Snapshot {
         step = S->step;
         time = S->time;
         skin = S->skin;
+        wide = S->wide;
         shape = S->pair_shape;
         return LQ_OK;
     }
@@ -920,19 +1040,21 @@ struct Snapshot {
                         "restore");
         S->step = step;
         S->time = time;
-        return set_flag(S, 1); /* lists are rebuilt before the next step */
+        return flag_full_rebuild(S); /* lists are rebuilt before the next step */
     }
 };
 
 int cuda_ok(cudaError_t e, const char* what) { return e == cudaSuccess ? LQ_OK : lqb::cuda_status(e, what); }
 
-/* ms per step of `steps` steps after two untimed ones. */
+/* ms per step of `steps` steps from a state flagged for a sort: the sort
+ * and list build that start every run are inside the window, so settings
+ * whose lists last long pay for one build in `steps` steps, not nothing. */
 int time_steps(LqSim* S, int steps, float* ms)
 {
     cudaEvent_t a, b;
     LQ_TRY_CUDA(cudaEventCreate(&a), "event");
     LQ_TRY_CUDA(cudaEventCreate(&b), "event");
-    int st = lq_sim_step(S, 2);
+    int st = LQ_OK;
     if (st == LQ_OK) st = cuda_ok(cudaEventRecord(a, S->stream), "event");
     if (st == LQ_OK) st = lq_sim_step(S, steps);
     if (st == LQ_OK) st = cuda_ok(cudaEventRecord(b, S->stream), "event");
@@ -956,13 +1078,15 @@ extern "C" int lq_sim_autotune(void* sim, int steps, int* shape_out, float* skin
     LQ_TRY(snap.take(S));
     const float h = S->ph.h;
     int best_shape = S->pair_shape;
-    float best_skin = S->skin, best_ms = 3.4e38f;
+    float best_skin = S->skin, best_wide = S->wide, best_ms = 3.4e38f;
     float best_factor = S->skin / h;   /* skin / h as the caller would pass it to lq_sim_set_skin */
     float factor = best_factor;
-    auto trial = [&](int shape, float skin) -> int {
+    auto trial = [&](int shape, float skin, float wide) -> int {
         LQ_TRY(snap.restore(S));
         S->pair_shape = shape;
         S->skin = skin;
+        if (wide > skin) LQ_TRY(ensure_wide_lists(S));
+        S->wide = wide;
         LQ_TRY(build_graphs(S));
         float ms = 0.0f;
         LQ_TRY(time_steps(S, steps, &ms));
@@ -970,23 +1094,34 @@ extern "C" int lq_sim_autotune(void* sim, int steps, int* shape_out, float* skin
             best_ms = ms;
             best_shape = shape;
             best_skin = skin;
+            best_wide = wide;
             best_factor = factor;
         }
         return LQ_OK;
     };
-    /* launch shapes at the current skin, then skins with the best shape */
+    /* launch shapes at the current lists, then one-level skins with the best
+     * shape, then two-level lists over the best skin whose wide margin
+     * (wide - skin <= 0.2 h) keeps a pair that the 3 x 3-column walk of the
+     * wide build leaves out below the kernel factor (0.2)^3, as the
+     * one-level skins do */
     int st = LQ_OK;
-    for (int k = 0; k < lqb::kPairShapeCount && st == LQ_OK; ++k) st = trial(k, snap.skin);
+    for (int k = 0; k < lqb::kPairShapeCount && st == LQ_OK; ++k) st = trial(k, snap.skin, snap.wide);
     const float skins[] = {0.02f, 0.05f, 0.1f, 0.2f};
     const int shape = best_shape;
     for (float f : skins) {
         factor = f;
-        if (st == LQ_OK && f * h != snap.skin) st = trial(shape, f * h);
+        if (st == LQ_OK && (f * h != snap.skin || snap.wide > snap.skin)) st = trial(shape, f * h, 0.0f);
     }
+    const float margins[] = {0.1f, 0.2f};
+    const float skin1 = best_skin;
+    factor = best_factor;
+    for (float m : margins)
+        if (st == LQ_OK) st = trial(shape, skin1, skin1 + m * h);
     /* back to the state before tuning, with the chosen configuration */
     int st2 = snap.restore(S);
     S->pair_shape = st == LQ_OK ? best_shape : snap.shape;
     S->skin = st == LQ_OK ? best_skin : snap.skin;
+    S->wide = st == LQ_OK ? best_wide : snap.wide;
     if (st2 == LQ_OK) st2 = build_graphs(S);
     if (st2 == LQ_OK) st2 = cuda_ok(cudaStreamSynchronize(S->stream), "autotune");
     if (st != LQ_OK) return st;
@@ -996,13 +1131,22 @@ extern "C" int lq_sim_autotune(void* sim, int steps, int* shape_out, float* skin
     return LQ_OK;
 }
 
+extern "C" int lq_sim_wide_skin(void* sim, float* wide_over_h)
+{
+    if (!sim || !wide_over_h) return lqb::set_error(LQ_ERR_ARG, "lq_sim_wide_skin: null argument");
+    LqSim* S = static_cast<LqSim*>(sim);
+    *wide_over_h = two_level(S) ? S->wide / S->ph.h : 0.0f;
+    return LQ_OK;
+}
+
 /* ------------------------------------------------------------ checkpoints */
 /* Binary checkpoint, little-endian as written by this library:
  *   "LQB200CK" | u32 version | u32 flags | i64 step | f64 time | f32 skin |
  *   i32 np, npb, npm | Parameters (208 B) |
  *   pospres, velrhop, idep (np x 16 B) | str, stn (np x 24 B) |
  *   [mixed form: x and v+rho in FP64, np x 32 B each] |
- *   i32 n + n x 5 f32 materials | i32 n + n x 10 f32 model-3 rows | i32 n + n x 2 i32 frames */
+ *   i32 n + n x 5 f32 materials | i32 n + n x 10 f32 model-3 rows | i32 n + n x 2 i32 frames |
+ *   [f32 wide: the two-level lists' cut-off beyond 2h; files without it load with one-level lists] */
 namespace {
 
 constexpr char kCkMagic[8] = {'L', 'Q', 'B', '2', '0', '0', 'C', 'K'};
@@ -1099,11 +1243,12 @@ extern "C" int lq_sim_save_checkpoint(void* sim, const char* path)
     w.put(S->vw_host.data(), S->vw_host.size() * sizeof(float));
     w.val((int32_t)S->fr.n);
     w.put(S->fr_host.data(), S->fr_host.size() * sizeof(int));
+    w.val(two_level(S) ? S->wide : 0.0f);
     const bool ok = w.ok && fclose(f) == 0;
     if (!ok) return lqb::set_error(LQ_ERR_IO, "write error on checkpoint %s", path);
     /* the run that continues searches before its next step, as a run
      * restarted from this file does, so both take identical steps */
-    return set_flag(S, 1);
+    return flag_full_rebuild(S);
 }
 
 extern "C" int lq_sim_load_checkpoint(const char* path, int flags, void** sim)
@@ -1170,7 +1315,8 @@ extern "C" int lq_sim_load_checkpoint(const char* path, int flags, void** sim)
     if (r.ok && nfr > 0)
         if (const char* p = r.take(2 * (size_t)nfr * sizeof(int)))
             fr.assign(reinterpret_cast<const int*>(p), reinterpret_cast<const int*>(p) + 2 * (size_t)nfr);
-    if (!r.ok || nmt < 0 || nvw < 0 || nfr < 0 || r.at != buf.size())
+    const float wide = (r.ok && buf.size() - r.at == sizeof(float)) ? r.val<float>() : 0.0f;
+    if (!r.ok || nmt < 0 || nvw < 0 || nfr < 0 || r.at != buf.size() || !(wide >= 0.0f))
         return lqb::set_error(LQ_ERR_IO, "%s: truncated or malformed checkpoint", path);
 
     /* aligned copies of the state arrays (the file offsets are not) */
@@ -1216,9 +1362,11 @@ extern "C" int lq_sim_load_checkpoint(const char* path, int flags, void** sim)
     if (st == LQ_OK && nmt > 0) st = lq_sim_set_materials(out, nmt, mt.data());
     if (st == LQ_OK && nvw > 0) st = lq_sim_set_hypoplastic(out, nvw, vw.data());
     if (st == LQ_OK && nfr > 0) st = lq_sim_set_frames(out, nfr, fr.data());
-    if (st == LQ_OK && skin != S->skin) {
+    if (st == LQ_OK && (skin != S->skin || wide > skin)) {
         S->skin = skin;            /* as saved, not through skin / h */
-        st = build_graphs(S);
+        if (wide > skin) st = ensure_wide_lists(S);
+        S->wide = wide;
+        if (st == LQ_OK) st = build_graphs(S);
     }
     if (st != LQ_OK) return fail(st);
     *sim = out;
@@ -1252,6 +1400,20 @@ extern "C" int lq_sim_rebuild_launches(void* sim, int* launches)
      * full pack of the neighbour data, tile segments and fill (tiled
      * shapes; their scan is a library kernel) */
     *launches = 4 + 1 + 1 + 1 + (S->npb > 0 ? 1 : 0) + 1 + (tiled(S) && S->npm > 0 ? 2 : 0);
+    /* with two-level lists the lists the stages read are renewed from the
+     * wide ones right after */
+    int renewal = 0;
+    LQ_TRY(lq_sim_renewal_launches(sim, &renewal));
+    *launches += renewal;
+    return LQ_OK;
+}
+
+extern "C" int lq_sim_renewal_launches(void* sim, int* launches)
+{
+    if (!sim || !launches) return lqb::set_error(LQ_ERR_ARG, "lq_sim_renewal_launches: null argument");
+    LqSim* S = static_cast<LqSim*>(sim);
+    /* material and boundary (when npb > 0) list renewal, positions record */
+    *launches = two_level(S) ? (S->npm > 0 ? 1 : 0) + (S->npb > 0 ? 1 : 0) + 1 : 0;
     return LQ_OK;
 }
 
@@ -1262,12 +1424,12 @@ namespace {
 /* Phases timed by lq_sim_profile: the reference's Timer phases
  * (reference include/types.h:158-173, src/loquat.cu:345-395) with the
  * search and the list build split out. */
-enum { PH_SEARCH = 0, PH_GATHER, PH_ADAMI, PH_INTERACTION, PH_INTEGRATE, PH_SHEPARD, PH_LIST, PH_COUNT };
+enum { PH_SEARCH = 0, PH_GATHER, PH_ADAMI, PH_INTERACTION, PH_INTEGRATE, PH_SHEPARD, PH_LIST, PH_RENEW, PH_COUNT };
 /* NVTX range names of the phases (host ranges around each phase's
  * launches; a tool such as ncu can select kernels by them with
  * --nvtx --nvtx-include "lq/interaction/") */
 const char* const kPhaseNames[PH_COUNT] = {"lq/search", "lq/gather", "lq/adami", "lq/interaction",
-                                           "lq/integrate", "lq/shepard", "lq/list"};
+                                           "lq/integrate", "lq/shepard", "lq/list", "lq/renew"};
 
 struct PhaseTimer {
     std::vector<cudaEvent_t> ev;
@@ -1296,21 +1458,27 @@ int profiled_step(LqSim* S, PhaseTimer& T)
     const Parameters* ph = &S->ph;
     const Parameters* pd = S->pd;
     cudaStream_t s = S->stream;
-    bool rebuild = false;
-    LQ_TRY(host_take_flag(S, &rebuild));
+    bool rebuild = false, renew = false;
+    LQ_TRY(host_take_flag(S, &rebuild, &renew));
     if (rebuild) {
         LQ_TRY(T.mark(s, PH_SEARCH));
         LQ_TRY(lqb::grid_search(ph, pd, S->S.pos, S->g, false, S->health, s, S->S.idep, S->fr));
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_GATHER));
         LQ_TRY(lqb::gather_state(S->np, S->g.part_idx, S->S, S->T, s));
-        k_copy_state<<<blocks(S->np), 256, 0, s>>>(S->np, S->npb, S->T, S->S, S->S2, S->xbuild);
+        k_copy_state<<<blocks(S->np), 256, 0, s>>>(S->np, S->npb, S->T, S->S, S->S2,
+                                                   two_level(S) ? S->xwide : S->xbuild);
         LQ_TRY_CUDA(cudaGetLastError(), "k_copy_state");
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_LIST));
         LQ_TRY(build_lists(S, s));
         LQ_TRY(lqb::launch_pack_neighbors(ph, S->S, S->rec, 0, s, S->flags & LQ_SIM_MIXED));
         LQ_TRY(lqb::launch_tile_order(ph, S->g.start, S->pair_shape, S->tile, s));
+        LQ_TRY(T.close(s));
+    }
+    if (renew) {
+        LQ_TRY(T.mark(s, PH_RENEW));
+        LQ_TRY(enqueue_renewal(S, s));
         LQ_TRY(T.close(s));
     }
     State* cur[2] = {&S->S, &S->S2};
@@ -1326,7 +1494,8 @@ int profiled_step(LqSim* S, PhaseTimer& T)
             LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt, S->vw));
         else {
             LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild,
-                                            S->skin, s, S->mt, S->vw));
+                                            S->skin, s, S->mt, S->vw, two_level(S) ? S->xwide : nullptr,
+                                            S->wide));
             LQ_TRY(enqueue_dynamic_dt(S, s));
         }
         LQ_TRY(T.close(s));
@@ -1341,7 +1510,7 @@ extern "C" int lq_sim_profile(void* sim, int nsteps, double* phase_ms, int* phas
     if (!sim || nsteps < 0 || !phase_ms) return lqb::set_error(LQ_ERR_ARG, "lq_sim_profile: bad argument");
     LqSim* S = static_cast<LqSim*>(sim);
     PhaseTimer T;
-    T.ev.resize((size_t)nsteps * 2 * (3 + 6 + 1) + 4);
+    T.ev.resize((size_t)nsteps * 2 * (4 + 6 + 2) + 4);   /* rebuild and renewal, two stages, filters */
     for (auto& e : T.ev) LQ_TRY_CUDA(cudaEventCreate(&e), "profile event create");
     int st = LQ_OK;
     const int N = S->ph.stress_shepard_filter;

@@ -509,6 +509,63 @@ __device__ __forceinline__ int ld_list(const int* p)
     return v;
 }
 
+/* Two-level lists: the lists the stages read (cut-off 2h + skin) renewed
+ * from wider ones (2h + wide, built after each sort) at the current
+ * positions, without a search.  Target t keeps, in their order, the entries
+ * of its wide list within the cut-off, so the result is the list a build
+ * with this cut-off over the same walk would give, as long as no pair within
+ * 2h + skin now was beyond 2h + wide when the wide lists were built (the
+ * corrector's check keeps every particle within (wide - skin) / 2 of its
+ * position then).  A wide list that overflowed (count above LQ_NBR_CAP) passes its
+ * count on: the pair kernel then walks that target's stencil, as after a
+ * direct build. */
+__global__ void __launch_bounds__(kBlock) k_list_refresh(int first, int ntarget, int np, float cut2,
+                                                         const float4* __restrict__ pos,
+                                                         const int* __restrict__ wlist,
+                                                         const int* __restrict__ wcount, int wstride,
+                                                         int* __restrict__ list, int* __restrict__ count,
+                                                         int stride)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntarget) return;
+    const int nw = __ldg(wcount + t);
+    if (nw > LQ_NBR_CAP) {
+        count[t] = nw;
+        return;
+    }
+    const int i = first + t;
+    const float4 xi = __ldg(pos + i);
+    const int* p = wlist + t;
+    /* groups of kG entries, the next group's entries fetched while this
+     * group's positions are gathered; the last group is filled up with the
+     * target's own slot (a valid address; never kept) */
+    constexpr int kG = 8;
+    int nxt[kG];
+#pragma unroll
+    for (int u = 0; u < kG; ++u) nxt[u] = u < nw ? ld_list(p + (size_t)u * wstride) : i;
+    int n = 0;
+    for (int k = 0; k < nw; k += kG) {
+        int j[kG];
+        float4 xj[kG];
+#pragma unroll
+        for (int u = 0; u < kG; ++u) {
+            j[u] = nxt[u];
+            nxt[u] = k + kG + u < nw ? ld_list(p + (size_t)(k + kG + u) * wstride) : i;
+        }
+#pragma unroll
+        for (int u = 0; u < kG; ++u) xj[u] = lq_in_range(j[u], np) ? __ldg(pos + j[u]) : xi;
+#pragma unroll
+        for (int u = 0; u < kG; ++u) {
+            const float dx = xi.x - xj[u].x, dy = xi.y - xj[u].y, dz = xi.z - xj[u].z;
+            if (k + u < nw && lq_in_range(j[u], np) && dx * dx + dy * dy + dz * dz < cut2) {
+                list[(size_t)n * stride + t] = j[u];
+                ++n;
+            }
+        }
+    }
+    count[t] = n;
+}
+
 /* The sums over one target's list (entry k at p[k * stride]), four
  * entries per group, the next group's entries fetched ahead so the
  * dependent neighbour loads do not wait on the list stream.  The last
@@ -1063,6 +1120,18 @@ int launch_neighbor_list(const Parameters* ph, const Parameters* pd, const float
                          const NeighborList& nl, cudaStream_t s)
 {
     return launch_neighbor_list_range(ph, pd, ph->npb, ph->npm, 0, 2.0f * ph->h * 1.00005f, pos, c, nl, nullptr, s);
+}
+
+int launch_list_refresh(const Parameters* ph, int first, int n, float cut, const float4* pos,
+                        const NeighborList& wide, const NeighborList& nl, cudaStream_t s)
+{
+    if (n <= 0) return LQ_OK;
+    if (nl.stride < n || wide.stride < n)
+        return set_error(LQ_ERR_ARG, "list refresh: strides %d / %d < targets %d", nl.stride, wide.stride, n);
+    k_list_refresh<<<blocks_for(n, kBlock), kBlock, 0, s>>>(first, n, ph->np, cut * cut, pos, wide.list, wide.count,
+                                                           wide.stride, nl.list, nl.count, nl.stride);
+    LQ_TRY_CUDA(cudaGetLastError(), "k_list_refresh");
+    return LQ_OK;
 }
 
 int launch_neighbor_list_range(const Parameters* ph, const Parameters* pd, int first, int n, int layer_lo, float cut,

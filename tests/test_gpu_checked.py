@@ -1,8 +1,9 @@
 """The bounds-checked build (-D LQ_CHECKED, loquat_b200/liblqb200_checked.so)
 stands in for a device memory checker: its list and grid kernels check every
 index they gather or scatter through.  Runs of the native driver (both
-precision forms, Shepard passes and list rebuilds, a batched ensemble with
-frames, the von Wolffersdorff model) must
+precision forms, Shepard passes and list rebuilds, two-level lists with
+their renewals, a batched ensemble with frames, the von Wolffersdorff
+model) must
 count no violation.  Each run is a child process that loads the checked
 library in place of the product one."""
 from __future__ import annotations
@@ -36,6 +37,14 @@ for shape in (0, 8):
     s.set_frames(comb.meta["frames"])
     s.set_pair_shape(shape)
     s.step(30)
+for mixed, shape in ((False, 0), (True, 9)):
+    s = lq.Simulation(c.par, *c.arrays(), mixed=mixed)
+    s.set_pair_shape(shape)
+    s.set_skin(0.02)
+    s.set_wide_skin(0.15)            # two-level lists: renewals from the wide lists
+    s.step(60)
+    assert s.renewals() >= 3 and s.rebuilds() >= 2
+    assert not s.health().any()
 v = cases.small_column(model=3, velocity_noise=0.05, shepard=7, seed=62)
 s = lq.Simulation(v.par, *v.arrays(), mixed=True)
 s.set_hypoplastic(v.meta["hypoplastic"])

@@ -1,0 +1,135 @@
+"""Two-level neighbour lists of the native driver (lq_sim_set_wide_skin):
+wide lists built after each sort, the lists the stages read renewed from
+them at the current positions without a search.
+
+* With fast particles (0.3 m/s noise) both renewals and new sorts happen
+  within 60 steps; the run agrees with the one-level run to float rounding
+  (both see every pair within 2h at every evaluation, summed in a
+  different order) and with the FP64 oracle within the bounds the one-level
+  driver is held to.
+* Graph-driven and eager steps take the same decisions and give
+  bit-identical results; a checkpoint keeps the setting, and the restored
+  run and the continued one stay bit-identical.
+* A batched ensemble with per-scenario materials and frames on two-level
+  lists against the oracle run per scenario after 100 steps.
+Reference step sequence: src/loquat.cu:322-409.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from loquat_b200 import cases
+from helpers import by_id, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def errors(got, want):
+    g, w = by_id(got), by_id(want)
+    mat = np.asarray(w[2])[:, 0] == 1
+    return dict(rho=rel_l2(g[1][mat, 3], w[1][mat, 3]), vel=rel_l2(g[1][mat, :3], w[1][mat, :3]),
+                str=rel_l2(g[3][mat], w[3][mat]), pos=rel_l2(g[0][mat, :3], w[0][mat, :3]))
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_two_level_lists_match_one_level_and_oracle(lq, orc, cuda, mixed):
+    c = cases.small_column(velocity_noise=0.3, shepard=7, seed=61).with_ids()
+    one = lq.Simulation(c.par, *c.arrays(), mixed=mixed)
+    one.set_skin(0.02)
+    two = lq.Simulation(c.par, *c.arrays(), mixed=mixed)
+    two.set_skin(0.02)
+    two.set_wide_skin(0.15)
+    assert two.wide_skin() == pytest.approx(0.15) and one.wide_skin() == 0.0
+    o = orc.OracleSim(c.par, *c.arrays())
+    for s in (one, two):
+        s.step(60)
+    o.step(60)
+    want = o.get()
+    o.close()
+    sorts, renewals = two.rebuilds(), two.renewals()
+    assert renewals >= 3 and sorts >= 2, (sorts, renewals)    # renewals and a second sort
+    assert sorts < one.rebuilds(), (sorts, one.rebuilds())
+    e12 = errors(two.download(), one.download())
+    e2o = errors(two.download(), want)
+    e1o = errors(one.download(), want)
+    print("mixed" if mixed else "plain", "sorts", sorts, "renewals", renewals, "one-level rebuilds", one.rebuilds(),
+          {k: f"{v:.1e}" for k, v in e12.items()}, {k: f"{v:.1e}" for k, v in e2o.items()})
+    for k in e12:
+        assert e12[k] < 1e-5, (k, e12)
+        assert e2o[k] < max(2.0 * e1o[k], 1e-6), (k, e2o, e1o)
+    assert not one.health().any() and not two.health().any()
+    one.close()
+    two.close()
+
+
+def test_two_level_graph_and_eager_steps_are_bit_identical(lq, cuda):
+    c = cases.small_column(velocity_noise=0.3, shepard=5, seed=62)
+    a = lq.Simulation(c.par, *c.arrays(), graph=True)
+    b = lq.Simulation(c.par, *c.arrays(), graph=False)
+    for s in (a, b):
+        s.set_skin(0.02)
+        s.set_wide_skin(0.12)
+        s.step(40)
+    assert (a.rebuilds(), a.renewals()) == (b.rebuilds(), b.renewals())
+    assert a.renewals() >= 2
+    for x, y in zip(a.download(), b.download()):
+        assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_two_level_checkpoint_restart_is_bit_identical(lq, cuda, tmp_path, mixed):
+    c = cases.small_column(velocity_noise=0.3, shepard=7, seed=63)
+    a = lq.Simulation(c.par, *c.arrays(), mixed=mixed)
+    a.set_skin(0.02)
+    a.set_wide_skin(0.15)
+    a.step(21)
+    path = tmp_path / "two.lqck"
+    a.save_checkpoint(path)
+    a.step(30)
+    b = lq.Simulation.load_checkpoint(path, mixed=mixed)
+    assert b.wide_skin() == pytest.approx(0.15)
+    b.step(30)
+    assert a.clock() == b.clock()
+    for k, (x, y) in enumerate(zip(a.download(), b.download())):
+        assert np.array_equal(x, y), k
+    assert b.renewals() >= 1
+
+
+def test_two_level_batched_ensemble_vs_oracle(lq, orc, cuda):
+    comb, parts = cases.ensemble(n=4, count_range=(2.0e3, 6.0e3), seed=13, shepard=7)
+    for k, p in enumerate(parts):
+        p.idep[:, 3] = np.arange(p.par.np, dtype=np.float32)
+        (b0, b1), (m0, m1) = comb.meta["slices"][k]
+        comb.idep[b0:b1, 3] = p.idep[: p.par.npb, 3]
+        comb.idep[m0:m1, 3] = p.idep[p.par.npb:, 3]
+    sim = lq.Simulation(comb.par, *comb.arrays(), mixed=True)
+    sim.set_materials(comb.meta["materials"])
+    sim.set_frames(comb.meta["frames"])
+    sim.set_skin(0.02)
+    sim.set_wide_skin(0.15)
+    sim.step(100)
+    batch = sim.download()
+    assert sim.renewals() >= 1
+    worst = {}
+    for k, p in enumerate(parts):
+        o = orc.OracleSim(p.par, *p.arrays())
+        o.step(100)
+        want = o.get()
+        o.close()
+        ow = np.argsort(want[2][:, 3], kind="stable")
+        want = [x[ow] for x in want]
+        sel = np.asarray(batch[2])[:, 0] == k + 1
+        got = [np.asarray(x)[sel] for x in batch]
+        og = np.argsort(got[2][:, 3], kind="stable")
+        got = [x[og] for x in got]
+        mat = want[2][:, 3] >= p.par.npb
+        for name, a, b in (("velocity", got[1][mat, :3], want[1][mat, :3]), ("stress", got[3][mat], want[3][mat]),
+                           ("density", got[1][mat, 3], want[1][mat, 3])):
+            worst[name] = max(worst.get(name, 0.0), rel_l2(a, b))
+    print("two-level ensemble", {k: f"{v:.2e}" for k, v in worst.items()}, "renewals", sim.renewals(),
+          "sorts", sim.rebuilds())
+    assert not sim.health().any()
+    sim.close()
+    for name, v in worst.items():
+        assert v <= 1e-3, (name, v)
