@@ -53,13 +53,27 @@ __device__ __forceinline__ void store_split(const State& out, int i, const doubl
     out.vel[i] = v;
 }
 
+/* A material slot's entry of the pair kernel's packed neighbour arrays from
+ * the position, velocity and stress just stored (what k_pack_neighbors
+ * would write from them), when nb is set: the native driver's integrators
+ * pack the slots they update, so a stage needs no pack of its own.  kPk
+ * (the mixed form) packs the velocity into two words. */
+template <bool kPk>
+__device__ __forceinline__ void pack_slot(const NbrArrays& nb, int i, const float4& x, const float4& v,
+                                          const tensor2d& s)
+{
+    if (!nb.xr) return;
+    nb.xr[i] = make_float4(x.x, x.y, x.z, v.w);
+    store_packed<kPk>(nb, i, v, s);
+}
+
 /* Half step of the material slots (reference src/predictor_corrector.cu:169-218):
  * v += dt/2 a; rho += dt/2 drho; x += dt/2 v_new; eps += dt/2 deps;
  * stress and plastic strain from the model at dt/2. */
 template <bool kMixed, bool kVW>
 __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_predict(const Parameters* __restrict__ P, int np, int npb, State in,
                                                     State out, State snap, bool do_snap, Rates rt, MaterialTable mt,
-                                                    MaterialTable vw)
+                                                    MaterialTable vw, NbrArrays nb)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
@@ -108,7 +122,9 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_predict(
             const float epf = (float)sqrt(2.0 / 3.0 * contract6(e, e));
             vw_update_d(vw_const(vw, id.x), hdt, de, w, sd, ev);
             out.idep[i] = make_float4(id.x, epf, (float)ev, id.w);
-            store_t2(out.str, i, narrow6(sd));
+            const tensor2d sn = narrow6(sd);
+            store_t2(out.str, i, sn);
+            pack_slot<kMixed>(nb, i, out.pos[i], out.vel[i], sn);   /* kinematics stored above */
             return;
         }
         if (M.model == 1) {
@@ -117,10 +133,15 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_predict(
             hypo_update_d(M, hdt, dd, w, sd);
             ep = sqrt(2.0 / 3.0 * contract6(e, e));
         }
-        store_split(out, i, xd, vd, (float)p);
+        float4 xh, vh;
+        split_words(out, i, xd, vd, (float)p, xh, vh);
+        out.pos[i] = xh;
+        out.vel[i] = vh;
         out.idep[i] = make_float4(id.x, (float)ep, (float)ev, id.w);
-        store_t2(out.str, i, narrow6(sd));
+        const tensor2d sn = narrow6(sd);
+        store_t2(out.str, i, sn);
         store_t2(out.stn, i, narrow6(e));
+        pack_slot<kMixed>(nb, i, xh, vh, sn);
         return;
     }
     float4 v = v0;
@@ -148,7 +169,9 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_predict(
         double evd = ev;
         vw_update_d(vw_const(vw, id.x), 0.5 * (double)dt, de, w, sd, evd);
         out.idep[i] = make_float4(id.x, epf, (float)evd, id.w);
-        store_t2(out.str, i, narrow6(sd));
+        const tensor2d sn = narrow6(sd);
+        store_t2(out.str, i, sn);
+        pack_slot<kMixed>(nb, i, out.pos[i], out.vel[i], sn);   /* kinematics stored above */
         return;
     }
     if (M.model == 1) {
@@ -163,6 +186,7 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_predict(
     out.idep[i] = make_float4(id.x, ep, ev, id.w);
     store_t2(out.str, i, s);
     store_t2(out.stn, i, e);
+    pack_slot<kMixed>(nb, i, x, v, s);
 }
 
 /* Full step from the snapshot (reference src/predictor_corrector.cu:256-307):
@@ -211,7 +235,7 @@ template <bool kMixed, bool kVW>
 __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(const Parameters* __restrict__ P, int np, int npb, State cur,
                                                     State ini, const int* __restrict__ ini_idx, State out, Rates rt,
                                                     int* __restrict__ health, VerletCheck verlet, int first,
-                                                    MaterialTable mt, MaterialTable vw)
+                                                    MaterialTable mt, MaterialTable vw, NbrArrays nb)
 {
     const int i = first + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
@@ -283,6 +307,7 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(
         const tensor2d s = narrow6(sd);
         out.idep[i] = make_float4(id.x, ep, (float)evd, id.w);
         store_t2(out.str, i, s);
+        pack_slot<kMixed>(nb, i, out.pos[i], out.vel[i], s);   /* kinematics stored above */
         if (health && (bad || !(isfinite(s.xx) && isfinite(s.yy) && isfinite(s.zz) && isfinite(s.xy) &&
                                 isfinite(s.xz) && isfinite(s.yz))))
             atomicAdd(health + HEALTH_NONFINITE, 1);
@@ -340,6 +365,7 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(
     out.idep[i] = make_float4(id.x, ep, ev, id.w);
     store_t2(out.str, i, s);
     store_t2(out.stn, i, e);
+    pack_slot<kMixed>(nb, i, x, v, s);
     if (health) {
         const bool ok = isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(v.x) && isfinite(v.y) &&
                         isfinite(v.z) && isfinite(v.w) && isfinite(s.xx) && isfinite(s.yy) && isfinite(s.zz) &&
@@ -352,7 +378,7 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(
 }  // namespace
 
 int launch_predict(const Parameters* ph, const Parameters* pd, const State& in, const State& out, const State* snap,
-                   const Rates& r, cudaStream_t s, const MaterialTable& mt, const MaterialTable& vw)
+                   const Rates& r, cudaStream_t s, const MaterialTable& mt, const MaterialTable& vw, float* rec)
 {
     if (ph->np <= 0) return LQ_OK;
     if (ph->constitutive_model == 3 && (!vw.p || vw.n <= 0))
@@ -363,12 +389,13 @@ int launch_predict(const Parameters* ph, const Parameters* pd, const State& in, 
      * more registers than the other models' kernels */
     const bool vwm = ph->constitutive_model == 3;
     const int nb = blocks_for(ph->np, kBlock);
+    const NbrArrays pk = rec ? nbr_arrays(rec, ph->np) : NbrArrays{nullptr, nullptr, nullptr, nullptr};
     if (in.xlo && out.xlo) {
-        if (vwm) k_predict<true, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw);
-        else k_predict<true, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw);
+        if (vwm) k_predict<true, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw, pk);
+        else k_predict<true, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw, pk);
     } else {
-        if (vwm) k_predict<false, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw);
-        else k_predict<false, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw);
+        if (vwm) k_predict<false, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw, pk);
+        else k_predict<false, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw, pk);
     }
     LQ_TRY_CUDA(cudaGetLastError(), "k_predict");
     return LQ_OK;
@@ -382,7 +409,8 @@ int launch_correct(const Parameters* ph, const Parameters* pd, const State& cur,
         return set_error(LQ_ERR_ARG, "corrector: constitutive model 3 needs a von Wolffersdorff table");
     k_correct<false, false><<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, ini_idx, cur, r, health,
                                                              VerletCheck{nullptr, nullptr, 0.0f, 0.0f, nullptr, 0.0f}, ph->npb,
-                                                             MaterialTable(), MaterialTable());
+                                                             MaterialTable(), MaterialTable(),
+                                                             NbrArrays{nullptr, nullptr, nullptr, nullptr});
     LQ_TRY_CUDA(cudaGetLastError(), "k_correct");
     return LQ_OK;
 }
@@ -390,7 +418,7 @@ int launch_correct(const Parameters* ph, const Parameters* pd, const State& cur,
 int launch_correct_into(const Parameters* ph, const Parameters* pd, const State& cur, const State& ini,
                         const State& out, const Rates& r, int* health, const float4* xbuild, int* rebuild,
                         float skin, cudaStream_t s, const MaterialTable& mt, const MaterialTable& vw,
-                        const float4* xwide, float wide)
+                        const float4* xwide, float wide, float* rec)
 {
     if (ph->np <= 0) return LQ_OK;
     if (ph->constitutive_model == 3 && (!vw.p || vw.n <= 0))
@@ -400,12 +428,13 @@ int launch_correct_into(const Parameters* ph, const Parameters* pd, const State&
     const VerletCheck vc{xbuild, rebuild, 0.5f * skin, ph->dt, xwide, 0.5f * (wide - skin)};
     const bool vwm = ph->constitutive_model == 3;
     const int nb = blocks_for(ph->np, kBlock);
+    const NbrArrays pk = rec ? nbr_arrays(rec, ph->np) : NbrArrays{nullptr, nullptr, nullptr, nullptr};
     if (cur.xlo && ini.xlo && out.xlo) {
-        if (vwm) k_correct<true, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw);
-        else k_correct<true, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw);
+        if (vwm) k_correct<true, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw, pk);
+        else k_correct<true, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw, pk);
     } else {
-        if (vwm) k_correct<false, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw);
-        else k_correct<false, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw);
+        if (vwm) k_correct<false, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw, pk);
+        else k_correct<false, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw, pk);
     }
     LQ_TRY_CUDA(cudaGetLastError(), "k_correct");
     return LQ_OK;

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 #include <types.h>
 #include "lq_internal.cuh"
+#include "lq_pack.h"
 
 namespace lqb {
 
@@ -533,6 +534,67 @@ __device__ __forceinline__ int vw_update_d(const VWConst& c, double dt, const te
         xe = e + h * ke1;
     }
     return steps;
+}
+
+/* Packed neighbour data for the list pair kernel: dense arrays over all
+ * slots, with s = sigma / rho^2,
+ *   nb.xr[j] = (x, y, z, rho), nb.sa[j] = (sxx, syy, szz, sxy),
+ *   nb.sb[j] = (sxz, syz, v0, v1),
+ * where the plain form keeps (v0, v1) = (vx, vy) and vz in nb.vz[j]
+ * (52 bytes per particle, four gathers per pair) and the mixed form packs
+ * the whole velocity into v0, v1 (pack_velocity: 48 bytes, three 16-byte
+ * gathers per pair).  The pair kernel is bound by the L1 data pipe: a
+ * warp's gathered neighbours sit close together in memory and the pipe's
+ * work follows the load instructions and the sectors each gathers, so the
+ * record holds only the 13 values a pair needs (no pressure word of
+ * pospres, no 24-byte stress records read as three 8-byte loads).
+ * 1 / rho is formed as the state-array pair body forms it. */
+struct NbrArrays {
+    float4* xr;
+    float4* sa;
+    float4* sb;
+    float* vz;
+};
+
+/* The mixed form's gathered velocity in two words (lq_pack.h: a shared
+ * exponent and three 18-bit mantissas). */
+__device__ __forceinline__ float2 pack_velocity(float vx, float vy, float vz)
+{
+    unsigned w0, w1;
+    pack_velocity_words(vx, vy, vz, w0, w1);
+    return make_float2(__uint_as_float(w0), __uint_as_float(w1));
+}
+
+__device__ __forceinline__ float3 unpack_velocity(float v0, float v1)
+{
+    float3 v;
+    unpack_velocity_words(__float_as_uint(v0), __float_as_uint(v1), v.x, v.y, v.z);
+    return v;
+}
+
+/* One slot's entry of the packed arrays from its velocity, density and
+ * stress (the pack kernel and the list-driven Adami write it alike). */
+template <bool kPk>
+__device__ __forceinline__ void store_packed(const NbrArrays& nb, int i, const float4& v, const tensor2d& str)
+{
+    const float rinv = __fdividef(1.0f, v.w);
+    const float r2 = rinv * rinv;
+    nb.sa[i] = make_float4(str.xx * r2, str.yy * r2, str.zz * r2, str.xy * r2);
+    if (kPk) {
+        const float2 w = pack_velocity(v.x, v.y, v.z);
+        nb.sb[i] = make_float4(str.xz * r2, str.yz * r2, w.x, w.y);
+    } else {
+        nb.sb[i] = make_float4(str.xz * r2, str.yz * r2, v.x, v.y);
+        nb.vz[i] = v.z;
+    }
+}
+
+/* The packed arrays inside `rec` (np x 13 floats, 16-byte aligned). */
+inline NbrArrays nbr_arrays(float* rec, int np)
+{
+    const size_t n = (size_t)np;
+    return NbrArrays{reinterpret_cast<float4*>(rec), reinterpret_cast<float4*>(rec) + n,
+                     reinterpret_cast<float4*>(rec) + 2 * n, rec + 12 * n};
 }
 
 }  // namespace lqb

@@ -205,10 +205,13 @@ int launch_shepard(const Parameters* par_host, const Parameters* par_dev, const 
 /* Predictor: out <- in advanced by dt/2 on material slots; when out != in
  * only the boundary slots' stress is copied (the rest of a boundary slot
  * never changes and must already be in `out`); `snap` (may be all-null)
- * receives a copy of `in`. */
+ * receives a copy of `in`.  With `rec` (the packed neighbour arrays) each
+ * material slot's entry is written from its new values, in the record of
+ * the form (the mixed form's packed velocity when the state has low
+ * words); the same holds for the corrector below. */
 int launch_predict(const Parameters* par_host, const Parameters* par_dev, const State& in, const State& out,
                    const State* snap, const Rates& r, cudaStream_t s, const MaterialTable& mt = MaterialTable(),
-                   const MaterialTable& vw = MaterialTable());
+                   const MaterialTable& vw = MaterialTable(), float* rec = nullptr);
 /* Corrector in place on `cur`; ini values read at ini_idx[i] (identity when
  * ini_idx is null).  Non-finite results are counted in health. */
 int launch_correct(const Parameters* par_host, const Parameters* par_dev, const State& cur, const State& ini,
@@ -225,7 +228,7 @@ int launch_correct_into(const Parameters* par_host, const Parameters* par_dev, c
                         const State& out, const Rates& r, int* health, const float4* xbuild, int* rebuild,
                         float skin, cudaStream_t s, const MaterialTable& mt = MaterialTable(),
                         const MaterialTable& vw = MaterialTable(), const float4* xwide = nullptr,
-                        float wide = 0.0f);
+                        float wide = 0.0f, float* rec = nullptr);
 
 /* List-driven Shepard filter (material targets and neighbours); a target
  * whose list overflowed walks its 27 cells in `c` instead. */
@@ -238,14 +241,19 @@ int launch_density_filter_list(const Parameters* par_host, const Parameters* par
                                const Frames& fr = Frames());
 /* Neighbour lists of targets [first, first + n) from grid layers
  * layer_lo..1 with cut-off radius `cut` (2h plus skin); list overflows are
- * counted in health[HEALTH_NBR_OVERFLOW]. */
+ * counted in health[HEALTH_NBR_OVERFLOW].  With `shell`, pairs at distance
+ * `inner` or more go to the shell list instead (wide build of two-level
+ * lists; nl.count then receives the inner counts). */
 int launch_neighbor_list_range(const Parameters* par_host, const Parameters* par_dev, int first, int n, int layer_lo,
                                float cut, const float4* pos, const Cells& c, const NeighborList& nl, int* health,
-                               cudaStream_t s, const float4* idep = nullptr, const Frames& fr = Frames());
-/* Lists of targets [first, first + n) with cut-off `cut` renewed from
- * their wide lists at the positions pos (two-level lists). */
+                               cudaStream_t s, const float4* idep = nullptr, const Frames& fr = Frames(),
+                               const NeighborList* shell = nullptr, float inner = 0.0f);
+/* Two-level lists of targets [first, first + n): rows [0, inner_count[t])
+ * of nl, written by the wide build, kept, and the entries of the shell list
+ * now within `cut` appended (positions pos). */
 int launch_list_refresh(const Parameters* par_host, int first, int n, float cut, const float4* pos,
-                        const NeighborList& wide, const NeighborList& nl, cudaStream_t s);
+                        const int* inner_count, const NeighborList& shell, const NeighborList& nl, int* health,
+                        cudaStream_t s);
 /* Fills n ints with v; adds v to one int. */
 int fill_int(int* p, int n, int v, cudaStream_t s);
 int add_int(int* p, int v, cudaStream_t s);

@@ -62,7 +62,9 @@ struct LqSim {
     float4* xbuild = nullptr;          /* positions when the lists were built */
     float wide = 0.0f;                 /* two-level lists: wide cut-off 2h + wide (0: one level) */
     float4* xwide = nullptr;           /* positions when the wide lists were built */
-    lqb::NeighborList wlm, wlb;        /* wide lists of material and boundary targets */
+    lqb::NeighborList wlm, wlb;        /* shell parts of the wide lists, material and boundary targets */
+    int* inner_m = nullptr;            /* inner parts' counts (their entries open the stages' lists) */
+    int* inner_b = nullptr;
     int* renewals = nullptr;           /* device counter of lists renewed from the wide ones */
     lqb::Rates R{};
     lqb::GridBuffers g;
@@ -116,6 +118,8 @@ int ensure_wide_lists(LqSim* S)
     S->wlb.stride = S->nlb.stride;
     LQ_TRY(dev_alloc(S, (void**)&S->wlb.list, sizeof(int) * (size_t)LQ_NBR_CAP * S->wlb.stride));
     LQ_TRY(dev_alloc(S, (void**)&S->wlb.count, sizeof(int) * (size_t)S->wlb.stride));
+    LQ_TRY(dev_alloc(S, (void**)&S->inner_m, sizeof(int) * (size_t)S->wlm.stride));
+    LQ_TRY(dev_alloc(S, (void**)&S->inner_b, sizeof(int) * (size_t)S->wlb.stride));
     return LQ_OK;
 }
 
@@ -322,18 +326,29 @@ __global__ void k_dt_update(Parameters* P, unsigned* m2, double* time)
 /* ------------------------------------------------------------ sequences */
 
 /* Material and boundary lists from the sorted state in S: the lists the
- * stages read, or with two-level lists the wide ones. */
+ * stages read, or with two-level lists the wide ones, whose pairs closer
+ * than 2h + 2 skin - wide (less a rounding margin of h / 1000) open the
+ * stages' lists and the rest form the shell lists that renewals filter. */
 int build_lists(LqSim* S, cudaStream_t s)
 {
     const Parameters* ph = &S->ph;
     const Parameters* pd = S->pd;
     const lqb::Cells cells{S->g.start, nullptr, nullptr};
-    const bool two = two_level(S);
-    const float cut = 2.0f * ph->h + (two ? S->wide : S->skin);
-    LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, S->npb, S->npm, 0, cut, S->S.pos, cells, two ? S->wlm : S->nlm,
-                                           S->health, s, S->S.idep, S->fr));
-    return lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, two ? S->wlb : S->nlb,
-                                           S->health, s, S->S.idep, S->fr);
+    if (!two_level(S)) {
+        const float cut = 2.0f * ph->h + S->skin;
+        LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, S->npb, S->npm, 0, cut, S->S.pos, cells, S->nlm, S->health,
+                                               s, S->S.idep, S->fr));
+        return lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, S->nlb, S->health, s,
+                                               S->S.idep, S->fr);
+    }
+    const float cut = 2.0f * ph->h + S->wide;
+    const float inner = 2.0f * ph->h + 2.0f * S->skin - S->wide - 1.0e-3f * ph->h;
+    const lqb::NeighborList im{S->nlm.list, S->inner_m, S->nlm.stride};
+    const lqb::NeighborList ib{S->nlb.list, S->inner_b, S->nlb.stride};
+    LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, S->npb, S->npm, 0, cut, S->S.pos, cells, im, S->health, s,
+                                           S->S.idep, S->fr, &S->wlm, inner));
+    return lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, ib, S->health, s, S->S.idep,
+                                           S->fr, &S->wlb, inner);
 }
 
 /* Two-level lists: the lists the stages read renewed from the wide ones at
@@ -342,8 +357,8 @@ int enqueue_renewal(LqSim* S, cudaStream_t s)
 {
     const Parameters* ph = &S->ph;
     const float cut = 2.0f * ph->h + S->skin;
-    LQ_TRY(lqb::launch_list_refresh(ph, S->npb, S->npm, cut, S->S.pos, S->wlm, S->nlm, s));
-    LQ_TRY(lqb::launch_list_refresh(ph, 0, S->npb, cut, S->S.pos, S->wlb, S->nlb, s));
+    LQ_TRY(lqb::launch_list_refresh(ph, S->npb, S->npm, cut, S->S.pos, S->inner_m, S->wlm, S->nlm, S->health, s));
+    LQ_TRY(lqb::launch_list_refresh(ph, 0, S->npb, cut, S->S.pos, S->inner_b, S->wlb, S->nlb, S->health, s));
     k_record_positions<<<blocks(S->np), 256, 0, s>>>(S->np, S->S.pos, S->xbuild);
     LQ_TRY_CUDA(cudaGetLastError(), "k_record_positions");
     return LQ_OK;
@@ -355,6 +370,12 @@ int enqueue_interaction(LqSim* S, const State& st, cudaStream_t s)
     const lqb::Cells cells{S->g.start, nullptr, nullptr};
     return lqb::launch_interaction_list(&S->ph, S->pd, st, S->R, cells, S->nlm, s, S->fr, S->flags & LQ_SIM_MIXED,
                                         S->rec, S->pair_shape, false, tile_order(S));
+}
+
+/* The material slots' packed neighbour data after a filter changed S. */
+int enqueue_material_pack(LqSim* S, cudaStream_t s)
+{
+    return lqb::launch_pack_neighbors(&S->ph, S->S, S->rec, S->npb, s, S->flags & LQ_SIM_MIXED);
 }
 
 /* Search, sort and list build; leaves the state in S with fresh lists. */
@@ -397,18 +418,20 @@ int enqueue_density_filter(LqSim* S, cudaStream_t s)
         k_set_density<<<blocks(S->npm), 256, 0, s>>>(S->npb, S->npm, S->rho_f, S->S.vel, S->S.vlo);
         LQ_TRY_CUDA(cudaGetLastError(), "k_set_density");
     }
-    return LQ_OK;
+    return enqueue_material_pack(S, s);
 }
 
-/* Adami for a stage.  The material slots are packed first, Adami reads
- * them and writes the boundary slots' packed stress itself (boundary
- * positions and velocities are packed at each list build and do not change
- * in between), so the pair kernel needs no pack. */
+/* Adami for a stage.  The material slots' packed neighbour data are
+ * current (the integrator that wrote the stage's state packed them, or the
+ * list build, or the filters' pack after them); Adami reads them and
+ * writes the boundary slots' packed stress itself (boundary positions and
+ * velocities are packed at each list build and do not change in between),
+ * so the pair kernel needs no pack. */
 int enqueue_adami_pack(LqSim* S, const State& st, cudaStream_t s)
 {
-    LQ_TRY(lqb::launch_pack_neighbors(&S->ph, st, S->rec, S->npb, s, S->flags & LQ_SIM_MIXED));
     return lqb::launch_adami_packed(&S->ph, S->pd, st, S->nlb, S->rec, s, S->flags & LQ_SIM_MIXED);
 }
+
 
 /* The two stages of a step on the current lists. */
 int enqueue_stages(LqSim* S, cudaStream_t s)
@@ -418,12 +441,12 @@ int enqueue_stages(LqSim* S, cudaStream_t s)
     /* predictor stage (reference src/loquat.cu:343-368) */
     LQ_TRY(enqueue_adami_pack(S, S->S, s));
     LQ_TRY(enqueue_interaction(S, S->S, s));
-    LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt, S->vw));
+    LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt, S->vw, S->rec));
     /* corrector stage (reference src/loquat.cu:371-396) */
     LQ_TRY(enqueue_adami_pack(S, S->S2, s));
     LQ_TRY(enqueue_interaction(S, S->S2, s));
     LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild, S->skin, s,
-                                    S->mt, S->vw, two_level(S) ? S->xwide : nullptr, S->wide));
+                                    S->mt, S->vw, two_level(S) ? S->xwide : nullptr, S->wide, S->rec));
     return enqueue_dynamic_dt(S, s);
 }
 
@@ -436,7 +459,7 @@ int enqueue_shepard(LqSim* S, cudaStream_t s)
         k_copy_t2<<<blocks(S->npm), 256, 0, s>>>(S->npb, S->npm, S->T.str, S->S.str);
         LQ_TRY_CUDA(cudaGetLastError(), "k_copy_t2");
     }
-    return LQ_OK;
+    return enqueue_material_pack(S, s);
 }
 
 /* An IF node on handle h after the capture's current dependencies, its body
@@ -952,13 +975,14 @@ extern "C" int lq_sim_launches_per_step(void* sim, int* plain, int* with_shepard
     if (!sim) return lqb::set_error(LQ_ERR_ARG, "lq_sim_launches_per_step: null sim");
     LqSim* S = static_cast<LqSim*>(sim);
     /* own kernels of a step without a rebuild: decide (graph only), Adami
-     * (when npb > 0), the material pack, interaction and integrator per
-     * stage; a Shepard pass adds the filter and its copy */
-    const int stage = (S->npb > 0 ? 1 : 0) + 2 + 1;
+     * (when npb > 0), interaction and integrator (which packs the material
+     * slots' neighbour data) per stage; a Shepard pass adds the filter, its
+     * copy and the material pack */
+    const int stage = (S->npb > 0 ? 1 : 0) + 1 + 1;
     const int decide = S->conditional ? 1 : 0;
     const int dyn = (S->flags & LQ_SIM_DYNAMIC_DT) ? (S->npm > 0 ? 2 : 1) : 0;
     if (plain) *plain = decide + 2 * stage + dyn;
-    if (with_shepard) *with_shepard = decide + 2 * stage + dyn + (S->npm > 0 ? 2 : 0);
+    if (with_shepard) *with_shepard = decide + 2 * stage + dyn + (S->npm > 0 ? 3 : 0);
     return LQ_OK;
 }
 
@@ -1491,11 +1515,11 @@ int profiled_step(LqSim* S, PhaseTimer& T)
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_INTEGRATE));
         if (stage == 0)
-            LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt, S->vw));
+            LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt, S->vw, S->rec));
         else {
             LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild,
                                             S->skin, s, S->mt, S->vw, two_level(S) ? S->xwide : nullptr,
-                                            S->wide));
+                                            S->wide, S->rec));
             LQ_TRY(enqueue_dynamic_dt(S, s));
         }
         LQ_TRY(T.close(s));

@@ -22,7 +22,6 @@
 #include <cub/device/device_scan.cuh>
 
 #include "lq_internal.cuh"
-#include "lq_pack.h"
 #include "lq_tile.h"
 #include "lq_device.cuh"
 #include <adami_boundary.h>
@@ -197,59 +196,6 @@ __device__ __forceinline__ void pair_body(const PairConst& K, const State& st, T
     T.l20 -= wz * gx; T.l21 -= wz * gy; T.l22 -= wz * gz;
 }
 
-/* Packed neighbour data for the list pair kernel: dense arrays over all
- * slots, with s = sigma / rho^2,
- *   nb.xr[j] = (x, y, z, rho), nb.sa[j] = (sxx, syy, szz, sxy),
- *   nb.sb[j] = (sxz, syz, v0, v1),
- * where the plain form keeps (v0, v1) = (vx, vy) and vz in nb.vz[j]
- * (52 bytes per particle, four gathers per pair) and the mixed form packs
- * the whole velocity into v0, v1 (pack_velocity: 48 bytes, three 16-byte
- * gathers per pair).  The pair kernel is bound by the L1 data pipe: a
- * warp's gathered neighbours sit close together in memory and the pipe's
- * work follows the load instructions and the sectors each gathers, so the
- * record holds only the 13 values a pair needs (no pressure word of
- * pospres, no 24-byte stress records read as three 8-byte loads).
- * 1 / rho is formed as the state-array pair body forms it. */
-struct NbrArrays {
-    float4* xr;
-    float4* sa;
-    float4* sb;
-    float* vz;
-};
-
-/* The mixed form's gathered velocity in two words (lq_pack.h: a shared
- * exponent and three 18-bit mantissas). */
-__device__ __forceinline__ float2 pack_velocity(float vx, float vy, float vz)
-{
-    unsigned w0, w1;
-    pack_velocity_words(vx, vy, vz, w0, w1);
-    return make_float2(__uint_as_float(w0), __uint_as_float(w1));
-}
-
-__device__ __forceinline__ float3 unpack_velocity(float v0, float v1)
-{
-    float3 v;
-    unpack_velocity_words(__float_as_uint(v0), __float_as_uint(v1), v.x, v.y, v.z);
-    return v;
-}
-
-/* One slot's entry of the packed arrays from its velocity, density and
- * stress (the pack kernel and the list-driven Adami write it alike). */
-template <bool kPk>
-__device__ __forceinline__ void store_packed(const NbrArrays& nb, int i, const float4& v, const tensor2d& str)
-{
-    const float rinv = __fdividef(1.0f, v.w);
-    const float r2 = rinv * rinv;
-    nb.sa[i] = make_float4(str.xx * r2, str.yy * r2, str.zz * r2, str.xy * r2);
-    if (kPk) {
-        const float2 w = pack_velocity(v.x, v.y, v.z);
-        nb.sb[i] = make_float4(str.xz * r2, str.yz * r2, w.x, w.y);
-    } else {
-        nb.sb[i] = make_float4(str.xz * r2, str.yz * r2, v.x, v.y);
-        nb.vz[i] = v.z;
-    }
-}
-
 /* One pair from the packed arrays, its density-rate and momentum terms
  * added to (drho, ax, ay, az) and its velocity-gradient terms to T.  The
  * viscosity term is always evaluated (K.avc is zero without viscosity), so
@@ -399,13 +345,20 @@ constexpr int kUnroll = 8;
  * apart when the list is built, so until the next build its distance stays
  * above 2h - skin (q > 2 - skin/h), where the kernel factor (2 - q)^3 stays
  * below (skin/h)^3.  Hits are staged per lane in shared memory and flushed
- * as coalesced rows. */
+ * in rows.
+ *
+ * With `shell` (the wide build of two-level lists) the hits are split: those
+ * with r^2 < inner2 go to `list` (count_out[t] of them) and the rest to
+ * shell (shell_count[t]), each list in hit order; each part stores at most
+ * LQ_NBR_CAP entries. */
+template <bool kSplit>
 __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __restrict__ P, int first, int ntarget,
                                                           int layer_lo, float cut2, const float4* __restrict__ pos,
                                                           Cells cells, int* __restrict__ list,
                                                           int* __restrict__ count_out, int stride,
                                                           int* __restrict__ health, const float4* __restrict__ idep,
-                                                          Frames fr)
+                                                          Frames fr, int* __restrict__ shell,
+                                                          int* __restrict__ shell_count, float inner2)
 {
     __shared__ int stage[kListWarps][kStage][32];
     const unsigned FULL = 0xffffffffu;
@@ -420,19 +373,29 @@ __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __re
     const float4 xi = active ? __ldg(pos + i) : make_float4(0.f, 0.f, 0.f, 0.f);
     int* my_stage = &stage[w][0][lane];
 
-    int staged = 0, total = 0;
+    /* staged hits carry bit 31 when they go to the shell part */
+    int staged = 0, ni = 0, ns = 0;
     auto flush = [&]() {
         const int maxc = (int)__reduce_max_sync(FULL, (unsigned)staged);
         for (int k = 0; k < maxc; ++k)
-            if (k < staged && total + k < LQ_NBR_CAP) list[(size_t)(total + k) * stride + t] = my_stage[32 * k];
-        total += staged;
+            if (k < staged) {
+                const int e = my_stage[32 * k];
+                if (kSplit && e < 0) {
+                    if (ns < LQ_NBR_CAP) shell[(size_t)ns * stride + t] = e & 0x7fffffff;
+                    ++ns;
+                } else {
+                    if (ni < LQ_NBR_CAP) list[(size_t)ni * stride + t] = e;
+                    ++ni;
+                }
+            }
         staged = 0;
         __syncwarp();
     };
     auto test = [&](bool mine, const float4& xj, int j) {
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        if (mine && dx * dx + dy * dy + dz * dz < cut2) {
-            my_stage[32 * staged] = j;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (mine && r2 < cut2) {
+            my_stage[32 * staged] = (kSplit && !(r2 < inner2)) ? (int)((unsigned)j | 0x80000000u) : j;
             ++staged;
         }
     };
@@ -483,8 +446,9 @@ __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __re
     }
     flush();
     if (active) {
-        count_out[t] = total;
-        if (total > LQ_NBR_CAP && health) atomicAdd(health + HEALTH_NBR_OVERFLOW, 1);
+        count_out[t] = ni;
+        if (kSplit) shell_count[t] = ns;
+        if ((ni > LQ_NBR_CAP || ns > LQ_NBR_CAP) && health) atomicAdd(health + HEALTH_NBR_OVERFLOW, 1);
     }
 }
 
@@ -510,60 +474,69 @@ __device__ __forceinline__ int ld_list(const int* p)
 }
 
 /* Two-level lists: the lists the stages read (cut-off 2h + skin) renewed
- * from wider ones (2h + wide, built after each sort) at the current
- * positions, without a search.  Target t keeps, in their order, the entries
- * of its wide list within the cut-off, so the result is the list a build
- * with this cut-off over the same walk would give, as long as no pair within
- * 2h + skin now was beyond 2h + wide when the wide lists were built (the
- * corrector's check keeps every particle within (wide - skin) / 2 of its
- * position then).  A wide list that overflowed (count above LQ_NBR_CAP) passes its
- * count on: the pair kernel then walks that target's stencil, as after a
- * direct build. */
+ * at the current positions without a search.  The wide build (cut-off
+ * 2h + wide) wrote each target's pairs closer than inner = 2h + 2 skin -
+ * wide into rows [0, ni) of the stages' list and the rest into its shell
+ * list.  While no particle has moved (wide - skin) / 2 from its position at
+ * that build (the corrector's check), a pair's distance has changed by less
+ * than wide - skin, so every inner pair is still within 2h + skin and every
+ * pair now within 2h + skin was within 2h + wide: the renewal keeps rows
+ * [0, ni) as they are and appends, in their order, the shell entries now
+ * within the cut-off.  Entries are fetched a group ahead so the position
+ * gathers overlap.  Overflows keep LQ_NBR_CAP valid rows and a count above
+ * it (the pair kernel then walks that target's stencil): a truncated shell
+ * list fills the rows after the inner part with its stored entries. */
 __global__ void __launch_bounds__(kBlock) k_list_refresh(int first, int ntarget, int np, float cut2,
                                                          const float4* __restrict__ pos,
-                                                         const int* __restrict__ wlist,
-                                                         const int* __restrict__ wcount, int wstride,
-                                                         int* __restrict__ list, int* __restrict__ count,
-                                                         int stride)
+                                                         const int* __restrict__ inner_count,
+                                                         const int* __restrict__ shell,
+                                                         const int* __restrict__ shell_count, int* __restrict__ list,
+                                                         int* __restrict__ count, int stride,
+                                                         int* __restrict__ health)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ntarget) return;
-    const int nw = __ldg(wcount + t);
-    if (nw > LQ_NBR_CAP) {
-        count[t] = nw;
+    const int ni = __ldg(inner_count + t), ns = __ldg(shell_count + t);
+    const int* p = shell + t;
+    if (ni > LQ_NBR_CAP) {
+        count[t] = ni;          /* rows [0, LQ_NBR_CAP) hold inner entries */
+        return;
+    }
+    if (ns > LQ_NBR_CAP) {
+        for (int k = 0; ni + k < LQ_NBR_CAP; ++k) list[(size_t)(ni + k) * stride + t] = ld_list(p + (size_t)k * stride);
+        count[t] = ni + ns;
         return;
     }
     const int i = first + t;
     const float4 xi = __ldg(pos + i);
-    const int* p = wlist + t;
-    /* groups of kG entries, the next group's entries fetched while this
-     * group's positions are gathered; the last group is filled up with the
-     * target's own slot (a valid address; never kept) */
+    /* groups of kG entries; the last group is filled up with the target's
+     * own slot (a valid address; never kept) */
     constexpr int kG = 8;
     int nxt[kG];
 #pragma unroll
-    for (int u = 0; u < kG; ++u) nxt[u] = u < nw ? ld_list(p + (size_t)u * wstride) : i;
-    int n = 0;
-    for (int k = 0; k < nw; k += kG) {
+    for (int u = 0; u < kG; ++u) nxt[u] = u < ns ? ld_list(p + (size_t)u * stride) : i;
+    int n = ni;
+    for (int k = 0; k < ns; k += kG) {
         int j[kG];
         float4 xj[kG];
 #pragma unroll
         for (int u = 0; u < kG; ++u) {
             j[u] = nxt[u];
-            nxt[u] = k + kG + u < nw ? ld_list(p + (size_t)(k + kG + u) * wstride) : i;
+            nxt[u] = k + kG + u < ns ? ld_list(p + (size_t)(k + kG + u) * stride) : i;
         }
 #pragma unroll
         for (int u = 0; u < kG; ++u) xj[u] = lq_in_range(j[u], np) ? __ldg(pos + j[u]) : xi;
 #pragma unroll
         for (int u = 0; u < kG; ++u) {
             const float dx = xi.x - xj[u].x, dy = xi.y - xj[u].y, dz = xi.z - xj[u].z;
-            if (k + u < nw && lq_in_range(j[u], np) && dx * dx + dy * dy + dz * dz < cut2) {
-                list[(size_t)n * stride + t] = j[u];
+            if (k + u < ns && lq_in_range(j[u], np) && dx * dx + dy * dy + dz * dz < cut2) {
+                if (n < LQ_NBR_CAP) list[(size_t)n * stride + t] = j[u];
                 ++n;
             }
         }
     }
     count[t] = n;
+    if (n > LQ_NBR_CAP && health) atomicAdd(health + HEALTH_NBR_OVERFLOW, 1);
 }
 
 /* The sums over one target's list (entry k at p[k * stride]), four
@@ -1077,12 +1050,6 @@ int tile_order_scratch(const Parameters* ph, int* nseg, size_t* scan_bytes)
     return LQ_OK;
 }
 
-static NbrArrays nbr_arrays(float* rec, int np)
-{
-    const size_t n = (size_t)np;
-    return NbrArrays{reinterpret_cast<float4*>(rec), reinterpret_cast<float4*>(rec) + n,
-                     reinterpret_cast<float4*>(rec) + 2 * n, rec + 12 * n};
-}
 
 int launch_tile_order(const Parameters* ph, const int* start, int shape, const TileOrder& to, cudaStream_t s)
 {
@@ -1123,26 +1090,37 @@ int launch_neighbor_list(const Parameters* ph, const Parameters* pd, const float
 }
 
 int launch_list_refresh(const Parameters* ph, int first, int n, float cut, const float4* pos,
-                        const NeighborList& wide, const NeighborList& nl, cudaStream_t s)
+                        const int* inner_count, const NeighborList& shell, const NeighborList& nl, int* health,
+                        cudaStream_t s)
 {
     if (n <= 0) return LQ_OK;
-    if (nl.stride < n || wide.stride < n)
-        return set_error(LQ_ERR_ARG, "list refresh: strides %d / %d < targets %d", nl.stride, wide.stride, n);
-    k_list_refresh<<<blocks_for(n, kBlock), kBlock, 0, s>>>(first, n, ph->np, cut * cut, pos, wide.list, wide.count,
-                                                           wide.stride, nl.list, nl.count, nl.stride);
+    if (nl.stride < n || shell.stride != nl.stride)
+        return set_error(LQ_ERR_ARG, "list renewal: strides %d / %d, targets %d", nl.stride, shell.stride, n);
+    k_list_refresh<<<blocks_for(n, kBlock), kBlock, 0, s>>>(first, n, ph->np, cut * cut, pos, inner_count, shell.list,
+                                                           shell.count, nl.list, nl.count, nl.stride, health);
     LQ_TRY_CUDA(cudaGetLastError(), "k_list_refresh");
     return LQ_OK;
 }
 
 int launch_neighbor_list_range(const Parameters* ph, const Parameters* pd, int first, int n, int layer_lo, float cut,
                                const float4* pos, const Cells& c, const NeighborList& nl, int* health,
-                               cudaStream_t s, const float4* idep, const Frames& fr)
+                               cudaStream_t s, const float4* idep, const Frames& fr, const NeighborList* shell,
+                               float inner)
 {
     if (fr.rows && !idep) return set_error(LQ_ERR_ARG, "neighbour list: frames need the idep array");
     if (n <= 0) return LQ_OK;
     if (nl.stride < n) return set_error(LQ_ERR_ARG, "neighbour list stride %d < targets %d", nl.stride, n);
-    k_neighbor_list<<<blocks_for(n, kBlock), kBlock, 0, s>>>(pd, first, n, layer_lo, cut * cut, pos, c, nl.list,
-                                                            nl.count, nl.stride, health, idep, fr);
+    if (shell && shell->stride != nl.stride)
+        return set_error(LQ_ERR_ARG, "neighbour list: shell stride %d differs from %d", shell->stride, nl.stride);
+    const float inner2 = inner > 0.0f ? inner * inner : 0.0f;
+    if (shell)
+        k_neighbor_list<true><<<blocks_for(n, kBlock), kBlock, 0, s>>>(pd, first, n, layer_lo, cut * cut, pos, c,
+                                                                      nl.list, nl.count, nl.stride, health, idep, fr,
+                                                                      shell->list, shell->count, inner2);
+    else
+        k_neighbor_list<false><<<blocks_for(n, kBlock), kBlock, 0, s>>>(pd, first, n, layer_lo, cut * cut, pos, c,
+                                                                       nl.list, nl.count, nl.stride, health, idep,
+                                                                       fr, nullptr, nullptr, 0.0f);
     LQ_TRY_CUDA(cudaGetLastError(), "k_neighbor_list");
     return LQ_OK;
 }

@@ -37,7 +37,7 @@ int main()
         (const void*)&lq_sim_synchronize, (const void*)&lq_sim_stream, (const void*)&lq_sim_upload,
         (const void*)&lq_sim_download, (const void*)&lq_sim_state, (const void*)&lq_sim_clock,
         (const void*)&lq_sim_health, (const void*)&lq_sim_launches_per_step, (const void*)&lq_sim_profile,
-        (const void*)&lq_sim_set_skin, (const void*)&lq_sim_set_materials, (const void*)&lq_sim_set_hypoplastic, (const void*)&lq_sim_set_frames, (const void*)&lq_sim_rebuilds, (const void*)&lq_sim_rebuild_launches, (const void*)&lq_sim_neighbor_entries, (const void*)&lq_debug_bounds_violations, (const void*)&lq_sim_set_pair_shape, (const void*)&lq_sim_pair_shape, (const void*)&lq_sim_autotune, (const void*)&lq_sim_save_checkpoint, (const void*)&lq_sim_load_checkpoint,
+        (const void*)&lq_sim_set_skin, (const void*)&lq_sim_set_materials, (const void*)&lq_sim_set_hypoplastic, (const void*)&lq_sim_set_frames, (const void*)&lq_sim_rebuilds, (const void*)&lq_sim_rebuild_launches, (const void*)&lq_sim_set_wide_skin, (const void*)&lq_sim_wide_skin, (const void*)&lq_sim_renewals, (const void*)&lq_sim_renewal_launches, (const void*)&lq_sim_neighbor_entries, (const void*)&lq_debug_bounds_violations, (const void*)&lq_sim_set_pair_shape, (const void*)&lq_sim_pair_shape, (const void*)&lq_sim_autotune, (const void*)&lq_sim_save_checkpoint, (const void*)&lq_sim_load_checkpoint,
         (const void*)&lq_io_load_parameters,
         (const void*)&lq_io_save_parameters, (const void*)&lq_io_load_hypoplastic, (const void*)&lq_io_save_parameters_vw, (const void*)&lq_io_load_particles, (const void*)&lq_io_save_particles,
         (const void*)&lq_io_save_vtu,
