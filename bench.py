@@ -587,8 +587,10 @@ def size_classes(counts, nclass=4):
     return [list(np.nonzero(cls == k)[0]) for k in range(nclass) if np.any(cls == k)]
 
 
-# timed steps of the ensemble measurement carried by the default line
+# timed steps of the ensemble measurement carried by the default line, and
+# steps of its per-phase profile
 ENSEMBLE_KEY_STEPS = 100
+ENSEMBLE_PROFILE_STEPS = 40
 
 
 def ensemble_measurement(args, torch, world, rank, local, dist, sample_clocks=False, steps=None):
@@ -647,6 +649,13 @@ def ensemble_measurement(args, torch, world, rank, local, dist, sample_clocks=Fa
             extra = {"clocks": clocks.stop() if clocks else None, "neighbour_list_rebuilds": sim.rebuilds() - rb0,
                      "neighbour_list_renewals": sim.renewals() - rn0,
                      "health": [int(x) for x in sim.health()], "gpu_launches_per_step": sim.launches_per_step()[0]}
+            if args.profile_steps > 0:
+                # per-phase device times of the same run (eager launches, CUDA
+                # events; long enough to hold sorts and renewals at their rate)
+                n = max(args.profile_steps, ENSEMBLE_PROFILE_STEPS)
+                prof = sim.profile(n)
+                extra["phases_ms_per_step"] = {k: v[0] / n for k, v in prof.items()}
+                extra["phase_launches"] = {k: v[1] for k, v in prof.items()}
         sim.close()
         forms[form] = {"value": total_npm * nsteps / (ms / 1e3), "ms_per_step": ms / nsteps}
         tuned_by_form[form] = tuned
@@ -724,6 +733,7 @@ def bench_ensemble(args):
             "autotuned": m["autotuned"], "gpu_launches_per_step": m["gpu_launches_per_step"],
             "neighbour_list_rebuilds": m["neighbour_list_rebuilds"],
             "neighbour_list_renewals": m["neighbour_list_renewals"], "health": m["health"],
+            "phases_ms_per_step": m.get("phases_ms_per_step"),
             "clocks": m["clocks"], "partition": m["partition"],
         }))
     if dist:
