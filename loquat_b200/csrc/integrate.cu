@@ -28,6 +28,15 @@ constexpr int kBlock = 128;
 #ifndef LQ_VW_MIN_BLOCKS
 #define LQ_VW_MIN_BLOCKS 4
 #endif
+/* resident blocks per SM asked of the other instantiations: 6 caps them at
+ * 80 registers (the mixed form's FP64 return map spills ~130 B), 24 warps
+ * per SM instead of 16 for the uncapped 117-120; on the 256-scenario
+ * ensemble the mixed integrators took 2.19 ms per step against 2.25 (5),
+ * 2.22 (7), 2.36 (8) and 2.49 uncapped; the plain ones (78 registers) are
+ * unaffected */
+#ifndef LQ_INT_MIN_BLOCKS
+#define LQ_INT_MIN_BLOCKS 6
+#endif
 
 inline int blocks_for(long long n, int b) { return (int)((n + b - 1) / b); }
 
@@ -71,7 +80,7 @@ __device__ __forceinline__ void pack_slot(const NbrArrays& nb, int i, const floa
  * v += dt/2 a; rho += dt/2 drho; x += dt/2 v_new; eps += dt/2 deps;
  * stress and plastic strain from the model at dt/2. */
 template <bool kMixed, bool kVW>
-__global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_predict(const Parameters* __restrict__ P, int np, int npb, State in,
+__global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : LQ_INT_MIN_BLOCKS) k_predict(const Parameters* __restrict__ P, int np, int npb, State in,
                                                     State out, State snap, bool do_snap, Rates rt, MaterialTable mt,
                                                     MaterialTable vw, NbrArrays nb)
 {
@@ -232,7 +241,7 @@ __device__ __forceinline__ void verlet_check(const VerletCheck& vc, int i, const
 }
 
 template <bool kMixed, bool kVW>
-__global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : 1) k_correct(const Parameters* __restrict__ P, int np, int npb, State cur,
+__global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : LQ_INT_MIN_BLOCKS) k_correct(const Parameters* __restrict__ P, int np, int npb, State cur,
                                                     State ini, const int* __restrict__ ini_idx, State out, Rates rt,
                                                     int* __restrict__ health, VerletCheck verlet, int first,
                                                     MaterialTable mt, MaterialTable vw, NbrArrays nb)
