@@ -243,11 +243,13 @@ int launch_density_filter_list(const Parameters* par_host, const Parameters* par
  * layer_lo..1 with cut-off radius `cut` (2h plus skin); list overflows are
  * counted in health[HEALTH_NBR_OVERFLOW].  With `shell`, pairs at distance
  * `inner` or more go to the shell list instead (wide build of two-level
- * lists; nl.count then receives the inner counts). */
+ * lists; nl.count then receives the inner counts).  With `gate` the
+ * kernel does nothing unless *gate is non-zero (a decision taken on the
+ * device). */
 int launch_neighbor_list_range(const Parameters* par_host, const Parameters* par_dev, int first, int n, int layer_lo,
                                float cut, const float4* pos, const Cells& c, const NeighborList& nl, int* health,
                                cudaStream_t s, const float4* idep = nullptr, const Frames& fr = Frames(),
-                               const NeighborList* shell = nullptr, float inner = 0.0f);
+                               const NeighborList* shell = nullptr, float inner = 0.0f, const int* gate = nullptr);
 /* Two-level lists of targets [first, first + n): rows [0, inner_count[t])
  * of nl, written by the wide build, kept, and the entries of the shell list
  * now within `cut` appended (positions pos). */

@@ -358,8 +358,10 @@ __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __re
                                                           int* __restrict__ count_out, int stride,
                                                           int* __restrict__ health, const float4* __restrict__ idep,
                                                           Frames fr, int* __restrict__ shell,
-                                                          int* __restrict__ shell_count, float inner2)
+                                                          int* __restrict__ shell_count, float inner2,
+                                                          const int* __restrict__ gate)
 {
+    if (gate && *gate == 0) return;     /* the whole grid leaves: no collective is split */
     __shared__ int stage[kListWarps][kStage][32];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1105,7 +1107,7 @@ int launch_list_refresh(const Parameters* ph, int first, int n, float cut, const
 int launch_neighbor_list_range(const Parameters* ph, const Parameters* pd, int first, int n, int layer_lo, float cut,
                                const float4* pos, const Cells& c, const NeighborList& nl, int* health,
                                cudaStream_t s, const float4* idep, const Frames& fr, const NeighborList* shell,
-                               float inner)
+                               float inner, const int* gate)
 {
     if (fr.rows && !idep) return set_error(LQ_ERR_ARG, "neighbour list: frames need the idep array");
     if (n <= 0) return LQ_OK;
@@ -1116,11 +1118,11 @@ int launch_neighbor_list_range(const Parameters* ph, const Parameters* pd, int f
     if (shell)
         k_neighbor_list<true><<<blocks_for(n, kBlock), kBlock, 0, s>>>(pd, first, n, layer_lo, cut * cut, pos, c,
                                                                       nl.list, nl.count, nl.stride, health, idep, fr,
-                                                                      shell->list, shell->count, inner2);
+                                                                      shell->list, shell->count, inner2, gate);
     else
         k_neighbor_list<false><<<blocks_for(n, kBlock), kBlock, 0, s>>>(pd, first, n, layer_lo, cut * cut, pos, c,
                                                                        nl.list, nl.count, nl.stride, health, idep,
-                                                                       fr, nullptr, nullptr, 0.0f);
+                                                                       fr, nullptr, nullptr, 0.0f, gate);
     LQ_TRY_CUDA(cudaGetLastError(), "k_neighbor_list");
     return LQ_OK;
 }
@@ -1291,12 +1293,12 @@ struct DropInWorkspace {
     int* build_of = nullptr;        /* np: identity -> slot at the build */
     int* cur_of = nullptr;          /* np: identity -> current slot */
     int* moved = nullptr;           /* device flag: a particle moved half the skin since the build */
-    int* moved_host = nullptr;      /* pinned copy of the flag */
+    int* tally = nullptr;           /* device counts of [0] builds and [1] reuses of carried lists */
     const int* key = nullptr;       /* the grid (its cell_beg) the carried lists belong to */
     long long gen = -1;
     int np_built = 0, npb_built = 0;
     bool built = false;
-    long long rebuilds = 0, reuses = 0;
+    long long rebuilds = 0, reuses = 0;   /* counts of earlier workspaces (tally holds this one's) */
     std::vector<void*> allocs;
 };
 std::mutex g_ws_mutex;
@@ -1305,7 +1307,6 @@ std::vector<DropInWorkspace> g_ws;
 void free_workspace(DropInWorkspace& w)
 {
     for (void* p : w.allocs) cudaFree(p);
-    if (w.moved_host) cudaFreeHost(w.moved_host);
     w = DropInWorkspace{};
 }
 
@@ -1328,8 +1329,17 @@ int size_workspace(DropInWorkspace& w, const Parameters* ph)
     LQ_TRY(lqb::scan_scratch_bytes(ncell, &cell_scan));
     if (np <= w.np && ncell <= w.ncell && nseg <= w.nseg && npm <= w.npm && w.rec) return LQ_OK;
     if (!w.allocs.empty()) LQ_TRY_CUDA(cudaDeviceSynchronize(), "interaction workspace");
+    long long rebuilds = w.rebuilds, reuses = w.reuses;
+    if (w.tally) {
+        int t[2] = {0, 0};
+        LQ_TRY_CUDA(cudaMemcpy(t, w.tally, sizeof(t), cudaMemcpyDeviceToHost), "interaction workspace");
+        rebuilds += t[0];
+        reuses += t[1];
+    }
     free_workspace(w);
     DropInWorkspace n;
+    n.rebuilds = rebuilds;
+    n.reuses = reuses;
     int st = LQ_OK;
     auto A = [&](void** p, size_t bytes) {
         if (st == LQ_OK) st = ws_alloc(n, p, bytes);
@@ -1353,9 +1363,10 @@ int size_workspace(DropInWorkspace& w, const Parameters* ph)
     A((void**)&n.build_of, sizeof(int) * (size_t)np);
     A((void**)&n.cur_of, sizeof(int) * (size_t)np);
     A((void**)&n.moved, sizeof(int));
+    A((void**)&n.tally, 2 * sizeof(int));
     if (st == LQ_OK) {
-        const cudaError_t e = cudaMallocHost((void**)&n.moved_host, sizeof(int));
-        if (e != cudaSuccess) st = lqb::set_error(LQ_ERR_ALLOC, "interaction workspace: %s", cudaGetErrorString(e));
+        const cudaError_t e = cudaMemset(n.tally, 0, 2 * sizeof(int));
+        if (e != cudaSuccess) st = lqb::set_error(LQ_ERR_CUDA, "interaction workspace: %s", cudaGetErrorString(e));
     }
     if (st != LQ_OK) {
         free_workspace(n);
@@ -1402,25 +1413,36 @@ __global__ void __launch_bounds__(256) k_moved_half_skin(int np, const float4* _
     if (far) *moved = 1;
 }
 
-__global__ void __launch_bounds__(256) k_identity_slots(int np, const int* __restrict__ ident, int* __restrict__ slot)
+/* The call's decision, counted: a build when a particle moved (or nothing
+ * was carried), else a reuse. */
+__global__ void k_tally_decision(const int* __restrict__ moved, int* __restrict__ tally)
+{
+    tally[*moved ? 0 : 1] += 1;
+}
+
+/* Reuse (skipped when *moved): identity -> current slot. */
+__global__ void __launch_bounds__(256) k_identity_slots(int np, const int* __restrict__ ident, int* __restrict__ slot,
+                                                        const int* __restrict__ moved)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= np) return;
+    if (c >= np || *moved) return;
     const int id = __ldg(ident + c);
     if ((unsigned)id < (unsigned)np) slot[id] = c;
 }
 
-/* The carried lists in the current slots: target t takes the list its
- * particle had at the build, each entry mapped from identity to slot. */
+/* The carried lists in the current slots (skipped when *moved): target t
+ * takes the list its particle had at the build, each entry mapped from
+ * identity to slot. */
 __global__ void __launch_bounds__(256) k_remap_lists(int np, int npb, int npm, const int* __restrict__ ident,
                                                      const int* __restrict__ build_of,
                                                      const int* __restrict__ list_id,
                                                      const int* __restrict__ count_b,
                                                      const int* __restrict__ cur_of, int* __restrict__ list,
-                                                     int* __restrict__ count, int stride)
+                                                     int* __restrict__ count, int stride,
+                                                     const int* __restrict__ moved)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= npm) return;
+    if (t >= npm || *moved) return;
     const int id = __ldg(ident + npb + t);
     const int b = (unsigned)id < (unsigned)np ? __ldg(build_of + id) - npb : -1;
     if (b < 0 || b >= npm) {
@@ -1436,16 +1458,17 @@ __global__ void __launch_bounds__(256) k_remap_lists(int np, int npb, int npm, c
     }
 }
 
-/* A fresh build stored for carrying: lists as identities, build positions
- * and slots by identity. */
+/* A fresh build stored for carrying (skipped unless *moved): lists as
+ * identities, build positions and slots by identity. */
 __global__ void __launch_bounds__(256) k_store_build(int np, int npb, int npm, const int* __restrict__ ident,
                                                      const float4* __restrict__ pos, const int* __restrict__ list,
                                                      const int* __restrict__ count, int stride,
                                                      int* __restrict__ list_id, int* __restrict__ count_b,
-                                                     float4* __restrict__ xbuild, int* __restrict__ build_of)
+                                                     float4* __restrict__ xbuild, int* __restrict__ build_of,
+                                                     const int* __restrict__ moved)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= np) return;
+    if (c >= np || !*moved) return;
     const int id = __ldg(ident + c);
     if ((unsigned)id < (unsigned)np) {
         xbuild[id] = __ldg(pos + c);
@@ -1487,8 +1510,15 @@ extern "C" int lq_interaction_stats(long long* rebuilds, long long* reuses)
     *rebuilds = 0;
     *reuses = 0;
     if (dev < (int)g_ws.size()) {
-        *rebuilds = g_ws[(size_t)dev].rebuilds;
-        *reuses = g_ws[(size_t)dev].reuses;
+        const DropInWorkspace& w = g_ws[(size_t)dev];
+        int t[2] = {0, 0};
+        if (w.tally) {
+            /* the decisions are counted on the device by the calls' streams */
+            LQ_TRY_CUDA(cudaDeviceSynchronize(), "interaction stats");
+            LQ_TRY_CUDA(cudaMemcpy(t, w.tally, sizeof(t), cudaMemcpyDeviceToHost), "interaction stats");
+        }
+        *rebuilds = w.rebuilds + t[0];
+        *reuses = w.reuses + t[1];
     }
     return LQ_OK;
 }
@@ -1539,39 +1569,38 @@ extern "C" int lq_particle_interaction(const void* par_host, const void* par_dev
     lqb::GridIdentity gi;
     if (lqb::identity_find(cell_beg, &gi) && gi.np == np) {
         /* the caller's grid tracks its particles: carry the lists while
-         * every particle stays within half the skin of its build position */
+         * every particle stays within half the skin of its build position.
+         * The device decides (no host synchronisation): both paths are
+         * enqueued and the one not taken returns at once. */
         const float skin = kDropInSkinOverH * ph->h;
-        bool reuse = false;
-        if (w->built && w->key == cell_beg && w->gen == gi.gen && w->np_built == np && w->npb_built == npb) {
+        const bool carried =
+            w->built && w->key == cell_beg && w->gen == gi.gen && w->np_built == np && w->npb_built == npb;
+        if (carried) {
             LQ_TRY_CUDA(cudaMemsetAsync(w->moved, 0, sizeof(int), s), "moved flag");
             k_moved_half_skin<<<nb256, 256, 0, s>>>(np, st.pos, gi.ident, w->xbuild, 0.25f * skin * skin, w->moved);
             LQ_TRY_CUDA(cudaGetLastError(), "k_moved_half_skin");
-            LQ_TRY_CUDA(cudaMemcpyAsync(w->moved_host, w->moved, sizeof(int), cudaMemcpyDeviceToHost, s),
-                        "moved flag");
-            LQ_TRY_CUDA(cudaStreamSynchronize(s), "moved flag");
-            reuse = *w->moved_host == 0;
-        }
-        if (reuse) {
-            k_identity_slots<<<nb256, 256, 0, s>>>(np, gi.ident, w->cur_of);
-            LQ_TRY_CUDA(cudaGetLastError(), "k_identity_slots");
-            k_remap_lists<<<(npm + 255) / 256, 256, 0, s>>>(np, npb, npm, gi.ident, w->build_of, w->list_id,
-                                                            w->count_b, w->cur_of, w->nl.list, w->nl.count,
-                                                            w->nl.stride);
-            LQ_TRY_CUDA(cudaGetLastError(), "k_remap_lists");
-            ++w->reuses;
         } else {
-            LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, npb, npm, 0, 2.0f * ph->h + skin, st.pos, c, w->nl,
-                                                   nullptr, s));
-            k_store_build<<<nb256, 256, 0, s>>>(np, npb, npm, gi.ident, st.pos, w->nl.list, w->nl.count,
-                                                w->nl.stride, w->list_id, w->count_b, w->xbuild, w->build_of);
-            LQ_TRY_CUDA(cudaGetLastError(), "k_store_build");
-            w->built = true;
-            w->key = cell_beg;
-            w->gen = gi.gen;
-            w->np_built = np;
-            w->npb_built = npb;
-            ++w->rebuilds;
+            LQ_TRY(lqb::fill_int(w->moved, 1, 1, s));
         }
+        k_tally_decision<<<1, 1, 0, s>>>(w->moved, w->tally);
+        LQ_TRY_CUDA(cudaGetLastError(), "k_tally_decision");
+        /* reuse */
+        k_identity_slots<<<nb256, 256, 0, s>>>(np, gi.ident, w->cur_of, w->moved);
+        LQ_TRY_CUDA(cudaGetLastError(), "k_identity_slots");
+        k_remap_lists<<<(npm + 255) / 256, 256, 0, s>>>(np, npb, npm, gi.ident, w->build_of, w->list_id, w->count_b,
+                                                        w->cur_of, w->nl.list, w->nl.count, w->nl.stride, w->moved);
+        LQ_TRY_CUDA(cudaGetLastError(), "k_remap_lists");
+        /* build */
+        LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, npb, npm, 0, 2.0f * ph->h + skin, st.pos, c, w->nl, nullptr,
+                                               s, nullptr, lqb::Frames(), nullptr, 0.0f, w->moved));
+        k_store_build<<<nb256, 256, 0, s>>>(np, npb, npm, gi.ident, st.pos, w->nl.list, w->nl.count, w->nl.stride,
+                                            w->list_id, w->count_b, w->xbuild, w->build_of, w->moved);
+        LQ_TRY_CUDA(cudaGetLastError(), "k_store_build");
+        w->built = true;
+        w->key = cell_beg;
+        w->gen = gi.gen;
+        w->np_built = np;
+        w->npb_built = npb;
     } else {
         /* the pair body's own cut-off test: q < 2 with the candidate slack
          * of the cell walk */

