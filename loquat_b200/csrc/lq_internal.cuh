@@ -156,15 +156,18 @@ int launch_neighbor_list(const Parameters* par_host, const Parameters* par_dev, 
  * sigma/rho^2: 52 bytes per particle, 48 in the compensated form, whose
  * velocity is packed into two words) that the pair kernel gathers; with
  * `pack` they are packed from the state first, in the form of
- * `compensated`. */
+ * `compensated`.  With `rows` (thread-per-target shapes, `pack` set)
+ * target t reads list row rows[t] (-1: walk the stencil), whose entries
+ * index records packed in another slot order: slot i's record goes to
+ * map[i], target t's own at npb + rows[t]. */
 int launch_interaction_list(const Parameters* par_host, const Parameters* par_dev, const State& st, const Rates& r,
                             const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr = Frames(),
                             bool compensated = false, float* rec = nullptr, int shape = 0, bool pack = true,
-                            const int* order = nullptr);
+                            const int* order = nullptr, const int* rows = nullptr, const int* map = nullptr);
 /* The packed neighbour arrays of slots [first, np) from the state;
  * packed_velocity selects the compensated pair kernel's record. */
 int launch_pack_neighbors(const Parameters* par_host, const State& st, float* rec, int first, cudaStream_t s,
-                          bool packed_velocity);
+                          bool packed_velocity, const int* map = nullptr);
 /* Adami over the boundary lists reading the packed arrays (material slots
  * packed), writing the boundary stress into the state and the packed
  * arrays. */

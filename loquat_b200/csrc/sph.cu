@@ -454,15 +454,23 @@ __global__ void __launch_bounds__(kBlock) k_neighbor_list(const Parameters* __re
     }
 }
 
+/* Slot i's packed record, at i or (with map) at map[i], the index lists
+ * of another slot order gather it at (slots with none are skipped). */
 template <bool kPk>
-__global__ void __launch_bounds__(kBlock) k_pack_neighbors(int first, int np, State st, NbrArrays nb)
+__global__ void __launch_bounds__(kBlock) k_pack_neighbors(int first, int np, State st, NbrArrays nb,
+                                                           const int* __restrict__ map)
 {
     const int i = first + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
+    int o = i;
+    if (map) {
+        o = __ldg(map + i);
+        if ((unsigned)o >= (unsigned)np) return;
+    }
     const float4 x = __ldg(st.pos + i);
     const float4 v = __ldg(st.vel + i);
-    nb.xr[i] = make_float4(x.x, x.y, x.z, v.w);
-    store_packed<kPk>(nb, i, v, load_t2(st.str, i));
+    nb.xr[o] = make_float4(x.x, x.y, x.z, v.w);
+    store_packed<kPk>(nb, o, v, load_t2(st.str, i));
 }
 
 /* A list entry: each 128-byte row of a list is read once per launch, so it
@@ -590,7 +598,8 @@ __device__ __forceinline__ void list_sums(const PairConst& K, const NbrArrays& n
 template <bool kKahan, int kThreads, int kMinBlocks>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) k_interaction_rec(
     const Parameters* __restrict__ P, int np, int npb, State st, Rates rt, Cells cells, const int* __restrict__ list,
-    const int* __restrict__ count, int stride, Frames fr, NbrArrays nb, const int* __restrict__ order)
+    const int* __restrict__ count, int stride, Frames fr, NbrArrays nb, const int* __restrict__ order,
+    const int* __restrict__ rows)
 {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= np - npb) return;
@@ -601,12 +610,20 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_interaction_rec(
     const PairConst K = load_pair_const(P);
     Target T;
     load_target(K, st, i, true, T);
-    const int n = __ldg(count + t);
+    /* with rows: target t's list is row rows[t] (-1: none), whose entries
+     * index records packed in that other slot order, the target's own at
+     * npb + row (the filler of the last group) */
+    int row = t, self = i;
+    if (rows) {
+        row = __ldg(rows + t);
+        self = npb + row;
+    }
+    const int n = row >= 0 ? __ldg(count + row) : LQ_NBR_CAP + 1;
     if (n <= LQ_NBR_CAP) {
         if (K.artp)
-            list_sums<kKahan, true>(K, nb, T, list + t, n, stride, i, np);
+            list_sums<kKahan, true>(K, nb, T, list + row, n, stride, self, np);
         else
-            list_sums<kKahan, false>(K, nb, T, list + t, n, stride, i, np);
+            list_sums<kKahan, false>(K, nb, T, list + row, n, stride, self, np);
     } else {
         walk_stencil(P, K, st, cells, i, T.x, [&](int j) { pair_body<kKahan>(K, st, T, j); }, fr);
     }
@@ -1128,15 +1145,15 @@ int launch_neighbor_list_range(const Parameters* ph, const Parameters* pd, int f
 }
 
 int launch_pack_neighbors(const Parameters* ph, const State& st, float* rec, int first, cudaStream_t s,
-                          bool packed_velocity)
+                          bool packed_velocity, const int* map)
 {
     const int n = ph->np - first;
     if (n <= 0) return LQ_OK;
     const NbrArrays nb = nbr_arrays(rec, ph->np);
     if (packed_velocity)
-        k_pack_neighbors<true><<<blocks_for(n, kBlock), kBlock, 0, s>>>(first, ph->np, st, nb);
+        k_pack_neighbors<true><<<blocks_for(n, kBlock), kBlock, 0, s>>>(first, ph->np, st, nb, map);
     else
-        k_pack_neighbors<false><<<blocks_for(n, kBlock), kBlock, 0, s>>>(first, ph->np, st, nb);
+        k_pack_neighbors<false><<<blocks_for(n, kBlock), kBlock, 0, s>>>(first, ph->np, st, nb, map);
     LQ_TRY_CUDA(cudaGetLastError(), "k_pack_neighbors");
     return LQ_OK;
 }
@@ -1168,22 +1185,26 @@ int launch_shepard_list(const Parameters* ph, const Parameters* pd, const State&
 
 int launch_interaction_list(const Parameters* ph, const Parameters* pd, const State& st, const Rates& r,
                             const Cells& c, const NeighborList& nl, cudaStream_t s, const Frames& fr,
-                            bool compensated, float* rec, int shape, bool pack, const int* order)
+                            bool compensated, float* rec, int shape, bool pack, const int* order,
+                            const int* rows, const int* map)
 {
     if (ph->npm <= 0) return LQ_OK;
     if (rec) {
         if (reinterpret_cast<uintptr_t>(rec) % 16 != 0)
             return set_error(LQ_ERR_ARG, "interaction: packed neighbour arrays must be 16-byte aligned");
         const NbrArrays nb = nbr_arrays(rec, ph->np);
-        if (pack) LQ_TRY(launch_pack_neighbors(ph, st, rec, 0, s, compensated));
+        if (rows && (!map || !pack || shape == 5 || shape == 6))
+            return set_error(LQ_ERR_ARG, "interaction: list rows need a record map, a pack and a thread-per-target "
+                             "shape");
+        if (pack) LQ_TRY(launch_pack_neighbors(ph, st, rec, 0, s, compensated, rows ? map : nullptr));
         if (shape >= 0 && shape < kPairShapeCount && kPairShapes[shape][2] == 1 && !order)
             return set_error(LQ_ERR_ARG, "interaction: launch shape %d needs the tile order", shape);
         if (shape < 0 || shape >= kPairShapeCount || kPairShapes[shape][2] != 1) order = nullptr;
 #define LQ_PAIR_LAUNCH(T, B)                                                                                \
     (compensated ? k_interaction_rec<true, T, B><<<blocks_for(ph->npm, T), T, 0, s>>>(                      \
-                       pd, ph->np, ph->npb, st, r, c, nl.list, nl.count, nl.stride, fr, nb, order)            \
+                       pd, ph->np, ph->npb, st, r, c, nl.list, nl.count, nl.stride, fr, nb, order, rows)       \
                  : k_interaction_rec<false, T, B><<<blocks_for(ph->npm, T), T, 0, s>>>(                     \
-                       pd, ph->np, ph->npb, st, r, c, nl.list, nl.count, nl.stride, fr, nb, order))
+                       pd, ph->np, ph->npb, st, r, c, nl.list, nl.count, nl.stride, fr, nb, order, rows))
         switch (shape) {
             case 7: LQ_PAIR_LAUNCH(768, 1); break;
             case 8: LQ_PAIR_LAUNCH(384, 2); break;
@@ -1287,11 +1308,10 @@ struct DropInWorkspace {
     lqb::NeighborList nl;           /* material targets' lists */
     float* rec = nullptr;           /* packed neighbour data, 13 floats per particle */
     /* lists carried across calls (caller grids that track identities) */
-    int* list_id = nullptr;         /* LQ_NBR_CAP x stride: the lists at their build, as particle identities */
-    int* count_b = nullptr;         /* stride: their counts, by target slot at the build */
     float4* xbuild = nullptr;       /* np: positions at the build, by identity */
     int* build_of = nullptr;        /* np: identity -> slot at the build */
-    int* cur_of = nullptr;          /* np: identity -> current slot */
+    int* rows = nullptr;            /* npm: target -> its list's row (the target's slot at the build) */
+    int* pidx = nullptr;            /* np: slot -> its particle's slot at the build (its record's index) */
     int* moved = nullptr;           /* device flag: a particle moved half the skin since the build */
     int* tally = nullptr;           /* device counts of [0] builds and [1] reuses of carried lists */
     const int* key = nullptr;       /* the grid (its cell_beg) the carried lists belong to */
@@ -1357,11 +1377,10 @@ int size_workspace(DropInWorkspace& w, const Parameters* ph)
     A((void**)&n.nl.list, sizeof(int) * (size_t)LQ_NBR_CAP * n.nl.stride);
     A((void**)&n.nl.count, sizeof(int) * (size_t)n.nl.stride);
     A((void**)&n.to.order, sizeof(int) * (size_t)npm);
-    A((void**)&n.list_id, sizeof(int) * (size_t)LQ_NBR_CAP * n.nl.stride);
-    A((void**)&n.count_b, sizeof(int) * (size_t)n.nl.stride);
     A((void**)&n.xbuild, sizeof(float4) * (size_t)np);
     A((void**)&n.build_of, sizeof(int) * (size_t)np);
-    A((void**)&n.cur_of, sizeof(int) * (size_t)np);
+    A((void**)&n.rows, sizeof(int) * (size_t)npm);
+    A((void**)&n.pidx, sizeof(int) * (size_t)np);
     A((void**)&n.moved, sizeof(int));
     A((void**)&n.tally, 2 * sizeof(int));
     if (st == LQ_OK) {
@@ -1393,9 +1412,14 @@ int dropin_workspace(const Parameters* ph, DropInWorkspace** out)
 }
 
 /* Carrying lists across calls.  The caller's grid gives each slot's
- * particle identity (lqb::identity_*); at a build the lists are stored as
- * identities with the build positions, and a later call whose particles
- * have all moved less than half the skin maps them to the current slots. */
+ * particle identity (lqb::identity_*).  A build keeps its lists as they are
+ * (rows and entries are slots at the build) and records, by identity, each
+ * particle's build slot and position.  Every call packs each particle's
+ * neighbour record at its build slot, so the pair kernel gathers through
+ * the stored entries as they are, each target reading the row of its build
+ * slot; a later call whose particles have all moved less than half the
+ * skin only maps slots to build slots (k_record_index).  The records stay
+ * in the cell order of the build. */
 __global__ void __launch_bounds__(256) k_moved_half_skin(int np, const float4* __restrict__ pos,
                                                          const int* __restrict__ ident,
                                                          const float4* __restrict__ xbuild, float half_skin2,
@@ -1420,52 +1444,28 @@ __global__ void k_tally_decision(const int* __restrict__ moved, int* __restrict_
     tally[*moved ? 0 : 1] += 1;
 }
 
-/* Reuse (skipped when *moved): identity -> current slot. */
-__global__ void __launch_bounds__(256) k_identity_slots(int np, const int* __restrict__ ident, int* __restrict__ slot,
-                                                        const int* __restrict__ moved)
+/* Each slot's record index, the build slot of its particle (-1 when its
+ * particle has none), and each material target's list row (its record
+ * index less npb; -1: no carried list, the pair kernel walks its
+ * stencil). */
+__global__ void __launch_bounds__(256) k_record_index(int np, int npb, const int* __restrict__ ident,
+                                                      const int* __restrict__ build_of, int* __restrict__ pidx,
+                                                      int* __restrict__ rows)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= np || *moved) return;
+    if (c >= np) return;
     const int id = __ldg(ident + c);
-    if ((unsigned)id < (unsigned)np) slot[id] = c;
+    const int b = (unsigned)id < (unsigned)np ? __ldg(build_of + id) : -1;
+    const int o = (unsigned)b < (unsigned)np ? b : -1;
+    pidx[c] = o;
+    if (c >= npb) rows[c - npb] = o >= npb ? o - npb : -1;
 }
 
-/* The carried lists in the current slots (skipped when *moved): target t
- * takes the list its particle had at the build, each entry mapped from
- * identity to slot. */
-__global__ void __launch_bounds__(256) k_remap_lists(int np, int npb, int npm, const int* __restrict__ ident,
-                                                     const int* __restrict__ build_of,
-                                                     const int* __restrict__ list_id,
-                                                     const int* __restrict__ count_b,
-                                                     const int* __restrict__ cur_of, int* __restrict__ list,
-                                                     int* __restrict__ count, int stride,
-                                                     const int* __restrict__ moved)
-{
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= npm || *moved) return;
-    const int id = __ldg(ident + npb + t);
-    const int b = (unsigned)id < (unsigned)np ? __ldg(build_of + id) - npb : -1;
-    if (b < 0 || b >= npm) {
-        count[t] = LQ_NBR_CAP + 1;    /* no carried list: the pair kernel walks the stencil */
-        return;
-    }
-    const int n = __ldg(count_b + b);
-    count[t] = n;
-    const int m = n < LQ_NBR_CAP ? n : LQ_NBR_CAP;
-    for (int k = 0; k < m; ++k) {
-        const int jid = __ldg(list_id + (size_t)k * stride + b);
-        list[(size_t)k * stride + t] = (unsigned)jid < (unsigned)np ? __ldg(cur_of + jid) : npb + t;
-    }
-}
-
-/* A fresh build stored for carrying (skipped unless *moved): lists as
- * identities, build positions and slots by identity. */
-__global__ void __launch_bounds__(256) k_store_build(int np, int npb, int npm, const int* __restrict__ ident,
-                                                     const float4* __restrict__ pos, const int* __restrict__ list,
-                                                     const int* __restrict__ count, int stride,
-                                                     int* __restrict__ list_id, int* __restrict__ count_b,
-                                                     float4* __restrict__ xbuild, int* __restrict__ build_of,
-                                                     const int* __restrict__ moved)
+/* A build recorded for carrying (skipped unless *moved): each particle's
+ * build slot and position, by identity. */
+__global__ void __launch_bounds__(256) k_store_build(int np, const int* __restrict__ ident,
+                                                     const float4* __restrict__ pos, float4* __restrict__ xbuild,
+                                                     int* __restrict__ build_of, const int* __restrict__ moved)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= np || !*moved) return;
@@ -1473,15 +1473,6 @@ __global__ void __launch_bounds__(256) k_store_build(int np, int npb, int npm, c
     if ((unsigned)id < (unsigned)np) {
         xbuild[id] = __ldg(pos + c);
         build_of[id] = c;
-    }
-    const int t = c - npb;
-    if (t < 0 || t >= npm) return;
-    const int n = __ldg(count + t);
-    count_b[t] = n;
-    const int m = n < LQ_NBR_CAP ? n : LQ_NBR_CAP;
-    for (int k = 0; k < m; ++k) {
-        const int j = __ldg(list + (size_t)k * stride + t);
-        list_id[(size_t)k * stride + t] = (unsigned)j < (unsigned)np ? __ldg(ident + j) : -1;
     }
 }
 
@@ -1584,30 +1575,32 @@ extern "C" int lq_particle_interaction(const void* par_host, const void* par_dev
         }
         k_tally_decision<<<1, 1, 0, s>>>(w->moved, w->tally);
         LQ_TRY_CUDA(cudaGetLastError(), "k_tally_decision");
-        /* reuse */
-        k_identity_slots<<<nb256, 256, 0, s>>>(np, gi.ident, w->cur_of, w->moved);
-        LQ_TRY_CUDA(cudaGetLastError(), "k_identity_slots");
-        k_remap_lists<<<(npm + 255) / 256, 256, 0, s>>>(np, npb, npm, gi.ident, w->build_of, w->list_id, w->count_b,
-                                                        w->cur_of, w->nl.list, w->nl.count, w->nl.stride, w->moved);
-        LQ_TRY_CUDA(cudaGetLastError(), "k_remap_lists");
-        /* build */
+        /* a build (skipped unless moved): fresh lists in the current
+         * slots, kept with each particle's build slot and position */
         LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, npb, npm, 0, 2.0f * ph->h + skin, st.pos, c, w->nl, nullptr,
                                                s, nullptr, lqb::Frames(), nullptr, 0.0f, w->moved));
-        k_store_build<<<nb256, 256, 0, s>>>(np, npb, npm, gi.ident, st.pos, w->nl.list, w->nl.count, w->nl.stride,
-                                            w->list_id, w->count_b, w->xbuild, w->build_of, w->moved);
+        k_store_build<<<nb256, 256, 0, s>>>(np, gi.ident, st.pos, w->xbuild, w->build_of, w->moved);
         LQ_TRY_CUDA(cudaGetLastError(), "k_store_build");
         w->built = true;
         w->key = cell_beg;
         w->gen = gi.gen;
         w->np_built = np;
         w->npb_built = npb;
-    } else {
-        /* the pair body's own cut-off test: q < 2 with the candidate slack
-         * of the cell walk */
-        const float cut = 2.0f * ph->h * sqrtf(1.0001f);
-        LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, npb, npm, 0, cut, st.pos, c, w->nl, nullptr, s));
-        w->built = false;
+        /* either way the pair kernel reads the lists of the last build,
+         * each target at the row of its build slot, with the records
+         * packed at the build slots: a reuse maps only slots */
+        k_record_index<<<nb256, 256, 0, s>>>(np, npb, gi.ident, w->build_of, w->pidx, w->rows);
+        LQ_TRY_CUDA(cudaGetLastError(), "k_record_index");
+        LQ_TRY(lqb::launch_tile_order(ph, w->start, kDropInShape, w->to, s));
+        return lqb::launch_interaction_list(ph, pd, st, r, c, w->nl, s, lqb::Frames(), false, w->rec, kDropInShape,
+                                            true, w->to.order, w->rows, w->pidx);
     }
+    /* a grid of the caller's own: lists built in its slots at every call,
+     * with the pair body's own cut-off test (q < 2 with the candidate
+     * slack of the cell walk) */
+    const float cut = 2.0f * ph->h * sqrtf(1.0001f);
+    LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, npb, npm, 0, cut, st.pos, c, w->nl, nullptr, s));
+    w->built = false;
     LQ_TRY(lqb::launch_tile_order(ph, w->start, kDropInShape, w->to, s));
     return lqb::launch_interaction_list(ph, pd, st, r, c, w->nl, s, lqb::Frames(), false, w->rec, kDropInShape, true,
                                         w->to.order);
