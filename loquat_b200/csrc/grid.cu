@@ -106,6 +106,11 @@ __global__ void __launch_bounds__(kBlock) k_cell_order(int ncell, const int* __r
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncell) return;
     const int s = __ldg(start + c), e = __ldg(start + c + 1);
+    /* most cells arrive in order (their particles came from one warp):
+     * a read-only pass finds them and leaves them untouched */
+    bool sorted = true;
+    for (int a = s + 1; a < e && sorted; ++a) sorted = part_idx[a - 1] < part_idx[a];
+    if (sorted) return;
     for (int a = s + 1; a < e; ++a) {
         const int v = part_idx[a];
         int b = a - 1;
