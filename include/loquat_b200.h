@@ -58,7 +58,11 @@ int lq_grid_create(int np, int ncell, void** grid);
 int lq_grid_resize(void* grid, int np, int ncell);
 int lq_grid_destroy(void* grid);
 /* Hash, stable sort and cell bounds (LoquatGrid::NeighborSearch,
- * reference src/loquat_grid.h:60).  pospres/idep: device float4[np]. */
+ * reference src/loquat_grid.h:60).  pospres/idep: device float4[np].  The
+ * stable order within a cell is restored by one thread per cell, in one
+ * read-only pass when the cell arrives in order (as it does when particles
+ * move little between searches) and by insertion otherwise: particles
+ * outside the lattice share one cell, so keep their number small. */
 int lq_grid_neighbor_search(void* grid, const void* par_host, const void* par_device,
                             const float* pospres, const float* idep, void* stream);
 /* Device pointers owned by the grid.  cell_start has ncell + 1 entries:
