@@ -853,8 +853,8 @@ __global__ void __launch_bounds__(kBlock) k_shepard(const Parameters* __restrict
 
 /* ------------------------------------------------- list-driven Adami */
 /* The Adami extrapolation of k_adami, summed over a boundary particle's
- * list of material neighbours (built with a skin; pairs at q >= 2 are
- * skipped exactly as the cell walk skips them), reading the neighbours from
+ * list of material neighbours (built with a skin; pairs at q >= 2 add
+ * exact zeros, as the cell walk skips them), reading the neighbours from
  * the packed arrays (sigma_j V_j W = s_j rho_j m W with s = sigma / rho^2),
  * and writing the
  * boundary particle's new stress both into the state and, scaled, into the
@@ -874,24 +874,43 @@ __global__ void __launch_bounds__(kBlock) k_adami_packed(const Parameters* __res
     const float4 xi = __ldg(st.pos + i);
     tensor2d S = make_tensor2d(0.0f);
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int k = 0; k < n; ++k) {
-        const int j = __ldg(list + (size_t)k * stride + i);
-        if (!lq_in_range(j, np_all)) continue;
-        const float4 xr = __ldg(nb.xr + j);
-        const float3 d = make_float3(xi.x - xr.x, xi.y - xr.y, xi.z - xr.z);
-        const float q = norm3df(d.x, d.y, d.z) * ih;
-        if (q < 2.0f) {
-            const float ker = Cw * (2.0f - q) * (2.0f - q) * (2.0f - q) * (2.0f - q) * (q + 0.5f);
-            const float vol = m / xr.w;
-            const float cs = m * xr.w * ker;
-            const float4 sa = __ldg(nb.sa + j);
-            const float2 sb = __ldg(reinterpret_cast<const float2*>(nb.sb + j));
-            S.xx += sa.x * cs;
-            S.yy += sa.y * cs;
-            S.zz += sa.z * cs;
-            S.xy += sa.w * cs;
-            S.xz += sb.x * cs;
-            S.yz += sb.y * cs;
+    /* groups of four entries, the next group's entries fetched ahead and
+     * every gather of a group issued together; a pair at q >= 2 (and the
+     * filler of the last group, the target's own record) gets the kernel
+     * factor 0 and adds exact zeros, so the loop has no branch */
+    const int* p = list + i;
+    int nxt[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) nxt[u] = u < n ? __ldg(p + (size_t)u * stride) : i;
+    for (int k = 0; k < n; k += 4) {
+        int j[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            j[u] = lq_in_range(nxt[u], np_all) ? nxt[u] : i;
+            nxt[u] = k + 4 + u < n ? __ldg(p + (size_t)(k + 4 + u) * stride) : i;
+        }
+        float4 xr[4], sa[4];
+        float2 sb[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            xr[u] = __ldg(nb.xr + j[u]);
+            sa[u] = __ldg(nb.sa + j[u]);
+            sb[u] = __ldg(reinterpret_cast<const float2*>(nb.sb + j[u]));
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const float3 d = make_float3(xi.x - xr[u].x, xi.y - xr[u].y, xi.z - xr[u].z);
+            const float q = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z) * ih;
+            const float t = k + u < n ? fmaxf(2.0f - q, 0.0f) : 0.0f;
+            const float ker = Cw * t * t * t * t * (q + 0.5f);
+            const float vol = m / xr[u].w;
+            const float cs = m * xr[u].w * ker;
+            S.xx += sa[u].x * cs;
+            S.yy += sa[u].y * cs;
+            S.zz += sa[u].z * cs;
+            S.xy += sa[u].w * cs;
+            S.xz += sb[u].x * cs;
+            S.yz += sb[u].y * cs;
             acc.x += d.x * ker * vol;
             acc.y += d.y * ker * vol;
             acc.z += d.z * ker * vol;
