@@ -625,7 +625,7 @@ def ensemble_measurement(args, torch, world, rank, local, dist, sample_clocks=Fa
         return e0.elapsed_time(e1)
 
     def batched(mixed):
-        sim = lq.Simulation(par, *comb.arrays(), mixed=mixed)
+        sim = lq.Simulation(par, *comb.arrays(), mixed=mixed, graph=not args.eager)
         sim.set_materials(comb.meta["materials"])
         sim.set_frames(comb.meta["frames"])
         sim.step(args.warmup)

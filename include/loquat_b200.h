@@ -266,8 +266,9 @@ int lq_sim_set_pair_shape(void* sim, int shape);
 int lq_sim_pair_shape(void* sim, int* shape);
 /* Autotuner: times `steps` steps for each pair kernel shape at the current
  * lists, then for one-level skins of 0.02, 0.05, 0.1 and 0.2 h with the
- * fastest shape, then two-level lists over the fastest skin with wide
- * margins of 0.1 and 0.2 h, and keeps the fastest setting (the wide one is
+ * fastest shape, then two-level lists with wide margins of 0.1 and 0.2 h
+ * over the fastest skin and over skins of 0.02 and 0.01 h narrower than
+ * it, and keeps the fastest setting (the wide one is
  * read with lq_sim_wide_skin).  Every trial starts from a device copy of
  * the state taken at the call and its window opens with the search and
  * list build that start every run, so settings whose lists last long pay

@@ -86,6 +86,9 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : LQ_INT_MIN_BL
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
+    /* boundary slots change only by Adami, which writes both state buffers
+     * of the native driver; without a snapshot there is nothing to do */
+    if (i < npb && !do_snap) return;
     const float4 x0 = in.pos[i];
     const float4 v0 = in.vel[i];
     const float4 id = in.idep[i];
@@ -99,10 +102,8 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : LQ_INT_MIN_BL
         store_t2(snap.stn, i, e0);
     }
     if (i < npb) {
-        /* a boundary slot of another output buffer takes only the stress
-         * (the Adami extrapolation): its position, velocity, idep and
-         * strain never change, and the native driver copies them whole at
-         * each list rebuild */
+        /* a boundary slot of another output buffer takes the stress (the
+         * Adami extrapolation); the rest never changes */
         if (out.pos != in.pos) store_t2(out.str, i, s0);
         return;
     }
@@ -248,12 +249,7 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : LQ_INT_MIN_BL
 {
     const int i = first + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
-    if (i < npb) {
-        /* boundary slots: the latest Adami stress; the rest of a boundary
-         * slot is the same in both buffers (see k_predict) */
-        store_t2(out.str, i, load_t2_rw(cur.str, i));
-        return;
-    }
+    if (i < npb) return;    /* boundary slots: Adami writes both buffers */
     const int k = ini_idx ? __ldg(ini_idx + i) : i;
     const float dt = __ldg(&P->dt);
     const float4 a = __ldg(rt.accad + i);
@@ -436,14 +432,17 @@ int launch_correct_into(const Parameters* ph, const Parameters* pd, const State&
     if (xwide && !(wide > skin)) return set_error(LQ_ERR_ARG, "corrector: the wide cut-off must exceed the skin");
     const VerletCheck vc{xbuild, rebuild, 0.5f * skin, ph->dt, xwide, 0.5f * (wide - skin)};
     const bool vwm = ph->constitutive_model == 3;
-    const int nb = blocks_for(ph->np, kBlock);
+    if (ph->npm <= 0) return LQ_OK;
+    /* material slots only: boundary slots are written by Adami into both
+     * buffers */
+    const int nb = blocks_for(ph->npm, kBlock), f = ph->npb;
     const NbrArrays pk = rec ? nbr_arrays(rec, ph->np) : NbrArrays{nullptr, nullptr, nullptr, nullptr};
     if (cur.xlo && ini.xlo && out.xlo) {
-        if (vwm) k_correct<true, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw, pk);
-        else k_correct<true, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw, pk);
+        if (vwm) k_correct<true, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, f, mt, vw, pk);
+        else k_correct<true, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, f, mt, vw, pk);
     } else {
-        if (vwm) k_correct<false, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw, pk);
-        else k_correct<false, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, 0, mt, vw, pk);
+        if (vwm) k_correct<false, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, f, mt, vw, pk);
+        else k_correct<false, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, cur, ini, nullptr, out, r, health, vc, f, mt, vw, pk);
     }
     LQ_TRY_CUDA(cudaGetLastError(), "k_correct");
     return LQ_OK;

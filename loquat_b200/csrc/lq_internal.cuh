@@ -169,10 +169,11 @@ int launch_interaction_list(const Parameters* par_host, const Parameters* par_de
 int launch_pack_neighbors(const Parameters* par_host, const State& st, float* rec, int first, cudaStream_t s,
                           bool packed_velocity, const int* map = nullptr);
 /* Adami over the boundary lists reading the packed arrays (material slots
- * packed), writing the boundary stress into the state and the packed
- * arrays. */
+ * packed), writing the boundary stress into the state, into str2 when set
+ * and into the packed arrays. */
 int launch_adami_packed(const Parameters* par_host, const Parameters* par_dev, const State& st,
-                        const NeighborList& nl, float* rec, cudaStream_t s, bool packed_velocity);
+                        const NeighborList& nl, float* rec, cudaStream_t s, bool packed_velocity,
+                        tensor2d* str2 = nullptr);
 /* Launch shapes of the packed pair kernel: {threads per block, resident
  * blocks per SM, tile order}, or {128, -G, 0} for the warp-cooperative form
  * with G lanes per target.  Shapes with the tile order take their targets
@@ -205,10 +206,10 @@ int launch_adami(const Parameters* par_host, const Parameters* par_dev, const St
  * from `st` to `out`, producing a complete new state. */
 int launch_shepard(const Parameters* par_host, const Parameters* par_dev, const State& st, tensor2d* out_str,
                    const State* full, const Cells& c, cudaStream_t s);
-/* Predictor: out <- in advanced by dt/2 on material slots; when out != in
- * only the boundary slots' stress is copied (the rest of a boundary slot
- * never changes and must already be in `out`); `snap` (may be all-null)
- * receives a copy of `in`.  With `rec` (the packed neighbour arrays) each
+/* Predictor: out <- in advanced by dt/2 on material slots; boundary slots
+ * are left alone (the native driver's Adami writes both of its state
+ * buffers), except that with a snapshot `snap` (may be all-null), which
+ * receives a copy of `in`, a separate `out` takes their stress.  With `rec` (the packed neighbour arrays) each
  * material slot's entry is written from its new values, in the record of
  * the form (the mixed form's packed velocity when the state has low
  * words); the same holds for the corrector below. */
@@ -220,9 +221,9 @@ int launch_predict(const Parameters* par_host, const Parameters* par_dev, const 
 int launch_correct(const Parameters* par_host, const Parameters* par_dev, const State& cur, const State& ini,
                    const int* ini_idx, const Rates& r, int* health, cudaStream_t s);
 
-/* Corrector from snapshot `ini` and current `cur` into `out` (boundary
- * slots take cur's stress; the rest of a boundary slot must already be the
- * same in both); material particles raise bit 1 of *rebuild when neighbour
+/* Corrector from snapshot `ini` and current `cur` into `out`, material
+ * slots only (boundary slots must already be the same in all three);
+ * material particles raise bit 1 of *rebuild when neighbour
  * lists built at xbuild with this skin may not hold through the next step,
  * and (with xwide) bit 2 when a particle has moved (wide - skin) / 2 or
  * more from xwide, where lists with cut-off 2h + wide were built: lists

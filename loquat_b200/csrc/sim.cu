@@ -17,6 +17,8 @@
  *      positions, build material and boundary lists]
  *     Adami(S), interaction(S), predictor S -> S2          (S is the snapshot)
  *     Adami(S2), interaction(S2), corrector (S2, S) -> S   (raises the flag)
+ *     (Adami writes the boundary stress into S and S2; the integrators
+ *     update the material slots only)
  *   every N steps: Shepard(S) -> T.str, copy back            (reference :400-409)
  *
  * The rebuild decision stays on the device: a one-thread kernel turns the
@@ -174,8 +176,9 @@ void release(LqSim* S)
 /* ------------------------------------------------------------- kernels */
 
 /* The gathered state back into S and the build positions; boundary slots
- * also into S2 (they never change between rebuilds, so the integrators
- * pass only their stress between the two buffers). */
+ * also into S2.  From then on only Adami changes a boundary slot, writing
+ * its stress into both buffers, so the integrators leave boundary slots
+ * alone. */
 __global__ void k_copy_state(int n, int npb, State in, State out, State out2, float4* __restrict__ xbuild)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -429,7 +432,10 @@ int enqueue_density_filter(LqSim* S, cudaStream_t s)
  * so the pair kernel needs no pack. */
 int enqueue_adami_pack(LqSim* S, const State& st, cudaStream_t s)
 {
-    return lqb::launch_adami_packed(&S->ph, S->pd, st, S->nlb, S->rec, s, S->flags & LQ_SIM_MIXED);
+    /* both state buffers take the boundary stress, so their boundary slots
+     * stay equal and the integrators never touch them */
+    tensor2d* other = st.str == S->S.str ? S->S2.str : S->S.str;
+    return lqb::launch_adami_packed(&S->ph, S->pd, st, S->nlb, S->rec, s, S->flags & LQ_SIM_MIXED, other);
 }
 
 
@@ -1136,11 +1142,19 @@ extern "C" int lq_sim_autotune(void* sim, int steps, int* shape_out, float* skin
         factor = f;
         if (st == LQ_OK && (f * h != snap.skin || snap.wide > snap.skin)) st = trial(shape, f * h, 0.0f);
     }
+    /* two-level lists over the best one-level skin and over narrow skins,
+     * whose lists hold fewer pairs beyond 2h while cheap renewals keep them
+     * current */
     const float margins[] = {0.1f, 0.2f};
-    const float skin1 = best_skin;
-    factor = best_factor;
-    for (float m : margins)
-        if (st == LQ_OK) st = trial(shape, skin1, skin1 + m * h);
+    const float best1 = best_factor;
+    const float two_skins[] = {best1, 0.02f, 0.01f};
+    for (int a = 0; a < 3 && st == LQ_OK; ++a) {
+        const float f = two_skins[a];
+        if (a > 0 && f >= best1) continue;       /* narrower than the best one-level skin only */
+        factor = f;
+        for (float m : margins)
+            if (st == LQ_OK) st = trial(shape, f * h, (f + m) * h);
+    }
     /* back to the state before tuning, with the chosen configuration */
     int st2 = snap.restore(S);
     S->pair_shape = st == LQ_OK ? best_shape : snap.shape;

@@ -857,13 +857,16 @@ __global__ void __launch_bounds__(kBlock) k_shepard(const Parameters* __restrict
  * exact zeros, as the cell walk skips them), reading the neighbours from
  * the packed arrays (sigma_j V_j W = s_j rho_j m W with s = sigma / rho^2),
  * and writing the
- * boundary particle's new stress both into the state and, scaled, into the
- * packed arrays, which then need no pack of the boundary slots before the
- * pair kernel.  Targets without neighbours keep both as they were. */
+ * boundary particle's new stress into the state (and into str2, the native
+ * driver's other state buffer, whose boundary slots so always equal the
+ * state's) and, scaled, into the packed arrays, which then need no pack of
+ * the boundary slots before the pair kernel.  Targets without neighbours
+ * keep all of them as they were. */
 template <bool kPk>
 __global__ void __launch_bounds__(kBlock) k_adami_packed(const Parameters* __restrict__ P, int npb, State st,
                                                          const int* __restrict__ list,
-                                                         const int* __restrict__ count, int stride, NbrArrays nb)
+                                                         const int* __restrict__ count, int stride, NbrArrays nb,
+                                                         tensor2d* __restrict__ str2)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= npb) return;
@@ -927,6 +930,7 @@ __global__ void __launch_bounds__(kBlock) k_adami_packed(const Parameters* __res
         out.xz = S.xz / acc.w;
         out.yz = S.yz / acc.w;
         store_t2(st.str, i, out);
+        if (str2) store_t2(str2, i, out);
         store_packed<kPk>(nb, i, __ldg(st.vel + i), out);
     }
 }
@@ -1178,16 +1182,16 @@ int launch_pack_neighbors(const Parameters* ph, const State& st, float* rec, int
 }
 
 int launch_adami_packed(const Parameters* ph, const Parameters* pd, const State& st, const NeighborList& nl,
-                        float* rec, cudaStream_t s, bool packed_velocity)
+                        float* rec, cudaStream_t s, bool packed_velocity, tensor2d* str2)
 {
     if (ph->npb <= 0) return LQ_OK;
     const NbrArrays nb = nbr_arrays(rec, ph->np);
     if (packed_velocity)
         k_adami_packed<true><<<blocks_for(ph->npb, kBlock), kBlock, 0, s>>>(pd, ph->npb, st, nl.list, nl.count,
-                                                                           nl.stride, nb);
+                                                                           nl.stride, nb, str2);
     else
         k_adami_packed<false><<<blocks_for(ph->npb, kBlock), kBlock, 0, s>>>(pd, ph->npb, st, nl.list, nl.count,
-                                                                            nl.stride, nb);
+                                                                            nl.stride, nb, str2);
     LQ_TRY_CUDA(cudaGetLastError(), "k_adami_packed");
     return LQ_OK;
 }
