@@ -862,8 +862,14 @@ __global__ void __launch_bounds__(kBlock) k_shepard(const Parameters* __restrict
  * state's) and, scaled, into the packed arrays, which then need no pack of
  * the boundary slots before the pair kernel.  Targets without neighbours
  * keep all of them as they were. */
+/* threads per block of the list-driven Adami: 128 measured against 64 and
+ * 256 (256: -4 % on the 256-scenario ensemble, +10 % on the cylinder; 64:
+ * +1 % and equal) */
+#ifndef LQ_ADAMI_BLOCK
+#define LQ_ADAMI_BLOCK 128
+#endif
 template <bool kPk>
-__global__ void __launch_bounds__(kBlock) k_adami_packed(const Parameters* __restrict__ P, int npb, State st,
+__global__ void __launch_bounds__(LQ_ADAMI_BLOCK) k_adami_packed(const Parameters* __restrict__ P, int npb, State st,
                                                          const int* __restrict__ list,
                                                          const int* __restrict__ count, int stride, NbrArrays nb,
                                                          tensor2d* __restrict__ str2)
@@ -1187,10 +1193,10 @@ int launch_adami_packed(const Parameters* ph, const Parameters* pd, const State&
     if (ph->npb <= 0) return LQ_OK;
     const NbrArrays nb = nbr_arrays(rec, ph->np);
     if (packed_velocity)
-        k_adami_packed<true><<<blocks_for(ph->npb, kBlock), kBlock, 0, s>>>(pd, ph->npb, st, nl.list, nl.count,
+        k_adami_packed<true><<<blocks_for(ph->npb, LQ_ADAMI_BLOCK), LQ_ADAMI_BLOCK, 0, s>>>(pd, ph->npb, st, nl.list, nl.count,
                                                                            nl.stride, nb, str2);
     else
-        k_adami_packed<false><<<blocks_for(ph->npb, kBlock), kBlock, 0, s>>>(pd, ph->npb, st, nl.list, nl.count,
+        k_adami_packed<false><<<blocks_for(ph->npb, LQ_ADAMI_BLOCK), LQ_ADAMI_BLOCK, 0, s>>>(pd, ph->npb, st, nl.list, nl.count,
                                                                             nl.stride, nb, str2);
     LQ_TRY_CUDA(cudaGetLastError(), "k_adami_packed");
     return LQ_OK;
