@@ -41,23 +41,26 @@ constexpr int kBlock = 128;
 inline int blocks_for(long long n, int b) { return (int)((n + b - 1) / b); }
 
 /* FP64 position (pressure p in the float word's w) and velocity into the
- * float high words x, v and the low words of `out` at slot i. */
+ * float high words x, v and, with `lo`, the low words of `out` at slot i. */
 __device__ __forceinline__ void split_words(const State& out, int i, const double4& xd, const double4& vd, float p,
-                                            float4& x, float4& v)
+                                            float4& x, float4& v, bool lo = true)
 {
     float4 xl, vl;
     split4(make_double4(xd.x, xd.y, xd.z, 0.0), x, xl);
     split4(vd, v, vl);
     x.w = p;
-    out.xlo[i] = xl;
-    out.vlo[i] = vl;
+    if (lo) {
+        out.xlo[i] = xl;
+        out.vlo[i] = vl;
+    }
 }
 
 /* The same, storing the high words too. */
-__device__ __forceinline__ void store_split(const State& out, int i, const double4& xd, const double4& vd, float p)
+__device__ __forceinline__ void store_split(const State& out, int i, const double4& xd, const double4& vd, float p,
+                                            bool lo = true)
 {
     float4 x, v;
-    split_words(out, i, xd, vd, p, x, v);
+    split_words(out, i, xd, vd, p, x, v, lo);
     out.pos[i] = x;
     out.vel[i] = v;
 }
@@ -78,11 +81,17 @@ __device__ __forceinline__ void pack_slot(const NbrArrays& nb, int i, const floa
 
 /* Half step of the material slots (reference src/predictor_corrector.cu:169-218):
  * v += dt/2 a; rho += dt/2 drho; x += dt/2 v_new; eps += dt/2 deps;
- * stress and plastic strain from the model at dt/2. */
+ * stress and plastic strain from the model at dt/2.  With `stage` the
+ * output is a stage buffer that only the neighbour kernels and the
+ * corrector read: the position and velocity high words (with the
+ * pressure), the object word and the stress; the corrector restarts the
+ * strain, the plastic strain and the FP64 kinematics from its snapshot, so
+ * the strain (neither read nor written), the low words and, for the
+ * hypoplastic model, the plastic strain are left out. */
 template <bool kMixed, bool kVW>
 __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : LQ_INT_MIN_BLOCKS) k_predict(const Parameters* __restrict__ P, int np, int npb, State in,
                                                     State out, State snap, bool do_snap, Rates rt, MaterialTable mt,
-                                                    MaterialTable vw, NbrArrays nb)
+                                                    MaterialTable vw, NbrArrays nb, bool stage)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
@@ -93,7 +102,7 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : LQ_INT_MIN_BL
     const float4 v0 = in.vel[i];
     const float4 id = in.idep[i];
     const tensor2d s0 = load_t2_rw(in.str, i);
-    const tensor2d e0 = load_t2_rw(in.stn, i);
+    const tensor2d e0 = stage ? make_tensor2d(0.0f) : load_t2_rw(in.stn, i);
     if (do_snap) {
         snap.pos[i] = x0;
         snap.vel[i] = v0;
@@ -127,9 +136,9 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : LQ_INT_MIN_BL
         if (kVW) {
             /* the kinematics are stored before the sub-stepping, whose FP64
              * registers then need not share the SM with them */
-            store_split(out, i, xd, vd, x0.w);
-            store_t2(out.stn, i, narrow6(e));
-            const float epf = (float)sqrt(2.0 / 3.0 * contract6(e, e));
+            store_split(out, i, xd, vd, x0.w, !stage);
+            if (!stage) store_t2(out.stn, i, narrow6(e));
+            const float epf = stage ? id.y : (float)sqrt(2.0 / 3.0 * contract6(e, e));
             vw_update_d(vw_const(vw, id.x), hdt, de, w, sd, ev);
             out.idep[i] = make_float4(id.x, epf, (float)ev, id.w);
             const tensor2d sn = narrow6(sd);
@@ -141,16 +150,16 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : LQ_INT_MIN_BL
             dp_update_d(M, hdt, w, dd, p, ep, sd);
         } else {
             hypo_update_d(M, hdt, dd, w, sd);
-            ep = sqrt(2.0 / 3.0 * contract6(e, e));
+            if (!stage) ep = sqrt(2.0 / 3.0 * contract6(e, e));
         }
         float4 xh, vh;
-        split_words(out, i, xd, vd, (float)p, xh, vh);
+        split_words(out, i, xd, vd, (float)p, xh, vh, !stage);
         out.pos[i] = xh;
         out.vel[i] = vh;
         out.idep[i] = make_float4(id.x, (float)ep, (float)ev, id.w);
         const tensor2d sn = narrow6(sd);
         store_t2(out.str, i, sn);
-        store_t2(out.stn, i, narrow6(e));
+        if (!stage) store_t2(out.stn, i, narrow6(e));
         pack_slot<kMixed>(nb, i, xh, vh, sn);
         return;
     }
@@ -173,8 +182,8 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : LQ_INT_MIN_BL
          * kinematics are stored first */
         out.pos[i] = x;
         out.vel[i] = v;
-        store_t2(out.stn, i, e);
-        const float epf = sqrtf(2.0f / 3.0f * J2(e));
+        if (!stage) store_t2(out.stn, i, e);
+        const float epf = stage ? id.y : sqrtf(2.0f / 3.0f * J2(e));
         T6d sd = widen6(s0);
         double evd = ev;
         vw_update_d(vw_const(vw, id.x), 0.5 * (double)dt, de, w, sd, evd);
@@ -188,14 +197,14 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : LQ_INT_MIN_BL
         dp_update(M, 0.5f * dt, w, de, p, ep, s);
     } else {
         hypo_update(M, 0.5f * dt, de, w, s);
-        ep = sqrtf(2.0f / 3.0f * J2(e));
+        if (!stage) ep = sqrtf(2.0f / 3.0f * J2(e));
     }
     x.w = p;
     out.pos[i] = x;
     out.vel[i] = v;
     out.idep[i] = make_float4(id.x, ep, ev, id.w);
     store_t2(out.str, i, s);
-    store_t2(out.stn, i, e);
+    if (!stage) store_t2(out.stn, i, e);
     pack_slot<kMixed>(nb, i, x, v, s);
 }
 
@@ -383,12 +392,15 @@ __global__ void __launch_bounds__(kBlock, kVW ? LQ_VW_MIN_BLOCKS : LQ_INT_MIN_BL
 }  // namespace
 
 int launch_predict(const Parameters* ph, const Parameters* pd, const State& in, const State& out, const State* snap,
-                   const Rates& r, cudaStream_t s, const MaterialTable& mt, const MaterialTable& vw, float* rec)
+                   const Rates& r, cudaStream_t s, const MaterialTable& mt, const MaterialTable& vw, float* rec,
+                   bool stage)
 {
     if (ph->np <= 0) return LQ_OK;
     if (ph->constitutive_model == 3 && (!vw.p || vw.n <= 0))
         return set_error(LQ_ERR_ARG, "predictor: constitutive model 3 needs a von Wolffersdorff table");
     const bool do_snap = snap && snap->pos;
+    if (stage && (do_snap || out.pos == in.pos))
+        return set_error(LQ_ERR_ARG, "predictor: a stage buffer needs its own output and no snapshot");
     State sn = do_snap ? *snap : State{nullptr, nullptr, nullptr, nullptr, nullptr};
     /* model 3 gets its own instantiation: its FP64 sub-stepping needs far
      * more registers than the other models' kernels */
@@ -396,11 +408,15 @@ int launch_predict(const Parameters* ph, const Parameters* pd, const State& in, 
     const int nb = blocks_for(ph->np, kBlock);
     const NbrArrays pk = rec ? nbr_arrays(rec, ph->np) : NbrArrays{nullptr, nullptr, nullptr, nullptr};
     if (in.xlo && out.xlo) {
-        if (vwm) k_predict<true, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw, pk);
-        else k_predict<true, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw, pk);
+        if (vwm) k_predict<true, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw, pk,
+                                                              stage);
+        else k_predict<true, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw, pk,
+                                                              stage);
     } else {
-        if (vwm) k_predict<false, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw, pk);
-        else k_predict<false, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw, pk);
+        if (vwm) k_predict<false, true><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw, pk,
+                                                              stage);
+        else k_predict<false, false><<<nb, kBlock, 0, s>>>(pd, ph->np, ph->npb, in, out, sn, do_snap, r, mt, vw, pk,
+                                                              stage);
     }
     LQ_TRY_CUDA(cudaGetLastError(), "k_predict");
     return LQ_OK;

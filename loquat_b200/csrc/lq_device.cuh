@@ -589,6 +589,17 @@ __device__ __forceinline__ void store_packed(const NbrArrays& nb, int i, const f
     }
 }
 
+/* The stress words of a slot's packed entry (sigma / rho^2, as
+ * store_packed writes them); its position, density and velocity words are
+ * left as they are. */
+__device__ __forceinline__ void store_packed_stress(const NbrArrays& nb, int i, float rho, const tensor2d& str)
+{
+    const float rinv = __fdividef(1.0f, rho);
+    const float r2 = rinv * rinv;
+    nb.sa[i] = make_float4(str.xx * r2, str.yy * r2, str.zz * r2, str.xy * r2);
+    *reinterpret_cast<float2*>(nb.sb + i) = make_float2(str.xz * r2, str.yz * r2);
+}
+
 /* The packed arrays inside `rec` (np x 13 floats, 16-byte aligned). */
 inline NbrArrays nbr_arrays(float* rec, int np)
 {

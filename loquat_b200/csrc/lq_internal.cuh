@@ -170,10 +170,19 @@ int launch_pack_neighbors(const Parameters* par_host, const State& st, float* re
                           bool packed_velocity, const int* map = nullptr);
 /* Adami over the boundary lists reading the packed arrays (material slots
  * packed), writing the boundary stress into the state, into str2 when set
- * and into the packed arrays. */
+ * and into the stress words of the packed arrays (the boundary slots'
+ * other words, from the last full pack, stay).  With act / nact (device;
+ * from launch_boundary_targets; act holds at least npb ints) only the
+ * slots act[0 .. *nact) are visited. */
 int launch_adami_packed(const Parameters* par_host, const Parameters* par_dev, const State& st,
-                        const NeighborList& nl, float* rec, cudaStream_t s, bool packed_velocity,
-                        tensor2d* str2 = nullptr);
+                        const NeighborList& nl, float* rec, cudaStream_t s, tensor2d* str2 = nullptr,
+                        const int* act = nullptr, const int* nact = nullptr);
+/* The boundary slots t < npb with count[t] > 0 or count2[t] > 0 (count2
+ * may be null), ascending, into act[0 .. *nact) on the device; temp holds
+ * boundary_targets_temp_bytes(npb) bytes of scratch. */
+size_t boundary_targets_temp_bytes(int npb);
+int launch_boundary_targets(int npb, const int* count, const int* count2, int* act, int* nact, void* temp,
+                            size_t temp_bytes, cudaStream_t s);
 /* Launch shapes of the packed pair kernel: {threads per block, resident
  * blocks per SM, tile order}, or {128, -G, 0} for the warp-cooperative form
  * with G lanes per target.  Shapes with the tile order take their targets
@@ -212,10 +221,13 @@ int launch_shepard(const Parameters* par_host, const Parameters* par_dev, const 
  * receives a copy of `in`, a separate `out` takes their stress.  With `rec` (the packed neighbour arrays) each
  * material slot's entry is written from its new values, in the record of
  * the form (the mixed form's packed velocity when the state has low
- * words); the same holds for the corrector below. */
+ * words); the same holds for the corrector below.  With `stage` (no
+ * snapshot, out distinct from in) out is a stage buffer read only by the
+ * neighbour kernels and launch_correct_into: its strain, its low words and
+ * its hypoplastic plastic strain are not written. */
 int launch_predict(const Parameters* par_host, const Parameters* par_dev, const State& in, const State& out,
                    const State* snap, const Rates& r, cudaStream_t s, const MaterialTable& mt = MaterialTable(),
-                   const MaterialTable& vw = MaterialTable(), float* rec = nullptr);
+                   const MaterialTable& vw = MaterialTable(), float* rec = nullptr, bool stage = false);
 /* Corrector in place on `cur`; ini values read at ini_idx[i] (identity when
  * ini_idx is null).  Non-finite results are counted in health. */
 int launch_correct(const Parameters* par_host, const Parameters* par_dev, const State& cur, const State& ini,
@@ -234,15 +246,20 @@ int launch_correct_into(const Parameters* par_host, const Parameters* par_dev, c
                         const MaterialTable& vw = MaterialTable(), const float4* xwide = nullptr,
                         float wide = 0.0f, float* rec = nullptr);
 
-/* List-driven Shepard filter (material targets and neighbours); a target
- * whose list overflowed walks its 27 cells in `c` instead. */
+/* List-driven Shepard filter (material targets and neighbours) reading
+ * the neighbours from the packed records `rec` (required; the material
+ * slots' records must hold the state st), targets in the tile order
+ * `order` when set; a target whose list overflowed walks its 27 cells in
+ * `c` over the state instead. */
 int launch_shepard_list(const Parameters* par_host, const Parameters* par_dev, const State& st, tensor2d* out_str,
-                        const NeighborList& nl, const Cells& c, cudaStream_t s, const Frames& fr = Frames());
+                        const NeighborList& nl, const Cells& c, cudaStream_t s, const Frames& fr, float* rec,
+                        const int* order = nullptr);
 /* Density Shepard filter of material slots into rho_out[npb, np) over the
- * material lists (overflowed lists walk their 27 cells in `c`). */
+ * material lists, from the packed records likewise (overflowed lists walk
+ * their 27 cells in `c`). */
 int launch_density_filter_list(const Parameters* par_host, const Parameters* par_dev, const State& st,
                                float* rho_out, const NeighborList& nl, const Cells& c, cudaStream_t s,
-                               const Frames& fr = Frames());
+                               const Frames& fr, float* rec, const int* order = nullptr);
 /* Neighbour lists of targets [first, first + n) from grid layers
  * layer_lo..1 with cut-off radius `cut` (2h plus skin); list overflows are
  * counted in health[HEALTH_NBR_OVERFLOW].  With `shell`, pairs at distance

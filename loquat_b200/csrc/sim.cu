@@ -18,7 +18,9 @@
  *     Adami(S), interaction(S), predictor S -> S2          (S is the snapshot)
  *     Adami(S2), interaction(S2), corrector (S2, S) -> S   (raises the flag)
  *     (Adami writes the boundary stress into S and S2; the integrators
- *     update the material slots only)
+ *     update the material slots only; S2 is a stage buffer: the predictor
+ *     writes what the neighbour kernels and the corrector read from it,
+ *     not its strain or low words)
  *   every N steps: Shepard(S) -> T.str, copy back            (reference :400-409)
  *
  * The rebuild decision stays on the device: a one-thread kernel turns the
@@ -71,6 +73,10 @@ struct LqSim {
     lqb::Rates R{};
     lqb::GridBuffers g;
     lqb::NeighborList nlm, nlb;        /* material targets, boundary targets */
+    int* bact = nullptr;               /* boundary slots whose lists can hold entries, ascending */
+    int* nbact = nullptr;              /* device count of bact */
+    void* bsel_tmp = nullptr;          /* scratch of their selection */
+    size_t bsel_bytes = 0;
     int* health = nullptr;
     int* rebuild = nullptr;            /* device flag: rebuild before the next step */
     int* rebuilds = nullptr;           /* device counter of rebuilds */
@@ -331,7 +337,10 @@ __global__ void k_dt_update(Parameters* P, unsigned* m2, double* time)
 /* Material and boundary lists from the sorted state in S: the lists the
  * stages read, or with two-level lists the wide ones, whose pairs closer
  * than 2h + 2 skin - wide (less a rounding margin of h / 1000) open the
- * stages' lists and the rest form the shell lists that renewals filter. */
+ * stages' lists and the rest form the shell lists that renewals filter.
+ * Then the boundary targets Adami visits: the slots with an entry, or with
+ * two-level lists an inner or shell entry (a renewal fills a row only from
+ * these, so the set holds until the next build). */
 int build_lists(LqSim* S, cudaStream_t s)
 {
     const Parameters* ph = &S->ph;
@@ -341,8 +350,10 @@ int build_lists(LqSim* S, cudaStream_t s)
         const float cut = 2.0f * ph->h + S->skin;
         LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, S->npb, S->npm, 0, cut, S->S.pos, cells, S->nlm, S->health,
                                                s, S->S.idep, S->fr));
-        return lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, S->nlb, S->health, s,
-                                               S->S.idep, S->fr);
+        LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, S->nlb, S->health, s,
+                                               S->S.idep, S->fr));
+        return lqb::launch_boundary_targets(S->npb, S->nlb.count, nullptr, S->bact, S->nbact, S->bsel_tmp,
+                                            S->bsel_bytes, s);
     }
     const float cut = 2.0f * ph->h + S->wide;
     const float inner = 2.0f * ph->h + 2.0f * S->skin - S->wide - 1.0e-3f * ph->h;
@@ -350,8 +361,10 @@ int build_lists(LqSim* S, cudaStream_t s)
     const lqb::NeighborList ib{S->nlb.list, S->inner_b, S->nlb.stride};
     LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, S->npb, S->npm, 0, cut, S->S.pos, cells, im, S->health, s,
                                            S->S.idep, S->fr, &S->wlm, inner));
-    return lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, ib, S->health, s, S->S.idep,
-                                           S->fr, &S->wlb, inner);
+    LQ_TRY(lqb::launch_neighbor_list_range(ph, pd, 0, S->npb, 1, cut, S->S.pos, cells, ib, S->health, s, S->S.idep,
+                                           S->fr, &S->wlb, inner));
+    return lqb::launch_boundary_targets(S->npb, S->inner_b, S->wlb.count, S->bact, S->nbact, S->bsel_tmp,
+                                        S->bsel_bytes, s);
 }
 
 /* Two-level lists: the lists the stages read renewed from the wide ones at
@@ -416,7 +429,8 @@ int enqueue_dynamic_dt(LqSim* S, cudaStream_t s)
 int enqueue_density_filter(LqSim* S, cudaStream_t s)
 {
     const lqb::Cells cells{S->g.start, nullptr, nullptr};
-    LQ_TRY(lqb::launch_density_filter_list(&S->ph, S->pd, S->S, S->rho_f, S->nlm, cells, s, S->fr));
+    LQ_TRY(lqb::launch_density_filter_list(&S->ph, S->pd, S->S, S->rho_f, S->nlm, cells, s, S->fr, S->rec,
+                                           tile_order(S)));
     if (S->npm > 0) {
         k_set_density<<<blocks(S->npm), 256, 0, s>>>(S->npb, S->npm, S->rho_f, S->S.vel, S->S.vlo);
         LQ_TRY_CUDA(cudaGetLastError(), "k_set_density");
@@ -435,7 +449,7 @@ int enqueue_adami_pack(LqSim* S, const State& st, cudaStream_t s)
     /* both state buffers take the boundary stress, so their boundary slots
      * stay equal and the integrators never touch them */
     tensor2d* other = st.str == S->S.str ? S->S2.str : S->S.str;
-    return lqb::launch_adami_packed(&S->ph, S->pd, st, S->nlb, S->rec, s, S->flags & LQ_SIM_MIXED, other);
+    return lqb::launch_adami_packed(&S->ph, S->pd, st, S->nlb, S->rec, s, other, S->bact, S->nbact);
 }
 
 
@@ -447,7 +461,7 @@ int enqueue_stages(LqSim* S, cudaStream_t s)
     /* predictor stage (reference src/loquat.cu:343-368) */
     LQ_TRY(enqueue_adami_pack(S, S->S, s));
     LQ_TRY(enqueue_interaction(S, S->S, s));
-    LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt, S->vw, S->rec));
+    LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt, S->vw, S->rec, true));
     /* corrector stage (reference src/loquat.cu:371-396) */
     LQ_TRY(enqueue_adami_pack(S, S->S2, s));
     LQ_TRY(enqueue_interaction(S, S->S2, s));
@@ -460,7 +474,7 @@ int enqueue_stages(LqSim* S, cudaStream_t s)
 int enqueue_shepard(LqSim* S, cudaStream_t s)
 {
     const lqb::Cells cells{S->g.start, nullptr, nullptr};
-    LQ_TRY(lqb::launch_shepard_list(&S->ph, S->pd, S->S, S->T.str, S->nlm, cells, s, S->fr));
+    LQ_TRY(lqb::launch_shepard_list(&S->ph, S->pd, S->S, S->T.str, S->nlm, cells, s, S->fr, S->rec, tile_order(S)));
     if (S->npm > 0) {
         k_copy_t2<<<blocks(S->npm), 256, 0, s>>>(S->npb, S->npm, S->T.str, S->S.str);
         LQ_TRY_CUDA(cudaGetLastError(), "k_copy_t2");
@@ -685,6 +699,10 @@ int create(LqSim* S, const Parameters* par, const float* pos, const float* vel, 
     S->nlb.stride = ((S->npb > 0 ? S->npb : 1) + 31) / 32 * 32;
     LQ_TRY(dev_alloc(S, (void**)&S->nlb.list, sizeof(int) * (size_t)LQ_NBR_CAP * S->nlb.stride));
     LQ_TRY(dev_alloc(S, (void**)&S->nlb.count, sizeof(int) * (size_t)S->nlb.stride));
+    LQ_TRY(dev_alloc(S, (void**)&S->bact, sizeof(int) * (size_t)S->nlb.stride));
+    LQ_TRY(dev_alloc(S, (void**)&S->nbact, sizeof(int)));
+    S->bsel_bytes = lqb::boundary_targets_temp_bytes(S->npb);
+    LQ_TRY(dev_alloc(S, &S->bsel_tmp, S->bsel_bytes));
     const int ncell = S->ph.ncell;
     lqb::GridBuffers& g = S->g;
     LQ_TRY(lqb::scan_scratch_bytes(ncell, &g.scan_bytes));
@@ -703,6 +721,7 @@ int create(LqSim* S, const Parameters* par, const float* pos, const float* vel, 
     LQ_TRY_CUDA(cudaMemsetAsync(S->R.acestn, 0, n * sizeof(tensor2d), S->stream), "zero rates");
     LQ_TRY_CUDA(cudaMemsetAsync(S->health, 0, sizeof(int) * lqb::HEALTH_WORDS, S->stream), "zero health");
     LQ_TRY_CUDA(cudaMemsetAsync(S->rebuilds, 0, sizeof(int), S->stream), "zero counter");
+    LQ_TRY_CUDA(cudaMemsetAsync(S->nbact, 0, sizeof(int), S->stream), "zero boundary targets");
     LQ_TRY_CUDA(cudaMemsetAsync(S->renewals, 0, sizeof(int), S->stream), "zero counter");
     LQ_TRY_CUDA(cudaMemcpyAsync(S->pd, &S->ph, sizeof(Parameters), cudaMemcpyHostToDevice, S->stream),
                 "upload Parameters");
@@ -1529,7 +1548,7 @@ int profiled_step(LqSim* S, PhaseTimer& T)
         LQ_TRY(T.close(s));
         LQ_TRY(T.mark(s, PH_INTEGRATE));
         if (stage == 0)
-            LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt, S->vw, S->rec));
+            LQ_TRY(lqb::launch_predict(ph, pd, S->S, S->S2, nullptr, S->R, s, S->mt, S->vw, S->rec, true));
         else {
             LQ_TRY(lqb::launch_correct_into(ph, pd, S->S2, S->S, S->S, S->R, S->health, S->xbuild, S->rebuild,
                                             S->skin, s, S->mt, S->vw, two_level(S) ? S->xwide : nullptr,

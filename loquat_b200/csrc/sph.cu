@@ -20,6 +20,8 @@
 #include <vector>
 
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+#include <cub/iterator/counting_input_iterator.cuh>
 
 #include "lq_internal.cuh"
 #include "lq_tile.h"
@@ -861,21 +863,33 @@ __global__ void __launch_bounds__(kBlock) k_shepard(const Parameters* __restrict
  * driver's other state buffer, whose boundary slots so always equal the
  * state's) and, scaled, into the packed arrays, which then need no pack of
  * the boundary slots before the pair kernel.  Targets without neighbours
- * keep all of them as they were. */
+ * keep all of them as they were.  With `act`, thread t takes the boundary
+ * slot act[t] for t < *nact (the slots whose lists can hold entries, in
+ * slot order, from launch_boundary_targets): most boundary particles of a
+ * wall have no material neighbour, and without the compaction a warp ran
+ * as long as its longest list over lanes that had none.  Each target's
+ * sums run in list order in one thread either way, so the results do not
+ * depend on the compaction. */
 /* threads per block of the list-driven Adami: 128 measured against 64 and
  * 256 (256: -4 % on the 256-scenario ensemble, +10 % on the cylinder; 64:
  * +1 % and equal) */
 #ifndef LQ_ADAMI_BLOCK
 #define LQ_ADAMI_BLOCK 128
 #endif
-template <bool kPk>
 __global__ void __launch_bounds__(LQ_ADAMI_BLOCK) k_adami_packed(const Parameters* __restrict__ P, int npb, State st,
                                                          const int* __restrict__ list,
                                                          const int* __restrict__ count, int stride, NbrArrays nb,
-                                                         tensor2d* __restrict__ str2)
+                                                         tensor2d* __restrict__ str2, const int* __restrict__ act,
+                                                         const int* __restrict__ nact)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= npb) return;
+    if (act) {
+        /* act holds npb slots, so both loads are issued together */
+        const int na = __ldg(nact), a = __ldg(act + i);
+        if (i >= na) return;
+        i = a;
+    }
     const int n = min(__ldg(count + i), LQ_NBR_CAP);
     if (n == 0) return;
     const int np_all = __ldg(&P->np);
@@ -909,10 +923,11 @@ __global__ void __launch_bounds__(LQ_ADAMI_BLOCK) k_adami_packed(const Parameter
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const float3 d = make_float3(xi.x - xr[u].x, xi.y - xr[u].y, xi.z - xr[u].z);
-            const float q = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z) * ih;
+            /* the approximate square root and quotient of the pair kernel */
+            const float q = sqrt_approx(d.x * d.x + d.y * d.y + d.z * d.z) * ih;
             const float t = k + u < n ? fmaxf(2.0f - q, 0.0f) : 0.0f;
             const float ker = Cw * t * t * t * t * (q + 0.5f);
-            const float vol = m / xr[u].w;
+            const float kv = ker * __fdividef(m, xr[u].w);
             const float cs = m * xr[u].w * ker;
             S.xx += sa[u].x * cs;
             S.yy += sa[u].y * cs;
@@ -920,112 +935,186 @@ __global__ void __launch_bounds__(LQ_ADAMI_BLOCK) k_adami_packed(const Parameter
             S.xy += sa[u].w * cs;
             S.xz += sb[u].x * cs;
             S.yz += sb[u].y * cs;
-            acc.x += d.x * ker * vol;
-            acc.y += d.y * ker * vol;
-            acc.z += d.z * ker * vol;
-            acc.w += ker * vol;
+            acc.x += d.x * kv;
+            acc.y += d.y * kv;
+            acc.z += d.z * kv;
+            acc.w += kv;
         }
     }
     if (acc.w > 0.0f) {
         const float rho0 = __ldg(&P->rho0);
+        const float inv = 1.0f / acc.w;
         tensor2d out;
-        out.xx = (S.xx - rho0 * __ldg(&P->acc_x) * acc.x) / acc.w;
-        out.yy = (S.yy - rho0 * __ldg(&P->acc_y) * acc.y) / acc.w;
-        out.zz = (S.zz - rho0 * __ldg(&P->acc_z) * acc.z) / acc.w;
-        out.xy = S.xy / acc.w;
-        out.xz = S.xz / acc.w;
-        out.yz = S.yz / acc.w;
+        out.xx = (S.xx - rho0 * __ldg(&P->acc_x) * acc.x) * inv;
+        out.yy = (S.yy - rho0 * __ldg(&P->acc_y) * acc.y) * inv;
+        out.zz = (S.zz - rho0 * __ldg(&P->acc_z) * acc.z) * inv;
+        out.xy = S.xy * inv;
+        out.xz = S.xz * inv;
+        out.yz = S.yz * inv;
         store_t2(st.str, i, out);
         if (str2) store_t2(str2, i, out);
-        store_packed<kPk>(nb, i, __ldg(st.vel + i), out);
+        /* a boundary particle's velocity and density stay as the list
+         * build packed them; only its stress words change */
+        store_packed_stress(nb, i, __ldg(&st.vel[i].w), out);
     }
 }
 
-/* ----------------------------------------------- list-driven Shepard */
-/* The Shepard filter of k_shepard over a material particle's list (its
- * boundary neighbours are skipped: the filter uses the material layer
- * only).  Writes the filtered stress of material slots to out_str. */
+/* ------------------------------------------ list-driven Shepard filters */
+/* The walk of the native driver's two filters over a material target's
+ * list, from the packed records (written from the state the filter reads:
+ * the corrector packs every material slot, and each filter packs again
+ * after changing the state): branch-free groups of four, the next group's
+ * entries fetched ahead.  add(W, xr, sa, sb) gets the kernel value of each
+ * entry, 0 for boundary neighbours (the filters use the material layer
+ * only), for pairs at q >= 2 and for the filler of the last group (the
+ * target's own slot); the list holds the target itself at q = 0.  kStress
+ * also gathers the sigma / rho^2 words. */
+template <bool kStress, class F>
+__device__ __forceinline__ void filter_groups(const NbrArrays& nb, const int* p, int n, int stride, int i, int npb,
+                                              int np, const float4& xi, float ih, float Cw, F&& add)
+{
+    int nxt[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) nxt[u] = u < n ? ld_list(p + (size_t)u * stride) : i;
+    for (int k = 0; k < n; k += 4) {
+        int j[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            j[u] = lq_in_range(nxt[u], np) ? nxt[u] : i;
+            nxt[u] = k + 4 + u < n ? ld_list(p + (size_t)(k + 4 + u) * stride) : i;
+        }
+        float4 xr[4], sa[4];
+        float2 sb[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            xr[u] = __ldg(nb.xr + j[u]);
+            if (kStress) {
+                sa[u] = __ldg(nb.sa + j[u]);
+                sb[u] = __ldg(reinterpret_cast<const float2*>(nb.sb + j[u]));
+            } else {
+                sa[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                sb[u] = make_float2(0.f, 0.f);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const float dx = xi.x - xr[u].x, dy = xi.y - xr[u].y, dz = xi.z - xr[u].z;
+            const float q = sqrt_approx(dx * dx + dy * dy + dz * dz) * ih;
+            const float t = (k + u < n && j[u] >= npb) ? fmaxf(2.0f - q, 0.0f) : 0.0f;
+            add(Cw * t * t * t * t * (q + 0.5f), xr[u], sa[u], sb[u]);
+        }
+    }
+}
+
+/* The Shepard stress filter of k_shepard over a material particle's list:
+ * sum sigma_j V_j W / sum V_j W over the material neighbours, with
+ * sigma_j V_j W = s_j rho_j m W from the packed records (s = sigma /
+ * rho^2, as Adami reads them).  Targets in the pair kernel's tile order
+ * when `order` is set.  A particle whose list overflowed walks its 27
+ * cells over the state instead.  Writes the filtered stress of material
+ * slots to out_str. */
 __global__ void __launch_bounds__(kBlock) k_shepard_list(const Parameters* __restrict__ P, int np, int npb, State st,
                                                          tensor2d* __restrict__ out_str,
                                                          const int* __restrict__ list,
                                                          const int* __restrict__ count, int stride, Cells cells,
-                                                         Frames fr)
+                                                         Frames fr, NbrArrays nb, const int* __restrict__ order)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= np - npb) return;
+    const int t = order ? __ldg(order + g) : g;
+    if (!lq_in_range(t, np - npb)) return;
     const int i = npb + t;
-    if (i >= np) return;
     const int n = __ldg(count + t);
     const float ih = __ldg(&P->i_h), m = __ldg(&P->m), Cw = __ldg(&P->kernel_normalization_par);
     const float4 xi = __ldg(st.pos + i);
     tensor2d S = make_tensor2d(0.0f);
     float w = 0.0f;
-    auto add = [&](int j) {
-        if (j < npb || !lq_in_range(j, np)) return;
-        const float4 xj = __ldg(st.pos + j);
-        const float3 d = make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
-        const float q = norm3df(d.x, d.y, d.z) * ih;
-        if (q < 2.0f) {
-            const float ker = Cw * (2.0f - q) * (2.0f - q) * (2.0f - q) * (2.0f - q) * (q + 0.5f);
-            const float vol = m / __ldg(&st.vel[j].w);
-            const tensor2d sj = load_t2(st.str, j);
-            S.xx += sj.xx * ker * vol;
-            S.yy += sj.yy * ker * vol;
-            S.zz += sj.zz * ker * vol;
-            S.xy += sj.xy * ker * vol;
-            S.xz += sj.xz * ker * vol;
-            S.yz += sj.yz * ker * vol;
-            w += ker * vol;
-        }
-    };
     if (n <= LQ_NBR_CAP) {
-        for (int k = 0; k < n; ++k) add(__ldg(list + (size_t)k * stride + t));
+        filter_groups<true>(nb, list + t, n, stride, i, npb, np, xi, ih, Cw,
+                            [&](float ker, const float4& xr, const float4& sa, const float2& sb) {
+                                const float cs = m * xr.w * ker;
+                                S.xx += sa.x * cs;
+                                S.yy += sa.y * cs;
+                                S.zz += sa.z * cs;
+                                S.xy += sa.w * cs;
+                                S.xz += sb.x * cs;
+                                S.yz += sb.y * cs;
+                                w += ker * __fdividef(m, xr.w);
+                            });
     } else {
         /* overflowed list (counted in the health word): the particle itself
          * and its 27-cell walk in the grid the lists were built from, as
          * the pair kernel does */
+        auto add = [&](int j) {
+            if (j < npb || !lq_in_range(j, np)) return;
+            const float4 xj = __ldg(st.pos + j);
+            const float3 d = make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
+            const float q = norm3df(d.x, d.y, d.z) * ih;
+            if (q < 2.0f) {
+                const float ker = Cw * (2.0f - q) * (2.0f - q) * (2.0f - q) * (2.0f - q) * (q + 0.5f);
+                const float vol = m / __ldg(&st.vel[j].w);
+                const tensor2d sj = load_t2(st.str, j);
+                S.xx += sj.xx * ker * vol;
+                S.yy += sj.yy * ker * vol;
+                S.zz += sj.zz * ker * vol;
+                S.xy += sj.xy * ker * vol;
+                S.xz += sj.xz * ker * vol;
+                S.yz += sj.yz * ker * vol;
+                w += ker * vol;
+            }
+        };
         add(i);
         walk_stencil(P, load_pair_const(P), st, cells, i, xi, add, fr);
     }
-    S.xx /= w;
-    S.yy /= w;
-    S.zz /= w;
-    S.xy /= w;
-    S.xz /= w;
-    S.yz /= w;
+    const float inv = 1.0f / w;
+    S.xx *= inv;
+    S.yy *= inv;
+    S.zz *= inv;
+    S.xy *= inv;
+    S.xz *= inv;
+    S.yz *= inv;
     store_t2(out_str, i, S);
 }
 
 /* Density Shepard filter over a material particle's list (boundary
  * neighbours skipped; the list holds the particle itself, at q = 0):
- * rho~_i = sum m W / sum (m / rho_j) W. */
+ * rho~_i = sum m W / sum (m / rho_j) W, from the packed records' positions
+ * and densities; targets in tile order when `order` is set. */
 __global__ void __launch_bounds__(kBlock) k_density_filter_list(const Parameters* __restrict__ P, int np, int npb,
                                                                 State st, float* __restrict__ rho_out,
                                                                 const int* __restrict__ list,
                                                                 const int* __restrict__ count, int stride,
-                                                                Cells cells, Frames fr)
+                                                                Cells cells, Frames fr, NbrArrays nb,
+                                                                const int* __restrict__ order)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= np - npb) return;
+    const int t = order ? __ldg(order + g) : g;
+    if (!lq_in_range(t, np - npb)) return;
     const int i = npb + t;
-    if (i >= np) return;
     const int n = __ldg(count + t);
     const float ih = __ldg(&P->i_h), m = __ldg(&P->m), Cw = __ldg(&P->kernel_normalization_par);
     const float4 xi = __ldg(st.pos + i);
     float num = 0.0f, den = 0.0f;
-    auto add = [&](int j) {
-        if (j < npb || !lq_in_range(j, np)) return;
-        const float4 xj = __ldg(st.pos + j);
-        const float3 d = make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
-        const float q = norm3df(d.x, d.y, d.z) * ih;
-        if (q < 2.0f) {
-            const float ker = Cw * (2.0f - q) * (2.0f - q) * (2.0f - q) * (2.0f - q) * (q + 0.5f);
-            num += m * ker;
-            den += ker * (m / __ldg(&st.vel[j].w));
-        }
-    };
     if (n <= LQ_NBR_CAP) {
-        for (int k = 0; k < n; ++k) add(__ldg(list + (size_t)k * stride + t));
+        filter_groups<false>(nb, list + t, n, stride, i, npb, np, xi, ih, Cw,
+                             [&](float ker, const float4& xr, const float4&, const float2&) {
+                                 num += m * ker;
+                                 den += ker * __fdividef(m, xr.w);
+                             });
     } else {
         /* overflowed list: the particle itself and its 27-cell walk */
+        auto add = [&](int j) {
+            if (j < npb || !lq_in_range(j, np)) return;
+            const float4 xj = __ldg(st.pos + j);
+            const float3 d = make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
+            const float q = norm3df(d.x, d.y, d.z) * ih;
+            if (q < 2.0f) {
+                const float ker = Cw * (2.0f - q) * (2.0f - q) * (2.0f - q) * (2.0f - q) * (q + 0.5f);
+                num += m * ker;
+                den += ker * (m / __ldg(&st.vel[j].w));
+            }
+        };
         add(i);
         walk_stencil(P, load_pair_const(P), st, cells, i, xi, add, fr);
     }
@@ -1035,11 +1124,14 @@ __global__ void __launch_bounds__(kBlock) k_density_filter_list(const Parameters
 }  // namespace
 
 int launch_density_filter_list(const Parameters* ph, const Parameters* pd, const State& st, float* rho_out,
-                               const NeighborList& nl, const Cells& c, cudaStream_t s, const Frames& fr)
+                               const NeighborList& nl, const Cells& c, cudaStream_t s, const Frames& fr,
+                               float* rec, const int* order)
 {
     if (ph->npm <= 0) return LQ_OK;
+    if (!rec) return set_error(LQ_ERR_ARG, "density filter: the packed neighbour records are required");
     k_density_filter_list<<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, rho_out, nl.list,
-                                                                        nl.count, nl.stride, c, fr);
+                                                                        nl.count, nl.stride, c, fr,
+                                                                        nbr_arrays(rec, ph->np), order);
     LQ_TRY_CUDA(cudaGetLastError(), "k_density_filter_list");
     return LQ_OK;
 }
@@ -1188,26 +1280,58 @@ int launch_pack_neighbors(const Parameters* ph, const State& st, float* rec, int
 }
 
 int launch_adami_packed(const Parameters* ph, const Parameters* pd, const State& st, const NeighborList& nl,
-                        float* rec, cudaStream_t s, bool packed_velocity, tensor2d* str2)
+                        float* rec, cudaStream_t s, tensor2d* str2, const int* act, const int* nact)
 {
     if (ph->npb <= 0) return LQ_OK;
+    if (!act != !nact) return set_error(LQ_ERR_ARG, "Adami: compacted targets need both act and nact");
+    if (nl.stride < ph->npb) return set_error(LQ_ERR_ARG, "Adami: list stride %d < %d targets", nl.stride, ph->npb);
     const NbrArrays nb = nbr_arrays(rec, ph->np);
-    if (packed_velocity)
-        k_adami_packed<true><<<blocks_for(ph->npb, LQ_ADAMI_BLOCK), LQ_ADAMI_BLOCK, 0, s>>>(pd, ph->npb, st, nl.list, nl.count,
-                                                                           nl.stride, nb, str2);
-    else
-        k_adami_packed<false><<<blocks_for(ph->npb, LQ_ADAMI_BLOCK), LQ_ADAMI_BLOCK, 0, s>>>(pd, ph->npb, st, nl.list, nl.count,
-                                                                            nl.stride, nb, str2);
+    k_adami_packed<<<blocks_for(ph->npb, LQ_ADAMI_BLOCK), LQ_ADAMI_BLOCK, 0, s>>>(pd, ph->npb, st, nl.list, nl.count,
+                                                                                nl.stride, nb, str2, act, nact);
     LQ_TRY_CUDA(cudaGetLastError(), "k_adami_packed");
     return LQ_OK;
 }
 
+namespace {
+/* A boundary list row that holds, or can gain by renewal, an entry. */
+struct HasEntries {
+    const int* a;
+    const int* b;
+    __device__ bool operator()(int i) const { return __ldg(a + i) > 0 || (b && __ldg(b + i) > 0); }
+};
+}   // namespace
+
+size_t boundary_targets_temp_bytes(int npb)
+{
+    size_t bytes = 0;
+    if (npb <= 0) return 0;
+    cub::DeviceSelect::If(nullptr, bytes, cub::CountingInputIterator<int>(0), (int*)nullptr, (int*)nullptr, npb,
+                          HasEntries{nullptr, nullptr});
+    return bytes;
+}
+
+int launch_boundary_targets(int npb, const int* count, const int* count2, int* act, int* nact, void* temp,
+                            size_t temp_bytes, cudaStream_t s)
+{
+    if (npb <= 0) return LQ_OK;
+    if (!count || !act || !nact || !temp)
+        return set_error(LQ_ERR_ARG, "boundary targets: missing count, output or scratch");
+    size_t bytes = temp_bytes;
+    LQ_TRY_CUDA(cub::DeviceSelect::If(temp, bytes, cub::CountingInputIterator<int>(0), act, nact, npb,
+                                      HasEntries{count, count2}, s),
+                "boundary targets (select)");
+    return LQ_OK;
+}
+
 int launch_shepard_list(const Parameters* ph, const Parameters* pd, const State& st, tensor2d* out_str,
-                        const NeighborList& nl, const Cells& c, cudaStream_t s, const Frames& fr)
+                        const NeighborList& nl, const Cells& c, cudaStream_t s, const Frames& fr, float* rec,
+                        const int* order)
 {
     if (ph->npm <= 0) return LQ_OK;
+    if (!rec) return set_error(LQ_ERR_ARG, "Shepard filter: the packed neighbour records are required");
     k_shepard_list<<<blocks_for(ph->npm, kBlock), kBlock, 0, s>>>(pd, ph->np, ph->npb, st, out_str, nl.list,
-                                                                 nl.count, nl.stride, c, fr);
+                                                                 nl.count, nl.stride, c, fr, nbr_arrays(rec, ph->np),
+                                                                 order);
     LQ_TRY_CUDA(cudaGetLastError(), "k_shepard_list");
     return LQ_OK;
 }
