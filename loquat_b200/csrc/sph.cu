@@ -21,7 +21,7 @@
 
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_select.cuh>
-#include <cub/iterator/counting_input_iterator.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include "lq_internal.cuh"
 #include "lq_tile.h"
@@ -1305,7 +1305,7 @@ size_t boundary_targets_temp_bytes(int npb)
 {
     size_t bytes = 0;
     if (npb <= 0) return 0;
-    cub::DeviceSelect::If(nullptr, bytes, cub::CountingInputIterator<int>(0), (int*)nullptr, (int*)nullptr, npb,
+    cub::DeviceSelect::If(nullptr, bytes, thrust::counting_iterator<int>(0), (int*)nullptr, (int*)nullptr, npb,
                           HasEntries{nullptr, nullptr});
     return bytes;
 }
@@ -1317,7 +1317,7 @@ int launch_boundary_targets(int npb, const int* count, const int* count2, int* a
     if (!count || !act || !nact || !temp)
         return set_error(LQ_ERR_ARG, "boundary targets: missing count, output or scratch");
     size_t bytes = temp_bytes;
-    LQ_TRY_CUDA(cub::DeviceSelect::If(temp, bytes, cub::CountingInputIterator<int>(0), act, nact, npb,
+    LQ_TRY_CUDA(cub::DeviceSelect::If(temp, bytes, thrust::counting_iterator<int>(0), act, nact, npb,
                                       HasEntries{count, count2}, s),
                 "boundary targets (select)");
     return LQ_OK;
