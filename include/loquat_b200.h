@@ -268,7 +268,9 @@ int lq_sim_pair_shape(void* sim, int* shape);
  * lists, then for one-level skins of 0.02, 0.05, 0.1 and 0.2 h with the
  * fastest shape, then two-level lists with wide margins of 0.1 and 0.2 h
  * over the fastest skin and over skins of 0.02 and 0.01 h narrower than
- * it, and keeps the fastest setting (the wide one is
+ * it; then it times again, over 2 x `steps` at the fastest lists, every
+ * shape that came within 5 % of the fastest in the first round (at most
+ * four), and keeps the fastest of that round (the wide setting is
  * read with lq_sim_wide_skin).  Every trial starts from a device copy of
  * the state taken at the call and its window opens with the search and
  * list build that start every run, so settings whose lists last long pay

@@ -36,6 +36,7 @@
  * (wide - skin) / 2 from its position at the wide build.  A second IF node
  * holds the renewal.
  */
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -1130,7 +1131,8 @@ extern "C" int lq_sim_autotune(void* sim, int steps, int* shape_out, float* skin
     float best_skin = S->skin, best_wide = S->wide, best_ms = 3.4e38f;
     float best_factor = S->skin / h;   /* skin / h as the caller would pass it to lq_sim_set_skin */
     float factor = best_factor;
-    auto trial = [&](int shape, float skin, float wide) -> int {
+    float shape_ms[lqb::kPairShapeCount];
+    auto trial = [&](int shape, float skin, float wide, int nsteps = 0) -> int {
         LQ_TRY(snap.restore(S));
         S->pair_shape = shape;
         S->skin = skin;
@@ -1138,7 +1140,8 @@ extern "C" int lq_sim_autotune(void* sim, int steps, int* shape_out, float* skin
         S->wide = wide;
         LQ_TRY(build_graphs(S));
         float ms = 0.0f;
-        LQ_TRY(time_steps(S, steps, &ms));
+        LQ_TRY(time_steps(S, nsteps > 0 ? nsteps : steps, &ms));
+        shape_ms[shape] = ms;
         if (ms < best_ms) {
             best_ms = ms;
             best_shape = shape;
@@ -1155,6 +1158,16 @@ extern "C" int lq_sim_autotune(void* sim, int steps, int* shape_out, float* skin
      * one-level skins do */
     int st = LQ_OK;
     for (int k = 0; k < lqb::kPairShapeCount && st == LQ_OK; ++k) st = trial(k, snap.skin, snap.wide);
+    /* the shapes within 5 % of the fastest at the starting lists (at most
+     * four): re-timed once the lists are chosen */
+    std::vector<int> contenders;
+    if (st == LQ_OK) {
+        const float first_best = best_ms;
+        for (int k = 0; k < lqb::kPairShapeCount; ++k)
+            if (shape_ms[k] <= 1.05f * first_best) contenders.push_back(k);
+        std::sort(contenders.begin(), contenders.end(), [&](int a, int b) { return shape_ms[a] < shape_ms[b]; });
+        if (contenders.size() > 4) contenders.resize(4);
+    }
     const float skins[] = {0.02f, 0.05f, 0.1f, 0.2f};
     const int shape = best_shape;
     for (float f : skins) {
@@ -1173,6 +1186,17 @@ extern "C" int lq_sim_autotune(void* sim, int steps, int* shape_out, float* skin
         factor = f;
         for (float m : margins)
             if (st == LQ_OK) st = trial(shape, f * h, (f + m) * h);
+    }
+    /* the contending shapes again at the chosen lists, each over twice the
+     * steps, the fastest of this round kept: a 40-step trial at the
+     * starting lists (mostly a list build) does not separate shapes a few
+     * percent apart at the lists they will run with */
+    if (st == LQ_OK && contenders.size() > 1) {
+        const float skin = best_skin, wide = best_wide;
+        factor = best_factor;
+        best_ms = 3.4e38f;
+        for (int k : contenders)
+            if (st == LQ_OK) st = trial(k, skin, wide, 2 * steps);
     }
     /* back to the state before tuning, with the chosen configuration */
     int st2 = snap.restore(S);
