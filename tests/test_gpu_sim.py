@@ -221,13 +221,16 @@ def subset(lq, case, keep_boundary, keep_material):
     return Case(case.name, par, *[a[idx].copy() for a in case.arrays()], dict(case.meta))
 
 
+@pytest.mark.parametrize("mixed", [False, True])
 @pytest.mark.parametrize("nb,nm", [(0, 10 ** 9), (10 ** 9, 0), (0, 1), (10 ** 9, 1), (5, 33)],
                          ids=["material-only", "boundary-only", "one-particle", "one-material", "ragged"])
-def test_degenerate_particle_sets_step_like_the_oracle(lq, orc, cuda, nb, nm):
-    """Material only (no Adami pass), boundary only (no interaction or
-    integration), a lone particle, and counts that fill no warp."""
+def test_degenerate_particle_sets_step_like_the_oracle(lq, orc, cuda, nb, nm, mixed):
+    """Material only (no boundary list, no Adami targets, no Adami pass),
+    boundary only (no interaction or integration), a lone particle, and
+    counts that fill no warp, in both precision forms (two Shepard passes
+    inside the nine steps)."""
     c = subset(lq, cases.small_column(velocity_noise=0.02, shepard=4, seed=41), nb, nm).with_ids()
-    sim = lq.Simulation(c.par, *c.arrays())
+    sim = lq.Simulation(c.par, *c.arrays(), mixed=mixed)
     osim = orc.OracleSim(c.par, *c.arrays())
     sim.step(9)
     osim.step(9)
