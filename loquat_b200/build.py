@@ -99,9 +99,13 @@ def build_checked(force: bool = False) -> Path:
     """The bounds-checked variant (-D LQ_CHECKED): every index the list and
     grid kernels gather or scatter through is checked before the access and
     a violation is counted (lq_debug_bounds_violations) instead of made.
-    It stands in for a device memory checker.  Loaded in place of the
-    product library by setting LOQUAT_B200_LIB to its path."""
-    return build(force=force, defines=["LQ_CHECKED"], out=CHECKED_LIB, build_dir=PKG / "_build_checked")
+    It stands in for a device memory checker.  Its Adami walks the lists in
+    pairs at every size (LQ_ADAMI_PAIR_TARGETS=0; the product build does so
+    from 4 M boundary particles on), so the checked runs cover that path.
+    Loaded in place of the product library by setting LOQUAT_B200_LIB to
+    its path."""
+    return build(force=force, defines=["LQ_CHECKED", "LQ_ADAMI_PAIR_TARGETS=0"], out=CHECKED_LIB,
+                 build_dir=PKG / "_build_checked")
 
 
 def build_app(force: bool = False) -> Path:

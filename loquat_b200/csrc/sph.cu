@@ -876,6 +876,21 @@ __global__ void __launch_bounds__(kBlock) k_shepard(const Parameters* __restrict
 #ifndef LQ_ADAMI_BLOCK
 #define LQ_ADAMI_BLOCK 128
 #endif
+/* Entries per group of the list-driven Adami, chosen per launch: groups of
+ * four where the targets fit in about one wave of the GPU (each thread's
+ * chain of dependent gathers is then the time: the cylinder's 0.34 M
+ * boundary particles, ~19 entries per active one), pairs from
+ * kAdamiPairTargets boundary particles on (48 registers against 62: more
+ * warps and fewer filler entries where enough targets keep the memory
+ * system busy; on the 256-scenario ensemble's 16.2 M, 1.17 against 1.28 ms
+ * per step, groups of eight 1.24).  The sums do not depend on the group
+ * size.  The bounds-checked build sets the threshold to 0, so its tests
+ * take the pairs path. */
+#ifndef LQ_ADAMI_PAIR_TARGETS
+#define LQ_ADAMI_PAIR_TARGETS (4 << 20)
+#endif
+constexpr int kAdamiPairTargets = LQ_ADAMI_PAIR_TARGETS;
+template <int kG>
 __global__ void __launch_bounds__(LQ_ADAMI_BLOCK) k_adami_packed(const Parameters* __restrict__ P, int npb, State st,
                                                          const int* __restrict__ list,
                                                          const int* __restrict__ count, int stride, NbrArrays nb,
@@ -897,31 +912,32 @@ __global__ void __launch_bounds__(LQ_ADAMI_BLOCK) k_adami_packed(const Parameter
     const float4 xi = __ldg(st.pos + i);
     tensor2d S = make_tensor2d(0.0f);
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    /* groups of four entries, the next group's entries fetched ahead and
+    /* groups of kG entries, the next group's entries fetched ahead and
      * every gather of a group issued together; a pair at q >= 2 (and the
      * filler of the last group, the target's own record) gets the kernel
-     * factor 0 and adds exact zeros, so the loop has no branch */
+     * factor 0 and adds exact zeros, so the loop has no branch and its sums
+     * do not depend on kG */
     const int* p = list + i;
-    int nxt[4];
+    int nxt[kG];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) nxt[u] = u < n ? __ldg(p + (size_t)u * stride) : i;
-    for (int k = 0; k < n; k += 4) {
-        int j[4];
+    for (int u = 0; u < kG; ++u) nxt[u] = u < n ? __ldg(p + (size_t)u * stride) : i;
+    for (int k = 0; k < n; k += kG) {
+        int j[kG];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < kG; ++u) {
             j[u] = lq_in_range(nxt[u], np_all) ? nxt[u] : i;
-            nxt[u] = k + 4 + u < n ? __ldg(p + (size_t)(k + 4 + u) * stride) : i;
+            nxt[u] = k + kG + u < n ? __ldg(p + (size_t)(k + kG + u) * stride) : i;
         }
-        float4 xr[4], sa[4];
-        float2 sb[4];
+        float4 xr[kG], sa[kG];
+        float2 sb[kG];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < kG; ++u) {
             xr[u] = __ldg(nb.xr + j[u]);
             sa[u] = __ldg(nb.sa + j[u]);
             sb[u] = __ldg(reinterpret_cast<const float2*>(nb.sb + j[u]));
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < kG; ++u) {
             const float3 d = make_float3(xi.x - xr[u].x, xi.y - xr[u].y, xi.z - xr[u].z);
             /* the approximate square root and quotient of the pair kernel */
             const float q = sqrt_approx(d.x * d.x + d.y * d.y + d.z * d.z) * ih;
@@ -1286,8 +1302,13 @@ int launch_adami_packed(const Parameters* ph, const Parameters* pd, const State&
     if (!act != !nact) return set_error(LQ_ERR_ARG, "Adami: compacted targets need both act and nact");
     if (nl.stride < ph->npb) return set_error(LQ_ERR_ARG, "Adami: list stride %d < %d targets", nl.stride, ph->npb);
     const NbrArrays nb = nbr_arrays(rec, ph->np);
-    k_adami_packed<<<blocks_for(ph->npb, LQ_ADAMI_BLOCK), LQ_ADAMI_BLOCK, 0, s>>>(pd, ph->npb, st, nl.list, nl.count,
-                                                                                nl.stride, nb, str2, act, nact);
+    const int grid = blocks_for(ph->npb, LQ_ADAMI_BLOCK);
+    if (ph->npb >= kAdamiPairTargets)
+        k_adami_packed<2><<<grid, LQ_ADAMI_BLOCK, 0, s>>>(pd, ph->npb, st, nl.list, nl.count, nl.stride, nb, str2, act,
+                                                          nact);
+    else
+        k_adami_packed<4><<<grid, LQ_ADAMI_BLOCK, 0, s>>>(pd, ph->npb, st, nl.list, nl.count, nl.stride, nb, str2, act,
+                                                          nact);
     LQ_TRY_CUDA(cudaGetLastError(), "k_adami_packed");
     return LQ_OK;
 }
