@@ -573,7 +573,8 @@ __device__ __forceinline__ float3 unpack_velocity(float v0, float v1)
 }
 
 /* One slot's entry of the packed arrays from its velocity, density and
- * stress (the pack kernel and the list-driven Adami write it alike). */
+ * stress (the pack kernel and the integrators write it alike; the
+ * list-driven Adami rewrites only the stress words, store_packed_stress). */
 template <bool kPk>
 __device__ __forceinline__ void store_packed(const NbrArrays& nb, int i, const float4& v, const tensor2d& str)
 {
