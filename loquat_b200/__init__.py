@@ -224,10 +224,13 @@ class Grid:
         h = _VP()
         check(lib().lq_grid_create(np_, ncell, ctypes.byref(h)), "lq_grid_create")
         self.handle = h
+        # held here so that a collection at interpreter exit, after the
+        # module's globals are gone, can still release the grid
+        self._destroy = lib().lq_grid_destroy
 
     def close(self):
-        if self.handle:
-            lib().lq_grid_destroy(self.handle)
+        if getattr(self, "handle", None):
+            self._destroy(self.handle)
             self.handle = None
 
     __del__ = close
@@ -267,6 +270,7 @@ class Simulation:
         check(lib().lq_sim_create(ctypes.byref(par), *[a.ctypes.data for a in arrs], flags, ctypes.byref(h)),
               "lq_sim_create")
         self.handle = h
+        self._destroy = lib().lq_sim_destroy    # usable at interpreter exit too
         self.np = par.np
         self.par = par.copy()
 
@@ -280,6 +284,7 @@ class Simulation:
         check(lib().lq_sim_load_checkpoint(os.fsencode(str(path)), flags, ctypes.byref(h)), "lq_sim_load_checkpoint")
         self = cls.__new__(cls)
         self.handle = h
+        self._destroy = lib().lq_sim_destroy
         with open(path, "rb") as f:
             f.seek(48)           # magic, version, flags, step, time, skin, three counts
             self.par = Parameters.from_bytes(f.read(ctypes.sizeof(Parameters)))
@@ -288,7 +293,7 @@ class Simulation:
 
     def close(self):
         if getattr(self, "handle", None):
-            lib().lq_sim_destroy(self.handle)
+            self._destroy(self.handle)
             self.handle = None
 
     __del__ = close

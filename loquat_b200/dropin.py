@@ -66,7 +66,7 @@ class ReferenceStep:
         self.time = 0.0
 
     def close(self):
-        if self.grid is not None:
+        if getattr(self, "grid", None) is not None:
             self.grid.close()
             self.grid = None
 
