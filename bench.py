@@ -67,7 +67,7 @@ def parse_args(argv=None):
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=["cylinder", "column", "ensemble", "slope", "inclined"], default="cylinder",
-                    help="slope / inclined: the von Wolffersdorff workloads (2.856 M soil at dr 5 mm; 16.0 M at "
+                    help="slope / inclined: the von Wolffersdorff workloads (2.85 M soil at dr 5 mm; 16.0 M at "
                          "dr 2.5 mm)")
     ap.add_argument("--scenarios", type=int, default=256, help="ensemble size (--config ensemble)")
     ap.add_argument("--dr", type=float, default=None, help="override the particle spacing")

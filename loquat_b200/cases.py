@@ -310,8 +310,9 @@ def slope_failure(dr=0.005, length=2.0, height=0.6, width=0.35, angle=45.0, runo
     x = 0, on a floor that runs `runout` beyond the toe.  Density
     rho_s / (1 + e0); geostatic stress from the local surface with
     K0 = 1 - sin(phi_c); void ratio e0 in idep.z.  At the defaults (2.0 x 0.6
-    x 0.35 m at dr = 5 mm) the soil holds 2.856 M particles: the stated
-    geometry at that spacing, not a 4.2 M count."""
+    x 0.35 m at dr = 5 mm) the soil holds 2,852,360 particles (642,780 in
+    the walls and floor): the stated geometry at that spacing, not a 4.2 M
+    count."""
     b = layers * dr
     rho = rho_s / (1.0 + e0)
     nsx, nsy, nsz = round(length / dr), round(width / dr), round(height / dr)
@@ -386,7 +387,7 @@ def inclined_block(dr=0.0025, length=1.0, width=1.0, height=0.25, angle=30.0, ru
 def config_case(index: int, **kw) -> Case:
     """Case of one of the benchmark configurations (0-based):
     0 column collapse 50k, 1 cylinder collapse ~1.96M (plain FP32 form),
-    2 von Wolffersdorff slope failure 2.856M, 4 von Wolffersdorff block on
+    2 von Wolffersdorff slope failure 2.85M, 4 von Wolffersdorff block on
     a 30 degree plane 16.0M (3 is the ensemble(), a set of cases)."""
     if index == 0:
         return column_collapse(**kw)

@@ -5,7 +5,7 @@ the FP64 oracle.
     python tests/golden/make_stated.py inclined [--out DIR]
 
 slope:    the sand slope failure, 2.0 x 0.6 x 0.35 m at 45 deg, dr = 5 mm
-          (2,856,000 soil + 639,140 boundary particles), seed 1 as the bench
+          (2,852,360 soil + 642,780 boundary particles), seed 1 as the bench
           generates it; a seeded 0.5 % sample of the soil particles.
 inclined: the block on the 30 deg plane, 1.0 x 1.0 x 0.25 m at dr = 2.5 mm
           (16.0 M soil + 1.63 M boundary particles), seed 1; a seeded 0.1 %

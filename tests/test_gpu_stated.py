@@ -2,7 +2,7 @@
 oracle (fixtures made by tests/golden/make_stated.py):
 
 * the sand slope failure, 2.0 x 0.6 x 0.35 m at 45 deg, dr = 5 mm
-  (2,856,000 soil + 639,140 boundary particles), on a seeded 0.5 % sample;
+  (2,852,360 soil + 642,780 boundary particles), on a seeded 0.5 % sample;
 * the block on the 30 deg plane at dr = 2.5 mm (16.0 M soil + 1.63 M
   boundary particles), on a seeded 0.1 % sample.
 
